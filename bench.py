@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark: converged T-matrices per second for a batch of 4096 spheroids.
+
+Workload (the batched-forward configuration): 4096 independent spheroids from
+a seeded generator -- size parameter x = 2 pi r_ev / lambda uniform in
+[0.1, 10], axis ratio log-uniform in [0.5, 2], Re m uniform in [1.3, 2.0],
+Im m log-uniform in [1e-3, 1], lambda = 1 um -- run through the task-based
+schedule (min_order 10, max_order 100, ngauss = 2 * order, tolerance 1e-4):
+the m = 0 convergence loop, every m block at the converged order, and the
+full Qsca/Qext sums. One step = one batch. Data are synthetic.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs its own batch (weak scaling, no
+data-path collective: the grains are independent); the time is the maximum
+over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRAINS = 4096
+SCHEDULE = dict(min_order=10, max_order=100, gauss_legendre_factor=2,
+                tolerance=1e-4)
+CPU_SAMPLE = 96  # grains per reference-CPU step (bounded sample)
+
+
+def grains(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.1, 10.0, n)
+    d = np.exp(rng.uniform(np.log(0.5), np.log(2.0), n))
+    mr = rng.uniform(1.3, 2.0, n)
+    mi = np.exp(rng.uniform(np.log(1e-3), np.log(1.0), n))
+    lam = 1e-6
+    r = x * lam / (2 * np.pi)
+    return r, np.full(n, lam), mr + 1j * mi, d
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier and max-reduction across ranks (NCCL when world > 1)."""
+
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            torch.cuda.set_device(local)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.td = td
+            self.torch = torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.td.barrier()
+
+    def max(self, v):
+        if self.world == 1:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.td.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                smax = float(p[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def flush_l2(buf):
+    # write a buffer larger than the 126 MB L2 between timed steps
+    buf.zero_()
+
+
+def reference_sample(nthreads, seed):
+    """One bounded sample of the same workload through the reference's own
+    task objects under QuickSched (oracle/_ref, built from the reference)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    r, lam, m, d = grains(CPU_SAMPLE, seed)
+    t = time.perf_counter()
+    out = O.ref_batch(r, lam, m, d, nthreads=nthreads, want_t=False, **{
+        "min_order": SCHEDULE["min_order"], "max_order": SCHEDULE["max_order"],
+        "glfac": SCHEDULE["gauss_legendre_factor"],
+        "tolerance": SCHEDULE["tolerance"]})
+    dt = time.perf_counter() - t
+    return len(out), dt
+
+
+def cpu_baseline_block(nthreads, steps=1):
+    vals = []
+    for s in range(steps):
+        n, dt = reference_sample(nthreads, 1000 + s)
+        vals.append(n / dt)
+    v = float(np.median(vals))
+    return {"value": v, "unit": "T-matrices/s", "cores": nthreads,
+            "kind": "reference",
+            "sample": "%d grains of the same distribution (seeded), reference "
+                      "task objects (InteractionTask/TMatrixM0Task chain + "
+                      "TMatrixMAllTask) under QuickSched, maximum_order 100, "
+                      "%d threads, median of %d" % (CPU_SAMPLE, nthreads, steps)}
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    nthreads = os.cpu_count() or 1
+    times = []
+    for s in range(args.warmup + args.steps):
+        n, dt = reference_sample(nthreads, 2000 + s)
+        if s >= args.warmup:
+            times.append(dt)
+    value = CPU_SAMPLE * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "T-matrices/s (converged, batched)",
+        "value": value, "unit": "T-matrices/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "batched T-matrices, config-2 distribution",
+                   "grains_per_step": CPU_SAMPLE, **SCHEDULE},
+        "cpu_baseline": {"value": value, "unit": "T-matrices/s",
+                         "cores": nthreads, "kind": "reference",
+                         "sample": "%d grains per step, reference QuickSched "
+                                   "path, %d threads" % (CPU_SAMPLE, nthreads)},
+        "e2e": {"value": value, "unit": "T-matrices/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    from costuum_b200 import _lib
+    from costuum_b200.tmatrix import Context
+
+    rank, world, local = dist_env()
+    dist = Dist(world, local)
+    ctx = Context(local)
+    lib = _lib.load()
+    h = ctx._h
+    dfma = ctx.probe_fp64(0)
+    dmma = ctx.probe_fp64(1)
+
+    r, lam, m, d = grains(N_GRAINS, 1 + rank)
+    mr = np.ascontiguousarray(m.real)
+    mi = np.ascontiguousarray(m.imag)
+    sched = _lib.TmxSchedule(SCHEDULE["min_order"], SCHEDULE["max_order"],
+                             SCHEDULE["gauss_legendre_factor"], 0,
+                             SCHEDULE["tolerance"])
+    P = _lib.ptr
+    _lib.check(h, lib.tmx_batch_upload(h, N_GRAINS, P(r), P(lam), P(mr), P(mi),
+                                       P(d), sched), "upload")
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda:%d" % local)
+
+    def step_device():
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        _lib.check(h, lib.tmx_timer_start(h), "timer")
+        _lib.check(h, lib.tmx_batch_compute(h), "compute")
+        ms = np.zeros(1)
+        _lib.check(h, lib.tmx_timer_stop(h, P(ms)), "timer")
+        return float(ms[0])
+
+    for _ in range(args.warmup):
+        step_device()
+    # ---- device-resident timed region
+    sampler = ClockSampler(local)
+    sampler.start()
+    lib.tmx_profile_enable(h, 1)
+    launches0 = ctx.kernel_launches
+    dist.barrier()
+    torch.cuda.synchronize()
+    total = 0.0
+    for _ in range(args.steps):
+        total += step_device()
+    torch.cuda.synchronize()
+    dist.barrier()
+    launches = ctx.kernel_launches - launches0
+    clocks = sampler.stop()
+    bk_ms = np.zeros(1)
+    bk_n = ctypes.c_int64()
+    bk_fl = np.zeros(1)
+    lib.tmx_profile_read(h, 0, P(bk_ms), ctypes.byref(bk_n), P(bk_fl))
+    tb_ms = np.zeros(1)
+    tb_n = ctypes.c_int64()
+    lib.tmx_profile_read(h, 1, P(tb_ms), ctypes.byref(tb_n), P(np.zeros(1)))
+    lib.tmx_profile_enable(h, 0)
+    flops_survey = lib.tmx_batch_flops_survey(h)
+    total_max = dist.max(total)
+    ms_step = total_max / args.steps
+    value = world * N_GRAINS / (ms_step * 1e-3)
+
+    # per-grain outcome of the last step
+    nmax = np.zeros(N_GRAINS, np.int32)
+    status = np.zeros(N_GRAINS, np.int32)
+    q = np.zeros((N_GRAINS, 6))
+    lib.tmx_batch_results(h, _lib.iptr(nmax), None, _lib.iptr(status), P(q))
+
+    # ---- end to end through the public API with host buffers
+    e2e_ms = 0.0
+    for s in range(max(1, args.steps)):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t0 = time.perf_counter()
+        res = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+        e2e_ms += (time.perf_counter() - t0) * 1e3
+    e2e_max = dist.max(e2e_ms) / max(1, args.steps)
+    h2d = N_GRAINS * 5 * 8
+    d2h = N_GRAINS * (3 * 4 + 6 * 8)
+
+    # roofline of the dominant kernel (block kernel: assembly + LU + solve)
+    bk_launches = max(1, bk_n.value)
+    per_launch_ms = bk_ms[0] / bk_launches
+    achieved = (bk_fl[0] / bk_launches) / (per_launch_ms * 1e-3) / 1e12
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.skip_cpu:
+            cpu = cpu_baseline_block(os.cpu_count() or 1, steps=1)
+        out = {
+            "metric": "T-matrices/s (converged, batched)",
+            "value": value, "unit": "T-matrices/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "batched T-matrices, config-2 distribution "
+                                   "(4096 spheroids, x in [0.1,10])",
+                       "grains_per_gpu": N_GRAINS, **SCHEDULE,
+                       "l2": "flushed between steps (256 MB write); working "
+                             "set > L2",
+                       "nmax_mean": float(nmax[nmax > 0].mean()),
+                       "nmax_max": int(nmax.max()),
+                       "status_nonzero": int((status != 0).sum())},
+            "e2e": {"value": world * N_GRAINS / (e2e_max * 1e-3),
+                    "unit": "T-matrices/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "tensor", "kernel": "k_blocks",
+                         "achieved": achieved, "peak": dmma,
+                         "unit": "TFLOP/s", "frac": achieved / dmma,
+                         "peak_kind": "measured FP64 DMMA (mma.sync m8n8k4 f64) "
+                                      "this run; DFMA peak %.1f" % dfma,
+                         "flops_model": "executed parity-class algorithm",
+                         "survey_model_tflops": (flops_survey * args.steps /
+                                                 (bk_ms[0] * 1e-3) / 1e12
+                                                 if bk_ms[0] > 0 else None),
+                         "launches": int(bk_n.value),
+                         "share_of_step": bk_ms[0] / max(total, 1e-9),
+                         "traffic": None},
+            "phases_ms_per_step": {"blocks": bk_ms[0] / args.steps,
+                                   "tables": tb_ms[0] / args.steps},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    ctx.close()
+    dist.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true",
+                    help="omit the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

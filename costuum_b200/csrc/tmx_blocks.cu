@@ -1,0 +1,707 @@
+// Block kernel: for one (grain, m, parity class) work item, assemble the
+// class sub-matrices of Q and RgQ by quadrature, factor Q with partial
+// pivoting in shared memory and solve T_c Q_c = -RgQ_c.
+//
+// Reference semantics (CosTuuM):
+//   assembly  TMatrixM0Task::execute   src/TMatrixResource.hpp:601-709 (m=0)
+//             TMatrixMAllTask::execute src/TMatrixResource.hpp:934-1100
+//   inversion Matrix::plu_inverse      src/Matrix.hpp:261-384
+//   T         T = -RgQ Q^-1            src/TMatrixResource.hpp:712-730
+//
+// Restructuring (same mathematics):
+//  * Parity classes. Q_m has non-zero entries only where the row label
+//    (i + n) % 2 equals the column label (m >= 1), and is block diagonal in i
+//    for m = 0. Partial pivoting never picks a row of another class (those
+//    entries are exact zeros) and elimination never mixes classes, so the
+//    reference's LU of the full 2nb x 2nb block performs, entry for entry,
+//    the LUs of the independent classes. Each class is one work item here.
+//  * Assembly as a GEMM. Every entry is sum_g sum_{t<4} F_t(g, n1) W_t(g, n2)
+//    with A-side vectors built from h_n1 = j + i y (or j alone for RgQ) and
+//    B-side vectors built from j_n2(m k r); see build_chunk().
+//  * T = -RgQ Q^-1 by two triangular solves on the LU factors instead of the
+//    explicit inverse followed by a product.
+#include "tmx_common.cuh"
+#include "tmx_kernels.h"
+
+#define TR 4 // rows per thread tile
+#define TC 4 // columns per thread tile (strided by the column-tile count)
+
+struct ClassDesc {
+  int nb;       // class size
+  int R0, R1;   // rows of group 0 / group 1
+  int R0p, NRp; // padded group-0 rows, padded total rows
+  int iA, iB;   // block index i of group 0 / group 1
+  int nA0, nB0; // first n of each group (n advances by 2)
+  int nbb;      // size nb of the full block (2 nbb x 2 nbb)
+  int nmin;     // smallest n in the block
+};
+
+__device__ __forceinline__ ClassDesc describe(int N, int m, int cls) {
+  ClassDesc D;
+  if (m == 0) {
+    D.iA = cls >> 1;
+    D.iB = D.iA;
+    D.nA0 = (cls & 1) ? 1 : 2;
+    D.R0 = (N >= D.nA0) ? (N - D.nA0) / 2 + 1 : 0;
+    D.nB0 = 0;
+    D.R1 = 0;
+    D.nbb = N;
+    D.nmin = 1;
+  } else {
+    D.iA = 0;
+    D.iB = 1;
+    D.nA0 = ((m & 1) == cls) ? m : m + 1;
+    D.R0 = (N >= D.nA0) ? (N - D.nA0) / 2 + 1 : 0;
+    D.nB0 = ((m & 1) == (cls ^ 1)) ? m : m + 1;
+    D.R1 = (N >= D.nB0) ? (N - D.nB0) / 2 + 1 : 0;
+    D.nbb = N + 1 - m;
+    D.nmin = m;
+  }
+  D.nb = D.R0 + D.R1;
+  D.R0p = (D.R0 + TR - 1) / TR * TR;
+  D.NRp = D.R0p + (D.R1 + TR - 1) / TR * TR;
+  return D;
+}
+
+__device__ __forceinline__ void member(const ClassDesc &D, int a, int &i,
+                                       int &n) {
+  if (a < D.R0) {
+    i = D.iA;
+    n = D.nA0 + 2 * a;
+  } else {
+    i = D.iB;
+    n = D.nB0 + 2 * (a - D.R0);
+  }
+}
+
+// padded row -> member (or -1 for padding)
+__device__ __forceinline__ int padded_member(const ClassDesc &D, int pr) {
+  if (pr < D.R0p) {
+    return (pr < D.R0) ? pr : -1;
+  }
+  const int a = D.R0 + (pr - D.R0p);
+  return (pr - D.R0p < D.R1) ? a : -1;
+}
+
+// complex offset of block m in a T-matrix of order N (reference layout)
+__device__ __host__ __forceinline__ int64_t block_offset(int N, int m) {
+  if (m == 0) {
+    return 0;
+  }
+  const int64_t a = N, b = N + 1 - m;
+  const int64_t sa = a * (a + 1) * (2 * a + 1) / 6;
+  const int64_t sb = b * (b + 1) * (2 * b + 1) / 6;
+  return 4 * (a * a + sa - sb);
+}
+
+__device__ __forceinline__ double a_n(int n) {
+  // a_n = sqrt((2n + 1) / (n (n + 1))) (NBasedResources.hpp:115-137)
+  return sqrt((2. * n + 1.) / ((n + 1.) * n));
+}
+
+// Shared-memory layout of the assembly phase for a chunk of G nodes:
+//   F[kk][pr]   double2 (F^j, F^y),  kk = 4 * gl + t,   pr < NRp
+//   W[rg][kk][b] double2 (complex),  rg = row group,    b < CT * TC
+struct AsmLayout {
+  int G, NRp, CT, ncol, ngroups;
+  size_t f_elems, w_elems;
+};
+
+// Build the A-side (F) and B-side (W) vectors of nodes [g0, g0 + G).
+//   F1 = a d h, F2 = a dd h, F3 = a d dh, F4 = a (dd dh + n(n+1) drr/kr d h)
+//   G1 = a d dj~, G2 = a (dd dj~ + drr/(m k r) n(n+1) d j~), G3 = a d j~,
+//   G4 = a dd j~  (j~ = j_n(m k r), dj~ its derivative form)
+//   alpha = w r^2, mu = m^2 / sin^2, beta = m w r^2 / sin
+//   Q11: W = (k2mr a mu G1, k2mr a G2, -k2 a mu G3, -k2 a G4)
+//   Q22: W = (k2 a mu G1, k2 a G2, -k2mr a mu G3, -k2mr a G4)
+//   Q12: W = i (k2mr b G4, k2mr b G3, k2 b G2, k2 b G1)
+//   Q21: W = i (k2 b G4, k2 b G3, k2mr b G2, k2mr b G1)
+// This is the expansion of the J11, J12, J21, J22 terms of
+// TMatrixResource.hpp:993-1097 into products of one n1 factor and one n2
+// factor per node.
+__device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
+                            int m, int ng, int g0, const double *__restrict__ T,
+                            const double *__restrict__ S,
+                            const double *__restrict__ Wg, double k2,
+                            cplx k2mr, cplx *Fs, cplx *Ws) {
+  const int G = L.G;
+  // A side
+  for (int u = threadIdx.x; u < G * L.NRp; u += blockDim.x) {
+    const int gl = u / L.NRp;
+    const int pr = u % L.NRp;
+    const int g = g0 + gl;
+    const int a = padded_member(D, pr);
+    cplx f1 = mkc(0., 0.), f2 = f1, f3 = f1, f4 = f1;
+    if (a >= 0 && g < ng) {
+      int i, n;
+      member(D, a, i, n);
+      const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+      const double j = t[TMX_Q_J], dj = t[TMX_Q_DJ];
+      const double y = t[TMX_Q_Y], dy = t[TMX_Q_DY];
+      const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
+      const double d = w[0], dd = w[1];
+      const double *s = S + (int64_t)g * TMX_NS;
+      const double an = a_n(n);
+      const double nn = n * (n + 1.);
+      const double q = nn * s[TMX_NS_DRR] * s[TMX_NS_KRINV] * d;
+      f1 = mkc(an * d * j, an * d * y);
+      f2 = mkc(an * dd * j, an * dd * y);
+      f3 = mkc(an * d * dj, an * d * dy);
+      f4 = mkc(an * (dd * dj + q * j), an * (dd * dy + q * y));
+    }
+    cplx *f = Fs + (int64_t)(4 * gl) * L.NRp + pr;
+    f[0] = f1;
+    f[L.NRp] = f2;
+    f[2 * L.NRp] = f3;
+    f[3 * L.NRp] = f4;
+  }
+  // B side
+  const int ncolp = L.CT * TC;
+  for (int u = threadIdx.x; u < G * ncolp; u += blockDim.x) {
+    const int gl = u / ncolp;
+    const int b = u % ncolp;
+    const int g = g0 + gl;
+    cplx w1[2], w2[2], w3[2], w4[2];
+    for (int rg = 0; rg < 2; ++rg) {
+      w1[rg] = w2[rg] = w3[rg] = w4[rg] = mkc(0., 0.);
+    }
+    if (b < D.nb && g < ng) {
+      int ib, n;
+      member(D, b, ib, n);
+      const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+      const cplx jm = mkc(t[TMX_Q_JM_RE], t[TMX_Q_JM_IM]);
+      const cplx djm = mkc(t[TMX_Q_DJM_RE], t[TMX_Q_DJM_IM]);
+      const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
+      const double d = w[0], dd = w[1];
+      const double *s = S + (int64_t)g * TMX_NS;
+      const double an = a_n(n);
+      const double nn = n * (n + 1.);
+      const cplx kmi = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
+      const cplx G1 = cscale(djm, an * d);
+      const cplx G2 = cscale(
+          cadd(cscale(djm, dd), cscale(cmul(kmi, jm), s[TMX_NS_DRR] * nn * d)),
+          an);
+      const cplx G3 = cscale(jm, an * d);
+      const cplx G4 = cscale(jm, an * dd);
+      const double wr2 = s[TMX_NS_W] * s[TMX_NS_R2];
+      const double mu = (double)(m * m) * s[TMX_NS_SIN2INV];
+      const double beta = s[TMX_NS_SININV] * m * wr2;
+      for (int rg = 0; rg < L.ngroups; ++rg) {
+        const int ia = (rg == 0) ? D.iA : D.iB;
+        if (ia == ib) {
+          // diagonal-type block: Q11 (i = 0) or Q22 (i = 1)
+          const cplx chi = (ia == 0) ? k2mr : mkc(k2, 0.);
+          const cplx clo = (ia == 0) ? mkc(-k2, 0.) : mkc(-k2mr.x, -k2mr.y);
+          w1[rg] = cmul(chi, cscale(G1, wr2 * mu));
+          w2[rg] = cmul(chi, cscale(G2, wr2));
+          w3[rg] = cmul(clo, cscale(G3, wr2 * mu));
+          w4[rg] = cmul(clo, cscale(G4, wr2));
+        } else {
+          // off-diagonal block: Q12 (ia = 0, ib = 1) or Q21 (ia = 1, ib = 0)
+          const cplx c1 = (ia == 0) ? k2mr : mkc(k2, 0.);
+          const cplx c2 = (ia == 0) ? mkc(k2, 0.) : k2mr;
+          const cplx ic1 = mkc(-c1.y * beta, c1.x * beta); // i c1 beta
+          const cplx ic2 = mkc(-c2.y * beta, c2.x * beta);
+          w1[rg] = cmul(ic1, G4);
+          w2[rg] = cmul(ic1, G3);
+          w3[rg] = cmul(ic2, G2);
+          w4[rg] = cmul(ic2, G1);
+        }
+      }
+    }
+    for (int rg = 0; rg < L.ngroups; ++rg) {
+      cplx *wp = Ws + ((int64_t)rg * 4 * G + 4 * gl) * ncolp + b;
+      wp[0] = w1[rg];
+      wp[ncolp] = w2[rg];
+      wp[2 * ncolp] = w3[rg];
+      wp[3 * ncolp] = w4[rg];
+    }
+  }
+}
+
+// hypot without the libm scaling path; the magnitudes here are far from
+// overflow/underflow
+__device__ __forceinline__ double cabs_dev(cplx a) { return hypot(a.x, a.y); }
+
+extern __shared__ __align__(16) unsigned char tmx_smem[];
+
+__global__ void __launch_bounds__(256)
+    k_blocks(TmxBlockArgs A, size_t smem_bytes) {
+  const int it = blockIdx.x;
+  if (it >= A.nitems) {
+    return;
+  }
+  const TmxItem item = A.items[it];
+  const TmxSlot sl = A.slots[item.slot];
+  const TmxGrain G = A.grains[sl.grain];
+  const int N = sl.nmax;
+  const int ng = sl.ngauss;
+  const int m = item.m;
+  const ClassDesc D = describe(N, m, item.cls);
+  const int nb = D.nb;
+  if (nb <= 0) {
+    return;
+  }
+  if (nb > TMX_MAX_NB) {
+    if (threadIdx.x == 0) {
+      atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
+    }
+    return;
+  }
+  const double *T = A.tab + sl.tab;
+  const double *S = A.nsc + sl.nsc;
+  const double *Wg = A.wig + A.wig_off[sl.wig_n] + (int64_t)m * ng * N * 2;
+  const double k2 = G.k * G.k;
+  const cplx k2mr = mkc(G.mr * k2, G.mi * k2);
+  cplx *Qs = A.scratch + item.scratch;
+  cplx *Rs = Qs + (int64_t)nb * nb;
+
+  // ------------------------------------------------------------ assembly
+  AsmLayout L;
+  L.G = A.chunk_nodes;
+  L.NRp = D.NRp;
+  L.CT = (nb + TC - 1) / TC;
+  L.ncol = L.CT * TC;
+  L.ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
+  const int RT = D.NRp / TR;
+  cplx *Fs = reinterpret_cast<cplx *>(tmx_smem);
+  cplx *Ws = Fs + (int64_t)4 * L.G * L.NRp;
+  const int ntiles = RT * L.CT;
+  const int tstep = (m == 0) ? 2 : 1; // m = 0: mu = 0 kills t = 0, 2
+  const int t0 = (m == 0) ? 1 : 0;
+  for (int tile0 = 0; tile0 < ntiles; tile0 += blockDim.x) {
+    const int tile = tile0 + threadIdx.x;
+    const bool active = tile < ntiles;
+    const int ct = active ? tile % L.CT : 0;
+    const int rt = active ? tile / L.CT : 0;
+    const int rg = (rt * TR < D.R0p) ? 0 : 1;
+    double aj[TR][TC][2], ay[TR][TC][2];
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        aj[r][c][0] = aj[r][c][1] = ay[r][c][0] = ay[r][c][1] = 0.;
+      }
+    }
+    for (int g0 = 0; g0 < ng; g0 += L.G) {
+      __syncthreads();
+      build_chunk(D, L, N, m, ng, g0, T, S, Wg, k2, k2mr, Fs, Ws);
+      __syncthreads();
+      if (active) {
+        const int kmax = 4 * min(L.G, ng - g0);
+        for (int kk = t0; kk < kmax; kk += tstep) {
+          const cplx *fr = Fs + (int64_t)kk * L.NRp + rt * TR;
+          const cplx *wr = Ws + ((int64_t)rg * 4 * L.G + kk) * L.ncol + ct;
+          cplx f[TR], w[TC];
+#pragma unroll
+          for (int r = 0; r < TR; ++r) {
+            f[r] = fr[r];
+          }
+#pragma unroll
+          for (int c = 0; c < TC; ++c) {
+            w[c] = wr[c * L.CT];
+          }
+#pragma unroll
+          for (int r = 0; r < TR; ++r) {
+#pragma unroll
+            for (int c = 0; c < TC; ++c) {
+              aj[r][c][0] = fma(f[r].x, w[c].x, aj[r][c][0]);
+              aj[r][c][1] = fma(f[r].x, w[c].y, aj[r][c][1]);
+              ay[r][c][0] = fma(f[r].y, w[c].x, ay[r][c][0]);
+              ay[r][c][1] = fma(f[r].y, w[c].y, ay[r][c][1]);
+            }
+          }
+        }
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int r = 0; r < TR; ++r) {
+        const int a = padded_member(D, rt * TR + r);
+        if (a < 0) {
+          continue;
+        }
+#pragma unroll
+        for (int c = 0; c < TC; ++c) {
+          const int b = ct + c * L.CT;
+          if (b >= nb) {
+            continue;
+          }
+          // Q = G^j + i G^y, RgQ = G^j
+          Qs[(int64_t)a * nb + b] =
+              mkc(aj[r][c][0] - ay[r][c][1], aj[r][c][1] + ay[r][c][0]);
+          Rs[(int64_t)a * nb + b] = mkc(aj[r][c][0], aj[r][c][1]);
+        }
+      }
+    }
+  }
+  __syncthreads();
+
+  // ------------------------------------------------------------------ LU
+  const int lda = nb | 1; // odd stride: conflict-free column access
+  cplx *Am = reinterpret_cast<cplx *>(tmx_smem);
+  cplx *uinv = Am + (int64_t)nb * lda;
+  int *piv = reinterpret_cast<int *>(uinv + nb);
+  int *perm = piv + nb;
+  int *flag = perm + nb;
+  size_t used = ((size_t)nb * lda + nb) * sizeof(cplx) + (3 * nb + 1) * sizeof(int);
+  used = (used + 15) & ~(size_t)15;
+  cplx *X = reinterpret_cast<cplx *>(tmx_smem + used);
+  int Rchunk = (int)((smem_bytes - used) / (sizeof(cplx) * lda));
+  if (Rchunk > nb) {
+    Rchunk = nb;
+  }
+  for (int u = threadIdx.x; u < nb * nb; u += blockDim.x) {
+    Am[(u / nb) * lda + (u % nb)] = Qs[u];
+  }
+  if (threadIdx.x == 0) {
+    *flag = 0;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  for (int i = 0; i < nb; ++i) {
+    if (warp == 0) {
+      double best = -1.;
+      int bi = i;
+      for (int j = i + lane; j < nb; j += 32) {
+        const double v = cabs_dev(Am[j * lda + i]);
+        if (v > best) {
+          best = v;
+          bi = j;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        piv[i] = bi;
+        if (!(best > 0.)) {
+          *flag = 1;
+        }
+      }
+    }
+    __syncthreads();
+    const int ip = piv[i];
+    if (ip != i) {
+      for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const cplx t = Am[i * lda + j];
+        Am[i * lda + j] = Am[ip * lda + j];
+        Am[ip * lda + j] = t;
+      }
+      __syncthreads();
+    }
+    const cplx pinv = cinv(Am[i * lda + i]);
+    for (int j = i + 1 + threadIdx.x; j < nb; j += blockDim.x) {
+      Am[j * lda + i] = cmul(Am[j * lda + i], pinv);
+    }
+    __syncthreads();
+    const int rem = nb - i - 1;
+    for (int u = threadIdx.x; u < rem * rem; u += blockDim.x) {
+      const int j = i + 1 + u / rem;
+      const int k = i + 1 + u % rem;
+      Am[j * lda + k] = csub(Am[j * lda + k], cmul(Am[j * lda + i], Am[i * lda + k]));
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+    uinv[j] = cinv(Am[j * lda + j]);
+  }
+  if (threadIdx.x == 0) {
+    // column exchanges of Matrix::plu_inverse step 4, as a gather index
+    for (int j = 0; j < nb; ++j) {
+      perm[j] = j;
+    }
+    for (int j = nb - 1; j >= 0; --j) {
+      const int p = piv[j];
+      const int t = perm[j];
+      perm[j] = perm[p];
+      perm[p] = t;
+    }
+    if (*flag) {
+      atomicOr(&A.status[sl.grain], TMX_ST_SINGULAR);
+    }
+  }
+  __syncthreads();
+
+  // --------------------------------------------- solve T_c Q_c = -RgQ_c
+  const bool chain = sl.tout < 0;
+  for (int r0 = 0; r0 < nb; r0 += Rchunk) {
+    const int R = min(Rchunk, nb - r0);
+    for (int u = threadIdx.x; u < R * nb; u += blockDim.x) {
+      const cplx v = Rs[(int64_t)(r0 + u / nb) * nb + (u % nb)];
+      X[(u / nb) * lda + (u % nb)] = mkc(-v.x, -v.y);
+    }
+    __syncthreads();
+    // Z U = X (forward over columns)
+    for (int j = 0; j < nb; ++j) {
+      for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        X[r * lda + j] = cmul(X[r * lda + j], uinv[j]);
+      }
+      __syncthreads();
+      const int rem = nb - j - 1;
+      for (int u = threadIdx.x; u < R * rem; u += blockDim.x) {
+        const int r = u / rem;
+        const int k = j + 1 + u % rem;
+        X[r * lda + k] = csub(X[r * lda + k], cmul(X[r * lda + j], Am[j * lda + k]));
+      }
+      __syncthreads();
+    }
+    // Y L = Z (backward over columns, L unit lower)
+    for (int j = nb - 1; j >= 1; --j) {
+      for (int u = threadIdx.x; u < R * j; u += blockDim.x) {
+        const int r = u / j;
+        const int k = u % j;
+        X[r * lda + k] = csub(X[r * lda + k], cmul(X[r * lda + j], Am[j * lda + k]));
+      }
+      __syncthreads();
+    }
+    // write out: T_c[a][b] = Y[a][perm[b]]
+    if (chain) {
+      for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        const int a = r0 + r;
+        int ia, na;
+        member(D, a, ia, na);
+        A.diag[sl.diag + ia * N + (na - 1)] = X[r * lda + perm[a]];
+      }
+    } else {
+      cplx *Tb = A.tout + sl.tout + block_offset(N, m);
+      const int w2 = 2 * D.nbb;
+      for (int u = threadIdx.x; u < R * nb; u += blockDim.x) {
+        const int r = u / nb;
+        const int b = u % nb;
+        const int a = r0 + r;
+        int ia, na, ib, nbn;
+        member(D, a, ia, na);
+        member(D, b, ib, nbn);
+        const int row = ia * D.nbb + (na - D.nmin);
+        const int col = ib * D.nbb + (nbn - D.nmin);
+        Tb[(int64_t)row * w2 + col] = X[r * lda + perm[b]];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
+  const int nrp = (max_nb + TR - 1) / TR * TR + TR;
+  const int ncol = (max_nb + TC - 1) / TC * TC;
+  const size_t asm_bytes =
+      ((size_t)4 * chunk_nodes * nrp + (size_t)2 * 4 * chunk_nodes * ncol) *
+      sizeof(cplx);
+  const int lda = max_nb | 1;
+  size_t lu = ((size_t)max_nb * lda + max_nb) * sizeof(cplx) +
+              (3 * max_nb + 1) * sizeof(int);
+  lu = (lu + 15) & ~(size_t)15;
+  // at least 8 rows of the right-hand side per solve chunk
+  const int rows = max_nb < 8 ? max_nb : 8;
+  size_t lu_total = lu + (size_t)rows * lda * sizeof(cplx);
+  // prefer the whole right-hand side when it fits in 200 KB
+  const size_t full = lu + (size_t)max_nb * lda * sizeof(cplx);
+  if (full <= 200 * 1024) {
+    lu_total = full;
+  }
+  return asm_bytes > lu_total ? asm_bytes : lu_total;
+}
+
+void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
+  if (a.nitems <= 0) {
+    return;
+  }
+  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    attr_set = true;
+  }
+  int threads = 256;
+  if (a.max_nb <= 16) {
+    threads = 64;
+  } else if (a.max_nb <= 32) {
+    threads = 128;
+  }
+  k_blocks<<<a.nitems, threads, smem, stream>>>(a, smem);
+}
+
+// ----------------------------------------------------------- convergence --
+
+// One thread per active slot: m = 0 sums of the latest order in the
+// reference's order (TMatrixResource.hpp:743-756) and the convergence test
+// (:758-775). Unconverged slots that have orders left go to the next list.
+__global__ void k_converge(const int32_t *__restrict__ active, int nactive,
+                           const TmxSlot *__restrict__ slots,
+                           const cplx *__restrict__ diag, TmxChainState *state,
+                           double tolerance, int order, int last_order,
+                           int32_t *next_active, int32_t *next_count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nactive) {
+    return;
+  }
+  const int g = active[p];
+  const TmxSlot sl = slots[p];
+  const cplx *dg = diag + sl.diag;
+  const int N = order;
+  double qs = 0., qe = 0.;
+  for (int n = 1; n < N + 1; ++n) {
+    const double dn1 = 2. * n + 1.;
+    const cplx a = dg[n - 1];
+    const cplx b = dg[N + n - 1];
+    qs += dn1 * (cnorm2(a) + cnorm2(b));
+    qe += dn1 * (a.x + b.x);
+  }
+  TmxChainState st = state[g];
+  const double old_qs = st.qsca, old_qe = st.qext;
+  st.qsca = qs;
+  st.qext = qe;
+  st.nmax = N;
+  st.ngauss = sl.ngauss;
+  if (st.dqs_t == -2.) {
+    st.dqs_t = -1.;
+    st.dqe_t = -1.;
+  } else {
+    st.dqs_t = fabs((old_qs - qs) / qs);
+    st.dqe_t = fabs((old_qe - qe) / qe);
+  }
+  if (st.dqs_t > 0.) {
+    st.dqs = st.dqs_t;
+    st.dqe = st.dqe_t;
+    if (st.dqs_t <= tolerance && st.dqe_t <= tolerance) {
+      st.converged = 1;
+    }
+  }
+  bool finite = isfinite(qs) && isfinite(qe);
+  if (!finite) {
+    st.status |= TMX_ST_NAN;
+  }
+  if (!st.converged && finite) {
+    if (order < last_order) {
+      const int q = atomicAdd(next_count, 1);
+      next_active[q] = g;
+    } else {
+      st.status |= TMX_ST_NOT_CONVERGED;
+    }
+  }
+  state[g] = st;
+}
+
+void tmx_launch_converge(const int32_t *active, int nactive,
+                         const TmxSlot *slots, const double2 *diag,
+                         TmxChainState *state, double tolerance, int order,
+                         int last_order, int32_t *next_active,
+                         int32_t *next_count, cudaStream_t stream) {
+  if (nactive <= 0) {
+    return;
+  }
+  k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
+      active, nactive, slots, diag, state, tolerance, order, last_order,
+      next_active, next_count);
+}
+
+// ------------------------------------------------------------- Q sums ------
+
+// TMatrixQTask::execute (TMatrixResource.hpp:1136-1210): full Qsca and Qext
+// over every m block, one thread per grain, in the reference's order.
+__global__ void k_qsums(const int64_t *__restrict__ t_off,
+                        const int32_t *__restrict__ nmaxv, int n,
+                        const cplx *__restrict__ T, double *q_out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) {
+    return;
+  }
+  const int N = nmaxv[g];
+  const cplx *Tg = T + t_off[g];
+  auto el = [&](int i1, int n1, int m, int i2, int n2) -> cplx {
+    const cplx *B = Tg + block_offset(N, m);
+    if (m > 0) {
+      const int nm = N + 1 - m;
+      return B[(int64_t)(i1 * nm + n1 - m) * (2 * nm) + i2 * nm + n2 - m];
+    }
+    return B[(int64_t)(i1 * N + n1 - 1) * (2 * N) + i2 * N + n2 - 1];
+  };
+  double qs = 0.;
+  for (int n1 = 1; n1 < N + 1; ++n1) {
+    for (int n2 = 1; n2 < N + 1; ++n2) {
+      const int mtop = min(n1, n2);
+      for (int m1 = 0; m1 <= mtop; ++m1) {
+        const double factor = (m1 > 0) ? 2. : 1.;
+        qs += factor * cnorm2(el(0, n1, m1, 0, n2));
+        qs += factor * cnorm2(el(0, n1, m1, 1, n2));
+        qs += factor * cnorm2(el(1, n1, m1, 0, n2));
+        qs += factor * cnorm2(el(1, n1, m1, 1, n2));
+      }
+    }
+  }
+  double qe = 0.;
+  for (int n1 = 1; n1 < N + 1; ++n1) {
+    for (int m1 = 0; m1 < n1 + 1; ++m1) {
+      const double factor = (m1 > 0) ? 2. : 1.;
+      qe += factor * el(0, n1, m1, 0, n1).x;
+      qe += factor * el(0, n1, m1, 1, n1).x;
+      qe += factor * el(1, n1, m1, 0, n1).x;
+      qe += factor * el(1, n1, m1, 1, n1).x;
+    }
+  }
+  q_out[2 * g] = qs;
+  q_out[2 * g + 1] = qe;
+}
+
+void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
+                      const double2 *T, double *q_out, cudaStream_t stream) {
+  if (n <= 0) {
+    return;
+  }
+  k_qsums<<<(n + 127) / 128, 128, 0, stream>>>(t_off, nmax, n, T, q_out);
+}
+
+// ------------------------------------------------------------ chain prep --
+
+// Slots and items of one order step: active position p gets the tables at
+// p * strides and the four m = 0 classes as items 4p .. 4p + 3.
+__global__ void k_chain_prep(const int32_t *__restrict__ active, int nactive,
+                             int order, int ngauss, int wig_n,
+                             int64_t tab_stride, int64_t nsc_stride,
+                             int64_t diag_stride, int64_t scr_stride,
+                             TmxSlot *slots, TmxItem *items) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nactive) {
+    return;
+  }
+  TmxSlot s;
+  s.grain = active[p];
+  s.nmax = order;
+  s.ngauss = ngauss;
+  s.wig_n = wig_n;
+  s.tab = p * tab_stride;
+  s.nsc = p * nsc_stride;
+  s.tout = -1;
+  s.diag = p * diag_stride;
+  slots[p] = s;
+  for (int c = 0; c < 4; ++c) {
+    TmxItem it;
+    it.slot = p;
+    it.m = 0;
+    it.cls = (int16_t)c;
+    it.scratch = (4 * (int64_t)p + c) * scr_stride;
+    items[4 * p + c] = it;
+  }
+}
+
+void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
+                           int ngauss, int wig_n, int64_t tab_stride,
+                           int64_t nsc_stride, int64_t diag_stride,
+                           int64_t scr_stride, TmxSlot *slots, TmxItem *items,
+                           cudaStream_t stream) {
+  if (nactive <= 0) {
+    return;
+  }
+  k_chain_prep<<<(nactive + 127) / 128, 128, 0, stream>>>(
+      active, nactive, order, ngauss, wig_n, tab_stride, nsc_stride,
+      diag_stride, scr_stride, slots, items);
+}

@@ -1,0 +1,1040 @@
+// Host driver of the T-matrix library: the B200 replacement of the
+// reference's TaskManager + QuickSched pair for the T-matrix path.
+//
+// Reference (CosTuuM): TaskManager::generate_tasks (src/TaskManager.hpp:
+// 445-1346) builds, per grain, a chain InteractionTask(order) ->
+// TMatrixM0Task(order) for order = min_order .. max_order - 1 that stops at
+// convergence, then one TMatrixMAllTask per m; QuickSched runs the graph on
+// host threads. Here the same schedule is a device work flow:
+//   1. order loop ("wavefront"): every still-active grain advances one order
+//      per step -- Bessel tables, the m = 0 classes (assembly + LU + solve),
+//      then the convergence test and a device-side compaction of the active
+//      list. The host only reads the active count between steps.
+//   2. blocks: all (grain, m, class) items at the converged (nmax, ngauss),
+//      bucketed by class size, largest first.
+//   3. full Q sums per grain (TMatrixQTask).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/tmx.h"
+#include "tmx_common.cuh"
+#include "tmx_kernels.h"
+
+namespace {
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+} // namespace
+
+struct tmx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  // Gauss-Legendre cache: lower-half nodes of the 2 * ngauss rule
+  std::vector<int64_t> gl_off_h;
+  std::vector<double> gl_x_h, gl_w_h;
+  DevBuf gl_x, gl_w, gl_off;
+  bool gl_dirty = true;
+  // Wigner d table sets, keyed by (nmax, ngauss, all m?)
+  std::map<std::tuple<int, int, int>, int> wig_sets;
+  std::vector<int64_t> wig_off_h;
+  int64_t wig_used = 0;
+  DevBuf wig, wig_off;
+  // batch buffers
+  DevBuf grains, state, state0, act0, act1, actinit, count, slots, items, tab,
+      nsc, scratch, diag, T, t_off, nmaxv, q, status, probe;
+  // uploaded batch (device-resident inputs)
+  bool uploaded = false;
+  int64_t up_n = 0;
+  int up_nact = 0;
+  tmx_schedule up_sched;
+  std::vector<int32_t> up_status;
+  int32_t *pinned = nullptr;
+  // timing: events on the library stream
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  bool profiling = false;
+  struct Prof {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    double ms = 0.;
+    int64_t launches = 0;
+    double flops = 0.;
+  } prof[2]; // 0: block kernel, 1: table kernel
+  double flops_survey = 0.; // survey-model flops of the last batch
+  // last batch
+  int64_t n = 0;
+  bool have_batch = false;
+  std::vector<int32_t> nmax_h, ngauss_h, status_h;
+  std::vector<double> q_h;
+  std::vector<int64_t> t_off_h;
+};
+
+#define CK(call)                                                               \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+      return TMX_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+#define LAUNCHED()                                                             \
+  do {                                                                         \
+    ++ctx->launches;                                                           \
+    CK(cudaGetLastError());                                                    \
+  } while (0)
+
+// executed flops of one class item: assembly (4 real FMAs per entry, node
+// and term; 2 terms for m = 0), LU (8/3 nb^3) and the two triangular solves
+// with nb right-hand sides (8 nb^3)
+static double item_flops(int nb, int m, int ng) {
+  const double b = nb;
+  const double terms = (m == 0) ? 2. : 4.;
+  return 8. * terms * b * b * ng + (8. / 3.) * b * b * b + 8. * b * b * b;
+}
+
+static int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a) {
+  if (!ctx->profiling) {
+    return 0;
+  }
+  CK(cudaEventCreate(a));
+  CK(cudaEventRecord(*a, ctx->stream));
+  (void)k;
+  return 0;
+}
+
+static int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops) {
+  if (!ctx->profiling) {
+    return 0;
+  }
+  cudaEvent_t b;
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(b, ctx->stream));
+  ctx->prof[k].pending.push_back({a, b});
+  ctx->prof[k].launches += 1;
+  ctx->prof[k].flops += flops;
+  return 0;
+}
+
+// resolve recorded event pairs (after the stream has been synchronised)
+static int prof_resolve(tmx_ctx *ctx) {
+  for (auto &p : ctx->prof) {
+    for (auto &e : p.pending) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e.first, e.second));
+      p.ms += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    p.pending.clear();
+  }
+  return 0;
+}
+
+static int fail(tmx_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) {
+    ctx->err = msg;
+  }
+  return code;
+}
+
+// grow-only device buffer; contents are not preserved
+static int ensure(tmx_ctx *ctx, DevBuf &b, size_t bytes) {
+  if (bytes == 0) {
+    bytes = 16;
+  }
+  if (b.cap >= bytes) {
+    return TMX_OK;
+  }
+  if (b.p) {
+    CK(cudaFreeAsync(b.p, ctx->stream));
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  size_t want = bytes + bytes / 4;
+  cudaError_t e = cudaMallocAsync(&b.p, want, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMallocAsync(&b.p, bytes, ctx->stream);
+    want = bytes;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, TMX_ERR_NOMEM,
+                "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  b.cap = want;
+  return TMX_OK;
+}
+
+// grow-only device buffer that keeps its first `keep` bytes
+static int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep) {
+  if (b.cap >= bytes) {
+    return TMX_OK;
+  }
+  DevBuf nb;
+  size_t want = std::max(bytes, b.cap * 2);
+  if (cudaMallocAsync(&nb.p, want, ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, TMX_ERR_NOMEM, "device allocation failed (table cache)");
+  }
+  nb.cap = want;
+  if (b.p) {
+    if (keep) {
+      CK(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+    }
+    CK(cudaFreeAsync(b.p, ctx->stream));
+  }
+  b = nb;
+  return TMX_OK;
+}
+
+// ----------------------------------------------------- Gauss-Legendre ----
+
+// Gauss-Legendre rule of the given order on [-1, 1]: Newton iteration on
+// P_n from the Lether & Wenston (1995) initial guess, ascending nodes with a
+// symmetric fill. Same recipe and operation order as the reference's
+// SpecialFunctions::get_gauss_legendre_points_and_weights
+// (src/SpecialFunctions.hpp:646-715), so the nodes are the same doubles.
+static void gauss_legendre(int order, double *points, double *weights) {
+  const unsigned ind = (unsigned)order % 2;
+  const unsigned k = (unsigned)order / 2 + ind;
+  for (unsigned i = 0; i < k; ++i) {
+    const double theta = M_PI * (i + 0.75) / (order + 0.5);
+    const double oi = 1. / order;
+    const double oi2 = oi * oi;
+    double x = (1. - 0.125 * oi2 + (5. / 38.) * oi * oi2 -
+                (2. / 25.) * oi2 * oi2 * (1. - (14. / 39.) / (theta * theta))) *
+               cos(theta);
+    unsigned it = 0;
+    double check = 1.e-16;
+    double pa = 0., pb = 0.;
+    do {
+      ++it;
+      if (it > 100) {
+        check *= 10.;
+      }
+      pb = 1.;
+      double pc = x;
+      for (unsigned j = 1; j < (unsigned)order; ++j) {
+        pa = pb;
+        pb = pc;
+        pc = x * pb + (x * pb - pa) * j / (j + 1.);
+      }
+      pa = 1. / ((pb - x * pc) * order);
+      pb = pa * pc * (1. - x * x);
+      x = x - pb;
+    } while (fabs(pb) > check * fabs(x));
+    const unsigned m = order - i - 1;
+    points[m] = x;
+    weights[m] = 2. * pa * pa * (1. - x * x);
+    if (i != k - 1 || ind != 1) {
+      points[i] = -points[m];
+      weights[i] = weights[m];
+    }
+  }
+}
+
+static int ensure_gl(tmx_ctx *ctx, const std::vector<int> &ngs) {
+  for (int ng : ngs) {
+    if ((int)ctx->gl_off_h.size() <= ng) {
+      ctx->gl_off_h.resize(ng + 1, -1);
+    }
+    if (ctx->gl_off_h[ng] >= 0) {
+      continue;
+    }
+    std::vector<double> x(2 * ng), w(2 * ng);
+    gauss_legendre(2 * ng, x.data(), w.data());
+    ctx->gl_off_h[ng] = (int64_t)ctx->gl_x_h.size();
+    ctx->gl_x_h.insert(ctx->gl_x_h.end(), x.begin(), x.begin() + ng);
+    ctx->gl_w_h.insert(ctx->gl_w_h.end(), w.begin(), w.begin() + ng);
+    ctx->gl_dirty = true;
+  }
+  if (ctx->gl_dirty) {
+    int rc;
+    const size_t nb = ctx->gl_x_h.size() * sizeof(double);
+    if ((rc = ensure(ctx, ctx->gl_x, nb)) || (rc = ensure(ctx, ctx->gl_w, nb)) ||
+        (rc = ensure(ctx, ctx->gl_off, ctx->gl_off_h.size() * sizeof(int64_t)))) {
+      return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->gl_x.p, ctx->gl_x_h.data(), nb,
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->gl_w.p, ctx->gl_w_h.data(), nb,
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->gl_off.p, ctx->gl_off_h.data(),
+                       ctx->gl_off_h.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    // the host vectors must stay unchanged until the copies ran
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->gl_dirty = false;
+  }
+  return TMX_OK;
+}
+
+// Wigner table sets for (nmax, ngauss); all_m selects m = 0..nmax, else m = 0
+static int ensure_wigner(tmx_ctx *ctx,
+                         const std::vector<std::pair<int, int>> &keys,
+                         bool all_m, std::vector<int> &set_ids) {
+  std::vector<TmxWigJob> jobs;
+  set_ids.clear();
+  int max_work = 0;
+  const int64_t old_used = ctx->wig_used;
+  for (auto &kv : keys) {
+    const auto key = std::make_tuple(kv.first, kv.second, all_m ? 1 : 0);
+    auto it = ctx->wig_sets.find(key);
+    if (it != ctx->wig_sets.end()) {
+      set_ids.push_back(it->second);
+      continue;
+    }
+    TmxWigJob J;
+    J.nmax = kv.first;
+    J.ngauss = kv.second;
+    J.m_lo = 0;
+    J.m_hi = all_m ? kv.first : 0;
+    J.out = ctx->wig_used;
+    const int64_t sz = (int64_t)(J.m_hi + 1) * J.ngauss * J.nmax * 2;
+    ctx->wig_used += sz;
+    const int id = (int)ctx->wig_off_h.size();
+    ctx->wig_off_h.push_back(J.out);
+    ctx->wig_sets[key] = id;
+    set_ids.push_back(id);
+    jobs.push_back(J);
+    max_work = std::max(max_work, (J.m_hi + 1) * J.ngauss);
+  }
+  if (jobs.empty()) {
+    return TMX_OK;
+  }
+  int rc = ensure_keep(ctx, ctx->wig, ctx->wig_used * sizeof(double),
+                       old_used * sizeof(double));
+  if (rc) {
+    return rc;
+  }
+  if ((rc = ensure(ctx, ctx->wig_off, ctx->wig_off_h.size() * sizeof(int64_t)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->wig_off.p, ctx->wig_off_h.data(),
+                     ctx->wig_off_h.size() * sizeof(int64_t),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  TmxWigJob *djobs = nullptr;
+  CK(cudaMallocAsync((void **)&djobs, jobs.size() * sizeof(TmxWigJob),
+                     ctx->stream));
+  CK(cudaMemcpyAsync(djobs, jobs.data(), jobs.size() * sizeof(TmxWigJob),
+                     cudaMemcpyHostToDevice, ctx->stream));
+  tmx_launch_wigner(djobs, (int)jobs.size(), max_work,
+                    (const double *)ctx->gl_x.p, (const int64_t *)ctx->gl_off.p,
+                    (double *)ctx->wig.p, ctx->stream);
+  LAUNCHED();
+  CK(cudaFreeAsync(djobs, ctx->stream));
+  // host vectors referenced by the async copies must outlive them
+  CK(cudaStreamSynchronize(ctx->stream));
+  return TMX_OK;
+}
+
+// ----------------------------------------------------------- class sizes --
+
+// number of members of class `cls` of block m at order N (see describe() in
+// tmx_blocks.cu)
+static int class_size(int N, int m, int cls) {
+  if (m == 0) {
+    const int n0 = (cls & 1) ? 1 : 2;
+    return (N >= n0) ? (N - n0) / 2 + 1 : 0;
+  }
+  const int nA0 = ((m & 1) == cls) ? m : m + 1;
+  const int nB0 = ((m & 1) == (cls ^ 1)) ? m : m + 1;
+  const int R0 = (N >= nA0) ? (N - nA0) / 2 + 1 : 0;
+  const int R1 = (N >= nB0) ? (N - nB0) / 2 + 1 : 0;
+  return R0 + R1;
+}
+
+static int chunk_nodes_for(int max_nb) {
+  const int nrp = (max_nb + 3) / 4 * 4 + 4;
+  const int ncol = (max_nb + 3) / 4 * 4;
+  const size_t per_node = (size_t)(4 * nrp + 8 * ncol) * 16;
+  const int lda = max_nb | 1;
+  const size_t lu = ((size_t)max_nb * lda + max_nb) * 16 * 2;
+  const size_t budget = std::max<size_t>(64 * 1024, std::min<size_t>(lu, 200 * 1024));
+  int G = (int)(budget / per_node);
+  return std::max(1, std::min(32, G));
+}
+
+extern "C" {
+
+int64_t tmx_tmatrix_size(int32_t nmax) {
+  if (nmax <= 0) {
+    return 0;
+  }
+  int64_t s = 4 * (int64_t)nmax * nmax;
+  for (int m = 1; m <= nmax; ++m) {
+    const int64_t nb = nmax + 1 - m;
+    s += 4 * nb * nb;
+  }
+  return s;
+}
+
+int tmx_create(tmx_ctx **out, int device) {
+  if (!out) {
+    return TMX_ERR_INVALID;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+    cudaGetLastError();
+    return TMX_ERR_NO_DEVICE;
+  }
+  tmx_ctx *ctx = new tmx_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) !=
+          cudaSuccess ||
+      cudaMallocHost((void **)&ctx->pinned, 64) != cudaSuccess) {
+    cudaGetLastError();
+    delete ctx;
+    return TMX_ERR_CUDA;
+  }
+  *out = ctx;
+  return TMX_OK;
+}
+
+void tmx_destroy(tmx_ctx *ctx) {
+  if (!ctx) {
+    return;
+  }
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->t0) {
+    cudaEventDestroy(ctx->t0);
+    cudaEventDestroy(ctx->t1);
+  }
+  DevBuf *bufs[] = {&ctx->state0, &ctx->actinit,
+                    &ctx->gl_x,  &ctx->gl_w,   &ctx->gl_off,  &ctx->wig,
+                    &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,
+                    &ctx->act1,  &ctx->count,  &ctx->slots,   &ctx->items,
+                    &ctx->tab,   &ctx->nsc,    &ctx->scratch, &ctx->diag,
+                    &ctx->T,     &ctx->t_off,  &ctx->nmaxv,   &ctx->q,
+                    &ctx->status, &ctx->probe};
+  for (DevBuf *b : bufs) {
+    if (b->p) {
+      cudaFreeAsync(b->p, ctx->stream);
+    }
+  }
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->pinned) {
+    cudaFreeHost(ctx->pinned);
+  }
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *tmx_last_error(const tmx_ctx *ctx) {
+  return ctx ? ctx->err.c_str() : "no context";
+}
+
+int64_t tmx_kernel_launches(const tmx_ctx *ctx) {
+  return ctx ? ctx->launches : 0;
+}
+
+int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                     const double *wavelength, const double *mr,
+                     const double *mi, const double *axis_ratio,
+                     const tmx_schedule *sched) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  if (n < 0 || (n > 0 && (!r_ev || !wavelength || !mr || !mi || !axis_ratio))) {
+    return fail(ctx, TMX_ERR_INVALID, "null input array or negative n");
+  }
+  tmx_schedule S = {10, 100, 2, 0, 1.e-4};
+  if (sched) {
+    S = *sched;
+  }
+  if (S.bessel_start <= 0) {
+    S.bessel_start = 800;
+  }
+  if (S.min_order < 2 || S.max_order <= S.min_order ||
+      S.gauss_legendre_factor < 1 || !(S.tolerance >= 0.)) {
+    return fail(ctx, TMX_ERR_INVALID,
+                "schedule needs 2 <= min_order < max_order, factor >= 1, "
+                "tolerance >= 0");
+  }
+  if (S.max_order - 1 > TMX_MAX_NB) {
+    return fail(ctx, TMX_ERR_INVALID,
+                "max_order - 1 exceeds the on-chip block limit " +
+                    std::to_string(TMX_MAX_NB));
+  }
+  if (S.bessel_start < S.max_order) {
+    return fail(ctx, TMX_ERR_INVALID, "bessel_start must be >= max_order");
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  ctx->uploaded = false;
+  ctx->have_batch = false;
+  int rc;
+
+  // ---- grains (host constants, as the reference computes them)
+  std::vector<TmxGrain> gr(n);
+  std::vector<int32_t> act;
+  act.reserve(n);
+  std::vector<TmxChainState> st0(n);
+  for (int64_t i = 0; i < n; ++i) {
+    TmxGrain &g = gr[i];
+    g.r_ev = r_ev[i];
+    g.k = 2. * M_PI / wavelength[i];
+    g.mr = mr[i];
+    g.mi = mi[i];
+    g.axis_ratio = axis_ratio[i];
+    g.cbrt_d = cbrt(axis_ratio[i]);
+    TmxChainState &s = st0[i];
+    s.qsca = s.qext = 0.;
+    s.dqs_t = s.dqe_t = -2.;
+    s.dqs = s.dqe = -1.;
+    s.nmax = s.ngauss = 0;
+    s.converged = 0;
+    s.status = 0;
+    const bool ok = std::isfinite(r_ev[i]) && r_ev[i] > 0. &&
+                    std::isfinite(wavelength[i]) && wavelength[i] > 0. &&
+                    std::isfinite(axis_ratio[i]) && axis_ratio[i] > 0. &&
+                    std::isfinite(mr[i]) && std::isfinite(mi[i]);
+    if (ok) {
+      act.push_back((int32_t)i);
+    } else {
+      s.status = TMX_ST_BAD_INPUT;
+    }
+  }
+  if ((rc = ensure(ctx, ctx->grains, n * sizeof(TmxGrain))) ||
+      (rc = ensure(ctx, ctx->state, n * sizeof(TmxChainState))) ||
+      (rc = ensure(ctx, ctx->state0, n * sizeof(TmxChainState))) ||
+      (rc = ensure(ctx, ctx->actinit, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->act0, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->act1, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->count, 16)) ||
+      (rc = ensure(ctx, ctx->status, n * sizeof(int32_t)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->grains.p, gr.data(), n * sizeof(TmxGrain),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->state0.p, st0.data(), n * sizeof(TmxChainState),
+                     cudaMemcpyHostToDevice, st));
+  if (!act.empty()) {
+    CK(cudaMemcpyAsync(ctx->actinit.p, act.data(), act.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+  }
+  // the host arrays above are about to go out of scope
+  CK(cudaStreamSynchronize(st));
+  ctx->up_n = n;
+  ctx->up_nact = (int)act.size();
+  ctx->up_sched = S;
+  ctx->up_status.resize(n);
+  for (int64_t i = 0; i < n; ++i) {
+    ctx->up_status[i] = st0[i].status;
+  }
+  ctx->uploaded = true;
+  return TMX_OK;
+}
+
+int tmx_batch_compute(tmx_ctx *ctx) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->uploaded) {
+    return fail(ctx, TMX_ERR_STATE, "no batch uploaded");
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->up_n;
+  const tmx_schedule S = ctx->up_sched;
+  const int glf = S.gauss_legendre_factor;
+  int rc;
+  ctx->have_batch = false;
+  ctx->n = n;
+  ctx->nmax_h.assign(n, 0);
+  ctx->ngauss_h.assign(n, 0);
+  ctx->status_h.assign(n, 0);
+  ctx->q_h.assign(6 * n, 0.);
+  ctx->t_off_h.assign(n, 0);
+  ctx->flops_survey = 0.;
+  if (n == 0) {
+    ctx->have_batch = true;
+    return TMX_OK;
+  }
+  std::vector<TmxChainState> st0(n);
+  CK(cudaMemcpyAsync(ctx->state.p, ctx->state0.p, n * sizeof(TmxChainState),
+                     cudaMemcpyDeviceToDevice, st));
+  if (ctx->up_nact > 0) {
+    CK(cudaMemcpyAsync(ctx->act0.p, ctx->actinit.p,
+                       ctx->up_nact * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                       st));
+  }
+  CK(cudaMemsetAsync(ctx->status.p, 0, n * sizeof(int32_t), st));
+
+  // ---- tables shared by all grains
+  std::vector<int> ngs;
+  std::vector<std::pair<int, int>> chain_keys;
+  for (int k = S.min_order; k < S.max_order; ++k) {
+    ngs.push_back(glf * k);
+    chain_keys.push_back({k, glf * k});
+  }
+  if ((rc = ensure_gl(ctx, ngs))) {
+    return rc;
+  }
+  std::vector<int> chain_sets;
+  if ((rc = ensure_wigner(ctx, chain_keys, false, chain_sets))) {
+    return rc;
+  }
+
+  // ---- 1. order loop
+  int nact = ctx->up_nact;
+  DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
+  const size_t budget = (size_t)8 << 30; // table bytes per chunk
+  for (int k = S.min_order; k < S.max_order && nact > 0; ++k) {
+    const int ng = glf * k;
+    const int64_t tab_stride = (int64_t)ng * k * TMX_NQ;
+    const int64_t nsc_stride = (int64_t)ng * TMX_NS;
+    const int cmax = (k + 1) / 2;
+    const int64_t scr_stride = 2 * (int64_t)cmax * cmax;
+    const size_t per_slot = (tab_stride + nsc_stride) * sizeof(double) +
+                            (4 * scr_stride + 2 * k) * sizeof(cplx);
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nact, budget / per_slot));
+    if ((rc = ensure(ctx, ctx->tab, chunk * tab_stride * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->nsc, chunk * nsc_stride * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->scratch, chunk * 4 * scr_stride * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->diag, (size_t)chunk * 2 * k * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->slots, chunk * sizeof(TmxSlot))) ||
+        (rc = ensure(ctx, ctx->items, 4 * (size_t)chunk * sizeof(TmxItem)))) {
+      return rc;
+    }
+    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(int32_t), st));
+    const int last = S.max_order - 1;
+    for (int c0 = 0; c0 < nact; c0 += chunk) {
+      const int cn = std::min(chunk, nact - c0);
+      const int32_t *a = (const int32_t *)cur->p + c0;
+      tmx_launch_chain_prep(a, cn, k, ng, chain_sets[k - S.min_order],
+                            tab_stride, nsc_stride, 2 * k, scr_stride,
+                            (TmxSlot *)ctx->slots.p, (TmxItem *)ctx->items.p, st);
+      LAUNCHED();
+      cudaEvent_t pe = nullptr;
+      if ((rc = prof_begin(ctx, 1, &pe))) {
+        return rc;
+      }
+      tmx_launch_tables((const TmxSlot *)ctx->slots.p, cn,
+                        (const TmxGrain *)ctx->grains.p,
+                        (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
+                        (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
+                        (double *)ctx->nsc.p, S.bessel_start, st);
+      LAUNCHED();
+      if ((rc = prof_end(ctx, 1, pe, 0.))) {
+        return rc;
+      }
+      TmxBlockArgs B;
+      B.items = (const TmxItem *)ctx->items.p;
+      B.nitems = 4 * cn;
+      B.slots = (const TmxSlot *)ctx->slots.p;
+      B.grains = (const TmxGrain *)ctx->grains.p;
+      B.tab = (const double *)ctx->tab.p;
+      B.nsc = (const double *)ctx->nsc.p;
+      B.wig = (const double *)ctx->wig.p;
+      B.wig_off = (const int64_t *)ctx->wig_off.p;
+      B.scratch = (cplx *)ctx->scratch.p;
+      B.tout = nullptr;
+      B.diag = (cplx *)ctx->diag.p;
+      B.status = (int32_t *)ctx->status.p;
+      B.max_nb = cmax;
+      B.chunk_nodes = chunk_nodes_for(cmax);
+      double fl = 0.;
+      for (int c = 0; c < 4; ++c) {
+        fl += item_flops(class_size(k, 0, c), 0, ng);
+      }
+      if ((rc = prof_begin(ctx, 0, &pe))) {
+        return rc;
+      }
+      tmx_launch_blocks(B, st);
+      LAUNCHED();
+      if ((rc = prof_end(ctx, 0, pe, fl * cn))) {
+        return rc;
+      }
+      tmx_launch_converge(a, cn, (const TmxSlot *)ctx->slots.p,
+                          (const cplx *)ctx->diag.p,
+                          (TmxChainState *)ctx->state.p, S.tolerance, k, last,
+                          (int32_t *)nxt->p, (int32_t *)ctx->count.p, st);
+      LAUNCHED();
+    }
+    CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    nact = ctx->pinned[0];
+    std::swap(cur, nxt);
+  }
+
+  // ---- per-grain outcome of the order loop
+  CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  std::vector<int32_t> p2; // grains that get blocks
+  for (int64_t i = 0; i < n; ++i) {
+    ctx->nmax_h[i] = st0[i].nmax;
+    ctx->ngauss_h[i] = st0[i].ngauss;
+    ctx->status_h[i] = st0[i].status | ctx->up_status[i];
+    ctx->q_h[6 * i + 0] = st0[i].qsca;
+    ctx->q_h[6 * i + 1] = st0[i].qext;
+    ctx->q_h[6 * i + 4] = st0[i].dqs;
+    ctx->q_h[6 * i + 5] = st0[i].dqe;
+    if (st0[i].nmax > 0) {
+      p2.push_back((int32_t)i);
+    }
+  }
+
+  // ---- 2. all blocks at the converged orders
+  const int np2 = (int)p2.size();
+  std::vector<TmxSlot> slots(np2);
+  std::vector<std::pair<int, int>> keys;
+  std::map<std::pair<int, int>, int> key_idx;
+  int64_t tab_total = 0, nsc_total = 0, t_total = 0;
+  for (int s = 0; s < np2; ++s) {
+    const int g = p2[s];
+    const int N = ctx->nmax_h[g], ng = ctx->ngauss_h[g];
+    auto kk = std::make_pair(N, ng);
+    if (!key_idx.count(kk)) {
+      key_idx[kk] = (int)keys.size();
+      keys.push_back(kk);
+    }
+    TmxSlot &sl = slots[s];
+    sl.grain = g;
+    sl.nmax = N;
+    sl.ngauss = ng;
+    sl.tab = tab_total;
+    sl.nsc = nsc_total;
+    sl.tout = t_total;
+    sl.diag = 0;
+    ctx->t_off_h[g] = t_total;
+    tab_total += (int64_t)ng * N * TMX_NQ;
+    nsc_total += (int64_t)ng * TMX_NS;
+    t_total += tmx_tmatrix_size(N);
+  }
+  std::vector<int> full_sets;
+  if ((rc = ensure_wigner(ctx, keys, true, full_sets))) {
+    return rc;
+  }
+  for (int s = 0; s < np2; ++s) {
+    slots[s].wig_n = full_sets[key_idx[std::make_pair(slots[s].nmax, slots[s].ngauss)]];
+  }
+  // items, bucketed by class size (largest first)
+  struct HItem {
+    int nb;
+    TmxItem it;
+  };
+  std::vector<HItem> hitems;
+  for (int s = 0; s < np2; ++s) {
+    const int N = slots[s].nmax;
+    for (int m = 0; m <= N; ++m) {
+      const int ncls = (m == 0) ? 4 : 2;
+      for (int c = 0; c < ncls; ++c) {
+        const int nb = class_size(N, m, c);
+        if (nb <= 0) {
+          continue;
+        }
+        HItem h;
+        h.nb = nb;
+        h.it.slot = s;
+        h.it.m = (int16_t)m;
+        h.it.cls = (int16_t)c;
+        h.it.scratch = 0;
+        hitems.push_back(h);
+      }
+    }
+  }
+  std::stable_sort(hitems.begin(), hitems.end(),
+                   [](const HItem &a, const HItem &b) { return a.nb > b.nb; });
+  std::vector<TmxItem> items(hitems.size());
+  int64_t scr_total = 0;
+  for (size_t i = 0; i < hitems.size(); ++i) {
+    items[i] = hitems[i].it;
+    items[i].scratch = scr_total;
+    scr_total += 2 * (int64_t)hitems[i].nb * hitems[i].nb;
+  }
+  if ((rc = ensure(ctx, ctx->tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->slots, std::max(1, np2) * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->items, std::max<size_t>(1, items.size()) * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
+    return rc;
+  }
+  if (np2 > 0) {
+    CK(cudaMemcpyAsync(ctx->slots.p, slots.data(), np2 * sizeof(TmxSlot),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(TmxItem),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->T.p, 0, t_total * sizeof(cplx), st));
+    cudaEvent_t pe = nullptr;
+    if ((rc = prof_begin(ctx, 1, &pe))) {
+      return rc;
+    }
+    tmx_launch_tables((const TmxSlot *)ctx->slots.p, np2,
+                      (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
+                      (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
+                      (double *)ctx->tab.p, (double *)ctx->nsc.p, S.bessel_start,
+                      st);
+    LAUNCHED();
+    if ((rc = prof_end(ctx, 1, pe, 0.))) {
+      return rc;
+    }
+    // buckets by class size
+    const int edges[] = {128, 64, 32, 16, 0};
+    size_t i0 = 0;
+    for (int b = 0; b < 4; ++b) {
+      size_t i1 = i0;
+      while (i1 < hitems.size() && hitems[i1].nb > edges[b + 1]) {
+        ++i1;
+      }
+      if (i1 > i0) {
+        TmxBlockArgs B;
+        B.items = (const TmxItem *)ctx->items.p + i0;
+        B.nitems = (int)(i1 - i0);
+        B.slots = (const TmxSlot *)ctx->slots.p;
+        B.grains = (const TmxGrain *)ctx->grains.p;
+        B.tab = (const double *)ctx->tab.p;
+        B.nsc = (const double *)ctx->nsc.p;
+        B.wig = (const double *)ctx->wig.p;
+        B.wig_off = (const int64_t *)ctx->wig_off.p;
+        B.scratch = (cplx *)ctx->scratch.p;
+        B.tout = (cplx *)ctx->T.p;
+        B.diag = nullptr;
+        B.status = (int32_t *)ctx->status.p;
+        B.max_nb = hitems[i0].nb;
+        B.chunk_nodes = chunk_nodes_for(B.max_nb);
+        double fl = 0.;
+        for (size_t q = i0; q < i1; ++q) {
+          fl += item_flops(hitems[q].nb, hitems[q].it.m,
+                           slots[hitems[q].it.slot].ngauss);
+        }
+        if ((rc = prof_begin(ctx, 0, &pe))) {
+          return rc;
+        }
+        tmx_launch_blocks(B, st);
+        LAUNCHED();
+        if ((rc = prof_end(ctx, 0, pe, fl))) {
+          return rc;
+        }
+      }
+      i0 = i1;
+    }
+    // ---- 3. full Q sums
+    std::vector<int32_t> nmv(n);
+    for (int64_t i = 0; i < n; ++i) {
+      nmv[i] = ctx->nmax_h[i];
+    }
+    CK(cudaMemcpyAsync(ctx->t_off.p, ctx->t_off_h.data(), n * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->nmaxv.p, nmv.data(), n * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    tmx_launch_qsums((const int64_t *)ctx->t_off.p, (const int32_t *)ctx->nmaxv.p,
+                     (int)n, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
+    LAUNCHED();
+    std::vector<double> q2(2 * n);
+    std::vector<int32_t> stb(n);
+    CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < n; ++i) {
+      if (ctx->nmax_h[i] > 0) {
+        ctx->q_h[6 * i + 2] = q2[2 * i];
+        ctx->q_h[6 * i + 3] = q2[2 * i + 1];
+      }
+      ctx->status_h[i] |= stb[i];
+    }
+  }
+  // survey-model flops (per grain: every order of the m = 0 chain on the
+  // unreduced 2k x 2k block, then every m >= 1 block on 2nm x 2nm)
+  for (int64_t i = 0; i < n; ++i) {
+    const int N = ctx->nmax_h[i];
+    if (N <= 0) {
+      continue;
+    }
+    for (int k = S.min_order; k <= N; ++k) {
+      const double b = k, g = glf * k, t = 2. * k;
+      ctx->flops_survey += 8. * 4. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+    }
+    for (int m = 1; m <= N; ++m) {
+      const double b = N + 1 - m, g = ctx->ngauss_h[i], t = 2. * b;
+      ctx->flops_survey += 8. * 10. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+    }
+  }
+  if ((rc = prof_resolve(ctx))) {
+    return rc;
+  }
+  ctx->have_batch = true;
+  return TMX_OK;
+}
+
+int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                      const double *wavelength, const double *mr,
+                      const double *mi, const double *axis_ratio,
+                      const tmx_schedule *sched) {
+  int rc = tmx_batch_upload(ctx, n, r_ev, wavelength, mr, mi, axis_ratio, sched);
+  if (rc) {
+    return rc;
+  }
+  return tmx_batch_compute(ctx);
+}
+
+int tmx_batch_results(tmx_ctx *ctx, int32_t *nmax, int32_t *ngauss,
+                      int32_t *status, double *q) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  const size_t n = ctx->n;
+  if (nmax) {
+    memcpy(nmax, ctx->nmax_h.data(), n * sizeof(int32_t));
+  }
+  if (ngauss) {
+    memcpy(ngauss, ctx->ngauss_h.data(), n * sizeof(int32_t));
+  }
+  if (status) {
+    memcpy(status, ctx->status_h.data(), n * sizeof(int32_t));
+  }
+  if (q) {
+    memcpy(q, ctx->q_h.data(), 6 * n * sizeof(double));
+  }
+  return TMX_OK;
+}
+
+int tmx_batch_tmatrix(tmx_ctx *ctx, int64_t grain, double *out) {
+  if (!ctx || !out) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch || grain < 0 || grain >= ctx->n) {
+    return fail(ctx, TMX_ERR_STATE, "grain index out of range");
+  }
+  const int64_t sz = tmx_tmatrix_size(ctx->nmax_h[grain]);
+  if (sz == 0) {
+    return TMX_OK;
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(out, (const cplx *)ctx->T.p + ctx->t_off_h[grain],
+                     sz * sizeof(cplx), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return TMX_OK;
+}
+
+int tmx_timer_start(tmx_ctx *ctx) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (!ctx->t0) {
+    CK(cudaEventCreate(&ctx->t0));
+    CK(cudaEventCreate(&ctx->t1));
+  }
+  CK(cudaEventRecord(ctx->t0, ctx->stream));
+  return TMX_OK;
+}
+
+int tmx_timer_stop(tmx_ctx *ctx, double *ms) {
+  if (!ctx || !ms || !ctx->t0) {
+    return TMX_ERR_INVALID;
+  }
+  CK(cudaEventRecord(ctx->t1, ctx->stream));
+  CK(cudaEventSynchronize(ctx->t1));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, ctx->t0, ctx->t1));
+  *ms = f;
+  return TMX_OK;
+}
+
+int tmx_profile_enable(tmx_ctx *ctx, int on) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  ctx->profiling = on != 0;
+  for (auto &p : ctx->prof) {
+    p.ms = 0.;
+    p.launches = 0;
+    p.flops = 0.;
+  }
+  return TMX_OK;
+}
+
+int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
+                     double *flops) {
+  if (!ctx || kernel < 0 || kernel > 1) {
+    return TMX_ERR_INVALID;
+  }
+  if (ms) {
+    *ms = ctx->prof[kernel].ms;
+  }
+  if (launches) {
+    *launches = ctx->prof[kernel].launches;
+  }
+  if (flops) {
+    *flops = ctx->prof[kernel].flops;
+  }
+  return TMX_OK;
+}
+
+double tmx_batch_flops_survey(const tmx_ctx *ctx) {
+  return ctx ? ctx->flops_survey : 0.;
+}
+
+int tmx_probe_fp64(tmx_ctx *ctx, int kind, double *tflops) {
+  if (!ctx || !tflops) {
+    return TMX_ERR_INVALID;
+  }
+  CK(cudaSetDevice(ctx->device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  const int blocks = sms * 8;
+  const int iters = 4096;
+  int rc;
+  if ((rc = ensure(ctx, ctx->probe, (size_t)blocks * 256 * sizeof(double)))) {
+    return rc;
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    CK(cudaEventRecord(e0, ctx->stream));
+    if (kind == 0) {
+      tmx_launch_probe_dfma((double *)ctx->probe.p, iters, blocks, ctx->stream);
+    } else {
+      tmx_launch_probe_dmma((double *)ctx->probe.p, iters, blocks, ctx->stream);
+    }
+    LAUNCHED();
+    CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) {
+      best = std::min(best, ms);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  double flops;
+  if (kind == 0) {
+    flops = 2.0 * 8 * iters * (double)blocks * 256;
+  } else {
+    flops = 512.0 * 8 * iters * (double)blocks * (256 / 32);
+  }
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return TMX_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,81 @@
+// Host-side launch wrappers of the CUDA kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tmx_internal.h"
+
+// One Wigner d table set: all m in [m_lo, m_hi] at the lower-half nodes of
+// the 2 ngauss Gauss-Legendre rule, n = 1..nmax.
+struct TmxWigJob {
+  int32_t nmax;
+  int32_t ngauss;
+  int32_t m_lo;
+  int32_t m_hi;
+  int64_t out; // offset (doubles) into the Wigner buffer
+};
+
+// Per-grain convergence state of the order loop (ConvergedSizeResources and
+// the Q sums kept in TMatrixResource).
+struct TmxChainState {
+  double qsca, qext;   // m = 0 sums of the latest order
+  double dqs_t, dqe_t; // TMatrixResource::_dQscattering/_dQextinction
+  double dqs, dqe;     // ConvergedSizeResources::_dQs/_dQe
+  int32_t nmax, ngauss;
+  int32_t converged;
+  int32_t status;
+};
+
+void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
+                       const double *gl_x, const double *gl_w,
+                       const int64_t *gl_off, double *tab, double *nsc,
+                       int bessel_start, cudaStream_t stream);
+
+void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,
+                       const double *gl_x, const int64_t *gl_off, double *out,
+                       cudaStream_t stream);
+
+// block kernel: assembly + LU + solve for a list of (slot, m, class) items
+struct TmxBlockArgs {
+  const TmxItem *items;
+  int nitems;
+  const TmxSlot *slots;
+  const TmxGrain *grains;
+  const double *tab;
+  const double *nsc;
+  const double *wig;           // Wigner buffer
+  const int64_t *wig_off;      // per Wigner set: offset of m = 0 (doubles)
+  double2 *scratch;            // per-item Q / RgQ scratch
+  double2 *tout;               // T-matrix storage (complex)
+  double2 *diag;               // chain-mode diagonal buffer
+  int32_t *status;             // per grain status bits
+  int chunk_nodes;             // quadrature nodes per shared-memory chunk
+  int max_nb;                  // largest class size in this launch
+};
+size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes);
+void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream);
+
+// slots and m = 0 items of one order step from the active list
+void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
+                           int ngauss, int wig_n, int64_t tab_stride,
+                           int64_t nsc_stride, int64_t diag_stride,
+                           int64_t scr_stride, TmxSlot *slots, TmxItem *items,
+                           cudaStream_t stream);
+
+// convergence step for the active slots of one order
+void tmx_launch_converge(const int32_t *active, int nactive,
+                         const TmxSlot *slots, const double2 *diag,
+                         TmxChainState *state, double tolerance, int order,
+                         int last_order, int32_t *next_active,
+                         int32_t *next_count, cudaStream_t stream);
+
+// full Q sums over all m blocks (TMatrixQTask)
+void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
+                      const double2 *T, double *q_out, cudaStream_t stream);
+
+// FP64 throughput probes (DFMA pipe and DMMA tensor pipe)
+void tmx_launch_probe_dfma(double *out, int iters, int blocks,
+                           cudaStream_t stream);
+void tmx_launch_probe_dmma(double *out, int iters, int blocks,
+                           cudaStream_t stream);

@@ -1,0 +1,290 @@
+// Table kernels: node scalars, spherical Bessel/Hankel tables and Wigner d
+// tables on device (sm_100a, FP64).
+//
+// This translation unit is compiled with --fmad=false: the recurrences below
+// follow the reference's operation order (src/SpecialFunctions.hpp) and, with
+// no fused multiply-add, round the way the reference's x86-64 build rounds.
+// Transcendentals (sin, cos, cosh, sinh) come from CUDA's libdevice and may
+// differ from the C library by an ulp.
+#include "tmx_common.cuh"
+#include "tmx_kernels.h"
+
+// ---------------------------------------------------------------- Bessel --
+
+// Spherical j_n and [z j_n]'/z, n = 1..nmax, for a real argument, by the
+// downward ratio recurrence rho_n = j_n / j_{n-1} started at n = nstart with
+// rho ~ z / (2 nstart + 1), then j_n = rho_n j_{n-1} upward
+// (SpecialFunctions::spherical_j_jdj_array, SpecialFunctions.hpp:201-240).
+// out[(n-1) * stride + 0] = j_n, [+1] = [z j_n]'/z
+__device__ static void bessel_j_real(int nmax, int nstart, double z,
+                                     double *out, int stride) {
+  const double zinv = 1. / z;
+  double cur = z / (2. * nstart + 1.);
+  for (int index = nstart - 1; index >= 1; --index) {
+    const double twoip1 = 2. * index + 1.;
+    const double nxt = 1. / (twoip1 * zinv - cur);
+    if (index - 1 < nmax) {
+      out[(index - 1) * stride] = nxt; // rho_{index-1} (0-based), kept
+    }
+    cur = nxt;
+  }
+  const double j0 = sin(z) * zinv;
+  double jprev = out[0] * j0;
+  out[0] = jprev;
+  out[1] = j0 - jprev * zinv;
+  for (int i = 1; i < nmax; ++i) {
+    const double ji = out[i * stride] * jprev;
+    const double ip1 = i + 1.;
+    out[i * stride] = ji;
+    out[i * stride + 1] = jprev - ip1 * zinv * ji;
+    jprev = ji;
+  }
+}
+
+// Spherical y_n and [z y_n]'/z by the upward recurrence from y_1, y_2
+// (SpecialFunctions::spherical_y_ydy_array, SpecialFunctions.hpp:106-140).
+__device__ static void bessel_y_real(int nmax, double z, double *out,
+                                     int stride) {
+  double sinz, cosz;
+  sincos(z, &sinz, &cosz);
+  const double zinv = 1. / z;
+  const double zinv2 = zinv * zinv;
+  const double zinv3 = zinv2 * zinv;
+  double y0 = -cosz * zinv2 - sinz * zinv;
+  double y1 = (-3. * zinv3 + zinv) * cosz - 3. * zinv2 * sinz;
+  out[0] = y0;
+  out[1] = -zinv * (cosz + y0);
+  if (nmax > 1) {
+    out[stride] = y1;
+    out[stride + 1] = y0 - 2. * zinv * y1;
+  }
+  for (int i = 2; i < nmax; ++i) {
+    const double twoip1 = 2. * i + 1.;
+    const double ip1 = i + 1.;
+    const double yi = twoip1 * zinv * y1 - y0;
+    out[i * stride] = yi;
+    out[i * stride + 1] = y1 - ip1 * zinv * yi;
+    y0 = y1;
+    y1 = yi;
+  }
+}
+
+// complex sine sin(x) cosh(y) + i cos(x) sinh(y)
+__device__ static cplx csin_dev(cplx z) {
+  double s, c;
+  sincos(z.x, &s, &c);
+  return mkc(s * cosh(z.y), c * sinh(z.y));
+}
+
+// Complex-argument version of bessel_j_real: every constant enters as a
+// complex number in the reference (std::complex arithmetic); multiplying by a
+// complex number with zero imaginary part equals scaling by its real part
+// bit for bit, which is what is done here.
+// out[(n-1) * stride + {0,1,2,3}] = (Re j, Im j, Re dj, Im dj)
+__device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
+                                        double *out, int stride) {
+  const cplx zinv = cinv(z);
+  cplx cur = cdiv(z, mkc(2. * nstart + 1., 0.));
+  for (int index = nstart - 1; index >= 1; --index) {
+    const double twoip1 = 2. * index + 1.;
+    const cplx nxt = cinv(csub(cscale(zinv, twoip1), cur));
+    if (index - 1 < nmax) {
+      out[(index - 1) * stride] = nxt.x;
+      out[(index - 1) * stride + 1] = nxt.y;
+    }
+    cur = nxt;
+  }
+  const cplx j0 = cmul(csin_dev(z), zinv);
+  cplx jprev = cmul(mkc(out[0], out[1]), j0);
+  out[0] = jprev.x;
+  out[1] = jprev.y;
+  const cplx dj0 = csub(j0, cmul(jprev, zinv));
+  out[2] = dj0.x;
+  out[3] = dj0.y;
+  for (int i = 1; i < nmax; ++i) {
+    const cplx rho = mkc(out[i * stride], out[i * stride + 1]);
+    const cplx ji = cmul(rho, jprev);
+    const cplx dji = csub(jprev, cmul(cscale(zinv, i + 1.), ji));
+    out[i * stride] = ji.x;
+    out[i * stride + 1] = ji.y;
+    out[i * stride + 2] = dji.x;
+    out[i * stride + 3] = dji.y;
+    jprev = ji;
+  }
+}
+
+// One block per slot; threads 0..ng-1 do the real-argument tables and node
+// scalars of node g, threads ng..2ng-1 the complex-argument tables.
+// Node scalars follow GaussBasedResources::execute (GaussBasedResources.hpp:
+// 132-152), get_r_dr_spheroid (SpecialFunctions.hpp:872-893) and
+// InteractionTask::execute (InteractionResource.hpp:478-527).
+__global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
+                         const TmxGrain *__restrict__ grains,
+                         const double *__restrict__ gl_x,
+                         const double *__restrict__ gl_w,
+                         const int64_t *__restrict__ gl_off, double *tab,
+                         double *nsc, int bessel_start) {
+  const int s = blockIdx.x;
+  if (s >= nslots) {
+    return;
+  }
+  const TmxSlot sl = slots[s];
+  const TmxGrain G = grains[sl.grain];
+  const int N = sl.nmax;
+  const int ng = sl.ngauss;
+  const double *x = gl_x + gl_off[ng];
+  const double *w = gl_w + gl_off[ng];
+  for (int u = threadIdx.x; u < 2 * ng; u += blockDim.x) {
+    const int g = u % ng;
+    const int kind = u / ng;
+    const double c = x[g];
+    const double s2 = (1. - c) * (1. + c);
+    const double sn = sqrt(s2);
+    const double a2 = G.cbrt_d * G.cbrt_d;
+    const double d2 = G.axis_ratio * G.axis_ratio;
+    const double d2m1 = d2 - 1.;
+    const double r2oa2 = 1. / (s2 + d2 * (c * c));
+    const double r2 = a2 * r2oa2;
+    const double drr = r2oa2 * c * sn * d2m1;
+    const double r = sqrt(r2);
+    double *T = tab + sl.tab + (int64_t)g * N * TMX_NQ;
+    if (kind == 0) {
+      const double kr = G.k * r * G.r_ev;
+      const double krinv = 1. / kr;
+      const cplx krmr = mkc(G.mr * G.k * r * G.r_ev, G.mi * G.k * r * G.r_ev);
+      const cplx krmrinv = cinv(krmr);
+      const double sin2inv = 1. / ((1. - c) * (1. + c));
+      double *S = nsc + sl.nsc + (int64_t)g * TMX_NS;
+      S[TMX_NS_KRINV] = krinv;
+      S[TMX_NS_KRMRINV_RE] = krmrinv.x;
+      S[TMX_NS_KRMRINV_IM] = krmrinv.y;
+      S[TMX_NS_R2] = r2;
+      S[TMX_NS_DRR] = drr;
+      S[TMX_NS_W] = w[g];
+      S[TMX_NS_COS] = c;
+      S[TMX_NS_SININV] = sqrt(sin2inv);
+      S[TMX_NS_SIN2INV] = sin2inv;
+      S[TMX_NS_PAD] = 0.;
+      bessel_j_real(N, bessel_start, kr, T + TMX_Q_J, TMX_NQ);
+      bessel_y_real(N, kr, T + TMX_Q_Y, TMX_NQ);
+    } else {
+      const cplx krmr = mkc(G.mr * G.k * r * G.r_ev, G.mi * G.k * r * G.r_ev);
+      bessel_j_complex(N, bessel_start, krmr, T + TMX_Q_JM_RE, TMX_NQ);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- Wigner --
+
+// d^n_{0m}(x) and d/dx for n = 1..nmax by forward recurrence in n
+// (SpecialFunctions::wigner_dn_0m, SpecialFunctions.hpp:302-371).
+// out[(n-1) * 2 + {0,1}] = (d, dd)
+__device__ static void wigner_d(double cosx, int nmax, int m, double *out) {
+  const double sinx = sqrt((1. - cosx) * (1. + cosx));
+  const double sinxinv = 1. / sinx;
+  if (m == 0) {
+    double d1 = 1.;
+    double d2 = cosx;
+    for (int n = 0; n < nmax; ++n) {
+      const double np1 = n + 1.;
+      const double np2 = n + 2.;
+      const double np12p1 = 2. * np1 + 1.;
+      const double dnp1 = (np12p1 * cosx * d2 - np1 * d1) / np2;
+      const double ddn = sinxinv * np1 * np2 * (dnp1 - d1) / np12p1;
+      out[2 * n] = d2;
+      out[2 * n + 1] = ddn;
+      d1 = d2;
+      d2 = dnp1;
+    }
+    return;
+  }
+  const double m2 = (double)(m * m);
+  double d1 = 0.;
+  double d2 = 1.;
+  for (int i = 0; i < m; ++i) {
+    const double i2 = 2. * (i + 1.);
+    d2 *= sqrt((i2 - 1.) / i2) * sinx;
+  }
+  for (int n = 0; n < m - 1; ++n) {
+    out[2 * n] = 0.;
+    out[2 * n + 1] = 0.;
+  }
+  for (int n = m - 1; n < nmax; ++n) {
+    const double np1 = n + 1.;
+    const double np2 = n + 2.;
+    const double np12p1 = 2. * np1 + 1.;
+    const double s12 = sqrt(np1 * np1 - m2);
+    const double s22 = sqrt(np2 * np2 - m2);
+    const double dnp1 = (np12p1 * cosx * d2 - s12 * d1) / s22;
+    const double ddn = sinxinv * (np1 * s22 * dnp1 - np2 * s12 * d1) / np12p1;
+    out[2 * n] = d2;
+    out[2 * n + 1] = ddn;
+    d1 = d2;
+    d2 = dnp1;
+  }
+}
+
+// Wigner tables at the lower-half quadrature nodes for one (nmax, ngauss):
+// for orders below 100 the values are those of the mirrored upper-half node
+// (cos = -x[g]) times (-1)^n (d) and -(-1)^n (dd), as WignerDResources
+// precomputes them (WignerDResources.hpp:147-174); from order 100 on they are
+// evaluated at the node itself (WignerDResources.hpp:232-247).
+// out[((m - m_lo) * ng + g) * nmax * 2 + (n - 1) * 2 + {0,1}]
+__global__ void k_wigner(const TmxWigJob *__restrict__ jobs, int njobs,
+                         const double *__restrict__ gl_x,
+                         const int64_t *__restrict__ gl_off, double *out) {
+  const int j = blockIdx.y;
+  if (j >= njobs) {
+    return;
+  }
+  const TmxWigJob J = jobs[j];
+  const int nm = J.m_hi - J.m_lo + 1;
+  const int total = nm * J.ngauss;
+  const double *x = gl_x + gl_off[J.ngauss];
+  for (int u = blockIdx.x * blockDim.x + threadIdx.x; u < total;
+       u += gridDim.x * blockDim.x) {
+    const int g = u % J.ngauss;
+    const int m = J.m_lo + u / J.ngauss;
+    double *o = out + J.out + ((int64_t)(m - J.m_lo) * J.ngauss + g) *
+                                  J.nmax * 2;
+    if (J.nmax < 100) {
+      wigner_d(-x[g], J.nmax, m, o);
+      double sign = 1.;
+      for (int n = 0; n < J.nmax; ++n) {
+        sign = -sign;
+        o[2 * n] = sign * o[2 * n];
+        o[2 * n + 1] = -sign * o[2 * n + 1];
+      }
+    } else {
+      wigner_d(x[g], J.nmax, m, o);
+    }
+  }
+}
+
+// --------------------------------------------------------- launchers ------
+
+void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
+                       const double *gl_x, const double *gl_w,
+                       const int64_t *gl_off, double *tab, double *nsc,
+                       int bessel_start, cudaStream_t stream) {
+  if (nslots <= 0) {
+    return;
+  }
+  k_tables<<<nslots, 128, 0, stream>>>(slots, nslots, grains, gl_x, gl_w,
+                                       gl_off, tab, nsc, bessel_start);
+}
+
+void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,
+                       const double *gl_x, const int64_t *gl_off, double *out,
+                       cudaStream_t stream) {
+  if (njobs <= 0) {
+    return;
+  }
+  const int threads = 128;
+  int bx = (max_work + threads - 1) / threads;
+  if (bx < 1) {
+    bx = 1;
+  }
+  dim3 grid(bx, njobs);
+  k_wigner<<<grid, threads, 0, stream>>>(jobs, njobs, gl_x, gl_off, out);
+}

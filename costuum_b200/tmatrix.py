@@ -1,0 +1,145 @@
+"""Batched T-matrices of independent spheroids on the GPU.
+
+This is the Python face of the C ABI in include/tmx.h. A batch runs the
+reference's task-based schedule (CosTuuM TaskManager: orders min_order ..
+max_order - 1 with ngauss = gauss_legendre_factor * order until the m = 0
+Qsca and Qext converge, then every m block) for every grain at once.
+"""
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+
+GRAIN_OK = 0
+GRAIN_NOT_CONVERGED = 1
+GRAIN_SINGULAR = 2
+GRAIN_NAN = 4
+GRAIN_BAD_INPUT = 8
+GRAIN_TOO_LARGE = 16
+
+
+def tmatrix_size(nmax):
+    """Complex elements of a T-matrix holding every m block up to nmax."""
+    return int(_lib.load().tmx_tmatrix_size(int(nmax)))
+
+
+def block_offset(nmax, m):
+    """Complex offset of block m inside a flat T-matrix."""
+    if m == 0:
+        return 0
+    nb = np.arange(nmax + 1 - (m - 1), nmax + 1)
+    return int(4 * nmax * nmax + 4 * int(np.sum(nb.astype(np.int64) ** 2)))
+
+
+def block(T, nmax, m):
+    """Block m of a flat T-matrix as a (2nb, 2nb) complex matrix."""
+    nb = nmax if m == 0 else nmax + 1 - m
+    off = block_offset(nmax, m)
+    return T[off:off + 4 * nb * nb].reshape(2 * nb, 2 * nb)
+
+
+class BatchResult:
+    """Per-grain outcome of Context.tmatrix_batch."""
+
+    def __init__(self, ctx, n, nmax, ngauss, status, q):
+        self._ctx = ctx
+        self.n = n
+        self.nmax = nmax
+        self.ngauss = ngauss
+        self.status = status
+        self.q = q  # [m0 Qsca, m0 Qext, full Qsca, full Qext, dQs, dQe]
+
+    @property
+    def qsca(self):
+        return self.q[:, 2]
+
+    @property
+    def qext(self):
+        return self.q[:, 3]
+
+    def tmatrix(self, i):
+        """Flat complex T-matrix of grain i (reference block layout)."""
+        N = int(self.nmax[i])
+        out = np.zeros(tmatrix_size(N), np.complex128)
+        if N > 0:
+            rc = _lib.load().tmx_batch_tmatrix(self._ctx._h, int(i), _lib.ptr(out))
+            _lib.check(self._ctx._h, rc, "tmx_batch_tmatrix")
+        return out
+
+
+class Context:
+    """A CUDA device context: owns device buffers and cached tables."""
+
+    def __init__(self, device=0):
+        lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = lib.tmx_create(ctypes.byref(h), int(device))
+        if rc != 0:
+            raise _lib.TmxError("tmx_create failed (%d): no usable CUDA device "
+                                "or CUDA error" % rc)
+        self._h = h
+        self.device = device
+        self._lock = threading.Lock()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().tmx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def kernel_launches(self):
+        return int(_lib.load().tmx_kernel_launches(self._h))
+
+    def probe_fp64(self, kind=0):
+        """Measured FP64 TFLOP/s: kind 0 DFMA pipe, 1 DMMA tensor pipe."""
+        v = np.zeros(1)
+        rc = _lib.load().tmx_probe_fp64(self._h, int(kind), _lib.ptr(v))
+        _lib.check(self._h, rc, "tmx_probe_fp64")
+        return float(v[0])
+
+    def tmatrix_batch(self, r_ev, wavelength, m, axis_ratio, min_order=10,
+                      max_order=100, gauss_legendre_factor=2, tolerance=1e-4,
+                      bessel_start=0):
+        """Converged T-matrices of independent grains (SI units)."""
+        r_ev = np.ascontiguousarray(r_ev, np.float64).ravel()
+        n = r_ev.size
+        wl = np.ascontiguousarray(np.broadcast_to(wavelength, (n,)), np.float64)
+        mm = np.broadcast_to(np.asarray(m, np.complex128), (n,))
+        mr = np.ascontiguousarray(mm.real)
+        mi = np.ascontiguousarray(mm.imag)
+        d = np.ascontiguousarray(np.broadcast_to(axis_ratio, (n,)), np.float64)
+        sched = _lib.TmxSchedule(int(min_order), int(max_order),
+                                 int(gauss_legendre_factor), int(bessel_start),
+                                 float(tolerance))
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_tmatrix_batch(self._h, n, _lib.ptr(r_ev), _lib.ptr(wl),
+                                       _lib.ptr(mr), _lib.ptr(mi), _lib.ptr(d),
+                                       ctypes.byref(sched))
+            _lib.check(self._h, rc, "tmx_tmatrix_batch")
+            nmax = np.zeros(n, np.int32)
+            ngauss = np.zeros(n, np.int32)
+            status = np.zeros(n, np.int32)
+            q = np.zeros((n, 6))
+            rc = lib.tmx_batch_results(self._h, _lib.iptr(nmax), _lib.iptr(ngauss),
+                                       _lib.iptr(status), _lib.ptr(q))
+            _lib.check(self._h, rc, "tmx_batch_results")
+        return BatchResult(self, n, nmax, ngauss, status, q)
+
+
+_default = None
+
+
+def default_context():
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default

@@ -1,0 +1,139 @@
+/* tmx.h -- C ABI of the B200 T-matrix library (libtmx.so).
+ *
+ * The library computes EBCM T-matrices of spheroids and their orientation-
+ * and shape-averaged observables on one NVIDIA B200 (sm_100a) in FP64. It is
+ * the drop-in replacement of the CosTuuM T-matrix path: the host drivers
+ * (CosTuuM's TaskManager + QuickSched, src/TaskManager.hpp:445-1346, and its
+ * Python module, src/CTMModule.cpp:146-478) bind these entry points instead
+ * of building and running a task graph on host threads.
+ *
+ * Conventions
+ *   - plain pointers and sizes only; every array argument is host memory
+ *     unless its name ends in _dev;
+ *   - complex numbers are interleaved (re, im) doubles;
+ *   - T-matrices use the reference's block layout (TMatrixResource,
+ *     src/TMatrixResource.hpp:195-213): block m (m = 0..nmax) is a
+ *     2nb x 2nb row-major complex matrix, nb = nmax for m = 0 and
+ *     nmax + 1 - m otherwise; row (i, n) sits at i * nb + n - max(m, 1);
+ *     blocks follow each other in m order (tmx_tmatrix_size());
+ *   - functions return TMX_OK (0) or a negative tmx_error; per-grain
+ *     outcomes are reported as status bits, never by aborting (the reference
+ *     calls abort() on non-convergence in its plain path).
+ */
+#ifndef TMX_H
+#define TMX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tmx_ctx tmx_ctx;
+
+enum tmx_error {
+  TMX_OK = 0,
+  TMX_ERR_INVALID = -1,  /* bad argument; see tmx_last_error() */
+  TMX_ERR_CUDA = -2,     /* a CUDA call failed */
+  TMX_ERR_NOMEM = -3,    /* device allocation failed */
+  TMX_ERR_STATE = -4,    /* no batch computed yet / index out of range */
+  TMX_ERR_NO_DEVICE = -5 /* no usable CUDA device */
+};
+
+/* per-grain status bits */
+enum tmx_grain_status {
+  TMX_GRAIN_OK = 0,
+  TMX_GRAIN_NOT_CONVERGED = 1, /* reached maximum_order - 1 (reference:
+                                  silent in the task path) */
+  TMX_GRAIN_SINGULAR = 2,      /* zero pivot in a Q block */
+  TMX_GRAIN_NAN = 4,           /* non-finite sums */
+  TMX_GRAIN_BAD_INPUT = 8,     /* r_ev, wavelength or axis ratio <= 0 */
+  TMX_GRAIN_TOO_LARGE = 16     /* block larger than the on-chip solver */
+};
+
+/* Convergence schedule of the task-based path (TaskManager(min_order,
+ * max_order, gauss_legendre_factor, tolerance), src/TaskManager.hpp:371):
+ * orders min_order .. max_order - 1 with ngauss = factor * order, stop at the
+ * first order whose m = 0 Qsca and Qext both change by <= tolerance. */
+typedef struct tmx_schedule {
+  int32_t min_order;             /* default 10 */
+  int32_t max_order;             /* default 100 (exclusive) */
+  int32_t gauss_legendre_factor; /* default 2 */
+  int32_t bessel_start;          /* start index of the downward j_n ratio
+                                    recurrence; 0 = 800, the reference's
+                                    SPECIALFUNCTIONS_BESSEL_NMAX */
+  double tolerance;              /* default 1e-4 */
+} tmx_schedule;
+
+/* Create a context on CUDA device `device` (the context owns a stream,
+ * device buffers and cached quadrature/Wigner tables). Replaces the
+ * QuickSched object + TMatrixAuxiliarySpaceManager of the reference
+ * (src/QuickSchedWrapper.hpp:302, src/TMatrixResource.hpp:376-435). */
+int tmx_create(tmx_ctx **ctx, int device);
+void tmx_destroy(tmx_ctx *ctx);
+const char *tmx_last_error(const tmx_ctx *ctx);
+
+/* Complex elements of a T-matrix with all m blocks up to nmax. */
+int64_t tmx_tmatrix_size(int32_t nmax);
+
+/* Converged T-matrices of n independent grains (the InteractionTask ->
+ * TMatrixM0Task convergence chain of TaskManager.hpp:1146-1197 followed by
+ * TMatrixMAllTask for every m, :1313-1327). Inputs are host arrays of length
+ * n: equal-volume radius and wavelength in metres, refractive index
+ * (mr + i mi), axis ratio d = a/b. The results stay on the device until the
+ * next batch; read them with tmx_batch_results / tmx_batch_tmatrix. */
+int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                      const double *wavelength, const double *mr,
+                      const double *mi, const double *axis_ratio,
+                      const tmx_schedule *schedule);
+
+/* The same computation in two steps: upload the inputs (host -> device),
+ * then compute from device-resident inputs (may be repeated). */
+int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                     const double *wavelength, const double *mr,
+                     const double *mi, const double *axis_ratio,
+                     const tmx_schedule *schedule);
+int tmx_batch_compute(tmx_ctx *ctx);
+
+/* Per-grain results of the last batch (any pointer may be NULL):
+ * nmax, ngauss, status bits, and q[6 * i + {0..5}] =
+ * {m=0 Qsca, m=0 Qext of the converged order, full Qsca, full Qext
+ *  (TMatrixQTask, src/TMatrixResource.hpp:1136-1210), dQs, dQe}.
+ * Qsca/Qext are the reference's unnormalised sums. */
+int tmx_batch_results(tmx_ctx *ctx, int32_t *nmax, int32_t *ngauss,
+                      int32_t *status, double *q);
+
+/* Copy the T-matrix of grain `grain` of the last batch into `out`
+ * (2 * tmx_tmatrix_size(nmax) doubles). */
+int tmx_batch_tmatrix(tmx_ctx *ctx, int64_t grain, double *out);
+
+/* Measured FP64 throughput of this device in TFLOP/s: kind 0 = DFMA pipe,
+ * kind 1 = DMMA tensor pipe (mma.sync m8n8k4 f64). */
+int tmx_probe_fp64(tmx_ctx *ctx, int kind, double *tflops);
+
+/* CUDA-event timer on the library's stream (the stream every kernel of the
+ * context is launched on). */
+int tmx_timer_start(tmx_ctx *ctx);
+int tmx_timer_stop(tmx_ctx *ctx, double *ms);
+
+/* Per-kernel device time: when enabled, every launch of kernel 0 (the block
+ * kernel: assembly + LU + solve) and kernel 1 (the Bessel table kernel) is
+ * bracketed by CUDA events on the library stream; tmx_profile_read returns
+ * the summed milliseconds, the launch count and the executed FP64 flops of
+ * the parity-class algorithm. Enabling resets the counters. */
+int tmx_profile_enable(tmx_ctx *ctx, int on);
+int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
+                     double *flops);
+
+/* FP64 flops of the last batch counted with the unreduced per-grain model
+ * (every chain order and every m block as a full 2nb x 2nb LU + solve). */
+double tmx_batch_flops_survey(const tmx_ctx *ctx);
+
+/* Number of this library's kernels launched since the context was created. */
+int64_t tmx_kernel_launches(const tmx_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMX_H */

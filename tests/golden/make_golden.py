@@ -1,0 +1,135 @@
+"""Generate the golden fixtures in tests/golden/ from the unmodified reference.
+
+Run in a container where the reference has been built (oracle/build_ref.sh):
+    python tests/golden/make_golden.py
+It imports the reference's own CPython module (oracle/_ref/CosTuuM*.so) and
+its task objects (oracle/_ref/libref_driver.so) and stores their outputs.
+The fixtures pin the C restatement in oracle/ (tests/test_oracle_golden.py).
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
+import oracle as O  # noqa: E402
+from oracle import _p  # noqa: E402
+
+
+def stages():
+    R = O.ref()
+    out = {}
+    for order in (1, 2, 3, 5, 20, 41, 80):
+        x = np.zeros(order)
+        w = np.zeros(order)
+        R.ref_gauss_legendre(order, _p(x), _p(w))
+        out["gl_%d_x" % order] = x
+        out["gl_%d_w" % order] = w
+    for i, z in enumerate((0.05, 1.3, 7.7, 33.1)):
+        j = np.zeros(30)
+        dj = np.zeros(30)
+        y = np.zeros(30)
+        dy = np.zeros(30)
+        R.ref_bessel_j_real(30, z, _p(j), _p(dj))
+        R.ref_bessel_y_real(30, z, _p(y), _p(dy))
+        out["bj_%d" % i] = np.stack([j, dj, y, dy])
+        out["bj_%d_z" % i] = np.array([z])
+    for i, z in enumerate((0.3 + 0.01j, 2.5 + 0.3j, 12.0 + 1.5j)):
+        j = np.zeros(30, complex)
+        dj = np.zeros(30, complex)
+        R.ref_bessel_j_complex(30, z.real, z.imag, _p(j), _p(dj))
+        out["bjc_%d" % i] = np.stack([j, dj])
+        out["bjc_%d_z" % i] = np.array([z])
+    for i, (c, m) in enumerate(((-0.99, 0), (-0.3, 1), (0.1, 3), (0.9999, 10))):
+        d = np.zeros(20)
+        dd = np.zeros(20)
+        R.ref_wigner_d(c, 20, m, _p(d), _p(dd))
+        out["wig_%d" % i] = np.stack([d, dd])
+        out["wig_%d_arg" % i] = np.array([c, m])
+    for i, (n1, n2, N) in enumerate(((1, 1, 0), (3, 5, 4), (10, 7, 12), (20, 20, 40))):
+        buf = np.zeros((N + 1) * (2 * n1 + 1))
+        k = R.ref_clebsch_gordan_row(n1, n2, N, _p(buf))
+        out["cg_%d" % i] = buf[:k].copy()
+        out["cg_%d_arg" % i] = np.array([n1, n2, N])
+    for i, (kind, par) in enumerate(((0, 0.), (1, 0.6), (2, 2.), (2, 0.5))):
+        c = np.zeros(21)
+        R.ref_orientation_coefficients(kind, par, 20, _p(c))
+        out["od_%d" % i] = c
+        out["od_%d_arg" % i] = np.array([kind, par])
+    A = (np.random.default_rng(0).standard_normal((7, 7))
+         + 1j * np.random.default_rng(1).standard_normal((7, 7)))
+    Ai = A.copy()
+    R.ref_plu_inverse(7, _p(Ai))
+    out["plu_a"] = A
+    out["plu_inv"] = Ai
+    out["rvrs"] = np.array([R.ref_rv_over_rs(d) for d in (0.5, 2.0, 1.0, 3.3)])
+    return out
+
+
+GRAINS = [  # r_ev (m), wavelength (m), m, axis ratio
+    (0.2e-6, 1e-6, 1.5 + 0.02j, 2.0),     # the one-grain configuration
+    (0.5e-6, 1e-6, 1.7 + 0.1j, 0.6),
+    (0.8e-6, 1e-6, 1.35 + 0.003j, 1.4),
+    (0.05e-6, 1e-6, 1.9 + 0.8j, 0.9),
+]
+
+
+def tmatrices():
+    out = {}
+    r = [g[0] for g in GRAINS]
+    lam = [g[1] for g in GRAINS]
+    m = [g[2] for g in GRAINS]
+    d = [g[3] for g in GRAINS]
+    res = O.ref_batch(r, lam, m, d, max_order=40, nthreads=2)
+    for i, rec in enumerate(res):
+        out["t_%d_T" % i] = rec["T"]
+        out["t_%d_meta" % i] = np.array([rec["nmax"], rec["ngauss"],
+                                         int(rec["converged"])])
+        out["t_%d_q" % i] = rec["q"]
+    out["t_grains"] = np.array([[g[0], g[1], g[2].real, g[2].imag, g[3]]
+                                for g in GRAINS])
+    return out
+
+
+def tables():
+    """get_table outputs of the reference's Python module."""
+    C = O.ref_module()
+    out = {}
+    th = np.arccos(np.linspace(-1, 1, 32))
+    # the one-grain configuration: Q_ext / Q_abs at 32 zenith angles
+    res = C.get_table(types=np.array([0]), sizes=np.array([0.2e-6]),
+                      wavelengths=np.array([1e-6]), thetas=th,
+                      shape_distribution=C.SingleShapeShapeDistribution(2.0),
+                      alignment_distribution=C.SizeBasedAlignmentDistribution(
+                          1e-5, C.DAVIS_GREENSTEIN_ALIGNMENT, maximum_order=40),
+                      dust_properties=C.CustomDustProperties(lambda w, s, t: 1.5 + 0.02j),
+                      number_of_threads=2, maximum_order=40, do_extinction=True)
+    out["gt1"] = res
+    out["gt1_theta"] = th
+    # a small grid with alignment, Draine-Hensley shapes, scattering
+    th2 = np.array([0.3, 1.2, 2.0])
+    sizes = np.array([0.05e-6, 0.3e-6])
+    lams = np.array([1.5e-6, 0.8e-6])
+    mfun = lambda w, s, t: (1.4 + 0.3 * s / 1e-6) + 0.05j * (1e-6 / w)  # noqa: E731
+    res2 = C.get_table(types=np.array([0]), sizes=sizes, wavelengths=lams,
+                       thetas=th2,
+                       shape_distribution=C.DraineHensleyShapeDistribution(4),
+                       alignment_distribution=C.SizeBasedAlignmentDistribution(
+                           0.1e-6, C.MISHCHENKO_ALIGNMENT, maximum_order=30),
+                       dust_properties=C.CustomDustProperties(mfun),
+                       number_of_threads=2, maximum_order=30,
+                       do_extinction=True, do_scattering=True)
+    out["gt2_qabs"] = res2[0]
+    out["gt2_z"] = res2[1]
+    out["gt2_theta"] = th2
+    out["gt2_sizes"] = sizes
+    out["gt2_lams"] = lams
+    return out
+
+
+if __name__ == "__main__":
+    np.savez_compressed(os.path.join(HERE, "stages.npz"), **stages())
+    np.savez_compressed(os.path.join(HERE, "tmatrices.npz"), **tmatrices())
+    np.savez_compressed(os.path.join(HERE, "tables.npz"), **tables())
+    print("golden fixtures written to", HERE)

@@ -43,6 +43,8 @@ SIGNATURES = {
     "tmx_profile_read": (ctypes.c_int, [_VP, ctypes.c_int, _D,
                                         ctypes.POINTER(ctypes.c_int64), _D]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
+    "tmx_tmatrix_fixed_noalloc": (ctypes.c_int, [ctypes.c_double] * 5
+                                  + [ctypes.c_int32, ctypes.c_int32, _VP, _VP]),
 }
 
 _lib = None

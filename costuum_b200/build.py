@@ -19,6 +19,7 @@ SOURCES = [
     ("tmx_observables.cu", []),
     ("tmx_probe.cu", []),
     ("tmx_host.cu", []),
+    ("tmx_noalloc.cu", []),
 ]
 
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -206,7 +206,7 @@ static int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep) {
 // symmetric fill. Same recipe and operation order as the reference's
 // SpecialFunctions::get_gauss_legendre_points_and_weights
 // (src/SpecialFunctions.hpp:646-715), so the nodes are the same doubles.
-static void gauss_legendre(int order, double *points, double *weights) {
+void tmx_host_gauss_legendre(int order, double *points, double *weights) {
   const unsigned ind = (unsigned)order % 2;
   const unsigned k = (unsigned)order / 2 + ind;
   for (unsigned i = 0; i < k; ++i) {
@@ -254,7 +254,7 @@ static int ensure_gl(tmx_ctx *ctx, const std::vector<int> &ngs) {
       continue;
     }
     std::vector<double> x(2 * ng), w(2 * ng);
-    gauss_legendre(2 * ng, x.data(), w.data());
+    tmx_host_gauss_legendre(2 * ng, x.data(), w.data());
     ctx->gl_off_h[ng] = (int64_t)ctx->gl_x_h.size();
     ctx->gl_x_h.insert(ctx->gl_x_h.end(), x.begin(), x.begin() + ng);
     ctx->gl_w_h.insert(ctx->gl_w_h.end(), w.begin(), w.begin() + ng);
@@ -344,7 +344,7 @@ static int ensure_wigner(tmx_ctx *ctx,
 
 // number of members of class `cls` of block m at order N (see describe() in
 // tmx_blocks.cu)
-static int class_size(int N, int m, int cls) {
+int tmx_host_class_size(int N, int m, int cls) {
   if (m == 0) {
     const int n0 = (cls & 1) ? 1 : 2;
     return (N >= n0) ? (N - n0) / 2 + 1 : 0;
@@ -356,7 +356,7 @@ static int class_size(int N, int m, int cls) {
   return R0 + R1;
 }
 
-static int chunk_nodes_for(int max_nb) {
+int tmx_host_chunk_nodes(int max_nb) {
   const int nrp = (max_nb + 3) / 4 * 4 + 4;
   const int ncol = (max_nb + 3) / 4 * 4;
   const size_t per_node = (size_t)(4 * nrp + 8 * ncol) * 16;
@@ -648,10 +648,10 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       B.diag = (cplx *)ctx->diag.p;
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = cmax;
-      B.chunk_nodes = chunk_nodes_for(cmax);
+      B.chunk_nodes = tmx_host_chunk_nodes(cmax);
       double fl = 0.;
       for (int c = 0; c < 4; ++c) {
-        fl += item_flops(class_size(k, 0, c), 0, ng);
+        fl += item_flops(tmx_host_class_size(k, 0, c), 0, ng);
       }
       if ((rc = prof_begin(ctx, 0, &pe))) {
         return rc;
@@ -737,7 +737,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     for (int m = 0; m <= N; ++m) {
       const int ncls = (m == 0) ? 4 : 2;
       for (int c = 0; c < ncls; ++c) {
-        const int nb = class_size(N, m, c);
+        const int nb = tmx_host_class_size(N, m, c);
         if (nb <= 0) {
           continue;
         }
@@ -813,7 +813,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
         B.diag = nullptr;
         B.status = (int32_t *)ctx->status.p;
         B.max_nb = hitems[i0].nb;
-        B.chunk_nodes = chunk_nodes_for(B.max_nb);
+        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
         double fl = 0.;
         for (size_t q = i0; q < i1; ++q) {
           fl += item_flops(hitems[q].nb, hitems[q].it.m,

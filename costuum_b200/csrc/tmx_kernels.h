@@ -79,3 +79,8 @@ void tmx_launch_probe_dfma(double *out, int iters, int blocks,
                            cudaStream_t stream);
 void tmx_launch_probe_dmma(double *out, int iters, int blocks,
                            cudaStream_t stream);
+
+// host helpers shared by the drivers (tmx_host.cu)
+void tmx_host_gauss_legendre(int order, double *points, double *weights);
+int tmx_host_class_size(int N, int m, int cls);
+int tmx_host_chunk_nodes(int max_nb);

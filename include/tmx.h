@@ -129,6 +129,24 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
  * (every chain order and every m block as a full 2nb x 2nb LU + solve). */
 double tmx_batch_flops_survey(const tmx_ctx *ctx);
 
+/* T-matrix of one grain at a fixed (nmax, ngauss), all m blocks, for callers
+ * that cannot allocate device memory -- e.g. a host application whose device
+ * memory is owned by another framework's caching allocator, or a per-call
+ * path that cannot pay cudaMalloc/cudaFree's implicit synchronisation. No
+ * counterpart in the reference. It calls no cudaMalloc/cudaFree: its
+ * intermediates live in one static device array of 2.25 MiB that every GPU
+ * loading the library keeps until exit. Limits: 2 <= nmax <= 32,
+ * 1 <= ngauss <= 64 (larger sizes return TMX_ERR_INVALID with a message on
+ * stderr). The caller passes the grain (SI units) and a device buffer T_dev
+ * of 2 * tmx_tmatrix_size(nmax) doubles; the work is enqueued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and is complete when that
+ * stream is. The first call on a device looks up the array's device address
+ * with that device current; make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race. */
+int tmx_tmatrix_fixed_noalloc(double r_ev, double wavelength, double mr,
+                              double mi, double axis_ratio, int32_t nmax,
+                              int32_t ngauss, double *T_dev, void *stream);
+
 /* Number of this library's kernels launched since the context was created. */
 int64_t tmx_kernel_launches(const tmx_ctx *ctx);
 

@@ -338,6 +338,7 @@ def run_ours(args):
 
 
 def main():
+    global N_GRAINS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -345,9 +346,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-cpu", action="store_true",
                     help="omit the CPU-baseline leg")
+    ap.add_argument("--grains", type=int, default=N_GRAINS,
+                    help="grains per GPU (smaller cases for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    N_GRAINS = args.grains
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -18,15 +18,24 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <string>
 #include <tuple>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/tmx.h"
 #include "tmx_common.cuh"
 #include "tmx_kernels.h"
 
 namespace {
+
+// NVTX range for the duration of a scope (phase markers for profilers)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
 
 struct DevBuf {
   void *p = nullptr;
@@ -595,6 +604,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   int nact = ctx->up_nact;
   DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
   const size_t budget = (size_t)8 << 30; // table bytes per chunk
+  std::unique_ptr<NvtxRange> chain_range(new NvtxRange("tmx_chain"));
   for (int k = S.min_order; k < S.max_order && nact > 0; ++k) {
     const int ng = glf * k;
     const int64_t tab_stride = (int64_t)ng * k * TMX_NQ;
@@ -674,6 +684,8 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     std::swap(cur, nxt);
   }
 
+  chain_range.reset();
+
   // ---- per-grain outcome of the order loop
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToHost, st));
@@ -693,6 +705,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   }
 
   // ---- 2. all blocks at the converged orders
+  NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
   std::vector<TmxSlot> slots(np2);
   std::vector<std::pair<int, int>> keys;

@@ -23,8 +23,10 @@
 #include "tmx_common.cuh"
 #include "tmx_kernels.h"
 
-#define TR 4 // rows per thread tile
-#define TC 4 // columns per thread tile (strided by the column-tile count)
+// Thread tiles: every thread of the assembly owns TR rows x TC columns of the
+// class matrix (columns strided by the column-tile count for conflict-free
+// shared-memory reads). Small classes use small tiles and small blocks so
+// that many blocks fit on an SM.
 
 struct ClassDesc {
   int nb;       // class size
@@ -36,6 +38,7 @@ struct ClassDesc {
   int nmin;     // smallest n in the block
 };
 
+template <int TR>
 __device__ __forceinline__ ClassDesc describe(int N, int m, int cls) {
   ClassDesc D;
   if (m == 0) {
@@ -119,6 +122,7 @@ struct AsmLayout {
 // This is the expansion of the J11, J12, J21, J22 terms of
 // TMatrixResource.hpp:993-1097 into products of one n1 factor and one n2
 // factor per node.
+template <int TC>
 __device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
                             int m, int ng, int g0, const double *__restrict__ T,
                             const double *__restrict__ S,
@@ -225,7 +229,8 @@ __device__ __forceinline__ double cabs_dev(cplx a) { return hypot(a.x, a.y); }
 
 extern __shared__ __align__(16) unsigned char tmx_smem[];
 
-__global__ void __launch_bounds__(256)
+template <int TR, int TC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_blocks(TmxBlockArgs A, size_t smem_bytes) {
   const int it = blockIdx.x;
   if (it >= A.nitems) {
@@ -237,7 +242,7 @@ __global__ void __launch_bounds__(256)
   const int N = sl.nmax;
   const int ng = sl.ngauss;
   const int m = item.m;
-  const ClassDesc D = describe(N, m, item.cls);
+  const ClassDesc D = describe<TR>(N, m, item.cls);
   const int nb = D.nb;
   if (nb <= 0) {
     return;
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(256)
   const int ntiles = RT * L.CT;
   const int tstep = (m == 0) ? 2 : 1; // m = 0: mu = 0 kills t = 0, 2
   const int t0 = (m == 0) ? 1 : 0;
-  for (int tile0 = 0; tile0 < ntiles; tile0 += blockDim.x) {
+  for (int tile0 = 0; tile0 < ntiles; tile0 += NT) {
     const int tile = tile0 + threadIdx.x;
     const bool active = tile < ntiles;
     const int ct = active ? tile % L.CT : 0;
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(256)
     }
     for (int g0 = 0; g0 < ng; g0 += L.G) {
       __syncthreads();
-      build_chunk(D, L, N, m, ng, g0, T, S, Wg, k2, k2mr, Fs, Ws);
+      build_chunk<TC>(D, L, N, m, ng, g0, T, S, Wg, k2, k2mr, Fs, Ws);
       __syncthreads();
       if (active) {
         const int kmax = 4 * min(L.G, ng - g0);
@@ -489,9 +494,11 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// shared memory of one block: the larger of the assembly chunk buffers and
+// the LU phase (factors, pivots and a right-hand-side chunk)
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
-  const int nrp = (max_nb + TR - 1) / TR * TR + TR;
-  const int ncol = (max_nb + TC - 1) / TC * TC;
+  const int nrp = (max_nb + 3) / 4 * 4 + 4;
+  const int ncol = (max_nb + 3) / 4 * 4;
   const size_t asm_bytes =
       ((size_t)4 * chunk_nodes * nrp + (size_t)2 * 4 * chunk_nodes * ncol) *
       sizeof(cplx);
@@ -510,24 +517,33 @@ size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
   return asm_bytes > lu_total ? asm_bytes : lu_total;
 }
 
+template <int TR, int TC, int NT, int MINB>
+static void launch_variant(const TmxBlockArgs &a, size_t smem,
+                           cudaStream_t stream) {
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_blocks<TR, TC, NT, MINB>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    attr_dev = dev;
+  }
+  k_blocks<TR, TC, NT, MINB><<<a.nitems, NT, smem, stream>>>(a, smem);
+}
+
 void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
   if (a.nitems <= 0) {
     return;
   }
   const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         227 * 1024);
-    attr_set = true;
-  }
-  int threads = 256;
   if (a.max_nb <= 16) {
-    threads = 64;
+    launch_variant<2, 2, 64, 8>(a, smem, stream);
   } else if (a.max_nb <= 32) {
-    threads = 128;
+    launch_variant<2, 4, 128, 4>(a, smem, stream);
+  } else {
+    launch_variant<4, 4, 256, 1>(a, smem, stream);
   }
-  k_blocks<<<a.nitems, threads, smem, stream>>>(a, smem);
 }
 
 // ----------------------------------------------------------- convergence --
@@ -606,50 +622,60 @@ void tmx_launch_converge(const int32_t *active, int nactive,
 
 // ------------------------------------------------------------- Q sums ------
 
-// TMatrixQTask::execute (TMatrixResource.hpp:1136-1210): full Qsca and Qext
-// over every m block, one thread per grain, in the reference's order.
-__global__ void k_qsums(const int64_t *__restrict__ t_off,
-                        const int32_t *__restrict__ nmaxv, int n,
-                        const cplx *__restrict__ T, double *q_out) {
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+// TMatrixQTask::execute (TMatrixResource.hpp:1136-1210): full Qsca and Qext.
+// The reference's quadruple loop over (n1, n2, m1, m2 = m1) visits every
+// entry of every m block once, so Qsca = sum_m f_m ||T_m||_F^2 and
+// Qext = sum_m f_m sum_n Re(T_m[(0,n),(0,n)] + T_m[(0,n),(1,n)] +
+// T_m[(1,n),(0,n)] + T_m[(1,n),(1,n)]), f_0 = 1, f_m = 2. One block per
+// grain reads each (contiguous) block coalesced; the reduction order is fixed.
+#define QS_THREADS 256
+__global__ void __launch_bounds__(QS_THREADS)
+    k_qsums(const int64_t *__restrict__ t_off, const int32_t *__restrict__ nmaxv,
+            int n, const cplx *__restrict__ T, double *q_out) {
+  const int g = blockIdx.x;
   if (g >= n) {
     return;
   }
   const int N = nmaxv[g];
   const cplx *Tg = T + t_off[g];
-  auto el = [&](int i1, int n1, int m, int i2, int n2) -> cplx {
+  double qs = 0., qe = 0.;
+  for (int m = 0; m <= N && N > 0; ++m) {
+    const int nb = (m == 0) ? N : N + 1 - m;
+    const int w = 2 * nb;
+    const double f = (m > 0) ? 2. : 1.;
     const cplx *B = Tg + block_offset(N, m);
-    if (m > 0) {
-      const int nm = N + 1 - m;
-      return B[(int64_t)(i1 * nm + n1 - m) * (2 * nm) + i2 * nm + n2 - m];
-    }
-    return B[(int64_t)(i1 * N + n1 - 1) * (2 * N) + i2 * N + n2 - 1];
-  };
-  double qs = 0.;
-  for (int n1 = 1; n1 < N + 1; ++n1) {
-    for (int n2 = 1; n2 < N + 1; ++n2) {
-      const int mtop = min(n1, n2);
-      for (int m1 = 0; m1 <= mtop; ++m1) {
-        const double factor = (m1 > 0) ? 2. : 1.;
-        qs += factor * cnorm2(el(0, n1, m1, 0, n2));
-        qs += factor * cnorm2(el(0, n1, m1, 1, n2));
-        qs += factor * cnorm2(el(1, n1, m1, 0, n2));
-        qs += factor * cnorm2(el(1, n1, m1, 1, n2));
+    double bs = 0., be = 0.;
+    for (int u = threadIdx.x; u < w * w; u += QS_THREADS) {
+      const cplx v = B[u];
+      bs += cnorm2(v);
+      if ((u / w) % nb == (u % w) % nb) {
+        be += v.x;
       }
     }
+    qs += f * bs;
+    qe += f * be;
   }
-  double qe = 0.;
-  for (int n1 = 1; n1 < N + 1; ++n1) {
-    for (int m1 = 0; m1 < n1 + 1; ++m1) {
-      const double factor = (m1 > 0) ? 2. : 1.;
-      qe += factor * el(0, n1, m1, 0, n1).x;
-      qe += factor * el(0, n1, m1, 1, n1).x;
-      qe += factor * el(1, n1, m1, 0, n1).x;
-      qe += factor * el(1, n1, m1, 1, n1).x;
+  __shared__ double red[2][QS_THREADS / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    qs += __shfl_down_sync(0xffffffffu, qs, o);
+    qe += __shfl_down_sync(0xffffffffu, qe, o);
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][warp] = qs;
+    red[1][warp] = qe;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0., b = 0.;
+    for (int i = 0; i < QS_THREADS / 32; ++i) {
+      a += red[0][i];
+      b += red[1][i];
     }
+    q_out[2 * g] = a;
+    q_out[2 * g + 1] = b;
   }
-  q_out[2 * g] = qs;
-  q_out[2 * g + 1] = qe;
 }
 
 void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
@@ -657,7 +683,7 @@ void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
   if (n <= 0) {
     return;
   }
-  k_qsums<<<(n + 127) / 128, 128, 0, stream>>>(t_off, nmax, n, T, q_out);
+  k_qsums<<<n, QS_THREADS, 0, stream>>>(t_off, nmax, n, T, q_out);
 }
 
 // ------------------------------------------------------------ chain prep --

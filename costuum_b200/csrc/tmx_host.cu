@@ -366,12 +366,17 @@ int tmx_host_class_size(int N, int m, int cls) {
 }
 
 int tmx_host_chunk_nodes(int max_nb) {
+  // quadrature nodes per shared-memory chunk: the assembly buffers may use
+  // what the LU phase needs anyway, but at least a small floor that grows
+  // with the class size (small classes keep small blocks)
   const int nrp = (max_nb + 3) / 4 * 4 + 4;
   const int ncol = (max_nb + 3) / 4 * 4;
   const size_t per_node = (size_t)(4 * nrp + 8 * ncol) * 16;
   const int lda = max_nb | 1;
   const size_t lu = ((size_t)max_nb * lda + max_nb) * 16 * 2;
-  const size_t budget = std::max<size_t>(64 * 1024, std::min<size_t>(lu, 200 * 1024));
+  const size_t floor =
+      max_nb <= 16 ? 12 * 1024 : (max_nb <= 32 ? 24 * 1024 : 64 * 1024);
+  const size_t budget = std::max<size_t>(floor, std::min<size_t>(lu, 200 * 1024));
   int G = (int)(budget / per_node);
   return std::max(1, std::min(32, G));
 }
@@ -466,8 +471,8 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   if (sched) {
     S = *sched;
   }
-  if (S.bessel_start <= 0) {
-    S.bessel_start = 800;
+  if (S.bessel_start < 0) {
+    S.bessel_start = 0;
   }
   if (S.min_order < 2 || S.max_order <= S.min_order ||
       S.gauss_legendre_factor < 1 || !(S.tolerance >= 0.)) {
@@ -480,8 +485,9 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
                 "max_order - 1 exceeds the on-chip block limit " +
                     std::to_string(TMX_MAX_NB));
   }
-  if (S.bessel_start < S.max_order) {
-    return fail(ctx, TMX_ERR_INVALID, "bessel_start must be >= max_order");
+  if (S.bessel_start > 0 && (S.bessel_start < S.max_order || S.bessel_start > 800)) {
+    return fail(ctx, TMX_ERR_INVALID,
+                "bessel_start must be 0 (automatic) or in [max_order, 800]");
   }
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;

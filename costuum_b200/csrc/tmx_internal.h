@@ -75,3 +75,7 @@ enum {
 };
 
 #define TMX_MAX_NB 128 // largest class size handled on chip
+
+// orders above max(nmax, |z|) at which the Bessel ratio recurrence starts
+// when no fixed start is requested
+#define TMX_BESSEL_MARGIN 64

@@ -11,6 +11,21 @@
 
 // ---------------------------------------------------------------- Bessel --
 
+// Start index of the downward ratio recurrence. The reference starts at
+// n = 800 for every argument (SPECIALFUNCTIONS_BESSEL_NMAX). Above
+// max(nmax, |z|) the recurrence contracts errors by about (|z| / 2n)^2 per
+// step, so a start 64 orders above max(nmax, |z|) reaches the same doubles
+// as a start at 800 (tests/test_bessel_start.py checks this bit for bit).
+// bessel_start > 0 forces a fixed start.
+__device__ __forceinline__ int bessel_nstart(int bessel_start, int nmax,
+                                             double absz) {
+  if (bessel_start > 0) {
+    return bessel_start;
+  }
+  const int hi = max(nmax, (int)ceil(absz)) + TMX_BESSEL_MARGIN;
+  return min(hi, 800);
+}
+
 // Spherical j_n and [z j_n]'/z, n = 1..nmax, for a real argument, by the
 // downward ratio recurrence rho_n = j_n / j_{n-1} started at n = nstart with
 // rho ~ z / (2 nstart + 1), then j_n = rho_n j_{n-1} upward
@@ -165,11 +180,13 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       S[TMX_NS_SININV] = sqrt(sin2inv);
       S[TMX_NS_SIN2INV] = sin2inv;
       S[TMX_NS_PAD] = 0.;
-      bessel_j_real(N, bessel_start, kr, T + TMX_Q_J, TMX_NQ);
+      bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
+                    TMX_NQ);
       bessel_y_real(N, kr, T + TMX_Q_Y, TMX_NQ);
     } else {
       const cplx krmr = mkc(G.mr * G.k * r * G.r_ev, G.mi * G.k * r * G.r_ev);
-      bessel_j_complex(N, bessel_start, krmr, T + TMX_Q_JM_RE, TMX_NQ);
+      bessel_j_complex(N, bessel_nstart(bessel_start, N, hypot(krmr.x, krmr.y)),
+                       krmr, T + TMX_Q_JM_RE, TMX_NQ);
     }
   }
 }

@@ -51,6 +51,11 @@ def lib():
         L.or_bessel_y_real.argtypes = [ctypes.c_int, ctypes.c_double, _D, _D]
         L.or_bessel_j_complex.argtypes = [ctypes.c_int, ctypes.c_double,
                                           ctypes.c_double, _D, _D]
+        L.or_bessel_j_real_start.argtypes = [ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, _D, _D]
+        L.or_bessel_j_complex_start.argtypes = [ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_double, ctypes.c_double,
+                                                _D, _D]
         L.or_wigner_d.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                   _D, _D]
         L.or_wigner_d_sinx.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int] * 2 + [_D, _D]
@@ -110,6 +115,20 @@ def bessel_j_complex(nmax, z):
     j = np.zeros(nmax, np.complex128)
     dj = np.zeros(nmax, np.complex128)
     lib().or_bessel_j_complex(nmax, z.real, z.imag, _p(j), _p(dj))
+    return j, dj
+
+
+def bessel_j_real_start(nmax, start, z):
+    j = np.zeros(nmax)
+    dj = np.zeros(nmax)
+    lib().or_bessel_j_real_start(nmax, start, z, _p(j), _p(dj))
+    return j, dj
+
+
+def bessel_j_complex_start(nmax, start, z):
+    j = np.zeros(nmax, np.complex128)
+    dj = np.zeros(nmax, np.complex128)
+    lib().or_bessel_j_complex_start(nmax, start, z.real, z.imag, _p(j), _p(dj))
     return j, dj
 
 

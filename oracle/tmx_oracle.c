@@ -113,12 +113,19 @@ static double gl_quadrature(double (*f)(double, const void *), const void *args,
  * downward ratio recurrence from n = 800, forward j_n = rho_n j_{n-1};
  * dj holds [z j_n(z)]' / z */
 void or_bessel_j_real(int nmax, double z, double *j, double *dj) {
+  or_bessel_j_real_start(nmax, BESSEL_START, z, j, dj);
+}
+
+/* the same recurrence started at an arbitrary index (for the start-index
+ * equivalence tests) */
+void or_bessel_j_real_start(int nmax, int start, double z, double *j,
+                            double *dj) {
   double rho[BESSEL_START];
   const double zinv = 1. / z;
-  const double twonp1 = 2. * BESSEL_START + 1.;
-  rho[BESSEL_START - 1] = z / twonp1;
-  for (unsigned i = 1; i < BESSEL_START; ++i) {
-    const unsigned index = BESSEL_START - i;
+  const double twonp1 = 2. * start + 1.;
+  rho[start - 1] = z / twonp1;
+  for (unsigned i = 1; i < (unsigned)start; ++i) {
+    const unsigned index = start - i;
     const double twoip1 = 2. * index + 1.;
     rho[index - 1] = 1. / (twoip1 * zinv - rho[index]);
   }
@@ -136,14 +143,19 @@ void or_bessel_j_real(int nmax, double z, double *j, double *dj) {
  * complex number, so products and quotients are full complex operations) */
 void or_bessel_j_complex(int nmax, double zr, double zi, double *jout,
                          double *djout) {
+  or_bessel_j_complex_start(nmax, BESSEL_START, zr, zi, jout, djout);
+}
+
+void or_bessel_j_complex_start(int nmax, int start, double zr, double zi,
+                               double *jout, double *djout) {
   cplx rho[BESSEL_START];
   const cplx z = CX(zr, zi);
   const cplx one = CX(1., 0.);
   const cplx zinv = one / z;
-  const cplx twonp1 = CX(2. * BESSEL_START + 1., 0.);
-  rho[BESSEL_START - 1] = z / twonp1;
-  for (unsigned i = 1; i < BESSEL_START; ++i) {
-    const unsigned index = BESSEL_START - i;
+  const cplx twonp1 = CX(2. * start + 1., 0.);
+  rho[start - 1] = z / twonp1;
+  for (unsigned i = 1; i < (unsigned)start; ++i) {
+    const unsigned index = start - i;
     const cplx twoip1 = CX(2. * index + 1., 0.);
     rho[index - 1] = one / (twoip1 * zinv - rho[index]);
   }

@@ -25,6 +25,11 @@ void or_gauss_legendre_ab(int order, double a, double b, double *x, double *w);
 void or_bessel_j_real(int nmax, double z, double *j, double *dj);
 void or_bessel_y_real(int nmax, double z, double *y, double *dy);
 void or_bessel_j_complex(int nmax, double zr, double zi, double *j, double *dj);
+/* the same recurrences started at index `start` instead of 800 */
+void or_bessel_j_real_start(int nmax, int start, double z, double *j,
+                            double *dj);
+void or_bessel_j_complex_start(int nmax, int start, double zr, double zi,
+                               double *j, double *dj);
 void or_wigner_d(double cosx, int nmax, int m, double *d, double *dd);
 void or_wigner_d_sinx(double cosx, double sinx, double sinx_inv, int nmax,
                       int m, double *d, double *dd);

@@ -79,3 +79,16 @@ def test_kernels_launched(ctx):
     before = ctx.kernel_launches
     ctx.tmatrix_batch([0.1e-6], 1e-6, 1.5 + 0.1j, 0.8)
     assert ctx.kernel_launches > before
+
+
+def test_bessel_start_automatic_equals_800(ctx):
+    """The automatic recurrence start gives the same T-matrices, bit for bit,
+    as the reference's fixed start at n = 800."""
+    r, lam, m, d = H.config2_sample(16, 5, xmax=10.0)
+    a = ctx.tmatrix_batch(r, lam, m, d, max_order=50, bessel_start=0)
+    Ta = [a.tmatrix(i) for i in range(len(r))]
+    na = a.nmax.copy()
+    b = ctx.tmatrix_batch(r, lam, m, d, max_order=50, bessel_start=800)
+    assert np.array_equal(na, b.nmax)
+    for i in range(len(r)):
+        assert np.array_equal(Ta[i], b.tmatrix(i)), i

@@ -43,6 +43,18 @@ SIGNATURES = {
     "tmx_profile_read": (ctypes.c_int, [_VP, ctypes.c_int, _D,
                                         ctypes.POINTER(ctypes.c_int64), _D]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
+    "tmx_orientation_coefficients": (ctypes.c_int, [ctypes.c_int, ctypes.c_double,
+                                                     ctypes.c_int, _VP, _VP, _D]),
+    "tmx_shape_distribution": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_double, ctypes.c_double,
+                                              _D, _D, _D]),
+    "tmx_rv_over_rs": (ctypes.c_double, [ctypes.c_double]),
+    "tmx_get_table": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, _D,
+                                     ctypes.c_int32, _D, ctypes.c_int32, _D,
+                                     ctypes.c_int32, _D, _D, _D, _D, _I32,
+                                     ctypes.c_int32, _D, ctypes.c_int32,
+                                     ctypes.c_int32, ctypes.c_int32,
+                                     ctypes.POINTER(TmxSchedule), _D, _D, _I32]),
     "tmx_tmatrix_fixed_noalloc": (ctypes.c_int, [ctypes.c_double] * 5
                                   + [ctypes.c_int32, ctypes.c_int32, _VP, _VP]),
 }
@@ -74,6 +86,10 @@ def ptr(a):
 
 def iptr(a):
     return a.ctypes.data_as(_I32)
+
+
+# p(beta) callback of a custom orientation distribution
+ORIENT_FN = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.c_double, ctypes.c_void_p)
 
 
 class TmxError(RuntimeError):

@@ -16,9 +16,10 @@ LIB = os.path.join(HERE, "libtmx.so")
 SOURCES = [
     ("tmx_tables.cu", ["--fmad=false"]),
     ("tmx_blocks.cu", []),
-    ("tmx_observables.cu", []),
+    ("tmx_observables.cu", ["--fmad=false"]),
     ("tmx_probe.cu", []),
     ("tmx_host.cu", []),
+    ("tmx_table.cu", []),
     ("tmx_noalloc.cu", []),
 ]
 

@@ -1,0 +1,201 @@
+// Internal: the context object shared by the host-side translation units.
+#pragma once
+
+#include <nvtx3/nvToolsExt.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/tmx.h"
+#include "tmx_common.cuh"
+#include "tmx_kernels.h"
+
+namespace {
+
+// NVTX range for the duration of a scope (phase markers for profilers)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+};
+
+} // namespace
+
+struct tmx_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+  // Gauss-Legendre cache: lower-half nodes of the 2 * ngauss rule
+  std::vector<int64_t> gl_off_h;
+  std::vector<double> gl_x_h, gl_w_h;
+  DevBuf gl_x, gl_w, gl_off;
+  bool gl_dirty = true;
+  // Wigner d table sets, keyed by (nmax, ngauss, all m?)
+  std::map<std::tuple<int, int, int>, int> wig_sets;
+  std::vector<int64_t> wig_off_h;
+  int64_t wig_used = 0;
+  DevBuf wig, wig_off;
+  // batch buffers
+  DevBuf grains, state, state0, act0, act1, actinit, count, slots, items, tab,
+      nsc, scratch, diag, T, t_off, nmaxv, q, status, probe;
+  // uploaded batch (device-resident inputs)
+  bool uploaded = false;
+  int64_t up_n = 0;
+  int up_nact = 0;
+  tmx_schedule up_sched;
+  std::vector<int32_t> up_status;
+  // observables (get_table): cached Clebsch-Gordan table and work buffers
+  DevBuf cg, cg_off;
+  int cg_nmax = 0;
+  DevBuf Ta, o_angles, o_phis, o_wts, o_coef, o_shw, o_og, o_work, o_sj, o_qj,
+      o_S, o_gq, o_gz, o_cq, o_cz;
+  int32_t *pinned = nullptr;
+  // timing: events on the library stream
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  bool profiling = false;
+  struct Prof {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+    double ms = 0.;
+    int64_t launches = 0;
+    double flops = 0.;
+  } prof[2]; // 0: block kernel, 1: table kernel
+  double flops_survey = 0.; // survey-model flops of the last batch
+  // last batch
+  int64_t n = 0;
+  bool have_batch = false;
+  std::vector<int32_t> nmax_h, ngauss_h, status_h;
+  std::vector<double> q_h;
+  std::vector<int64_t> t_off_h;
+};
+
+#define CK(call)                                                               \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess) {                                                   \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+      return TMX_ERR_CUDA;                                                     \
+    }                                                                          \
+  } while (0)
+
+#define LAUNCHED()                                                             \
+  do {                                                                         \
+    ++ctx->launches;                                                           \
+    CK(cudaGetLastError());                                                    \
+  } while (0)
+
+// executed flops of one class item: assembly (4 real FMAs per entry, node
+// and term; 2 terms for m = 0), LU (8/3 nb^3) and the two triangular solves
+// with nb right-hand sides (8 nb^3)
+static inline double item_flops(int nb, int m, int ng) {
+  const double b = nb;
+  const double terms = (m == 0) ? 2. : 4.;
+  return 8. * terms * b * b * ng + (8. / 3.) * b * b * b + 8. * b * b * b;
+}
+
+static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a) {
+  if (!ctx->profiling) {
+    return 0;
+  }
+  CK(cudaEventCreate(a));
+  CK(cudaEventRecord(*a, ctx->stream));
+  (void)k;
+  return 0;
+}
+
+static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops) {
+  if (!ctx->profiling) {
+    return 0;
+  }
+  cudaEvent_t b;
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(b, ctx->stream));
+  ctx->prof[k].pending.push_back({a, b});
+  ctx->prof[k].launches += 1;
+  ctx->prof[k].flops += flops;
+  return 0;
+}
+
+// resolve recorded event pairs (after the stream has been synchronised)
+static inline int prof_resolve(tmx_ctx *ctx) {
+  for (auto &p : ctx->prof) {
+    for (auto &e : p.pending) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e.first, e.second));
+      p.ms += ms;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    p.pending.clear();
+  }
+  return 0;
+}
+
+static inline int fail(tmx_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) {
+    ctx->err = msg;
+  }
+  return code;
+}
+
+// grow-only device buffer; contents are not preserved
+static inline int ensure(tmx_ctx *ctx, DevBuf &b, size_t bytes) {
+  if (bytes == 0) {
+    bytes = 16;
+  }
+  if (b.cap >= bytes) {
+    return TMX_OK;
+  }
+  if (b.p) {
+    CK(cudaFreeAsync(b.p, ctx->stream));
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  size_t want = bytes + bytes / 4;
+  cudaError_t e = cudaMallocAsync(&b.p, want, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    e = cudaMallocAsync(&b.p, bytes, ctx->stream);
+    want = bytes;
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, TMX_ERR_NOMEM,
+                "device allocation of " + std::to_string(bytes) + " bytes failed");
+  }
+  b.cap = want;
+  return TMX_OK;
+}
+
+// grow-only device buffer that keeps its first `keep` bytes
+static inline int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep) {
+  if (b.cap >= bytes) {
+    return TMX_OK;
+  }
+  DevBuf nb;
+  size_t want = std::max(bytes, b.cap * 2);
+  if (cudaMallocAsync(&nb.p, want, ctx->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, TMX_ERR_NOMEM, "device allocation failed (table cache)");
+  }
+  nb.cap = want;
+  if (b.p) {
+    if (keep) {
+      CK(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice,
+                         ctx->stream));
+    }
+    CK(cudaFreeAsync(b.p, ctx->stream));
+  }
+  b = nb;
+  return TMX_OK;
+}
+
+// Clebsch-Gordan table for all (n1, n2) <= nmax (tmx_table.cu)
+int tmx_ensure_cg(tmx_ctx *ctx, int nmax);

@@ -84,3 +84,58 @@ void tmx_launch_probe_dmma(double *out, int iters, int blocks,
 void tmx_host_gauss_legendre(int order, double *points, double *weights);
 int tmx_host_class_size(int N, int m, int cls);
 int tmx_host_chunk_nodes(int max_nb);
+
+// ------------------------------------------------------------ observables --
+
+// per-grain descriptor of the observable kernels
+struct TmxObsGrain {
+  int32_t nmax;
+  int32_t coef_set; // orientation coefficient set, -1: no averaging
+  int64_t t_off;    // complex offset of the grain's T-matrix
+  double k;         // wavenumber
+  double r_ev;      // equal-volume radius
+};
+
+// cos, sin, 1/sin of a zenith angle as the reference's grids compute them
+struct TmxAngle {
+  double c, s, si;
+};
+
+// forward-amplitude job: S(theta_in -> theta_out) for nphi azimuths
+struct TmxSJob {
+  int32_t grain;
+  int32_t angle_in;
+  int32_t angle_out;
+  int32_t nphi;
+  int64_t phi0; // first e^{i phi} of the job in the azimuth table
+  int64_t out;  // first S (4 complex each) of the job
+};
+
+// Q job for one (grain, theta): main amplitude and, with the scattering
+// subtraction, nacc x nacc amplitudes starting at s_acc
+struct TmxQJob {
+  int32_t grain;
+  int32_t pad;
+  int64_t out;
+  int64_t s_main;
+  int64_t s_acc;
+};
+
+void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
+                   int blocks, cudaStream_t stream);
+void tmx_launch_orient_avg(const TmxObsGrain *og, int ngrains, const double2 *T,
+                           double2 *Ta, const double *coeffs, int ncoef,
+                           const int64_t *cg_off, const double *cg, int cg_nmax,
+                           double2 *work, int wstride, int blocks, int threads,
+                           cudaStream_t stream);
+void tmx_launch_forward_s(const TmxSJob *jobs, int njobs, const TmxObsGrain *og,
+                          const double2 *Ta, const TmxAngle *angles,
+                          const double2 *phis, double2 *S, cudaStream_t stream);
+void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,
+                           const double2 *S, const double *wts, int nacc,
+                           double *qout, int qstride, int do_abs, int do_ext,
+                           cudaStream_t stream);
+void tmx_launch_z_epilogue(int n, const double2 *S, double *zout,
+                           cudaStream_t stream);
+void tmx_launch_shape_avg(int ncells, int nshape, int nper, const double *in,
+                          const double *w, double *out, cudaStream_t stream);

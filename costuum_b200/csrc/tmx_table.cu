@@ -1,0 +1,695 @@
+// Host side of the orientation/shape-averaged observables: orientation
+// distribution coefficients, shape distribution nodes, and the get_table
+// pipeline (T-matrices -> orientation average -> S -> Q / Z -> shape average).
+//
+// Reference (CosTuuM): CTMModule.cpp:146-478 (get_table), TaskManager.hpp:
+// 445-1346 (the per-grain task graph), OrientationDistribution.hpp:220-243,
+// MishchenkoOrientationDistribution.hpp:107-118,
+// DavisGreensteinOrientationDistribution.hpp:81-102,
+// ShapeDistribution.hpp:95-106, DraineHensleyShapeDistribution.hpp.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tmx_ctx.h"
+
+// ------------------------------------------------------ quadrature tools --
+
+// Gauss-Legendre rule on [a, b] (get_gauss_legendre_points_and_weights_ab,
+// SpecialFunctions.hpp:737-751)
+static void gl_ab(int order, double a, double b, double *x, double *w) {
+  tmx_host_gauss_legendre(order, x, w);
+  const double wfac = 0.5 * (b - a);
+  const double xterm = 0.5 * (a + b);
+  for (int i = 0; i < order; ++i) {
+    x[i] = wfac * x[i] + xterm;
+    w[i] *= wfac;
+  }
+}
+
+// Adaptive Gauss-Legendre quadrature that raises the order by one until
+// either the absolute or the relative change is below its target
+// (gauss_legendre_quadrature, SpecialFunctions.hpp:771-810).
+template <typename F>
+static double gl_quadrature(F f, double lower, double upper, int start,
+                            int maximum, double abs_tol, double rel_tol) {
+  int order = start;
+  double old_q = 0.;
+  double absd = abs_tol + 1.;
+  double reld = rel_tol + 1.;
+  std::vector<double> x(maximum > 0 ? maximum : 1), w(x.size());
+  while (order < maximum && absd > abs_tol && reld > rel_tol) {
+    gl_ab(order, lower, upper, x.data(), w.data());
+    double q = 0.;
+    for (int i = 0; i < order; ++i) {
+      q += w[i] * f(x[i]);
+    }
+    absd = fabs(q - old_q);
+    reld = absd / fabs(q + old_q);
+    old_q = q;
+    ++order;
+  }
+  return old_q;
+}
+
+// Legendre P_n(cos beta) = d^n_00(beta) by the m = 0 recurrence of
+// SpecialFunctions::wigner_dn_0m (SpecialFunctions.hpp:302-371)
+static double wigner_d00(double cosx, int order) {
+  if (order == 0) {
+    return 1.;
+  }
+  double d1 = 1., d2 = cosx, last = cosx;
+  for (int n = 0; n < order; ++n) {
+    const double np1 = n + 1.;
+    const double np2 = n + 2.;
+    const double np12p1 = 2. * np1 + 1.;
+    const double dnp1 = (np12p1 * cosx * d2 - np1 * d1) / np2;
+    last = d2;
+    d1 = d2;
+    d2 = dnp1;
+  }
+  return last;
+}
+
+// ------------------------------------------------------- distributions ---
+
+extern "C" int tmx_orientation_coefficients(int kind, double param, int order,
+                                            double (*fn)(double, void *),
+                                            void *arg, double *out) {
+  if (order < 0 || !out || kind < 0 || kind > 3 || (kind == 3 && !fn)) {
+    return TMX_ERR_INVALID;
+  }
+  for (int i = 0; i <= order; ++i) {
+    out[i] = 0.;
+  }
+  if (kind == 1) {
+    // Mishchenko: p(beta) = 1/2 + 5/4 p2 (3 cos^2 - 1), p2 = 3/2 <cos^2> - 1/2
+    out[0] = 1.;
+    if (order >= 2) {
+      out[2] = 1.5 * param - 0.5;
+    }
+    return TMX_OK;
+  }
+  if (kind == 2) {
+    // Davis-Greenstein perfect alignment
+    if (param < 1.) {
+      double nominator = 1., denominator = 2.;
+      out[0] = 1.;
+      for (int i = 1; 2 * i < order + 1; ++i) {
+        const int sign = (i % 2 == 0) ? 1 : -1;
+        out[2 * i] = sign * nominator / denominator;
+        nominator *= 2. * i + 1.;
+        denominator *= 2. * (i + 1.);
+      }
+    } else {
+      for (int i = 0; i <= order; ++i) {
+        out[i] = 1.;
+      }
+    }
+    return TMX_OK;
+  }
+  // numerical: random (p = 1/2; tolerances 1e-10 / 1e-5) or custom
+  // (Python function; tolerances 1e-4 / 1e-4, PyOrientationDistribution.hpp)
+  auto p = [&](double beta) { return kind == 0 ? 0.5 : fn(beta, arg); };
+  const double at = (kind == 0) ? 1.e-10 : 1.e-4;
+  const double rt = (kind == 0) ? 1.e-5 : 1.e-4;
+  const double norm = gl_quadrature(
+      [&](double beta) { return sin(beta) * p(beta); }, 0., M_PI, 100, 1000,
+      at, rt);
+  const double nf = 1. / norm;
+  out[0] = 1.;
+  for (int i = 1; i <= order; ++i) {
+    out[i] = gl_quadrature(
+        [&](double beta) {
+          const double cb = cos(beta);
+          const double sb = sin(beta);
+          const double pb = nf * p(beta);
+          return sb * pb * wigner_d00(cb, i);
+        },
+        0., M_PI, 2 * (i + 1), 100 * (i + 1), at, rt);
+  }
+  return TMX_OK;
+}
+
+namespace {
+
+// DraineHensleyShapeDistribution helpers (DraineHensleyShapeDistribution.hpp)
+double dh_shape_factor(double d) {
+  if (d < 1.) {
+    const double e2 = 1. - d * d;
+    const double e = sqrt(e2);
+    return (1. - e2) * (0.5 * log((1. + e) / (1. - e)) / e - 1.) / e2;
+  } else if (d > 1.) {
+    const double e2 = 1. - 1. / (d * d);
+    const double e = sqrt(e2);
+    return (1. - sqrt(1. - e2) * asin(e) / e) / e2;
+  }
+  return 1. / 3.;
+}
+
+double dh_jacobian(double d) {
+  if (d < 1.) {
+    const double e2 = 1. - d * d;
+    if (e2 < 1.e-5) {
+      return 4. / 15. + 2. * e2 / 21. + 3. * e2 * e2 / 70.;
+    }
+    const double e = sqrt(e2);
+    return 0.5 * sqrt(1. - e2) * ((3. - e2) * log((1. + e) / (1. - e)) - 6. * e) /
+           (e2 * e2 * e);
+  } else if (d > 1.) {
+    const double e2 = 1. - 1. / (d * d);
+    if (e2 < 1.e-5) {
+      return 4. / 15. - 2. * e2 / 21. - 11. * e2 * e2 / 210.;
+    }
+    const double e = sqrt(e2);
+    return (1. - e2) * ((3. - 2. * e2) * asin(e) - 3. * e * sqrt(1. - e2)) /
+           (e2 * e2 * e);
+  }
+  return 4. / 15.;
+}
+
+double dh_cde2(double L) {
+  const double Lm1 = L - 1.;
+  return 12. * L * Lm1 * Lm1;
+}
+
+double dh_eval(double d) { return dh_cde2(dh_shape_factor(d)) * dh_jacobian(d); }
+
+} // namespace
+
+// kind 0: the default ShapeDistribution (exp(-(d-1)^2 / (2 x 0.027777778))
+// on [0.5, 1.5]); kind 1: Draine & Hensley (2017) CDE2 with a probability
+// cutoff (param1) or a prolate/oblate fraction (param2 > 0)
+extern "C" int tmx_shape_distribution(int kind, int npoints, double param1,
+                                      double param2, double *shapes,
+                                      double *weights, double *limits) {
+  if (npoints < 1 || !shapes || !weights || kind < 0 || kind > 1) {
+    return TMX_ERR_INVALID;
+  }
+  double dmin = 0.5, dmax = 1.5;
+  auto pdf = [&](double d) -> double {
+    if (kind == 0) {
+      if (d >= 0.5 && d <= 1.5) {
+        const double x = d - 1.;
+        return exp(-0.5 * x * x / 0.027777778);
+      }
+      return 0.;
+    }
+    return (d >= dmin && d <= dmax) ? dh_eval(d) : 0.;
+  };
+  if (kind == 1) {
+    const double cutoff = param1, fraction = param2;
+    if (fraction > 0.) {
+      auto integ = [&](double a, double b) {
+        return gl_quadrature([&](double d) { return dh_eval(d); }, a, b, 10,
+                             1000, 1.e-10, 1.e-10);
+      };
+      const double prolate_fraction = integ(0., 1.);
+      const double prolate_target = fraction * prolate_fraction;
+      double lower = 0., upper = 1., half = 0.5;
+      double integral = integ(half, 1.);
+      int guard = 0;
+      while (fabs(integral - prolate_target) >
+                 0.005 * fabs(integral + prolate_target) &&
+             ++guard < 200) {
+        if (integral > prolate_target) {
+          lower = half;
+        } else {
+          upper = half;
+        }
+        half = 0.5 * (lower + upper);
+        integral = integ(half, 1.);
+      }
+      dmin = half;
+      const double oblate_target = fraction * (1. - prolate_fraction);
+      lower = 1.;
+      upper = 2.;
+      integral = integ(1., upper);
+      guard = 0;
+      while (integral < oblate_target && ++guard < 60) {
+        upper *= 2.;
+        integral = integ(1., upper);
+      }
+      half = 0.5 * (lower + upper);
+      integral = integ(1., half);
+      guard = 0;
+      while (fabs(integral - oblate_target) > 1.e-5 * fabs(integral + oblate_target) &&
+             ++guard < 200) {
+        if (integral > oblate_target) {
+          upper = half;
+        } else {
+          lower = half;
+        }
+        half = 0.5 * (lower + upper);
+        integral = integ(1., half);
+      }
+      dmax = half;
+    } else {
+      dmin = 1.;
+      dmax = 1.;
+      double valmin = pdf(dmin) - cutoff;
+      int guard = 0;
+      while (valmin > 0. && ++guard < 200) {
+        dmin *= 0.5;
+        valmin = pdf(dmin) - cutoff;
+      }
+      double ub = 1.;
+      guard = 0;
+      while (fabs(dmin - ub) > 0.005 * fabs(dmin + ub) && ++guard < 200) {
+        const double mid = 0.5 * (dmin + ub);
+        const double v = pdf(mid) - cutoff;
+        if (v < 0.) {
+          dmin = mid;
+        } else {
+          ub = mid;
+        }
+      }
+      double valmax = pdf(dmax) - cutoff;
+      guard = 0;
+      while (valmax > 0. && ++guard < 1000) {
+        dmax += 1.;
+        valmax = pdf(dmax) - cutoff;
+      }
+      double lb = 1.;
+      guard = 0;
+      while (fabs(dmax - lb) > 0.005 * fabs(dmax + lb) && ++guard < 200) {
+        const double mid = 0.5 * (lb + dmax);
+        const double v = pdf(mid) - cutoff;
+        if (v > 0.) {
+          lb = mid;
+        } else {
+          dmax = mid;
+        }
+      }
+    }
+  }
+  if (limits) {
+    limits[0] = dmin;
+    limits[1] = dmax;
+  }
+  // ShapeDistribution::evaluate: GL nodes on [dmin, dmax], weight x p(d)
+  gl_ab(npoints, dmin, dmax, shapes, weights);
+  for (int i = 0; i < npoints; ++i) {
+    weights[i] *= pdf(shapes[i]);
+  }
+  return TMX_OK;
+}
+
+// R_V / R_S of a spheroid (get_equal_volume_to_equal_surface_area_sphere_
+// ratio, SpecialFunctions.hpp:557-583)
+extern "C" double tmx_rv_over_rs(double d) {
+  if (d > 1.) {
+    const double d2 = d * d;
+    const double e = sqrt(1. - 1. / d2);
+    const double cbrtd2 = cbrt(d2);
+    return 1. / sqrt(0.25 * (2. * cbrtd2 +
+                             log((1. + e) / (1. - e)) / (e * cbrtd2 * cbrtd2)));
+  } else if (d < 1.) {
+    const double cbrtd = cbrt(d);
+    const double e = sqrt(1. - d * d);
+    return 1. / sqrt(0.5 * (cbrtd * cbrtd + asin(e) / (e * cbrtd)));
+  }
+  return 1.;
+}
+
+// -------------------------------------------------------------- get_table --
+
+namespace {
+
+// zenith angle as the reference's grids compute it
+TmxAngle make_angle(double cost) {
+  TmxAngle a;
+  a.c = cost;
+  a.s = sqrt((1. - cost) * (1. + cost));
+  a.si = (a.s != 0.) ? 1. / a.s : 9000.;
+  return a;
+}
+
+int64_t est_nmax(double x, int min_order, int max_order) {
+  double e = x + 4.05 * cbrt(x) + 8.;
+  e = std::max<double>(e, min_order);
+  return std::min<int64_t>((int64_t)e, max_order - 1);
+}
+
+} // namespace
+
+extern "C" int tmx_get_table(
+    tmx_ctx *ctx, int32_t ntypes, int32_t nsizes, const double *sizes,
+    int32_t nlambda, const double *lambdas, int32_t ntheta,
+    const double *thetas, int32_t nshape, const double *shapes,
+    const double *shape_weights, const double *mr, const double *mi,
+    const int32_t *orient_set, int32_t nsets, const double *coeffs,
+    int32_t ncoef, int32_t flags, int32_t ngauss, const tmx_schedule *sched,
+    double *out_q, double *out_z, int32_t *grain_status) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  const bool do_abs = flags & TMX_TABLE_ABSORPTION;
+  const bool do_ext = flags & TMX_TABLE_EXTINCTION;
+  const bool do_sca = flags & TMX_TABLE_SCATTERING;
+  const bool account = (flags & TMX_TABLE_ACCOUNT_FOR_SCATTERING) && do_abs;
+  if (ntypes < 0 || nsizes < 0 || nlambda < 0 || ntheta < 0 || nshape < 1 ||
+      !sizes || !lambdas || (ntheta > 0 && !thetas) || !shapes ||
+      !shape_weights || !mr || !mi || !orient_set || nsets < 0 ||
+      (nsets > 0 && (!coeffs || ncoef < 1)) || (account && ngauss < 1) ||
+      ((do_abs || do_ext) && !out_q) || (do_sca && !out_z)) {
+    return fail(ctx, TMX_ERR_INVALID, "tmx_get_table: invalid arguments");
+  }
+  tmx_schedule S = {10, 100, 2, 0, 1.e-4};
+  if (sched) {
+    S = *sched;
+  }
+  for (int i = 0; i < nsizes * nshape; ++i) {
+    if (orient_set[i] >= nsets) {
+      return fail(ctx, TMX_ERR_INVALID, "tmx_get_table: orientation set index");
+    }
+  }
+  const int nq = (do_abs ? 2 : 0) + (do_ext ? 3 : 0);
+  const int nphi_sca = 2 * ntheta;
+  const int64_t ncells = (int64_t)ntypes * nsizes * nlambda;
+  if (ncells == 0 || ntheta == 0 || (!do_abs && !do_ext && !do_sca)) {
+    return TMX_OK;
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  int rc;
+  NvtxRange range("tmx_get_table");
+
+  // ---- angle and azimuth tables
+  std::vector<TmxAngle> ang;
+  for (int i = 0; i < ntheta; ++i) {
+    ang.push_back(make_angle(cos(thetas[i])));
+  }
+  const int acc_a0 = (int)ang.size();
+  std::vector<double> acc_w; // [theta weights (ngauss), phi weights (ngauss)]
+  std::vector<cplx> phis;
+  phis.push_back(mkc(1., 0.)); // azimuth 0 for the theta -> theta amplitude
+  int64_t acc_p0 = 0, sca_p0 = 0;
+  if (account) {
+    std::vector<double> ct(ngauss), wt(ngauss), ph(ngauss), wp(ngauss);
+    tmx_host_gauss_legendre(ngauss, ct.data(), wt.data());
+    gl_ab(ngauss, 0., 2. * M_PI, ph.data(), wp.data());
+    for (int i = 0; i < ngauss; ++i) {
+      ang.push_back(make_angle(ct[i]));
+    }
+    acc_w = wt;
+    acc_w.insert(acc_w.end(), wp.begin(), wp.end());
+    acc_p0 = (int64_t)phis.size();
+    for (int i = 0; i < ngauss; ++i) {
+      phis.push_back(mkc(cos(ph[i]), -sin(ph[i])));
+    }
+  }
+  int sca_ain = -1, sca_a0 = -1;
+  if (do_sca) {
+    sca_ain = (int)ang.size();
+    ang.push_back(make_angle(cos(M_PI_2)));
+    sca_a0 = (int)ang.size();
+    std::vector<double> ct(ntheta), wt(ntheta), ph(nphi_sca), wp(nphi_sca);
+    tmx_host_gauss_legendre(ntheta, ct.data(), wt.data());
+    for (int i = 0; i < ntheta; ++i) {
+      // theta_out = acos(GL node); the grid keeps cos(theta_out) = node
+      ang.push_back(make_angle(ct[i]));
+    }
+    gl_ab(nphi_sca, 0., 2. * M_PI, ph.data(), wp.data());
+    sca_p0 = (int64_t)phis.size();
+    for (int i = 0; i < nphi_sca; ++i) {
+      phis.push_back(mkc(cos(ph[i]), sin(ph[i])));
+    }
+  }
+  if ((rc = ensure(ctx, ctx->o_angles, ang.size() * sizeof(TmxAngle))) ||
+      (rc = ensure(ctx, ctx->o_phis, phis.size() * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->o_wts, std::max<size_t>(1, acc_w.size()) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->o_coef, std::max<int64_t>(1, (int64_t)nsets * ncoef) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->o_shw, nshape * sizeof(double)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->o_phis.p, phis.data(), phis.size() * sizeof(cplx),
+                     cudaMemcpyHostToDevice, st));
+  if (!acc_w.empty()) {
+    CK(cudaMemcpyAsync(ctx->o_wts.p, acc_w.data(), acc_w.size() * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
+  }
+  if (nsets > 0) {
+    CK(cudaMemcpyAsync(ctx->o_coef.p, coeffs, (int64_t)nsets * ncoef * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaMemcpyAsync(ctx->o_shw.p, shape_weights, nshape * sizeof(double),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st)); // host vectors above are about to change
+
+  // ---- chunks of whole cells (all shapes of a cell stay together)
+  const int64_t per_grain_s =
+      ntheta + (account ? (int64_t)ntheta * ngauss * ngauss : 0) +
+      (do_sca ? (int64_t)ntheta * nphi_sca : 0);
+  const double budget = 6.e9; // bytes for T, Ta and S of one chunk
+  std::vector<double> gr_r, gr_l, gr_mr, gr_mi, gr_d;
+  int64_t c0 = 0;
+  while (c0 < ncells) {
+    // grow the chunk until the estimated memory reaches the budget
+    int64_t c1 = c0;
+    double bytes = 0.;
+    while (c1 < ncells) {
+      const int64_t isz = (c1 / nlambda) % nsizes;
+      const int64_t il = c1 % nlambda;
+      double cell = 0.;
+      for (int s = 0; s < nshape; ++s) {
+        const double x = 2. * M_PI * sizes[isz] / lambdas[il] * std::max(1., cbrt(shapes[s]));
+        const int64_t N = est_nmax(x, S.min_order, S.max_order);
+        cell += 2. * tmx_tmatrix_size((int32_t)N) * 16. + per_grain_s * 64.;
+      }
+      if (c1 > c0 && bytes + cell > budget) {
+        break;
+      }
+      bytes += cell;
+      ++c1;
+      if ((c1 - c0) * nshape >= 32768) {
+        break;
+      }
+    }
+    const int64_t nc = c1 - c0;
+    const int64_t ng = nc * nshape;
+    gr_r.resize(ng);
+    gr_l.resize(ng);
+    gr_mr.resize(ng);
+    gr_mi.resize(ng);
+    gr_d.resize(ng);
+    for (int64_t c = 0; c < nc; ++c) {
+      const int64_t cell = c0 + c;
+      const int64_t isz = (cell / nlambda) % nsizes;
+      const int64_t il = cell % nlambda;
+      for (int s = 0; s < nshape; ++s) {
+        const int64_t g = c * nshape + s;
+        gr_r[g] = sizes[isz];
+        gr_l[g] = lambdas[il];
+        gr_mr[g] = mr[cell];
+        gr_mi[g] = mi[cell];
+        gr_d[g] = shapes[s];
+      }
+    }
+    if ((rc = tmx_batch_upload(ctx, ng, gr_r.data(), gr_l.data(), gr_mr.data(),
+                               gr_mi.data(), gr_d.data(), &S)) ||
+        (rc = tmx_batch_compute(ctx))) {
+      return rc;
+    }
+    if (grain_status) {
+      for (int64_t g = 0; g < ng; ++g) {
+        grain_status[c0 * nshape + g] = ctx->status_h[g];
+      }
+    }
+    // ---- per-grain observable descriptors
+    int nmax_chunk = 1;
+    std::vector<TmxObsGrain> og(ng);
+    int64_t t_total = 0;
+    for (int64_t g = 0; g < ng; ++g) {
+      const int64_t cell = c0 + g / nshape;
+      const int64_t isz = (cell / nlambda) % nsizes;
+      const int s = (int)(g % nshape);
+      og[g].nmax = ctx->nmax_h[g];
+      og[g].coef_set = orient_set[isz * nshape + s];
+      og[g].t_off = ctx->t_off_h[g];
+      og[g].k = 2. * M_PI / lambdas[cell % nlambda];
+      og[g].r_ev = sizes[isz];
+      nmax_chunk = std::max(nmax_chunk, og[g].nmax);
+      if (og[g].nmax > 0) {
+        t_total = std::max<int64_t>(t_total, og[g].t_off + tmx_tmatrix_size(og[g].nmax));
+      }
+      if (og[g].coef_set >= 0 && 2 * og[g].nmax + 1 > ncoef) {
+        return fail(ctx, TMX_ERR_INVALID,
+                    "tmx_get_table: orientation coefficients shorter than 2 nmax + 1");
+      }
+    }
+    if ((rc = tmx_ensure_cg(ctx, nmax_chunk))) {
+      return rc;
+    }
+    // ---- orientation average (disabled alignment keeps T)
+    const int oa_blocks = (int)std::min<int64_t>(ng, 4 * 148);
+    const int oa_threads = 128;
+    const int wstride = 2 * (2 * nmax_chunk + 1);
+    if ((rc = ensure(ctx, ctx->o_og, ng * sizeof(TmxObsGrain))) ||
+        (rc = ensure(ctx, ctx->Ta, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->o_work, (size_t)oa_blocks * oa_threads * wstride * sizeof(cplx)))) {
+      return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), ng * sizeof(TmxObsGrain),
+                       cudaMemcpyHostToDevice, st));
+    if (t_total > 0) {
+      CK(cudaMemcpyAsync(ctx->Ta.p, ctx->T.p, t_total * sizeof(cplx),
+                         cudaMemcpyDeviceToDevice, st));
+    }
+    tmx_launch_orient_avg((const TmxObsGrain *)ctx->o_og.p, (int)ng,
+                          (const cplx *)ctx->T.p, (cplx *)ctx->Ta.p,
+                          (const double *)ctx->o_coef.p, ncoef,
+                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
+                          ctx->cg_nmax, (cplx *)ctx->o_work.p, wstride, oa_blocks,
+                          oa_threads, st);
+    LAUNCHED();
+    // ---- amplitude jobs
+    std::vector<TmxSJob> sj;
+    std::vector<TmxQJob> qj;
+    int64_t sidx = 0;
+    const int64_t sca_base = ng * ntheta * (1 + (account ? (int64_t)ngauss * ngauss : 0));
+    for (int64_t g = 0; g < ng; ++g) {
+      if (og[g].nmax <= 0) {
+        continue;
+      }
+      for (int t = 0; t < ntheta; ++t) {
+        TmxQJob q;
+        q.grain = (int32_t)g;
+        q.pad = 0;
+        q.out = g * ntheta + t;
+        TmxSJob j;
+        j.grain = (int32_t)g;
+        j.angle_in = t;
+        j.angle_out = t;
+        j.nphi = 1;
+        j.phi0 = 0;
+        j.out = sidx;
+        q.s_main = sidx;
+        sidx += 1;
+        sj.push_back(j);
+        q.s_acc = sidx;
+        if (account) {
+          for (int ti = 0; ti < ngauss; ++ti) {
+            TmxSJob a;
+            a.grain = (int32_t)g;
+            a.angle_in = acc_a0 + ti;
+            a.angle_out = t;
+            a.nphi = ngauss;
+            a.phi0 = acc_p0;
+            a.out = sidx;
+            sidx += ngauss;
+            sj.push_back(a);
+          }
+        }
+        qj.push_back(q);
+      }
+    }
+    int64_t nsca = 0;
+    if (do_sca) {
+      for (int64_t g = 0; g < ng; ++g) {
+        for (int t = 0; t < ntheta; ++t) {
+          if (og[g].nmax > 0) {
+            TmxSJob j;
+            j.grain = (int32_t)g;
+            j.angle_in = sca_ain;
+            j.angle_out = sca_a0 + t;
+            j.nphi = nphi_sca;
+            j.phi0 = sca_p0;
+            j.out = sca_base + (g * ntheta + t) * nphi_sca;
+            sj.push_back(j);
+          }
+        }
+      }
+      nsca = ng * ntheta * nphi_sca;
+    }
+    const int64_t s_total = sca_base + nsca;
+    if ((rc = ensure(ctx, ctx->o_sj, std::max<size_t>(1, sj.size()) * sizeof(TmxSJob))) ||
+        (rc = ensure(ctx, ctx->o_qj, std::max<size_t>(1, qj.size()) * sizeof(TmxQJob))) ||
+        (rc = ensure(ctx, ctx->o_S, std::max<int64_t>(1, s_total) * 4 * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, ng * ntheta * nq) * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->o_gz, std::max<int64_t>(1, do_sca ? nsca * 16 : 1) * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->o_cq, std::max<int64_t>(1, nc * ntheta * nq) * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->o_cz, std::max<int64_t>(1, do_sca ? nc * ntheta * nphi_sca * 16 : 1) * sizeof(double)))) {
+      return rc;
+    }
+    CK(cudaMemsetAsync(ctx->o_S.p, 0, s_total * 4 * sizeof(cplx), st));
+    if (!sj.empty()) {
+      CK(cudaMemcpyAsync(ctx->o_sj.p, sj.data(), sj.size() * sizeof(TmxSJob),
+                         cudaMemcpyHostToDevice, st));
+    }
+    if (!qj.empty()) {
+      CK(cudaMemcpyAsync(ctx->o_qj.p, qj.data(), qj.size() * sizeof(TmxQJob),
+                         cudaMemcpyHostToDevice, st));
+    }
+    tmx_launch_forward_s((const TmxSJob *)ctx->o_sj.p, (int)sj.size(),
+                         (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->Ta.p,
+                         (const TmxAngle *)ctx->o_angles.p,
+                         (const cplx *)ctx->o_phis.p, (cplx *)ctx->o_S.p, st);
+    LAUNCHED();
+    if (nq > 0) {
+      CK(cudaMemsetAsync(ctx->o_gq.p, 0, ng * ntheta * nq * sizeof(double), st));
+      tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, (int)qj.size(),
+                            (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->o_S.p,
+                            (const double *)ctx->o_wts.p, account ? ngauss : 0,
+                            (double *)ctx->o_gq.p, nq, do_abs, do_ext, st);
+      LAUNCHED();
+      tmx_launch_shape_avg((int)nc, nshape, ntheta * nq, (const double *)ctx->o_gq.p,
+                           (const double *)ctx->o_shw.p, (double *)ctx->o_cq.p, st);
+      LAUNCHED();
+      CK(cudaMemcpyAsync(out_q + c0 * ntheta * nq, ctx->o_cq.p,
+                         nc * ntheta * nq * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    if (do_sca) {
+      tmx_launch_z_epilogue((int)nsca, (const cplx *)ctx->o_S.p + sca_base * 4,
+                            (double *)ctx->o_gz.p, st);
+      LAUNCHED();
+      tmx_launch_shape_avg((int)nc, nshape, ntheta * nphi_sca * 16,
+                           (const double *)ctx->o_gz.p, (const double *)ctx->o_shw.p,
+                           (double *)ctx->o_cz.p, st);
+      LAUNCHED();
+      CK(cudaMemcpyAsync(out_z + c0 * ntheta * nphi_sca * 16, ctx->o_cz.p,
+                         nc * ntheta * nphi_sca * 16 * sizeof(double),
+                         cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    c0 = c1;
+  }
+  return TMX_OK;
+}
+
+// Clebsch-Gordan table for every (n1, n2) up to nmax (cached; rebuilt when a
+// larger nmax is needed)
+int tmx_ensure_cg(tmx_ctx *ctx, int nmax) {
+  if (ctx->cg_nmax >= nmax && ctx->cg_nmax > 0) {
+    return TMX_OK;
+  }
+  nmax = std::max(nmax, ctx->cg_nmax);
+  cudaStream_t st = ctx->stream;
+  std::vector<int64_t> off((size_t)nmax * nmax);
+  int64_t tot = 0;
+  for (int n1 = 1; n1 <= nmax; ++n1) {
+    for (int n2 = 1; n2 <= nmax; ++n2) {
+      const int M = std::min(n1, n2);
+      off[(size_t)(n1 - 1) * nmax + (n2 - 1)] = tot;
+      tot += (int64_t)(2 * M + 1) * (M + 1);
+    }
+  }
+  const int blocks = 4 * 148;
+  int rc;
+  if ((rc = ensure(ctx, ctx->cg, tot * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->cg_off, off.size() * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->o_work,
+                   (size_t)blocks * 128 * 2 * (2 * nmax + 1) * sizeof(double)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->cg_off.p, off.data(), off.size() * sizeof(int64_t),
+                     cudaMemcpyHostToDevice, st));
+  tmx_launch_cg(nmax, (const int64_t *)ctx->cg_off.p, (double *)ctx->cg.p,
+                (double *)ctx->o_work.p, blocks, st);
+  LAUNCHED();
+  CK(cudaStreamSynchronize(st));
+  ctx->cg_nmax = nmax;
+  return TMX_OK;
+}

@@ -132,6 +132,63 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
  * (every chain order and every m block as a full 2nb x 2nb LU + solve). */
 double tmx_batch_flops_survey(const tmx_ctx *ctx);
 
+/* ------------------------------------------------ averaged observables ---
+ *
+ * Orientation distribution expansion coefficients p_0 .. p_order
+ * (OrientationDistribution::initialise, src/OrientationDistribution.hpp:
+ * 220-243 and its subclasses): kind 0 random orientation (p(beta) = 1/2,
+ * numerical quadrature), 1 Mishchenko (param = <cos^2 beta>,
+ * src/MishchenkoOrientationDistribution.hpp:107-118), 2 Davis-Greenstein
+ * perfect alignment (param = axis ratio,
+ * src/DavisGreensteinOrientationDistribution.hpp:81-102), 3 custom p(beta)
+ * given by fn(beta, arg) (src/PyOrientationDistribution.hpp:458-600). */
+int tmx_orientation_coefficients(int kind, double param, int order,
+                                 double (*fn)(double, void *), void *arg,
+                                 double *out);
+
+/* Shape distribution quadrature nodes and weights (ShapeDistribution::
+ * evaluate, src/ShapeDistribution.hpp:95-106): kind 0 the default
+ * distribution on [0.5, 1.5], kind 1 Draine & Hensley
+ * (src/DraineHensleyShapeDistribution.hpp; param1 = cutoff, param2 =
+ * fraction, as its constructor). limits (may be NULL) receives the minimum
+ * and maximum axis ratio. */
+int tmx_shape_distribution(int kind, int npoints, double param1, double param2,
+                           double *shapes, double *weights, double *limits);
+
+/* R_V / R_S, the ratio of the equal-volume and equal-surface-area sphere
+ * radii of a spheroid with axis ratio d
+ * (src/SpecialFunctions.hpp:557-583; CTMModule.cpp:66-95). */
+double tmx_rv_over_rs(double axis_ratio);
+
+enum tmx_table_flags {
+  TMX_TABLE_ABSORPTION = 1,
+  TMX_TABLE_EXTINCTION = 2,
+  TMX_TABLE_SCATTERING = 4,
+  TMX_TABLE_ACCOUNT_FOR_SCATTERING = 8
+};
+
+/* The get_table computation (src/CTMModule.cpp:146-478 with the task graph of
+ * src/TaskManager.hpp:445-1346) for a grid of compositions x sizes x
+ * wavelengths x shapes. sizes and lambdas must already be sorted ascending
+ * (the reference sorts them). mr/mi[(type * nsizes + size) * nlambda + l] is
+ * the refractive index of each cell; orient_set[size * nshape + shape] picks a
+ * row of coeffs[nsets][ncoef] (or -1: no orientation averaging); ncoef must
+ * exceed 2 nmax. Outputs (host): out_q[cell][theta][k] with k = (Qabs,
+ * Qabspol) if TMX_TABLE_ABSORPTION then (Qext, Qextpol, Qextcpol) if
+ * TMX_TABLE_EXTINCTION; out_z[cell][theta][phi][4][4] on the reference's
+ * scattering grid (theta_in = pi/2, ntheta Gauss-Legendre zenith angles,
+ * 2 ntheta Gauss-Legendre azimuths); grain_status[cell][shape] (may be
+ * NULL). ngauss is number_of_quadrature_angles of the scattering
+ * subtraction. */
+int tmx_get_table(tmx_ctx *ctx, int32_t ntypes, int32_t nsizes,
+                  const double *sizes, int32_t nlambda, const double *lambdas,
+                  int32_t ntheta, const double *thetas, int32_t nshape,
+                  const double *shapes, const double *shape_weights,
+                  const double *mr, const double *mi, const int32_t *orient_set,
+                  int32_t nsets, const double *coeffs, int32_t ncoef,
+                  int32_t flags, int32_t ngauss, const tmx_schedule *schedule,
+                  double *out_q, double *out_z, int32_t *grain_status);
+
 /* T-matrix of one grain at a fixed (nmax, ngauss), all m blocks, for callers
  * that cannot allocate device memory -- e.g. a host application whose device
  * memory is owned by another framework's caching allocator, or a per-call

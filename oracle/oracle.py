@@ -287,6 +287,9 @@ def ref():
         L.ref_plu_inverse.argtypes = [ctypes.c_int, _D]
         L.ref_orientation_coefficients.argtypes = [ctypes.c_int, ctypes.c_double,
                                                    ctypes.c_int, _D]
+        L.ref_custom_orientation_coefficients.argtypes = [ctypes.c_int, _D]
+        L.ref_draine_hensley.argtypes = [ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, _D, _D, _D]
         L.ref_batch_create.restype = ctypes.c_void_p
         L.ref_batch_create.argtypes = ([ctypes.c_int] + [_D] * 5 + [ctypes.c_int] * 3
                                        + [ctypes.c_double, ctypes.c_int])

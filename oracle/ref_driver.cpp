@@ -20,6 +20,7 @@
 #include "AlignmentAverageTask.hpp"
 #include "ConvergedSizeResources.hpp"
 #include "DavisGreensteinOrientationDistribution.hpp"
+#include "DraineHensleyShapeDistribution.hpp"
 #include "GaussBasedResources.hpp"
 #include "InteractionResource.hpp"
 #include "Matrix.hpp"
@@ -137,6 +138,41 @@ void ref_orientation_coefficients(int kind, double param, int order,
     out[i] = od->get_coefficient(i);
   }
   delete od;
+}
+
+// an orientation distribution with a user-defined p(beta), initialised with
+// the tolerances the Python module's custom distribution uses
+// (PyOrientationDistribution.hpp: initialise(1e-4, 1e-4))
+class RefCustomOrientation : public OrientationDistribution {
+public:
+  RefCustomOrientation(int order) : OrientationDistribution(order) {
+    initialise(1.e-4, 1.e-4);
+  }
+  virtual float_type operator()(const float_type beta, const float_type cosbeta,
+                                const float_type sinbeta) const {
+    return 0.5 + 0.3 * cosbeta * cosbeta;
+  }
+};
+
+// p(beta) = 0.5 + 0.3 cos^2(beta)
+void ref_custom_orientation_coefficients(int order, double *out) {
+  RefCustomOrientation od(order);
+  for (int i = 0; i <= order; ++i) {
+    out[i] = od.get_coefficient(i);
+  }
+}
+
+// nodes, weights and limits of DraineHensleyShapeDistribution(npoints,
+// cutoff, fraction)
+void ref_draine_hensley(int npoints, double cutoff, double fraction,
+                        double *shapes, double *weights, double *limits) {
+  DraineHensleyShapeDistribution sd(npoints, cutoff, fraction);
+  for (int i = 0; i < npoints; ++i) {
+    shapes[i] = sd.get_shape(i);
+    weights[i] = sd.get_weight(i);
+  }
+  limits[0] = sd.get_minimum_axis_ratio();
+  limits[1] = sd.get_maximum_axis_ratio();
 }
 
 // ----------------------------------------------------------------- batch ---

@@ -64,6 +64,16 @@ def stages():
     out["plu_a"] = A
     out["plu_inv"] = Ai
     out["rvrs"] = np.array([R.ref_rv_over_rs(d) for d in (0.5, 2.0, 1.0, 3.3)])
+    c = np.zeros(41)
+    R.ref_custom_orientation_coefficients(40, _p(c))
+    out["od_custom"] = c  # p(beta) = 0.5 + 0.3 cos^2 beta
+    for i, (n, cut, frac) in enumerate(((20, 0.15, -1.), (7, 0.3, -1.), (10, 0.15, 0.5))):
+        sh = np.zeros(n)
+        w = np.zeros(n)
+        lim = np.zeros(2)
+        R.ref_draine_hensley(n, cut, frac, _p(sh), _p(w), _p(lim))
+        out["dh_%d" % i] = np.concatenate([sh, w, lim])
+        out["dh_%d_arg" % i] = np.array([n, cut, frac])
     return out
 
 
@@ -125,6 +135,41 @@ def tables():
     out["gt2_theta"] = th2
     out["gt2_sizes"] = sizes
     out["gt2_lams"] = lams
+    # scattering subtraction, Davis-Greenstein alignment, two compositions
+    th3 = np.array([0.1, 1.0, 2.5])
+    res3 = C.get_table(types=np.array([0, 2]), sizes=np.array([0.4e-6]),
+                       wavelengths=np.array([1e-6, 2e-6]), thetas=th3,
+                       shape_distribution=C.SingleShapeShapeDistribution(1.5),
+                       alignment_distribution=C.SizeBasedAlignmentDistribution(
+                           1e-7, C.DAVIS_GREENSTEIN_ALIGNMENT, maximum_order=30),
+                       dust_properties=C.CustomDustProperties(
+                           lambda w, s, t: (1.4 + 0.1 * t) + 0.05j),
+                       number_of_threads=2, maximum_order=30,
+                       number_of_quadrature_angles=6,
+                       account_for_scattering=True)
+    out["gt3"] = res3
+    out["gt3_theta"] = th3
+    # disabled alignment (prolate) and custom alignment (oblate/prolate)
+    th4 = np.array([0.5, 1.5])
+    res4 = C.get_table(types=np.array([0]), sizes=np.array([0.3e-6]),
+                       wavelengths=np.array([1e-6]), thetas=th4,
+                       shape_distribution=C.SingleShapeShapeDistribution(0.7),
+                       alignment_distribution=C.SizeBasedAlignmentDistribution(
+                           1e-7, C.DISABLE_ALIGNMENT, maximum_order=30),
+                       dust_properties=C.CustomDustProperties(lambda w, s, t: 1.6 + 0.2j),
+                       number_of_threads=2, maximum_order=30, do_extinction=True)
+    out["gt4"] = res4
+    out["gt4_theta"] = th4
+    ob = C.MishchenkoOrientationDistribution(0.7, 60)
+    pr = C.DavisGreensteinOrientationDistribution(0.5, 60)
+    res5 = C.get_table(types=np.array([0]), sizes=np.array([0.3e-6]),
+                       wavelengths=np.array([1e-6]), thetas=th4,
+                       shape_distribution=C.SingleShapeShapeDistribution(0.7),
+                       alignment_distribution=C.SizeBasedAlignmentDistribution(
+                           1e-7, C.CUSTOM_ALIGNMENT, 30, ob, pr),
+                       dust_properties=C.CustomDustProperties(lambda w, s, t: 1.6 + 0.2j),
+                       number_of_threads=2, maximum_order=30, do_extinction=True)
+    out["gt5"] = res5
     return out
 
 

@@ -33,7 +33,13 @@ SIGNATURES = {
     "tmx_batch_upload": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D, _D,
                                         _D, ctypes.POINTER(TmxSchedule)]),
     "tmx_batch_compute": (ctypes.c_int, [_VP]),
+    "tmx_tmatrix_batch_fixed": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D,
+                                               _D, _D, _I32, _I32]),
     "tmx_batch_results": (ctypes.c_int, [_VP, _I32, _I32, _I32, _D]),
+    "tmx_batch_observables": (ctypes.c_int, [_VP, ctypes.c_int32, _D, _D,
+                                             ctypes.c_int32, _D]),
+    "tmx_batch_gradients": (ctypes.c_int, [_VP, ctypes.c_int32, _D, _D,
+                                           ctypes.c_int32, _D, _D]),
     "tmx_batch_tmatrix": (ctypes.c_int, [_VP, ctypes.c_int64, _D]),
     "tmx_probe_fp64": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "tmx_kernel_launches": (ctypes.c_int64, [_VP]),

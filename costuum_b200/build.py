@@ -16,6 +16,7 @@ LIB = os.path.join(HERE, "libtmx.so")
 SOURCES = [
     ("tmx_tables.cu", ["--fmad=false"]),
     ("tmx_blocks.cu", []),
+    ("tmx_tangent.cu", []),
     ("tmx_observables.cu", ["--fmad=false"]),
     ("tmx_probe.cu", []),
     ("tmx_host.cu", []),

@@ -52,6 +52,7 @@ struct tmx_ctx {
   int up_nact = 0;
   tmx_schedule up_sched;
   std::vector<int32_t> up_status;
+  std::vector<TmxGrain> up_grains;
   // observables (get_table): cached Clebsch-Gordan table and work buffers
   DevBuf cg, cg_off;
   int cg_nmax = 0;
@@ -74,6 +75,13 @@ struct tmx_ctx {
   std::vector<int32_t> nmax_h, ngauss_h, status_h;
   std::vector<double> q_h;
   std::vector<int64_t> t_off_h;
+  // block schedule of the last batch (phase 2), reused by the tangents
+  std::vector<TmxSlot> p2_slots;
+  std::vector<TmxItem> p2_items;
+  std::vector<int> p2_nb;
+  int64_t p2_scr_total = 0, p2_t_total = 0;
+  DevBuf lu, dT, tscr, dTa, dS; // tangent buffers
+  int o_nsj = 0, o_nqj = 0;     // per-grain observable job counts
 };
 
 #define CK(call)                                                               \

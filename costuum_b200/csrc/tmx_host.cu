@@ -246,7 +246,8 @@ void tmx_destroy(tmx_ctx *ctx) {
     cudaEventDestroy(ctx->t0);
     cudaEventDestroy(ctx->t1);
   }
-  DevBuf *bufs[] = {&ctx->cg, &ctx->cg_off, &ctx->Ta, &ctx->o_angles,
+  DevBuf *bufs[] = {&ctx->lu, &ctx->dT, &ctx->tscr, &ctx->dTa, &ctx->dS,
+                    &ctx->cg, &ctx->cg_off, &ctx->Ta, &ctx->o_angles,
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
                     &ctx->o_og, &ctx->o_work, &ctx->o_sj, &ctx->o_qj, &ctx->o_S,
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
@@ -367,6 +368,7 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   // the host arrays above are about to go out of scope
   CK(cudaStreamSynchronize(st));
   ctx->up_n = n;
+  ctx->up_grains = gr;
   ctx->up_nact = (int)act.size();
   ctx->up_sched = S;
   ctx->up_status.resize(n);
@@ -376,6 +378,212 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   ctx->uploaded = true;
   return TMX_OK;
 }
+
+// Phase 2 of a batch: every (grain, m, class) block at the grain's order in
+// ctx->nmax_h / ctx->ngauss_h (grains listed in p2), then the full Q sums.
+// The block schedule is kept in the context for the tangent kernels.
+static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  const tmx_schedule S = ctx->up_sched;
+  const int glf = S.gauss_legendre_factor;
+  int rc;
+  // ---- 2. all blocks at the converged orders
+  NvtxRange blocks_range("tmx_blocks");
+  const int np2 = (int)p2.size();
+  std::vector<TmxSlot> slots(np2);
+  std::vector<std::pair<int, int>> keys;
+  std::map<std::pair<int, int>, int> key_idx;
+  int64_t tab_total = 0, nsc_total = 0, t_total = 0;
+  for (int s = 0; s < np2; ++s) {
+    const int g = p2[s];
+    const int N = ctx->nmax_h[g], ng = ctx->ngauss_h[g];
+    auto kk = std::make_pair(N, ng);
+    if (!key_idx.count(kk)) {
+      key_idx[kk] = (int)keys.size();
+      keys.push_back(kk);
+    }
+    TmxSlot &sl = slots[s];
+    sl.grain = g;
+    sl.nmax = N;
+    sl.ngauss = ng;
+    sl.tab = tab_total;
+    sl.nsc = nsc_total;
+    sl.tout = t_total;
+    sl.diag = 0;
+    ctx->t_off_h[g] = t_total;
+    tab_total += (int64_t)ng * N * TMX_NQ;
+    nsc_total += (int64_t)ng * TMX_NS;
+    t_total += tmx_tmatrix_size(N);
+  }
+  std::vector<int> full_sets;
+  if ((rc = ensure_wigner(ctx, keys, true, full_sets))) {
+    return rc;
+  }
+  for (int s = 0; s < np2; ++s) {
+    slots[s].wig_n = full_sets[key_idx[std::make_pair(slots[s].nmax, slots[s].ngauss)]];
+  }
+  // items, bucketed by class size (largest first)
+  struct HItem {
+    int nb;
+    TmxItem it;
+  };
+  std::vector<HItem> hitems;
+  for (int s = 0; s < np2; ++s) {
+    const int N = slots[s].nmax;
+    for (int m = 0; m <= N; ++m) {
+      const int ncls = (m == 0) ? 4 : 2;
+      for (int c = 0; c < ncls; ++c) {
+        const int nb = tmx_host_class_size(N, m, c);
+        if (nb <= 0) {
+          continue;
+        }
+        HItem h;
+        h.nb = nb;
+        h.it.slot = s;
+        h.it.m = (int16_t)m;
+        h.it.cls = (int16_t)c;
+        h.it.scratch = 0;
+        hitems.push_back(h);
+      }
+    }
+  }
+  std::stable_sort(hitems.begin(), hitems.end(),
+                   [](const HItem &a, const HItem &b) { return a.nb > b.nb; });
+  ctx->p2_slots = slots;
+  ctx->p2_items.resize(hitems.size());
+  ctx->p2_nb.resize(hitems.size());
+  std::vector<TmxItem> items(hitems.size());
+  int64_t scr_total = 0;
+  for (size_t i = 0; i < hitems.size(); ++i) {
+    items[i] = hitems[i].it;
+    items[i].scratch = scr_total;
+    ctx->p2_items[i] = items[i];
+    ctx->p2_nb[i] = hitems[i].nb;
+    scr_total += 2 * (int64_t)hitems[i].nb * hitems[i].nb;
+  }
+  ctx->p2_scr_total = scr_total;
+  ctx->p2_t_total = t_total;
+  if ((rc = ensure(ctx, ctx->tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->slots, std::max(1, np2) * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->items, std::max<size_t>(1, items.size()) * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
+    return rc;
+  }
+  if (np2 > 0) {
+    CK(cudaMemcpyAsync(ctx->slots.p, slots.data(), np2 * sizeof(TmxSlot),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(TmxItem),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->T.p, 0, t_total * sizeof(cplx), st));
+    cudaEvent_t pe = nullptr;
+    if ((rc = prof_begin(ctx, 1, &pe))) {
+      return rc;
+    }
+    tmx_launch_tables((const TmxSlot *)ctx->slots.p, np2,
+                      (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
+                      (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
+                      (double *)ctx->tab.p, (double *)ctx->nsc.p, S.bessel_start,
+                      st);
+    LAUNCHED();
+    if ((rc = prof_end(ctx, 1, pe, 0.))) {
+      return rc;
+    }
+    // buckets by class size
+    const int edges[] = {128, 64, 32, 16, 0};
+    size_t i0 = 0;
+    for (int b = 0; b < 4; ++b) {
+      size_t i1 = i0;
+      while (i1 < hitems.size() && hitems[i1].nb > edges[b + 1]) {
+        ++i1;
+      }
+      if (i1 > i0) {
+        TmxBlockArgs B;
+        B.items = (const TmxItem *)ctx->items.p + i0;
+        B.nitems = (int)(i1 - i0);
+        B.slots = (const TmxSlot *)ctx->slots.p;
+        B.grains = (const TmxGrain *)ctx->grains.p;
+        B.tab = (const double *)ctx->tab.p;
+        B.nsc = (const double *)ctx->nsc.p;
+        B.wig = (const double *)ctx->wig.p;
+        B.wig_off = (const int64_t *)ctx->wig_off.p;
+        B.scratch = (cplx *)ctx->scratch.p;
+        B.tout = (cplx *)ctx->T.p;
+        B.diag = nullptr;
+        B.status = (int32_t *)ctx->status.p;
+        B.max_nb = hitems[i0].nb;
+        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+        double fl = 0.;
+        for (size_t q = i0; q < i1; ++q) {
+          fl += item_flops(hitems[q].nb, hitems[q].it.m,
+                           slots[hitems[q].it.slot].ngauss);
+        }
+        if ((rc = prof_begin(ctx, 0, &pe))) {
+          return rc;
+        }
+        tmx_launch_blocks(B, st);
+        LAUNCHED();
+        if ((rc = prof_end(ctx, 0, pe, fl))) {
+          return rc;
+        }
+      }
+      i0 = i1;
+    }
+    // ---- 3. full Q sums
+    std::vector<int32_t> nmv(n);
+    for (int64_t i = 0; i < n; ++i) {
+      nmv[i] = ctx->nmax_h[i];
+    }
+    CK(cudaMemcpyAsync(ctx->t_off.p, ctx->t_off_h.data(), n * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->nmaxv.p, nmv.data(), n * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    tmx_launch_qsums((const int64_t *)ctx->t_off.p, (const int32_t *)ctx->nmaxv.p,
+                     (int)n, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
+    LAUNCHED();
+    std::vector<double> q2(2 * n);
+    std::vector<int32_t> stb(n);
+    CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < n; ++i) {
+      if (ctx->nmax_h[i] > 0) {
+        ctx->q_h[6 * i + 2] = q2[2 * i];
+        ctx->q_h[6 * i + 3] = q2[2 * i + 1];
+      }
+      ctx->status_h[i] |= stb[i];
+    }
+  }
+  // survey-model flops (per grain: every order of the m = 0 chain on the
+  // unreduced 2k x 2k block, then every m >= 1 block on 2nm x 2nm)
+  for (int64_t i = 0; i < n; ++i) {
+    const int N = ctx->nmax_h[i];
+    if (N <= 0) {
+      continue;
+    }
+    for (int k = S.min_order; k <= N; ++k) {
+      const double b = k, g = glf * k, t = 2. * k;
+      ctx->flops_survey += 8. * 4. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+    }
+    for (int m = 1; m <= N; ++m) {
+      const double b = N + 1 - m, g = ctx->ngauss_h[i], t = 2. * b;
+      ctx->flops_survey += 8. * 10. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+    }
+  }
+  if ((rc = prof_resolve(ctx))) {
+    return rc;
+  }
+  ctx->have_batch = true;
+  return TMX_OK;
+}
+
 
 int tmx_batch_compute(tmx_ctx *ctx) {
   if (!ctx) {
@@ -531,193 +739,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
   }
 
-  // ---- 2. all blocks at the converged orders
-  NvtxRange blocks_range("tmx_blocks");
-  const int np2 = (int)p2.size();
-  std::vector<TmxSlot> slots(np2);
-  std::vector<std::pair<int, int>> keys;
-  std::map<std::pair<int, int>, int> key_idx;
-  int64_t tab_total = 0, nsc_total = 0, t_total = 0;
-  for (int s = 0; s < np2; ++s) {
-    const int g = p2[s];
-    const int N = ctx->nmax_h[g], ng = ctx->ngauss_h[g];
-    auto kk = std::make_pair(N, ng);
-    if (!key_idx.count(kk)) {
-      key_idx[kk] = (int)keys.size();
-      keys.push_back(kk);
-    }
-    TmxSlot &sl = slots[s];
-    sl.grain = g;
-    sl.nmax = N;
-    sl.ngauss = ng;
-    sl.tab = tab_total;
-    sl.nsc = nsc_total;
-    sl.tout = t_total;
-    sl.diag = 0;
-    ctx->t_off_h[g] = t_total;
-    tab_total += (int64_t)ng * N * TMX_NQ;
-    nsc_total += (int64_t)ng * TMX_NS;
-    t_total += tmx_tmatrix_size(N);
-  }
-  std::vector<int> full_sets;
-  if ((rc = ensure_wigner(ctx, keys, true, full_sets))) {
-    return rc;
-  }
-  for (int s = 0; s < np2; ++s) {
-    slots[s].wig_n = full_sets[key_idx[std::make_pair(slots[s].nmax, slots[s].ngauss)]];
-  }
-  // items, bucketed by class size (largest first)
-  struct HItem {
-    int nb;
-    TmxItem it;
-  };
-  std::vector<HItem> hitems;
-  for (int s = 0; s < np2; ++s) {
-    const int N = slots[s].nmax;
-    for (int m = 0; m <= N; ++m) {
-      const int ncls = (m == 0) ? 4 : 2;
-      for (int c = 0; c < ncls; ++c) {
-        const int nb = tmx_host_class_size(N, m, c);
-        if (nb <= 0) {
-          continue;
-        }
-        HItem h;
-        h.nb = nb;
-        h.it.slot = s;
-        h.it.m = (int16_t)m;
-        h.it.cls = (int16_t)c;
-        h.it.scratch = 0;
-        hitems.push_back(h);
-      }
-    }
-  }
-  std::stable_sort(hitems.begin(), hitems.end(),
-                   [](const HItem &a, const HItem &b) { return a.nb > b.nb; });
-  std::vector<TmxItem> items(hitems.size());
-  int64_t scr_total = 0;
-  for (size_t i = 0; i < hitems.size(); ++i) {
-    items[i] = hitems[i].it;
-    items[i].scratch = scr_total;
-    scr_total += 2 * (int64_t)hitems[i].nb * hitems[i].nb;
-  }
-  if ((rc = ensure(ctx, ctx->tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->slots, std::max(1, np2) * sizeof(TmxSlot))) ||
-      (rc = ensure(ctx, ctx->items, std::max<size_t>(1, items.size()) * sizeof(TmxItem))) ||
-      (rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
-      (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
-      (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
-    return rc;
-  }
-  if (np2 > 0) {
-    CK(cudaMemcpyAsync(ctx->slots.p, slots.data(), np2 * sizeof(TmxSlot),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(TmxItem),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(ctx->T.p, 0, t_total * sizeof(cplx), st));
-    cudaEvent_t pe = nullptr;
-    if ((rc = prof_begin(ctx, 1, &pe))) {
-      return rc;
-    }
-    tmx_launch_tables((const TmxSlot *)ctx->slots.p, np2,
-                      (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
-                      (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
-                      (double *)ctx->tab.p, (double *)ctx->nsc.p, S.bessel_start,
-                      st);
-    LAUNCHED();
-    if ((rc = prof_end(ctx, 1, pe, 0.))) {
-      return rc;
-    }
-    // buckets by class size
-    const int edges[] = {128, 64, 32, 16, 0};
-    size_t i0 = 0;
-    for (int b = 0; b < 4; ++b) {
-      size_t i1 = i0;
-      while (i1 < hitems.size() && hitems[i1].nb > edges[b + 1]) {
-        ++i1;
-      }
-      if (i1 > i0) {
-        TmxBlockArgs B;
-        B.items = (const TmxItem *)ctx->items.p + i0;
-        B.nitems = (int)(i1 - i0);
-        B.slots = (const TmxSlot *)ctx->slots.p;
-        B.grains = (const TmxGrain *)ctx->grains.p;
-        B.tab = (const double *)ctx->tab.p;
-        B.nsc = (const double *)ctx->nsc.p;
-        B.wig = (const double *)ctx->wig.p;
-        B.wig_off = (const int64_t *)ctx->wig_off.p;
-        B.scratch = (cplx *)ctx->scratch.p;
-        B.tout = (cplx *)ctx->T.p;
-        B.diag = nullptr;
-        B.status = (int32_t *)ctx->status.p;
-        B.max_nb = hitems[i0].nb;
-        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
-        double fl = 0.;
-        for (size_t q = i0; q < i1; ++q) {
-          fl += item_flops(hitems[q].nb, hitems[q].it.m,
-                           slots[hitems[q].it.slot].ngauss);
-        }
-        if ((rc = prof_begin(ctx, 0, &pe))) {
-          return rc;
-        }
-        tmx_launch_blocks(B, st);
-        LAUNCHED();
-        if ((rc = prof_end(ctx, 0, pe, fl))) {
-          return rc;
-        }
-      }
-      i0 = i1;
-    }
-    // ---- 3. full Q sums
-    std::vector<int32_t> nmv(n);
-    for (int64_t i = 0; i < n; ++i) {
-      nmv[i] = ctx->nmax_h[i];
-    }
-    CK(cudaMemcpyAsync(ctx->t_off.p, ctx->t_off_h.data(), n * sizeof(int64_t),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->nmaxv.p, nmv.data(), n * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, st));
-    tmx_launch_qsums((const int64_t *)ctx->t_off.p, (const int32_t *)ctx->nmaxv.p,
-                     (int)n, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
-    LAUNCHED();
-    std::vector<double> q2(2 * n);
-    std::vector<int32_t> stb(n);
-    CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    for (int64_t i = 0; i < n; ++i) {
-      if (ctx->nmax_h[i] > 0) {
-        ctx->q_h[6 * i + 2] = q2[2 * i];
-        ctx->q_h[6 * i + 3] = q2[2 * i + 1];
-      }
-      ctx->status_h[i] |= stb[i];
-    }
-  }
-  // survey-model flops (per grain: every order of the m = 0 chain on the
-  // unreduced 2k x 2k block, then every m >= 1 block on 2nm x 2nm)
-  for (int64_t i = 0; i < n; ++i) {
-    const int N = ctx->nmax_h[i];
-    if (N <= 0) {
-      continue;
-    }
-    for (int k = S.min_order; k <= N; ++k) {
-      const double b = k, g = glf * k, t = 2. * k;
-      ctx->flops_survey += 8. * 4. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
-    }
-    for (int m = 1; m <= N; ++m) {
-      const double b = N + 1 - m, g = ctx->ngauss_h[i], t = 2. * b;
-      ctx->flops_survey += 8. * 10. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
-    }
-  }
-  if ((rc = prof_resolve(ctx))) {
-    return rc;
-  }
-  ctx->have_batch = true;
-  return TMX_OK;
+  return run_blocks(ctx, p2);
 }
 
 int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,
@@ -729,6 +751,59 @@ int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,
     return rc;
   }
   return tmx_batch_compute(ctx);
+}
+
+int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                            const double *wavelength, const double *mr,
+                            const double *mi, const double *axis_ratio,
+                            const int32_t *nmax, const int32_t *ngauss) {
+  if (!ctx) {
+    return TMX_ERR_INVALID;
+  }
+  if (n > 0 && (!nmax || !ngauss)) {
+    return fail(ctx, TMX_ERR_INVALID, "null nmax/ngauss");
+  }
+  int32_t top = 2;
+  for (int64_t i = 0; i < n; ++i) {
+    if (nmax[i] < 1 || nmax[i] > TMX_MAX_NB || ngauss[i] < 1) {
+      return fail(ctx, TMX_ERR_INVALID, "nmax must be in [1, 128], ngauss >= 1");
+    }
+    top = std::max(top, nmax[i]);
+  }
+  tmx_schedule S = {2, std::max(top + 1, 3), 1, 0, 1.e-4};
+  int rc = tmx_batch_upload(ctx, n, r_ev, wavelength, mr, mi, axis_ratio, &S);
+  if (rc) {
+    return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  ctx->have_batch = false;
+  ctx->n = n;
+  ctx->nmax_h.assign(n, 0);
+  ctx->ngauss_h.assign(n, 0);
+  ctx->status_h.assign(n, 0);
+  ctx->q_h.assign(6 * n, 0.);
+  ctx->t_off_h.assign(n, 0);
+  ctx->flops_survey = 0.;
+  std::vector<int32_t> p2;
+  std::vector<int> ngs;
+  for (int64_t i = 0; i < n; ++i) {
+    ctx->status_h[i] = ctx->up_status[i];
+    if (ctx->up_status[i] == 0) {
+      ctx->nmax_h[i] = nmax[i];
+      ctx->ngauss_h[i] = ngauss[i];
+      p2.push_back((int32_t)i);
+      ngs.push_back(ngauss[i]);
+    }
+  }
+  if ((rc = ensure_gl(ctx, ngs))) {
+    return rc;
+  }
+  CK(cudaMemsetAsync(ctx->status.p, 0, n * sizeof(int32_t), ctx->stream));
+  if (n == 0) {
+    ctx->have_batch = true;
+    return TMX_OK;
+  }
+  return run_blocks(ctx, p2);
 }
 
 int tmx_batch_results(tmx_ctx *ctx, int32_t *nmax, int32_t *ngauss,

@@ -27,6 +27,11 @@ enum {
   TMX_NS_COS,
   TMX_NS_SININV,
   TMX_NS_SIN2INV,
+  TMX_NS_KR,        // k r R_V
+  TMX_NS_KRMR_RE,   // m k r R_V
+  TMX_NS_KRMR_IM,
+  TMX_NS_DLNR2_DD,  // d ln(r^2) / d(axis ratio)
+  TMX_NS_DDRR_DD,   // d (r'/r) / d(axis ratio)
   TMX_NS_PAD,
   TMX_NS
 };

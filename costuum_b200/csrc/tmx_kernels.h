@@ -52,6 +52,8 @@ struct TmxBlockArgs {
   int32_t *status;             // per grain status bits
   int chunk_nodes;             // quadrature nodes per shared-memory chunk
   int max_nb;                  // largest class size in this launch
+  double2 *lu = nullptr;       // if set: LU factors + pivots saved per item
+                               // at the item's scratch offset (2 nb^2)
 };
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes);
 void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream);
@@ -137,5 +139,36 @@ void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og
                            cudaStream_t stream);
 void tmx_launch_z_epilogue(int n, const double2 *S, double *zout,
                            cudaStream_t stream);
+void tmx_launch_dq_epilogue(const TmxQJob *jobs, int njobs,
+                            const TmxObsGrain *og, const double2 *S,
+                            const double2 *dSm, const double2 *dSr,
+                            const double2 *dSd, double *dq, cudaStream_t stream);
 void tmx_launch_shape_avg(int ncells, int nshape, int nper, const double *in,
                           const double *w, double *out, cudaStream_t stream);
+
+// ---------------------------------------------------------------- tangents --
+
+// d/dp of every class block for p = refractive index (complex derivative),
+// equal-volume radius, axis ratio: dT = -(dRgQ + T dQ) Q^-1 with the LU
+// factors saved by the forward block kernel.
+struct TmxTangentArgs {
+  const TmxItem *items;
+  int nitems;
+  int nparams;                 // parameters per item (param = blockIdx.y)
+  const TmxSlot *slots;
+  const TmxGrain *grains;
+  const double *tab;
+  const double *nsc;
+  const double *wig;
+  const int64_t *wig_off;
+  const double2 *lu;           // saved LU factors / pivots (forward)
+  const double2 *T;            // forward T-matrices
+  double2 *scratch;            // per (item, param): dQ, dRgQ (2 nb^2)
+  int64_t scratch_stride;      // complex elements per parameter
+  double2 *dT;                 // tangent T-matrices, one set per parameter
+  int64_t dT_stride;           // complex elements per parameter set
+  int chunk_nodes;
+  int max_nb;
+};
+size_t tmx_tangent_smem_bytes(int max_nb, int chunk_nodes);
+void tmx_launch_tangents(const TmxTangentArgs &a, cudaStream_t stream);

@@ -443,6 +443,50 @@ __global__ void k_q_epilogue(const TmxQJob *__restrict__ jobs, int njobs,
   }
 }
 
+// One thread per (grain, theta): derivatives of (Qext, Qextpol, Qextcpol)
+// with respect to (Re m, Im m, R_V, d) from the tangent amplitudes. S is
+// linear in T, and T is holomorphic in m, so dS/d(Im m) = i dS/d(Re m); the
+// normalisation 1/(pi R_V^2) adds -2 Q / R_V to the R_V derivative.
+// dq[(job.out * 3 + k) * 4 + p]
+__global__ void k_dq_epilogue(const TmxQJob *__restrict__ jobs, int njobs,
+                              const TmxObsGrain *__restrict__ og,
+                              const cplx *__restrict__ S,
+                              const cplx *__restrict__ dSm,
+                              const cplx *__restrict__ dSr,
+                              const cplx *__restrict__ dSd,
+                              double *__restrict__ dq) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= njobs) {
+    return;
+  }
+  const TmxQJob J = jobs[u];
+  const TmxObsGrain G = og[J.grain];
+  const double f = (2. * M_PI / G.k) / (M_PI * G.r_ev * G.r_ev);
+  const cplx *s = S + J.s_main * 4;
+  const double q[3] = {f * (s[0].y + s[3].y), f * (s[0].y - s[3].y),
+                       f * (s[3].x - s[0].x)};
+  const cplx *dm = dSm + J.s_main * 4;
+  const cplx *dr = dSr + J.s_main * 4;
+  const cplx *dd = dSd + J.s_main * 4;
+  double *o = dq + J.out * 12;
+  // Re m
+  o[0 * 4 + 0] = f * (dm[0].y + dm[3].y);
+  o[1 * 4 + 0] = f * (dm[0].y - dm[3].y);
+  o[2 * 4 + 0] = f * (dm[3].x - dm[0].x);
+  // Im m: Im(i z) = Re z, Re(i z) = -Im z
+  o[0 * 4 + 1] = f * (dm[0].x + dm[3].x);
+  o[1 * 4 + 1] = f * (dm[0].x - dm[3].x);
+  o[2 * 4 + 1] = -f * (dm[3].y - dm[0].y);
+  // R_V
+  o[0 * 4 + 2] = f * (dr[0].y + dr[3].y) - 2. * q[0] / G.r_ev;
+  o[1 * 4 + 2] = f * (dr[0].y - dr[3].y) - 2. * q[1] / G.r_ev;
+  o[2 * 4 + 2] = f * (dr[3].x - dr[0].x) - 2. * q[2] / G.r_ev;
+  // axis ratio
+  o[0 * 4 + 3] = f * (dd[0].y + dd[3].y);
+  o[1 * 4 + 3] = f * (dd[0].y - dd[3].y);
+  o[2 * 4 + 3] = f * (dd[3].x - dd[0].x);
+}
+
 // one thread per (grain, theta_out, phi_out): the 4x4 matrix of
 // ScatteringMatrixTask::execute from S, row major
 __global__ void k_z_epilogue(int n, const cplx *__restrict__ S,
@@ -533,6 +577,17 @@ void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og
   }
   k_q_epilogue<<<(njobs + 127) / 128, 128, 0, stream>>>(
       jobs, njobs, og, S, wts, nacc, qout, qstride, do_abs, do_ext);
+}
+
+void tmx_launch_dq_epilogue(const TmxQJob *jobs, int njobs,
+                            const TmxObsGrain *og, const double2 *S,
+                            const double2 *dSm, const double2 *dSr,
+                            const double2 *dSd, double *dq, cudaStream_t stream) {
+  if (njobs <= 0) {
+    return;
+  }
+  k_dq_epilogue<<<(njobs + 127) / 128, 128, 0, stream>>>(jobs, njobs, og, S,
+                                                         dSm, dSr, dSd, dq);
 }
 
 void tmx_launch_z_epilogue(int n, const double2 *S, double *zout,

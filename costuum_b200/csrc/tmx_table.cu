@@ -693,3 +693,275 @@ int tmx_ensure_cg(tmx_ctx *ctx, int nmax) {
   ctx->cg_nmax = nmax;
   return TMX_OK;
 }
+
+// ------------------------------------------- per-grain observables / grads --
+
+namespace {
+
+// orientation-averaged theta -> theta amplitudes of every grain of the last
+// batch for the T-matrices at `Tsrc`; S[(grain * ntheta + t) * 4]
+int batch_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int ntheta,
+                     bool average, int ncoef, cplx *S_out) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  int rc;
+  int nmax_b = 1;
+  for (int64_t g = 0; g < n; ++g) {
+    nmax_b = std::max(nmax_b, ctx->nmax_h[g]);
+  }
+  const int64_t t_total = ctx->p2_t_total;
+  if (t_total <= 0) {
+    return TMX_OK;
+  }
+  const int oa_blocks = (int)std::min<int64_t>(n, 4 * 148);
+  const int wstride = 2 * (2 * nmax_b + 1);
+  if ((rc = ensure(ctx, ctx->Ta, t_total * sizeof(cplx)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->Ta.p, Tsrc, t_total * sizeof(cplx),
+                     cudaMemcpyDeviceToDevice, st));
+  if (average) {
+    if ((rc = tmx_ensure_cg(ctx, nmax_b)) ||
+        (rc = ensure(ctx, ctx->o_work, (size_t)oa_blocks * 128 * wstride * sizeof(cplx)))) {
+      return rc;
+    }
+    tmx_launch_orient_avg((const TmxObsGrain *)ctx->o_og.p, (int)n, Tsrc,
+                          (cplx *)ctx->Ta.p, (const double *)ctx->o_coef.p, ncoef,
+                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
+                          ctx->cg_nmax, (cplx *)ctx->o_work.p, wstride, oa_blocks,
+                          128, st);
+    LAUNCHED();
+  }
+  CK(cudaMemsetAsync(S_out, 0, n * ntheta * 4 * sizeof(cplx), st));
+  tmx_launch_forward_s((const TmxSJob *)ctx->o_sj.p, ctx->o_nsj,
+                       (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->Ta.p,
+                       (const TmxAngle *)ctx->o_angles.p, (const cplx *)ctx->o_phis.p,
+                       S_out, st);
+  LAUNCHED();
+  return TMX_OK;
+}
+
+// descriptors shared by the per-grain observable and gradient passes
+int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
+                           const double *coeffs, int ncoef) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  int rc;
+  std::vector<TmxAngle> ang(ntheta);
+  for (int i = 0; i < ntheta; ++i) {
+    ang[i] = make_angle(cos(thetas[i]));
+  }
+  std::vector<cplx> phis(1, mkc(1., 0.));
+  std::vector<TmxObsGrain> og(n);
+  std::vector<TmxSJob> sj;
+  std::vector<TmxQJob> qj;
+  for (int64_t g = 0; g < n; ++g) {
+    og[g].nmax = ctx->nmax_h[g];
+    og[g].coef_set = coeffs ? 0 : -1;
+    og[g].t_off = ctx->t_off_h[g];
+    og[g].k = ctx->up_grains[g].k;
+    og[g].r_ev = ctx->up_grains[g].r_ev;
+    if (coeffs && 2 * og[g].nmax + 1 > ncoef) {
+      return fail(ctx, TMX_ERR_INVALID,
+                  "orientation coefficients shorter than 2 nmax + 1");
+    }
+    if (og[g].nmax <= 0) {
+      continue;
+    }
+    for (int t = 0; t < ntheta; ++t) {
+      TmxSJob j;
+      j.grain = (int32_t)g;
+      j.angle_in = t;
+      j.angle_out = t;
+      j.nphi = 1;
+      j.phi0 = 0;
+      j.out = g * ntheta + t;
+      sj.push_back(j);
+      TmxQJob q;
+      q.grain = (int32_t)g;
+      q.pad = 0;
+      q.out = g * ntheta + t;
+      q.s_main = g * ntheta + t;
+      q.s_acc = 0;
+      qj.push_back(q);
+    }
+  }
+  if ((rc = ensure(ctx, ctx->o_angles, std::max(1, ntheta) * sizeof(TmxAngle))) ||
+      (rc = ensure(ctx, ctx->o_phis, sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->o_og, std::max<int64_t>(1, n) * sizeof(TmxObsGrain))) ||
+      (rc = ensure(ctx, ctx->o_sj, std::max<size_t>(1, sj.size()) * sizeof(TmxSJob))) ||
+      (rc = ensure(ctx, ctx->o_qj, std::max<size_t>(1, qj.size()) * sizeof(TmxQJob))) ||
+      (rc = ensure(ctx, ctx->o_coef, std::max(1, ncoef) * sizeof(double)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ntheta * sizeof(TmxAngle),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->o_phis.p, phis.data(), sizeof(cplx),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
+                     cudaMemcpyHostToDevice, st));
+  if (!sj.empty()) {
+    CK(cudaMemcpyAsync(ctx->o_sj.p, sj.data(), sj.size() * sizeof(TmxSJob),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->o_qj.p, qj.data(), qj.size() * sizeof(TmxQJob),
+                       cudaMemcpyHostToDevice, st));
+  }
+  if (coeffs) {
+    CK(cudaMemcpyAsync(ctx->o_coef.p, coeffs, ncoef * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
+  }
+  ctx->o_nsj = (int)sj.size();
+  ctx->o_nqj = (int)qj.size();
+  CK(cudaStreamSynchronize(st));
+  return TMX_OK;
+}
+
+} // namespace
+
+extern "C" int tmx_batch_observables(tmx_ctx *ctx, int32_t ntheta,
+                                     const double *thetas, const double *coeffs,
+                                     int32_t ncoef, double *q) {
+  if (!ctx || ntheta < 1 || !thetas || !q) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  int rc;
+  if ((rc = batch_observable_setup(ctx, ntheta, thetas, coeffs, ncoef)) ||
+      (rc = ensure(ctx, ctx->o_S, std::max<int64_t>(1, n * ntheta) * 4 * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double)))) {
+    return rc;
+  }
+  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, coeffs != nullptr,
+                             ncoef, (cplx *)ctx->o_S.p))) {
+    return rc;
+  }
+  CK(cudaMemsetAsync(ctx->o_gq.p, 0, n * ntheta * 3 * sizeof(double), st));
+  tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
+                        (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->o_S.p,
+                        nullptr, 0, (double *)ctx->o_gq.p, 3, 0, 1, st);
+  LAUNCHED();
+  CK(cudaMemcpyAsync(q, ctx->o_gq.p, n * ntheta * 3 * sizeof(double),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return TMX_OK;
+}
+
+extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
+                                   const double *thetas, const double *coeffs,
+                                   int32_t ncoef, double *q, double *dq) {
+  if (!ctx || ntheta < 1 || !thetas || !dq) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  const int64_t nitems = (int64_t)ctx->p2_items.size();
+  const int64_t scr = ctx->p2_scr_total;
+  const int64_t tt = ctx->p2_t_total;
+  int rc;
+  NvtxRange range("tmx_gradients");
+  if ((rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, scr) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->tscr, std::max<int64_t>(1, 3 * scr) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->dT, std::max<int64_t>(1, 3 * tt) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->dS, std::max<int64_t>(1, 4 * n * ntheta) * 4 * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->o_gz, std::max<int64_t>(1, n * ntheta * 12) * sizeof(double)))) {
+    return rc;
+  }
+  if (nitems > 0) {
+    CK(cudaMemsetAsync(ctx->dT.p, 0, 3 * tt * sizeof(cplx), st));
+    // forward blocks again, now keeping the LU factors, then the tangents;
+    // both in the class-size buckets of the forward schedule
+    const int edges[] = {128, 64, 32, 16, 0};
+    int64_t i0 = 0;
+    for (int b = 0; b < 4; ++b) {
+      int64_t i1 = i0;
+      while (i1 < nitems && ctx->p2_nb[i1] > edges[b + 1]) {
+        ++i1;
+      }
+      if (i1 > i0) {
+        const int max_nb = ctx->p2_nb[i0];
+        TmxBlockArgs B;
+        B.items = (const TmxItem *)ctx->items.p + i0;
+        B.nitems = (int)(i1 - i0);
+        B.slots = (const TmxSlot *)ctx->slots.p;
+        B.grains = (const TmxGrain *)ctx->grains.p;
+        B.tab = (const double *)ctx->tab.p;
+        B.nsc = (const double *)ctx->nsc.p;
+        B.wig = (const double *)ctx->wig.p;
+        B.wig_off = (const int64_t *)ctx->wig_off.p;
+        B.scratch = (cplx *)ctx->scratch.p;
+        B.tout = (cplx *)ctx->T.p;
+        B.diag = nullptr;
+        B.status = (int32_t *)ctx->status.p;
+        B.max_nb = max_nb;
+        B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
+        B.lu = (cplx *)ctx->lu.p;
+        tmx_launch_blocks(B, st);
+        LAUNCHED();
+        TmxTangentArgs A;
+        A.items = B.items;
+        A.nitems = B.nitems;
+        A.nparams = 3;
+        A.slots = B.slots;
+        A.grains = B.grains;
+        A.tab = B.tab;
+        A.nsc = B.nsc;
+        A.wig = B.wig;
+        A.wig_off = B.wig_off;
+        A.lu = (const cplx *)ctx->lu.p;
+        A.T = (const cplx *)ctx->T.p;
+        A.scratch = (cplx *)ctx->tscr.p;
+        A.scratch_stride = scr;
+        A.dT = (cplx *)ctx->dT.p;
+        A.dT_stride = tt;
+        A.chunk_nodes = std::max(1, tmx_host_chunk_nodes(max_nb) / 2);
+        A.max_nb = max_nb;
+        tmx_launch_tangents(A, st);
+        LAUNCHED();
+      }
+      i0 = i1;
+    }
+  }
+  if ((rc = batch_observable_setup(ctx, ntheta, thetas, coeffs, ncoef))) {
+    return rc;
+  }
+  cplx *S = (cplx *)ctx->dS.p;
+  const int64_t sz = n * ntheta * 4;
+  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, coeffs != nullptr,
+                             ncoef, S))) {
+    return rc;
+  }
+  for (int p = 0; p < 3; ++p) {
+    if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->dT.p + p * tt, ntheta,
+                               coeffs != nullptr, ncoef, S + (1 + p) * sz))) {
+      return rc;
+    }
+  }
+  CK(cudaMemsetAsync(ctx->o_gq.p, 0, n * ntheta * 3 * sizeof(double), st));
+  CK(cudaMemsetAsync(ctx->o_gz.p, 0, n * ntheta * 12 * sizeof(double), st));
+  tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
+                        (const TmxObsGrain *)ctx->o_og.p, S, nullptr, 0,
+                        (double *)ctx->o_gq.p, 3, 0, 1, st);
+  LAUNCHED();
+  tmx_launch_dq_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
+                         (const TmxObsGrain *)ctx->o_og.p, S, S + sz, S + 2 * sz,
+                         S + 3 * sz, (double *)ctx->o_gz.p, st);
+  LAUNCHED();
+  if (q) {
+    CK(cudaMemcpyAsync(q, ctx->o_gq.p, n * ntheta * 3 * sizeof(double),
+                       cudaMemcpyDeviceToHost, st));
+  }
+  CK(cudaMemcpyAsync(dq, ctx->o_gz.p, n * ntheta * 12 * sizeof(double),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return TMX_OK;
+}

@@ -179,6 +179,17 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       S[TMX_NS_COS] = c;
       S[TMX_NS_SININV] = sqrt(sin2inv);
       S[TMX_NS_SIN2INV] = sin2inv;
+      S[TMX_NS_KR] = kr;
+      S[TMX_NS_KRMR_RE] = krmr.x;
+      S[TMX_NS_KRMR_IM] = krmr.y;
+      // r^2 = d^{2/3} / (sin^2 + d^2 cos^2) (unit equal-volume radius):
+      // d ln r^2 / dd = 2 / (3 d) - 2 d cos^2 / (sin^2 + d^2 cos^2);
+      // r'/r = r2oa2 cos sin (d^2 - 1):
+      // d(r'/r)/dd = 2 d cos sin r2oa2 (1 - cos^2 r2oa2 (d^2 - 1))
+      const double dd = G.axis_ratio;
+      S[TMX_NS_DLNR2_DD] = 2. / (3. * dd) - 2. * dd * (c * c) * r2oa2;
+      S[TMX_NS_DDRR_DD] =
+          2. * dd * c * sn * r2oa2 * (1. - (c * c) * r2oa2 * d2m1);
       S[TMX_NS_PAD] = 0.;
       bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
                     TMX_NQ);

@@ -125,14 +125,77 @@ class Context:
                                        _lib.ptr(mr), _lib.ptr(mi), _lib.ptr(d),
                                        ctypes.byref(sched))
             _lib.check(self._h, rc, "tmx_tmatrix_batch")
-            nmax = np.zeros(n, np.int32)
-            ngauss = np.zeros(n, np.int32)
-            status = np.zeros(n, np.int32)
-            q = np.zeros((n, 6))
-            rc = lib.tmx_batch_results(self._h, _lib.iptr(nmax), _lib.iptr(ngauss),
-                                       _lib.iptr(status), _lib.ptr(q))
-            _lib.check(self._h, rc, "tmx_batch_results")
+            return self._results(n)
+
+
+    def tmatrix_batch_fixed(self, r_ev, wavelength, m, axis_ratio, nmax, ngauss):
+        """All m blocks of each grain at a given (nmax, ngauss), without the
+        convergence loop."""
+        r_ev = np.ascontiguousarray(r_ev, np.float64).ravel()
+        n = r_ev.size
+        wl = np.ascontiguousarray(np.broadcast_to(wavelength, (n,)), np.float64)
+        mm = np.broadcast_to(np.asarray(m, np.complex128), (n,))
+        mr = np.ascontiguousarray(mm.real)
+        mi = np.ascontiguousarray(mm.imag)
+        d = np.ascontiguousarray(np.broadcast_to(axis_ratio, (n,)), np.float64)
+        nm = np.ascontiguousarray(np.broadcast_to(nmax, (n,)), np.int32)
+        ng = np.ascontiguousarray(np.broadcast_to(ngauss, (n,)), np.int32)
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_tmatrix_batch_fixed(self._h, n, _lib.ptr(r_ev), _lib.ptr(wl),
+                                             _lib.ptr(mr), _lib.ptr(mi), _lib.ptr(d),
+                                             _lib.iptr(nm), _lib.iptr(ng))
+            _lib.check(self._h, rc, "tmx_tmatrix_batch_fixed")
+            return self._results(n)
+
+    def _results(self, n):
+        self._n = n
+        lib = _lib.load()
+        nmax = np.zeros(n, np.int32)
+        ngauss = np.zeros(n, np.int32)
+        status = np.zeros(n, np.int32)
+        q = np.zeros((n, 6))
+        rc = lib.tmx_batch_results(self._h, _lib.iptr(nmax), _lib.iptr(ngauss),
+                                   _lib.iptr(status), _lib.ptr(q))
+        _lib.check(self._h, rc, "tmx_batch_results")
         return BatchResult(self, n, nmax, ngauss, status, q)
+
+    def observables(self, thetas, coefficients=None):
+        """(n, ntheta, 3) array of (Qext, Qextpol, Qextcpol) of the last batch,
+        orientation-averaged with the given expansion coefficients."""
+        th = np.ascontiguousarray(np.atleast_1d(thetas), np.float64)
+        c = None if coefficients is None else np.ascontiguousarray(coefficients, np.float64)
+        lib = _lib.load()
+        n = self._last_n()
+        q = np.zeros((n, len(th), 3))
+        with self._lock:
+            rc = lib.tmx_batch_observables(self._h, len(th), _lib.ptr(th),
+                                           None if c is None else _lib.ptr(c),
+                                           0 if c is None else len(c), _lib.ptr(q))
+            _lib.check(self._h, rc, "tmx_batch_observables")
+        return q
+
+    def gradients(self, thetas, coefficients=None):
+        """(q, dq): q as observables(); dq (n, ntheta, 3, 4) derivatives with
+        respect to (Re m, Im m, r_ev, axis ratio) at the batch's orders."""
+        th = np.ascontiguousarray(np.atleast_1d(thetas), np.float64)
+        c = None if coefficients is None else np.ascontiguousarray(coefficients, np.float64)
+        lib = _lib.load()
+        n = self._last_n()
+        q = np.zeros((n, len(th), 3))
+        dq = np.zeros((n, len(th), 3, 4))
+        with self._lock:
+            rc = lib.tmx_batch_gradients(self._h, len(th), _lib.ptr(th),
+                                         None if c is None else _lib.ptr(c),
+                                         0 if c is None else len(c), _lib.ptr(q),
+                                         _lib.ptr(dq))
+            _lib.check(self._h, rc, "tmx_batch_gradients")
+        return q, dq
+
+    def _last_n(self):
+        if getattr(self, "_n", None) is None:
+            raise _lib.TmxError("no batch has been computed")
+        return self._n
 
 
 _default = None

@@ -98,6 +98,16 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
                      const tmx_schedule *schedule);
 int tmx_batch_compute(tmx_ctx *ctx);
 
+/* The block computation of a batch at given orders, without the convergence
+ * loop: grain i gets all m blocks at (nmax[i], ngauss[i]) (the state of a
+ * TMatrixMAllTask run after ConvergedSizeResources fixed the order,
+ * src/TMatrixResource.hpp:893-1120, plus its m = 0 block). For finite
+ * differences and gradients at a fixed order. */
+int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                            const double *wavelength, const double *mr,
+                            const double *mi, const double *axis_ratio,
+                            const int32_t *nmax, const int32_t *ngauss);
+
 /* Per-grain results of the last batch (any pointer may be NULL):
  * nmax, ngauss, status bits, and q[6 * i + {0..5}] =
  * {m=0 Qsca, m=0 Qext of the converged order, full Qsca, full Qext
@@ -188,6 +198,26 @@ int tmx_get_table(tmx_ctx *ctx, int32_t ntypes, int32_t nsizes,
                   int32_t nsets, const double *coeffs, int32_t ncoef,
                   int32_t flags, int32_t ngauss, const tmx_schedule *schedule,
                   double *out_q, double *out_z, int32_t *grain_status);
+
+/* Orientation-averaged extinction coefficients of every grain of the last
+ * batch at the zenith angles thetas (ExtinctionCoefficientTask::execute,
+ * src/ExtinctionCoefficientTask.hpp:626-653, on the AlignmentAverageTask
+ * output): q[(grain * ntheta + t) * 3 + {0,1,2}] = {Qext, Qextpol,
+ * Qextcpol}. Without the scattering subtraction the reference's Qabs and
+ * Qabspol equal Qext and Qextpol. coeffs (ncoef >= 2 nmax + 1 values) are
+ * the orientation distribution's expansion coefficients; NULL keeps the
+ * particle-frame T-matrix. */
+int tmx_batch_observables(tmx_ctx *ctx, int32_t ntheta, const double *thetas,
+                          const double *coeffs, int32_t ncoef, double *q);
+
+/* Derivatives of those coefficients at the orders of the last batch with
+ * respect to (Re m, Im m, r_ev, axis ratio): dq[((grain * ntheta + t) * 3 +
+ * k) * 4 + p]. Forward-mode through dT = -(dRgQ + T dQ) Q^-1 with the LU
+ * factors of each block; no counterpart in the reference (which has no
+ * derivatives). q (may be NULL) receives the coefficients themselves. */
+int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta, const double *thetas,
+                        const double *coeffs, int32_t ncoef, double *q,
+                        double *dq);
 
 /* T-matrix of one grain at a fixed (nmax, ngauss), all m blocks, for callers
  * that cannot allocate device memory -- e.g. a host application whose device

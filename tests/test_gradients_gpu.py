@@ -1,0 +1,142 @@
+"""Derivatives of orientation-averaged extinction coefficients with respect
+to (Re m, Im m, r_ev, axis ratio): the tangent kernels against central finite
+differences at the converged order, of the GPU forward and of the CPU oracle.
+Tolerance 1e-6 relative (per grain, coefficient and parameter, over the
+angles).
+
+A central difference has its own error: truncation O(h^2) for large steps,
+rounding noise of the forward divided by h for small ones. For weakly
+polarised grains (Qextpol ~ 1e-3 Qext) the noise floor of a 1e-6 relative
+step is itself ~1e-6, so each derivative is compared with central
+differences at relative steps 1e-6 and 1e-5 and the closer one must agree."""
+import numpy as np
+import pytest
+
+import _helpers as H
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FD_STEP = 1e-6
+TOL = 1e-6
+
+
+def _step(params, p):
+    """Relative step: 1e-6 of r_ev and of d; for Re m and Im m 1e-6 of |m|
+    (Im m can be 1e-3, where 1e-6 of it would put the forward's rounding
+    noise at the 1e-6 level of the derivative)."""
+    if p < 2:
+        return FD_STEP * np.hypot(params[..., 0], params[..., 1])
+    return FD_STEP * np.abs(params[..., p])
+THETAS = np.array([0.3, 1.1, 1.9, 2.7])
+
+
+def _coeffs(kind, param, order=120):
+    return O.orientation_coefficients(kind, param, order)
+
+
+def _fd_gpu(ctx, params, lam, nmax, ngauss, coeffs, rel=FD_STEP):
+    n = len(params)
+    fd = np.zeros((n, len(THETAS), 3, 4))
+    for p in range(4):
+        h = _step(params, p) * (rel / FD_STEP)
+        out = []
+        for sgn in (1, -1):
+            q = params.copy()
+            q[:, p] += sgn * h
+            ctx.tmatrix_batch_fixed(q[:, 2], lam, q[:, 0] + 1j * q[:, 1], q[:, 3],
+                                    nmax, ngauss)
+            out.append(ctx.observables(THETAS, coeffs))
+        fd[:, :, :, p] = (out[0] - out[1]) / (2 * h[:, None, None])
+    return fd
+
+
+def _compare(dq, fds, q):
+    """Relative error per (grain, coefficient, parameter). A coefficient that
+    is zero up to rounding (Qextpol and Qextcpol under random orientation)
+    has derivatives at the noise level of the same parameter's Qext
+    derivative; there both must stay below 1e-6 of that scale."""
+    worst = 0.0
+    for i in range(dq.shape[0]):
+        for p in range(4):
+            scale = np.linalg.norm(dq[i, :, 0, p])
+            for k in range(3):
+                a = dq[i, :, k, p]
+                errs = []
+                for fd in fds:
+                    b = fd[i, :, k, p]
+                    nb = np.linalg.norm(b)
+                    if nb < 1e-6 * scale:
+                        # zero up to rounding: the tangent must be as well
+                        errs.append(0.0 if np.linalg.norm(a) < 1e-6 * scale else 1.0)
+                    else:
+                        errs.append(np.linalg.norm(a - b) / nb)
+                err = min(errs)
+                worst = max(worst, err)
+                assert err <= TOL, (i, k, p, err)
+    return worst
+
+
+@pytest.mark.parametrize("kind,param", [(0, 0.0), (2, 2.0), (1, 0.3)])
+def test_tangents_vs_central_differences(ctx, kind, param):
+    r, lam, m, d = H.config2_sample(8, 17, xmax=6.0)
+    params = np.stack([m.real, m.imag, r, d], axis=1)
+    res = ctx.tmatrix_batch(r, lam, m, d, max_order=60)
+    nmax, ngauss = res.nmax.copy(), res.ngauss.copy()
+    coeffs = _coeffs(kind, param)
+    ctx.tmatrix_batch_fixed(r, lam, m, d, nmax, ngauss)
+    q, dq = ctx.gradients(THETAS, coeffs)
+    assert np.allclose(q, ctx.observables(THETAS, coeffs), rtol=1e-12, atol=0)
+    fds = [_fd_gpu(ctx, params, lam, nmax, ngauss, coeffs, rel)
+           for rel in (1e-6, 1e-5)]
+    worst = _compare(dq, fds, q)
+    print("worst relative error vs central FD: %.3g" % worst)
+
+
+def _oracle_q(r, lam, m, d, nmax, ngauss, coeffs):
+    T, _ = H.oracle_at(r, lam, m, d, nmax, ngauss)
+    Ta = O.orientation_average(T, nmax, coeffs)
+    return O.extinction(Ta, nmax, lam, r, THETAS)
+
+
+def test_tangents_vs_oracle_finite_differences(ctx):
+    r, lam, m, d = H.config2_sample(3, 23, xmax=4.0)
+    res = ctx.tmatrix_batch(r, lam, m, d, max_order=40)
+    nmax, ngauss = res.nmax.copy(), res.ngauss.copy()
+    coeffs = _coeffs(2, 0.5)
+    ctx.tmatrix_batch_fixed(r, lam, m, d, nmax, ngauss)
+    q, dq = ctx.gradients(THETAS, coeffs)
+    params = np.stack([m.real, m.imag, r, d], axis=1)
+    fds = []
+    for rel in (1e-6, 1e-5):
+        fd = np.zeros_like(dq)
+        for i in range(3):
+            for p in range(4):
+                h = _step(params[i], p) * (rel / FD_STEP)
+                vals = []
+                for sgn in (1, -1):
+                    x = params[i].copy()
+                    x[p] += sgn * h
+                    vals.append(_oracle_q(x[2], lam, x[0] + 1j * x[1], x[3],
+                                          int(nmax[i]), int(ngauss[i]), coeffs))
+                fd[i, :, :, p] = (vals[0] - vals[1]) / (2 * h)
+        fds.append(fd)
+    _compare(dq, fds, q)
+
+
+def test_autograd_function(ctx):
+    import torch
+    from costuum_b200.autograd import extinction
+    r, lam, m, d = H.config2_sample(4, 29, xmax=5.0)
+    coeffs = _coeffs(2, 2.0)
+    params = torch.tensor(np.stack([m.real, m.imag, r, d], axis=1),
+                          dtype=torch.float64, requires_grad=True)
+    q = extinction(params, lam, THETAS, coeffs, max_order=50)
+    w = torch.tensor(np.random.default_rng(0).standard_normal(q.shape))
+    (q * w).sum().backward()
+    res = ctx.tmatrix_batch(r, lam, m, d, max_order=50)
+    ctx.tmatrix_batch_fixed(r, lam, m, d, res.nmax, res.ngauss)
+    qq, dq = ctx.gradients(THETAS, coeffs)
+    assert np.allclose(q.detach().numpy(), qq, rtol=1e-12)
+    want = np.einsum("ntk,ntkp->np", w.numpy(), dq)
+    assert np.allclose(params.grad.numpy(), want, rtol=1e-12, atol=0)

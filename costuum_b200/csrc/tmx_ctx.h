@@ -57,7 +57,10 @@ struct tmx_ctx {
   DevBuf cg, cg_off;
   int cg_nmax = 0;
   DevBuf Ta, o_angles, o_phis, o_wts, o_coef, o_shw, o_og, o_work, o_sj, o_qj,
-      o_S, o_gq, o_gz, o_cq, o_cz;
+      o_S, o_gq, o_gz, o_cq, o_cz, o_pairs, o_grp, o_x;
+  // plan of the observable kernels (first pair of each grain, job groups)
+  int64_t o_ngrains = 0, o_npairs = 0;
+  int o_nbmax = 1, o_ngrp = 0;
   int32_t *pinned = nullptr;
   // timing: events on the library stream
   cudaEvent_t t0 = nullptr, t1 = nullptr;

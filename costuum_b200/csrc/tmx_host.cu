@@ -251,6 +251,7 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
                     &ctx->o_og, &ctx->o_work, &ctx->o_sj, &ctx->o_qj, &ctx->o_S,
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
+                    &ctx->o_pairs, &ctx->o_grp, &ctx->o_x,
                     &ctx->state0, &ctx->actinit,
                     &ctx->gl_x,  &ctx->gl_w,   &ctx->gl_off,  &ctx->wig,
                     &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,

@@ -113,6 +113,13 @@ struct TmxSJob {
   int64_t out;  // first S (4 complex each) of the job
 };
 
+// consecutive amplitude jobs of one grain handled by one CTA (at most 32)
+struct TmxAmpGroup {
+  int32_t grain;
+  int32_t njobs;
+  int64_t job0;
+};
+
 // Q job for one (grain, theta): main amplitude and, with the scattering
 // subtraction, nacc x nacc amplitudes starting at s_acc
 struct TmxQJob {
@@ -125,14 +132,21 @@ struct TmxQJob {
 
 void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
                    int blocks, cudaStream_t stream);
-void tmx_launch_orient_avg(const TmxObsGrain *og, int ngrains, const double2 *T,
-                           double2 *Ta, const double *coeffs, int ncoef,
-                           const int64_t *cg_off, const double *cg, int cg_nmax,
-                           double2 *work, int wstride, int blocks, int threads,
-                           cudaStream_t stream);
-void tmx_launch_forward_s(const TmxSJob *jobs, int njobs, const TmxObsGrain *og,
-                          const double2 *Ta, const TmxAngle *angles,
-                          const double2 *phis, double2 *S, cudaStream_t stream);
+// orientation average (coef_set >= 0) or copy of every grain's T-matrix
+// with the amplitude factors c_{n' n} folded in; pair_base[g] = first
+// (n1, n2) pair of grain g (nmax^2 pairs per grain), mmax >= every nmax
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
+                             int ngrains, int64_t npairs, const double2 *T,
+                             double2 *Ta, const double *coeffs, int ncoef,
+                             const int64_t *cg_off, const double *cg,
+                             int cg_nmax, int mmax, cudaStream_t stream);
+// CTAs of the amplitude kernel at full occupancy for nbmax (its work slots:
+// grid x 32 x (nbmax + 1) x 4 complex)
+int tmx_amp_grid(int nbmax);
+void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
+                    const TmxObsGrain *og, const double2 *Ta,
+                    const TmxAngle *angles, const double2 *phis, double2 *S,
+                    double2 *xslot, int nbmax, int grid, cudaStream_t stream);
 void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,
                            const double2 *S, const double *wts, int nacc,
                            double *qout, int qstride, int do_abs, int do_ext,

@@ -22,6 +22,8 @@
 //
 // Compiled with --fmad=false, like the table kernels, so the recurrences
 // round as the reference's build does.
+#include <algorithm>
+
 #include "tmx_common.cuh"
 #include "tmx_kernels.h"
 
@@ -124,90 +126,153 @@ __device__ __forceinline__ int64_t telem(int N, int m, int i1, int n1, int i2,
          n2 - nmin;
 }
 
-__device__ static void orient_avg_grain(const TmxObsGrain G,
-                                        const cplx *__restrict__ T,
-                                        cplx *__restrict__ Ta,
-                                        const double *__restrict__ coeffs,
-                                        int ncoef,
-                                        const int64_t *__restrict__ cg_off,
-                                        const double *__restrict__ cg,
-                                        int cg_nmax, cplx *S) {
-  const int N = G.nmax;
-  if (N <= 0 || G.coef_set < 0) {
-    return; // disabled alignment: copied by the host
-  }
-  const double *p = coeffs + (int64_t)G.coef_set * ncoef;
-  const cplx *Tg = T + G.t_off;
-  cplx *Tag = Ta + G.t_off;
-  for (int u = threadIdx.x; u < N * N; u += blockDim.x) {
-    const int n1 = u / N + 1;
-    const int n2 = u % N + 1;
-    const int M = min(n1, n2);
-    const int lo = abs(n1 - n2);
-    const int hi = n1 + n2;
-    const double *C = cg + cg_off[(n1 - 1) * cg_nmax + (n2 - 1)];
-    // pass 1: S_a(N') = sum_m1 f(m1) (-1)^m1 CG(m1) T_m1(type a)
-    for (int Np = lo; Np <= hi; ++Np) {
-      const double *Cr = C + (int64_t)(Np - lo) * (M + 1);
-      const bool even = ((Np + hi) % 2 == 0);
-      const int i1a = 0, i2a = even ? 0 : 1;
-      const int i1b = 1, i2b = even ? 1 : 0;
-      cplx sa = mkc(0., 0.), sb = mkc(0., 0.);
-      for (int m1 = 0; m1 <= M; ++m1) {
-        const double f = ((m1 == 0) ? 1. : 2.) * ((m1 & 1) ? -1. : 1.) * Cr[m1];
-        const cplx ta = Tg[telem(N, m1, i1a, n1, i2a, n2)];
-        const cplx tb = Tg[telem(N, m1, i1b, n1, i2b, n2)];
-        sa = cadd(sa, cscale(ta, f));
-        sb = cadd(sb, cscale(tb, f));
-      }
-      S[2 * (Np - lo)] = sa;
-      S[2 * (Np - lo) + 1] = sb;
-    }
-    // pass 2: Tavg_m = sum_N' p_N' (-1)^m CG(m) S(N')
-    for (int m = 0; m <= M; ++m) {
-      cplx e00 = mkc(0., 0.), e11 = e00, e01 = e00, e10 = e00;
-      const double ms = (m & 1) ? -1. : 1.;
-      for (int Np = lo; Np <= hi; ++Np) {
-        const double f = ms * p[Np] * C[(int64_t)(Np - lo) * (M + 1) + m];
-        const cplx sa = S[2 * (Np - lo)];
-        const cplx sb = S[2 * (Np - lo) + 1];
-        if ((Np + hi) % 2 == 0) {
-          e00 = cadd(e00, cscale(sa, f));
-          e11 = cadd(e11, cscale(sb, f));
-        } else {
-          e01 = cadd(e01, cscale(sa, f));
-          e10 = cadd(e10, cscale(sb, f));
-        }
-      }
-      Tag[telem(N, m, 0, n1, 0, n2)] = e00;
-      Tag[telem(N, m, 1, n1, 1, n2)] = e11;
-      Tag[telem(N, m, 0, n1, 1, n2)] = e01;
-      Tag[telem(N, m, 1, n1, 0, n2)] = e10;
-    }
+// acc += t * a (complex times real), fused; this file is compiled without
+// automatic contraction, so the contractions are spelled out
+__device__ __forceinline__ void cfma(cplx &acc, cplx t, double a) {
+  acc.x = __fma_rn(t.x, a, acc.x);
+  acc.y = __fma_rn(t.y, a, acc.y);
+}
+
+// sqrt((2n + 1) / ((n + 1) n)), the factor of a_{n n'} for one order
+__device__ __forceinline__ double a_fac(int n) {
+  return sqrt((2. * n + 1.) / ((n + 1.) * n));
+}
+
+// c_{n' n} z for c_{n' n} = i^{n' - n - 1} a_{n' n} (NBasedResources::get_cnn,
+// NBasedResources.hpp:115-137); n' is the incoming order (column), n the
+// outgoing one (row)
+__device__ __forceinline__ cplx c_fold(int nin, int nout, double a, cplx z) {
+  const cplx s = cscale(z, a);
+  switch ((((nin - nout - 1) % 4) + 4) % 4) {
+  case 0:
+    return s;
+  case 1:
+    return mkc(-s.y, s.x);
+  case 2:
+    return mkc(-s.x, -s.y);
+  default:
+    return mkc(s.y, -s.x);
   }
 }
 
-
-// Blocks stride over grains; threads over (n1, n2) of a grain. S[N'] (2
-// complex per N') lives in a per-thread work slot of wstride elements.
-__global__ void k_orient_avg(const TmxObsGrain *__restrict__ og, int ngrains,
-                             const cplx *__restrict__ T, cplx *__restrict__ Ta,
-                             const double *__restrict__ coeffs, int ncoef,
-                             const int64_t *__restrict__ cg_off,
-                             const double *__restrict__ cg, int cg_nmax,
-                             cplx *__restrict__ work, int wstride) {
-  cplx *S = work + ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * wstride;
-  for (int gi = blockIdx.x; gi < ngrains; gi += gridDim.x) {
-    orient_avg_grain(og[gi], T, Ta, coeffs, ncoef, cg_off, cg, cg_nmax, S);
+// One warp per (grain, n1, n2). AlignmentAverageTask::execute (Alignment
+// AverageTask.hpp:115-215) forms, for every m,
+//   Ta_m = sum_N' p_N' (-1)^m CG(n1 m n2 -m|N'0) sum_m1 f(m1) (-1)^m1
+//          CG(n1 m1 n2 -m1|N'0) T_m1,
+// with f = 1 for m1 = 0 and 2 otherwise; the m1 sum does not depend on m, so
+// pass 1 forms it once per N' (lanes over N') and pass 2 contracts over N'
+// (lanes over m): O(n^2) per pair instead of O(n^3). Even N' - |n1 - n2|
+// couple the (0,0) and (1,1) sub-blocks, odd ones (0,1) and (1,0). Grains
+// without an orientation distribution (coef_set < 0) are copied. Either way
+// the output carries the factor c_{n2 n1} of the amplitude sums, so that
+// the amplitude kernel contracts Ta with real vectors only.
+// Shared memory per warp: t[4][M + 1] and S[2][2M + 1] complex.
+__global__ void __launch_bounds__(256)
+k_orient_pairs(const TmxObsGrain *__restrict__ og,
+               const int64_t *__restrict__ pair_base, int ngrains,
+               int64_t npairs, const cplx *__restrict__ T,
+               cplx *__restrict__ Ta, const double *__restrict__ coeffs,
+               int ncoef, const int64_t *__restrict__ cg_off,
+               const double *__restrict__ cg, int cg_nmax, int wcap) {
+  extern __shared__ cplx osh[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  cplx *tv = osh + (int64_t)warp * wcap;
+  for (int64_t w = (int64_t)blockIdx.x * nwarps + warp; w < npairs;
+       w += (int64_t)gridDim.x * nwarps) {
+    // grain of pair w: the last g with pair_base[g] <= w
+    int lo = 0, hi = ngrains - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pair_base[mid] <= w) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    const TmxObsGrain G = og[lo];
+    const int N = G.nmax;
+    const int pair = (int)(w - pair_base[lo]);
+    const int n1 = pair / N + 1;
+    const int n2 = pair % N + 1;
+    const int M = min(n1, n2);
+    const cplx *Tg = T + G.t_off;
+    cplx *Tag = Ta + G.t_off;
+    const double afold = a_fac(n1) * a_fac(n2);
+    if (G.coef_set < 0) {
+      for (int m = lane; m <= M; m += 32) {
+        for (int q = 0; q < 4; ++q) {
+          const int i1 = q >> 1, i2 = q & 1;
+          const int64_t e = telem(N, m, i1, n1, i2, n2);
+          Tag[e] = c_fold(n2, n1, afold, Tg[e]);
+        }
+      }
+      continue;
+    }
+    const double *p = coeffs + (int64_t)G.coef_set * ncoef;
+    const int nN = 2 * M + 1;
+    const int Nlo = abs(n1 - n2);
+    const double *C = cg + cg_off[(n1 - 1) * cg_nmax + (n2 - 1)];
+    cplx *t00 = tv, *t11 = tv + (M + 1), *t01 = tv + 2 * (M + 1),
+         *t10 = tv + 3 * (M + 1);
+    cplx *S = tv + 4 * (M + 1);
+    for (int m1 = lane; m1 <= M; m1 += 32) {
+      // f(m1) (-1)^m1 is a power of two with a sign: the product is exact
+      const double f = ((m1 == 0) ? 1. : 2.) * ((m1 & 1) ? -1. : 1.);
+      t00[m1] = cscale(Tg[telem(N, m1, 0, n1, 0, n2)], f);
+      t11[m1] = cscale(Tg[telem(N, m1, 1, n1, 1, n2)], f);
+      t01[m1] = cscale(Tg[telem(N, m1, 0, n1, 1, n2)], f);
+      t10[m1] = cscale(Tg[telem(N, m1, 1, n1, 0, n2)], f);
+    }
+    __syncwarp();
+    // pass 1: S(N') for the two sub-blocks of its parity
+    for (int j = lane; j < nN; j += 32) {
+      const double *Cr = C + (int64_t)j * (M + 1);
+      const cplx *ta = (j & 1) ? t01 : t00;
+      const cplx *tb = (j & 1) ? t10 : t11;
+      cplx sa = mkc(0., 0.), sb = sa;
+      for (int m1 = 0; m1 <= M; ++m1) {
+        const double c = Cr[m1];
+        cfma(sa, ta[m1], c);
+        cfma(sb, tb[m1], c);
+      }
+      S[2 * j] = sa;
+      S[2 * j + 1] = sb;
+    }
+    __syncwarp();
+    // pass 2: Ta_m = sum_N' p_N' (-1)^m CG(m) S(N')
+    for (int m = lane; m <= M; m += 32) {
+      cplx e00 = mkc(0., 0.), e11 = e00, e01 = e00, e10 = e00;
+      const double ms = (m & 1) ? -1. : 1.;
+      for (int j = 0; j < nN; j += 2) {
+        const double f = ms * p[Nlo + j] * C[(int64_t)j * (M + 1) + m];
+        cfma(e00, S[2 * j], f);
+        cfma(e11, S[2 * j + 1], f);
+      }
+      for (int j = 1; j < nN; j += 2) {
+        const double f = ms * p[Nlo + j] * C[(int64_t)j * (M + 1) + m];
+        cfma(e01, S[2 * j], f);
+        cfma(e10, S[2 * j + 1], f);
+      }
+      Tag[telem(N, m, 0, n1, 0, n2)] = c_fold(n2, n1, afold, e00);
+      Tag[telem(N, m, 1, n1, 1, n2)] = c_fold(n2, n1, afold, e11);
+      Tag[telem(N, m, 0, n1, 1, n2)] = c_fold(n2, n1, afold, e01);
+      Tag[telem(N, m, 1, n1, 0, n2)] = c_fold(n2, n1, afold, e10);
+    }
+    __syncwarp();
   }
 }
 
 // -------------------------------------------------- forward amplitude ----
 
-// d^n_{0m}(x) / sin x and d/dx for one m, n = 1..nmax
+// pi_n = m d^n_{0m}(x) / sin x and tau_n = d/dx d^n_{0m}(x) for one m and
+// n = nmin..nmax, written to pi[(n - nmin) * stride], tau[...]
 // (SpecialFunctions::wigner_dn_0m_sinx, SpecialFunctions.hpp:397-495)
-__device__ static void wigner_sinx(double cosx, double sinx, double sinx_inv,
-                                   int nmax, int m, double *y, double *dy) {
+__device__ static void wigner_col(double cosx, double sinx, double sinx_inv,
+                                  int nmax, int m, double *pi, double *tau,
+                                  int stride) {
+  const int nmin = (m > 1) ? m : 1;
   if (fabs(1. - fabs(cosx)) <= 1.e-10) {
     if (m == 1) {
       int sign = 1;
@@ -216,17 +281,17 @@ __device__ static void wigner_sinx(double cosx, double sinx, double sinx_inv,
         if (cosx < 0.) {
           dn *= sign;
         }
-        y[n - 1] = dn;
+        pi[(n - nmin) * stride] = m * dn;
         if (cosx < 0.) {
           dn = -dn;
         }
-        dy[n - 1] = dn;
+        tau[(n - nmin) * stride] = dn;
         sign = -sign;
       }
     } else {
-      for (int i = 0; i < nmax; ++i) {
-        y[i] = 0.;
-        dy[i] = 0.;
+      for (int n = nmin; n <= nmax; ++n) {
+        pi[(n - nmin) * stride] = 0.;
+        tau[(n - nmin) * stride] = 0.;
       }
     }
     return;
@@ -240,8 +305,8 @@ __device__ static void wigner_sinx(double cosx, double sinx, double sinx_inv,
       const double np12p1 = 2. * np1 + 1.;
       const double dnp1 = (np12p1 * cosx * d2 - np1 * d1) / np2;
       const double ddn = sinx_inv * np1 * np2 * (dnp1 - d1) / np12p1;
-      y[n] = d2 * sinx_inv;
-      dy[n] = ddn;
+      pi[n * stride] = 0.;
+      tau[n * stride] = ddn;
       d1 = d2;
       d2 = dnp1;
     }
@@ -254,10 +319,6 @@ __device__ static void wigner_sinx(double cosx, double sinx, double sinx_inv,
     const double i2 = 2. * (i + 1.);
     d2 *= sqrt((i2 - 1.) / i2) * sinx;
   }
-  for (int n = 0; n < m - 1; ++n) {
-    y[n] = 0.;
-    dy[n] = 0.;
-  }
   for (int n = m - 1; n < nmax; ++n) {
     const double np1 = n + 1.;
     const double np2 = n + 2.;
@@ -266,128 +327,152 @@ __device__ static void wigner_sinx(double cosx, double sinx, double sinx_inv,
     const double s22 = sqrt(np2 * np2 - m2);
     const double dnp1 = (np12p1 * cosx * d2 - s12 * d1) / s22;
     const double ddn = sinx_inv * (np1 * s22 * dnp1 - np2 * s12 * d1) / np12p1;
-    y[n] = d2 * sinx_inv;
-    dy[n] = ddn;
+    pi[(n + 1 - nmin) * stride] = m * (d2 * sinx_inv);
+    tau[(n + 1 - nmin) * stride] = ddn;
     d1 = d2;
     d2 = dnp1;
   }
 }
 
-__device__ __forceinline__ double a_nn(int n1, int n2) {
-  const double s1 = sqrt((2. * n1 + 1.) / ((n1 + 1.) * n1));
-  const double s2 = sqrt((2. * n2 + 1.) / ((n2 + 1.) * n2));
-  return s1 * s2;
-}
-
-// c_{n1 n2} = i^{n1 - n2 - 1} a_{n1 n2} (NBasedResources::get_cnn)
-__device__ __forceinline__ cplx c_nn(int n1, int n2) {
-  const double a = a_nn(n1, n2);
-  switch ((((n1 - n2 - 1) % 4) + 4) % 4) {
-  case 0:
-    return mkc(a, 0.);
-  case 1:
-    return mkc(0., a);
-  case 2:
-    return mkc(-a, 0.);
-  default:
-    return mkc(0., -a);
-  }
-}
-
-// One block per job (grain, theta_in, theta_out, azimuth list). Thread m
-// forms X_m, the four (n, n') sums of order m without the azimuthal factor;
-// then every azimuth p gets S = (1/k) sum_m (2 cos m phi, 2 sin m phi) X_m
+// One CTA per group of up to 32 amplitude jobs of one grain (lane = job).
+// For every m, with u = (pi_n, tau_n) at the outgoing angle and v at the
+// incoming one (n the row order, n' the column order of block m),
+//   X0 = u^T Tc v,  X1 = u^T Tc v',  X2 = u'^T Tc v,  X3 = u'^T Tc v'
+// where Tc is block m with the c_{n' n} factors folded in and u', v' swap
+// the pi and tau halves: the four (n, n') sums of
+// ExtinctionCoefficientTask.hpp:517-619 as one (2nb x 2nb) x (2nb x 64)
+// product per m. Warps own rows; lanes own jobs; the T row is read once per
+// warp (a broadcast) and the angle vectors come from shared memory. X is
+// kept in this CTA's global slot; the azimuth pass then forms
+//   S = (1/k) sum_m (2 cos m phi, 2 sin m phi) X_m
 // with e^{i m phi} built by repeated multiplication as in the reference.
-__global__ void k_forward_s(const TmxSJob *__restrict__ jobs, int njobs,
-                            const TmxObsGrain *__restrict__ og,
-                            const cplx *__restrict__ Ta,
-                            const TmxAngle *__restrict__ angles,
-                            const cplx *__restrict__ phis,
-                            cplx *__restrict__ S_out) {
-  const int j = blockIdx.x;
-  if (j >= njobs) {
-    return;
-  }
-  const TmxSJob J = jobs[j];
-  const TmxObsGrain G = og[J.grain];
-  const int N = G.nmax;
-  const cplx *T = Ta + G.t_off;
-  __shared__ cplx X[TMX_MAX_NB + 2][4];
-  const TmxAngle ai = angles[J.angle_in];
-  const TmxAngle ao = angles[J.angle_out];
-  double din[TMX_MAX_NB], ddin[TMX_MAX_NB], dout[TMX_MAX_NB], ddout[TMX_MAX_NB];
-  for (int m = threadIdx.x; m <= N; m += blockDim.x) {
-    wigner_sinx(ai.c, ai.s, ai.si, N, m, din, ddin);
-    wigner_sinx(ao.c, ao.s, ao.si, N, m, dout, ddout);
-    const int nmin = (m > 1) ? m : 1;
-    cplx x0 = mkc(0., 0.), x1 = x0, x2 = x0, x3 = x0;
-    for (int nn = nmin; nn < N + 1; ++nn) {
-      const double pi_nn = m * din[nn - 1];
-      const double tau_nn = ddin[nn - 1];
-      for (int n = nmin; n < N + 1; ++n) {
-        const double pi_n = m * dout[n - 1];
-        const double tau_n = ddout[n - 1];
-        const cplx c = c_nn(nn, n);
-        const cplx T11 = T[telem(N, m, 0, n, 0, nn)];
-        const cplx T22 = T[telem(N, m, 1, n, 1, nn)];
-        if (m == 0) {
-          const cplx f = cscale(cscale(c, tau_n), tau_nn);
-          x0 = cadd(x0, cmul(f, T22));
-          x3 = cadd(x3, cmul(f, T11));
+__global__ void __launch_bounds__(256)
+k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
+      const TmxSJob *__restrict__ jobs, const TmxObsGrain *__restrict__ og,
+      const cplx *__restrict__ Ta, const TmxAngle *__restrict__ angles,
+      const cplx *__restrict__ phis, cplx *__restrict__ S_out,
+      cplx *__restrict__ xslot, int nbmax) {
+  extern __shared__ double ash[];
+  double *po = ash;
+  double *to = po + nbmax * 32;
+  double *pi = to + nbmax * 32;
+  double *ti = pi + nbmax * 32;
+  cplx *red = (cplx *)(ti + nbmax * 32); // [8 warps][4][32 lanes]
+  __shared__ TmxSJob sj[32];
+  __shared__ int pref[33];
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  cplx *X = xslot + (int64_t)blockIdx.x * 32 * (nbmax + 1) * 4;
+  for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+    const TmxAmpGroup grp = groups[gi];
+    const TmxObsGrain G = og[grp.grain];
+    const int N = G.nmax;
+    const int nj = grp.njobs;
+    const cplx *Tg = Ta + G.t_off;
+    if (tid < nj) {
+      sj[tid] = jobs[grp.job0 + tid];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      pref[0] = 0;
+      for (int p = 0; p < nj; ++p) {
+        pref[p + 1] = pref[p] + sj[p].nphi;
+      }
+    }
+    for (int m = 0; m <= N; ++m) {
+      const int nmin = (m > 1) ? m : 1;
+      const int nb = N + 1 - nmin;
+      if (tid < 64) {
+        const int p = tid & 31;
+        const int side = tid >> 5; // 0: outgoing angle, 1: incoming angle
+        double *P = side ? pi : po;
+        double *Tt = side ? ti : to;
+        if (p < nj) {
+          const TmxAngle a = angles[side ? sj[p].angle_in : sj[p].angle_out];
+          wigner_col(a.c, a.s, a.si, N, m, P + p, Tt + p, 32);
         } else {
-          const cplx T12 = T[telem(N, m, 0, n, 1, nn)];
-          const cplx T21 = T[telem(N, m, 1, n, 0, nn)];
-          const double pp = pi_n * pi_nn, pt = pi_n * tau_nn;
-          const double tp = tau_n * pi_nn, tt = tau_n * tau_nn;
-          const cplx s0 = cadd(cadd(cadd(cscale(T11, pp), cscale(T21, tp)),
-                                    cscale(T12, pt)),
-                               cscale(T22, tt));
-          const cplx s1 = cadd(cadd(cadd(cscale(T11, pt), cscale(T21, tt)),
-                                    cscale(T12, pp)),
-                               cscale(T22, tp));
-          const cplx s2 = cadd(cadd(cadd(cscale(T11, tp), cscale(T21, pp)),
-                                    cscale(T12, tt)),
-                               cscale(T22, pt));
-          const cplx s3 = cadd(cadd(cadd(cscale(T11, tt), cscale(T21, pt)),
-                                    cscale(T12, tp)),
-                               cscale(T22, pp));
-          x0 = cadd(x0, cmul(c, s0));
-          x1 = cadd(x1, cmul(c, s1));
-          x2 = cadd(x2, cmul(c, s2));
-          x3 = cadd(x3, cmul(c, s3));
+          for (int k = 0; k < nb; ++k) {
+            P[k * 32 + p] = 0.;
+            Tt[k * 32 + p] = 0.;
+          }
+        }
+      }
+      __syncthreads();
+      cplx x0 = mkc(0., 0.), x1 = x0, x2 = x0, x3 = x0;
+      const cplx *Tm = Tg + tblock(N, m);
+      for (int r = warp; r < 2 * nb; r += 8) {
+        const cplx *Tr = Tm + (int64_t)r * 2 * nb;
+        cplx y0 = mkc(0., 0.), y1 = y0;
+#pragma unroll 4
+        for (int k = 0; k < nb; ++k) {
+          const double a = pi[k * 32 + lane];
+          const double b = ti[k * 32 + lane];
+          const cplx t0 = Tr[k];
+          const cplx t1 = Tr[nb + k];
+          cfma(y0, t0, a);
+          cfma(y0, t1, b);
+          cfma(y1, t0, b);
+          cfma(y1, t1, a);
+        }
+        const int kr = (r < nb) ? r : r - nb;
+        const double u = (r < nb) ? po[kr * 32 + lane] : to[kr * 32 + lane];
+        const double up = (r < nb) ? to[kr * 32 + lane] : po[kr * 32 + lane];
+        cfma(x0, y0, u);
+        cfma(x1, y1, u);
+        cfma(x2, y0, up);
+        cfma(x3, y1, up);
+      }
+      red[(warp * 4 + 0) * 32 + lane] = x0;
+      red[(warp * 4 + 1) * 32 + lane] = x1;
+      red[(warp * 4 + 2) * 32 + lane] = x2;
+      red[(warp * 4 + 3) * 32 + lane] = x3;
+      __syncthreads();
+      if (tid < 128) {
+        const int k = tid >> 5;
+        cplx s = red[k * 32 + lane];
+        for (int w = 1; w < 8; ++w) {
+          s = cadd(s, red[(w * 4 + k) * 32 + lane]);
+        }
+        if (lane < nj) {
+          X[((int64_t)lane * (N + 1) + m) * 4 + k] = s;
         }
       }
     }
-    X[m][0] = x0;
-    X[m][1] = x1;
-    X[m][2] = x2;
-    X[m][3] = x3;
-  }
-  __syncthreads();
-  const double kinv = 1. / G.k;
-  for (int p = threadIdx.x; p < J.nphi; p += blockDim.x) {
-    const cplx e1 = phis[J.phi0 + p];
-    cplx e = mkc(1., 0.);
-    cplx s0 = mkc(0., 0.), s1 = s0, s2 = s0, s3 = s0;
-    for (int m = 0; m <= N; ++m) {
-      const double fcos = 2. * e.x;
-      const double fsin = 2. * e.y;
-      e = cmul(e, e1);
-      if (m == 0) {
-        s0 = cadd(s0, X[0][0]);
-        s3 = cadd(s3, X[0][3]);
-      } else {
-        s0 = cadd(s0, cscale(X[m][0], fcos));
-        s1 = cadd(s1, cscale(X[m][1], fsin));
-        s2 = csub(s2, cscale(X[m][2], fsin));
-        s3 = cadd(s3, cscale(X[m][3], fcos));
+    __syncthreads();
+    const double kinv = 1. / G.k;
+    for (int item = tid; item < pref[nj]; item += blockDim.x) {
+      int p = 0;
+      while (pref[p + 1] <= item) {
+        ++p;
       }
+      const TmxSJob J = sj[p];
+      const int f = item - pref[p];
+      const cplx e1 = phis[J.phi0 + f];
+      const cplx *Xp = X + (int64_t)p * (N + 1) * 4;
+      cplx e = mkc(1., 0.);
+      cplx s0 = mkc(0., 0.), s1 = s0, s2 = s0, s3 = s0;
+      for (int m = 0; m <= N; ++m) {
+        const double fcos = 2. * e.x;
+        const double fsin = 2. * e.y;
+        e = cmul(e, e1);
+        if (m == 0) {
+          s0 = cadd(s0, Xp[0]);
+          s3 = cadd(s3, Xp[3]);
+        } else {
+          s0 = cadd(s0, cscale(Xp[m * 4 + 0], fcos));
+          s1 = cadd(s1, cscale(Xp[m * 4 + 1], fsin));
+          s2 = csub(s2, cscale(Xp[m * 4 + 2], fsin));
+          s3 = cadd(s3, cscale(Xp[m * 4 + 3], fcos));
+        }
+      }
+      cplx *o = S_out + (J.out + f) * 4;
+      o[0] = cscale(s0, kinv);
+      o[1] = cscale(s1, kinv);
+      o[2] = cscale(s2, kinv);
+      o[3] = cscale(s3, kinv);
     }
-    cplx *o = S_out + (J.out + p) * 4;
-    o[0] = cscale(s0, kinv);
-    o[1] = cscale(s1, kinv);
-    o[2] = cscale(s2, kinv);
-    o[3] = cscale(s3, kinv);
+    __syncthreads();
   }
 }
 
@@ -547,25 +632,49 @@ void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
   k_cg<<<blocks, 128, 0, stream>>>(nmax, cg_off, cg, work);
 }
 
-void tmx_launch_orient_avg(const TmxObsGrain *og, int ngrains, const double2 *T,
-                           double2 *Ta, const double *coeffs, int ncoef,
-                           const int64_t *cg_off, const double *cg, int cg_nmax,
-                           double2 *work, int wstride, int blocks, int threads,
-                           cudaStream_t stream) {
-  if (ngrains <= 0) {
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
+                             int ngrains, int64_t npairs, const double2 *T,
+                             double2 *Ta, const double *coeffs, int ncoef,
+                             const int64_t *cg_off, const double *cg,
+                             int cg_nmax, int mmax, cudaStream_t stream) {
+  if (npairs <= 0) {
     return;
   }
-  k_orient_avg<<<blocks, threads, 0, stream>>>(og, ngrains, T, Ta, coeffs, ncoef,
-                                               cg_off, cg, cg_nmax, work, wstride);
+  const int wcap = 4 * (mmax + 1) + 2 * (2 * mmax + 1);
+  const size_t smem = (size_t)8 * wcap * sizeof(double2);
+  cudaFuncSetAttribute(k_orient_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int64_t want = (npairs + 7) / 8;
+  const int blocks = (int)std::min<int64_t>(want, 148 * 8);
+  k_orient_pairs<<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs, T,
+                                                Ta, coeffs, ncoef, cg_off, cg,
+                                                cg_nmax, wcap);
 }
 
-void tmx_launch_forward_s(const TmxSJob *jobs, int njobs, const TmxObsGrain *og,
-                          const double2 *Ta, const TmxAngle *angles,
-                          const double2 *phis, double2 *S, cudaStream_t stream) {
-  if (njobs <= 0) {
+static size_t amp_smem(int nbmax) {
+  return (size_t)4 * nbmax * 32 * sizeof(double) + 8 * 4 * 32 * sizeof(double2);
+}
+
+int tmx_amp_grid(int nbmax) {
+  cudaFuncSetAttribute(k_amp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)amp_smem(TMX_MAX_NB));
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp, 256, amp_smem(nbmax));
+  return std::max(1, sms * std::max(1, per_sm));
+}
+
+void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
+                    const TmxObsGrain *og, const double2 *Ta,
+                    const TmxAngle *angles, const double2 *phis, double2 *S,
+                    double2 *xslot, int nbmax, int grid, cudaStream_t stream) {
+  if (ngroups <= 0) {
     return;
   }
-  k_forward_s<<<njobs, 128, 0, stream>>>(jobs, njobs, og, Ta, angles, phis, S);
+  const int blocks = std::min(grid, ngroups);
+  k_amp<<<blocks, 256, amp_smem(nbmax), stream>>>(groups, ngroups, jobs, og, Ta,
+                                                  angles, phis, S, xslot, nbmax);
 }
 
 void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,

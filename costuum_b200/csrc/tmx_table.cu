@@ -331,6 +331,89 @@ int64_t est_nmax(double x, int min_order, int max_order) {
   return std::min<int64_t>((int64_t)e, max_order - 1);
 }
 
+// Work plan of the observable kernels for the grains `og` (already on the
+// device in ctx->o_og) and the amplitude jobs `sj` (already in ctx->o_sj):
+// the first (n1, n2) pair of every grain for the orientation kernel and
+// groups of at most 32 consecutive jobs of one grain for the amplitude
+// kernel.
+int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
+                    const std::vector<TmxSJob> &sj) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = (int64_t)og.size();
+  std::vector<int64_t> base(std::max<int64_t>(1, n), 0);
+  int64_t npairs = 0;
+  int nbmax = 1;
+  for (int64_t g = 0; g < n; ++g) {
+    base[g] = npairs;
+    const int64_t N = std::max(0, og[g].nmax);
+    npairs += N * N;
+    nbmax = std::max(nbmax, og[g].nmax);
+  }
+  std::vector<TmxAmpGroup> grp;
+  for (size_t j = 0; j < sj.size(); ++j) {
+    if (grp.empty() || grp.back().grain != sj[j].grain || grp.back().njobs == 32) {
+      TmxAmpGroup a;
+      a.grain = sj[j].grain;
+      a.njobs = 0;
+      a.job0 = (int64_t)j;
+      grp.push_back(a);
+    }
+    grp.back().njobs += 1;
+  }
+  int rc;
+  if ((rc = ensure(ctx, ctx->o_pairs, base.size() * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->o_grp, std::max<size_t>(1, grp.size()) * sizeof(TmxAmpGroup)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->o_pairs.p, base.data(), base.size() * sizeof(int64_t),
+                     cudaMemcpyHostToDevice, st));
+  if (!grp.empty()) {
+    CK(cudaMemcpyAsync(ctx->o_grp.p, grp.data(), grp.size() * sizeof(TmxAmpGroup),
+                       cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaStreamSynchronize(st));
+  ctx->o_ngrains = n;
+  ctx->o_npairs = npairs;
+  ctx->o_nbmax = nbmax;
+  ctx->o_ngrp = (int)grp.size();
+  return TMX_OK;
+}
+
+// Ta = orientation average (or copy) of Tsrc with the amplitude factors
+// folded in, then the amplitudes S of every job (zeroed first: grains with
+// nmax 0 have no jobs)
+int run_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int64_t t_total, int ncoef,
+                   cplx *S_out, int64_t s_total) {
+  cudaStream_t st = ctx->stream;
+  int rc;
+  if ((rc = ensure(ctx, ctx->Ta, std::max<int64_t>(1, t_total) * sizeof(cplx)))) {
+    return rc;
+  }
+  CK(cudaMemsetAsync(S_out, 0, std::max<int64_t>(0, s_total) * 4 * sizeof(cplx), st));
+  if (t_total <= 0 || ctx->o_npairs <= 0) {
+    return TMX_OK;
+  }
+  tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
+                          (const int64_t *)ctx->o_pairs.p, (int)ctx->o_ngrains,
+                          ctx->o_npairs, Tsrc, (cplx *)ctx->Ta.p,
+                          (const double *)ctx->o_coef.p, ncoef,
+                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
+                          ctx->cg_nmax, ctx->o_nbmax, st);
+  LAUNCHED();
+  const int grid = tmx_amp_grid(ctx->o_nbmax);
+  if ((rc = ensure(ctx, ctx->o_x,
+                   (size_t)grid * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
+    return rc;
+  }
+  tmx_launch_amp((const TmxAmpGroup *)ctx->o_grp.p, ctx->o_ngrp,
+                 (const TmxSJob *)ctx->o_sj.p, (const TmxObsGrain *)ctx->o_og.p,
+                 (const cplx *)ctx->Ta.p, (const TmxAngle *)ctx->o_angles.p,
+                 (const cplx *)ctx->o_phis.p, S_out, (cplx *)ctx->o_x.p,
+                 ctx->o_nbmax, grid, st);
+  LAUNCHED();
+  return TMX_OK;
+}
+
 } // namespace
 
 extern "C" int tmx_get_table(
@@ -523,28 +606,11 @@ extern "C" int tmx_get_table(
     if ((rc = tmx_ensure_cg(ctx, nmax_chunk))) {
       return rc;
     }
-    // ---- orientation average (disabled alignment keeps T)
-    const int oa_blocks = (int)std::min<int64_t>(ng, 4 * 148);
-    const int oa_threads = 128;
-    const int wstride = 2 * (2 * nmax_chunk + 1);
-    if ((rc = ensure(ctx, ctx->o_og, ng * sizeof(TmxObsGrain))) ||
-        (rc = ensure(ctx, ctx->Ta, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
-        (rc = ensure(ctx, ctx->o_work, (size_t)oa_blocks * oa_threads * wstride * sizeof(cplx)))) {
+    if ((rc = ensure(ctx, ctx->o_og, ng * sizeof(TmxObsGrain)))) {
       return rc;
     }
     CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), ng * sizeof(TmxObsGrain),
                        cudaMemcpyHostToDevice, st));
-    if (t_total > 0) {
-      CK(cudaMemcpyAsync(ctx->Ta.p, ctx->T.p, t_total * sizeof(cplx),
-                         cudaMemcpyDeviceToDevice, st));
-    }
-    tmx_launch_orient_avg((const TmxObsGrain *)ctx->o_og.p, (int)ng,
-                          (const cplx *)ctx->T.p, (cplx *)ctx->Ta.p,
-                          (const double *)ctx->o_coef.p, ncoef,
-                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
-                          ctx->cg_nmax, (cplx *)ctx->o_work.p, wstride, oa_blocks,
-                          oa_threads, st);
-    LAUNCHED();
     // ---- amplitude jobs
     std::vector<TmxSJob> sj;
     std::vector<TmxQJob> qj;
@@ -614,7 +680,6 @@ extern "C" int tmx_get_table(
         (rc = ensure(ctx, ctx->o_cz, std::max<int64_t>(1, do_sca ? nc * ntheta * nphi_sca * 16 : 1) * sizeof(double)))) {
       return rc;
     }
-    CK(cudaMemsetAsync(ctx->o_S.p, 0, s_total * 4 * sizeof(cplx), st));
     if (!sj.empty()) {
       CK(cudaMemcpyAsync(ctx->o_sj.p, sj.data(), sj.size() * sizeof(TmxSJob),
                          cudaMemcpyHostToDevice, st));
@@ -623,11 +688,11 @@ extern "C" int tmx_get_table(
       CK(cudaMemcpyAsync(ctx->o_qj.p, qj.data(), qj.size() * sizeof(TmxQJob),
                          cudaMemcpyHostToDevice, st));
     }
-    tmx_launch_forward_s((const TmxSJob *)ctx->o_sj.p, (int)sj.size(),
-                         (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->Ta.p,
-                         (const TmxAngle *)ctx->o_angles.p,
-                         (const cplx *)ctx->o_phis.p, (cplx *)ctx->o_S.p, st);
-    LAUNCHED();
+    if ((rc = upload_obs_plan(ctx, og, sj)) ||
+        (rc = run_amplitudes(ctx, (const cplx *)ctx->T.p, t_total, ncoef,
+                             (cplx *)ctx->o_S.p, s_total))) {
+      return rc;
+    }
     if (nq > 0) {
       CK(cudaMemsetAsync(ctx->o_gq.p, 0, ng * ntheta * nq * sizeof(double), st));
       tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, (int)qj.size(),
@@ -700,45 +765,10 @@ namespace {
 
 // orientation-averaged theta -> theta amplitudes of every grain of the last
 // batch for the T-matrices at `Tsrc`; S[(grain * ntheta + t) * 4]
-int batch_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int ntheta,
-                     bool average, int ncoef, cplx *S_out) {
-  cudaStream_t st = ctx->stream;
-  const int64_t n = ctx->n;
-  int rc;
-  int nmax_b = 1;
-  for (int64_t g = 0; g < n; ++g) {
-    nmax_b = std::max(nmax_b, ctx->nmax_h[g]);
-  }
-  const int64_t t_total = ctx->p2_t_total;
-  if (t_total <= 0) {
-    return TMX_OK;
-  }
-  const int oa_blocks = (int)std::min<int64_t>(n, 4 * 148);
-  const int wstride = 2 * (2 * nmax_b + 1);
-  if ((rc = ensure(ctx, ctx->Ta, t_total * sizeof(cplx)))) {
-    return rc;
-  }
-  CK(cudaMemcpyAsync(ctx->Ta.p, Tsrc, t_total * sizeof(cplx),
-                     cudaMemcpyDeviceToDevice, st));
-  if (average) {
-    if ((rc = tmx_ensure_cg(ctx, nmax_b)) ||
-        (rc = ensure(ctx, ctx->o_work, (size_t)oa_blocks * 128 * wstride * sizeof(cplx)))) {
-      return rc;
-    }
-    tmx_launch_orient_avg((const TmxObsGrain *)ctx->o_og.p, (int)n, Tsrc,
-                          (cplx *)ctx->Ta.p, (const double *)ctx->o_coef.p, ncoef,
-                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
-                          ctx->cg_nmax, (cplx *)ctx->o_work.p, wstride, oa_blocks,
-                          128, st);
-    LAUNCHED();
-  }
-  CK(cudaMemsetAsync(S_out, 0, n * ntheta * 4 * sizeof(cplx), st));
-  tmx_launch_forward_s((const TmxSJob *)ctx->o_sj.p, ctx->o_nsj,
-                       (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->Ta.p,
-                       (const TmxAngle *)ctx->o_angles.p, (const cplx *)ctx->o_phis.p,
-                       S_out, st);
-  LAUNCHED();
-  return TMX_OK;
+int batch_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int ntheta, int ncoef,
+                     cplx *S_out) {
+  return run_amplitudes(ctx, Tsrc, ctx->p2_t_total, ncoef, S_out,
+                        ctx->n * ntheta);
 }
 
 // descriptors shared by the per-grain observable and gradient passes
@@ -812,8 +842,16 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
   }
   ctx->o_nsj = (int)sj.size();
   ctx->o_nqj = (int)qj.size();
-  CK(cudaStreamSynchronize(st));
-  return TMX_OK;
+  if (coeffs) {
+    int nmax_b = 1;
+    for (int64_t g = 0; g < n; ++g) {
+      nmax_b = std::max(nmax_b, og[g].nmax);
+    }
+    if ((rc = tmx_ensure_cg(ctx, nmax_b))) {
+      return rc;
+    }
+  }
+  return upload_obs_plan(ctx, og, sj);
 }
 
 } // namespace
@@ -836,8 +874,8 @@ extern "C" int tmx_batch_observables(tmx_ctx *ctx, int32_t ntheta,
       (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double)))) {
     return rc;
   }
-  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, coeffs != nullptr,
-                             ncoef, (cplx *)ctx->o_S.p))) {
+  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, ncoef,
+                             (cplx *)ctx->o_S.p))) {
     return rc;
   }
   CK(cudaMemsetAsync(ctx->o_gq.p, 0, n * ntheta * 3 * sizeof(double), st));
@@ -936,13 +974,12 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   }
   cplx *S = (cplx *)ctx->dS.p;
   const int64_t sz = n * ntheta * 4;
-  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, coeffs != nullptr,
-                             ncoef, S))) {
+  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, ncoef, S))) {
     return rc;
   }
   for (int p = 0; p < 3; ++p) {
     if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->dT.p + p * tt, ntheta,
-                               coeffs != nullptr, ncoef, S + (1 + p) * sz))) {
+                               ncoef, S + (1 + p) * sz))) {
       return rc;
     }
   }

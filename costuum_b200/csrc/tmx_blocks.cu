@@ -20,6 +20,8 @@
 //    B-side vectors built from j_n2(m k r); see build_chunk().
 //  * T = -RgQ Q^-1 by two triangular solves on the LU factors instead of the
 //    explicit inverse followed by a product.
+#include <algorithm>
+
 #include "tmx_blocks_common.cuh"
 
 // Build the A-side (F) and B-side (W) vectors of nodes [g0, g0 + G).
@@ -34,6 +36,88 @@
 // This is the expansion of the J11, J12, J21, J22 terms of
 // TMatrixResource.hpp:993-1097 into products of one n1 factor and one n2
 // factor per node.
+// A-side vectors (F^j, F^y) of row member a at node g, stored to f[t * ts]
+__device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
+                                       const double *__restrict__ T,
+                                       const double *__restrict__ S,
+                                       const double *__restrict__ Wg, cplx *f,
+                                       int ts) {
+  int i, n;
+  member(D, a, i, n);
+  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+  const double j = t[TMX_Q_J], dj = t[TMX_Q_DJ];
+  const double y = t[TMX_Q_Y], dy = t[TMX_Q_DY];
+  const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
+  const double d = w[0], dd = w[1];
+  const double *s = S + (int64_t)g * TMX_NS;
+  const double an = a_n(n);
+  const double nn = n * (n + 1.);
+  const double q = nn * s[TMX_NS_DRR] * s[TMX_NS_KRINV] * d;
+  f[0] = mkc(an * d * j, an * d * y);
+  f[ts] = mkc(an * dd * j, an * dd * y);
+  f[2 * ts] = mkc(an * d * dj, an * d * dy);
+  f[3 * ts] = mkc(an * (dd * dj + q * j), an * (dd * dy + q * y));
+}
+
+// B-side vectors of column member b at node g for each row group, stored to
+// w[rg * gs + t * ts] (rg = 0 rows of block index D.iA, rg = 1 rows of D.iB)
+__device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
+                                       int g, int ngroups,
+                                       const double *__restrict__ T,
+                                       const double *__restrict__ S,
+                                       const double *__restrict__ Wg, double k2,
+                                       cplx k2mr, cplx *w, int ts, int gs) {
+  int ib, n;
+  member(D, b, ib, n);
+  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+  const cplx jm = mkc(t[TMX_Q_JM_RE], t[TMX_Q_JM_IM]);
+  const cplx djm = mkc(t[TMX_Q_DJM_RE], t[TMX_Q_DJM_IM]);
+  const double *wg = Wg + ((int64_t)g * N + (n - 1)) * 2;
+  const double d = wg[0], dd = wg[1];
+  const double *s = S + (int64_t)g * TMX_NS;
+  const double an = a_n(n);
+  const double nn = n * (n + 1.);
+  const cplx kmi = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
+  const cplx G1 = cscale(djm, an * d);
+  const cplx G2 = cscale(
+      cadd(cscale(djm, dd), cscale(cmul(kmi, jm), s[TMX_NS_DRR] * nn * d)), an);
+  const cplx G3 = cscale(jm, an * d);
+  const cplx G4 = cscale(jm, an * dd);
+  const double wr2 = s[TMX_NS_W] * s[TMX_NS_R2];
+  const double mu = (double)(m * m) * s[TMX_NS_SIN2INV];
+  const double beta = s[TMX_NS_SININV] * m * wr2;
+  for (int rg = 0; rg < ngroups; ++rg) {
+    const int ia = (rg == 0) ? D.iA : D.iB;
+    cplx *wr = w + rg * gs;
+    if (ia == ib) {
+      // diagonal-type block: Q11 (i = 0) or Q22 (i = 1)
+      const cplx chi = (ia == 0) ? k2mr : mkc(k2, 0.);
+      const cplx clo = (ia == 0) ? mkc(-k2, 0.) : mkc(-k2mr.x, -k2mr.y);
+      wr[0] = cmul(chi, cscale(G1, wr2 * mu));
+      wr[ts] = cmul(chi, cscale(G2, wr2));
+      wr[2 * ts] = cmul(clo, cscale(G3, wr2 * mu));
+      wr[3 * ts] = cmul(clo, cscale(G4, wr2));
+    } else {
+      // off-diagonal block: Q12 (ia = 0, ib = 1) or Q21 (ia = 1, ib = 0)
+      const cplx c1 = (ia == 0) ? k2mr : mkc(k2, 0.);
+      const cplx c2 = (ia == 0) ? mkc(k2, 0.) : k2mr;
+      const cplx ic1 = mkc(-c1.y * beta, c1.x * beta); // i c1 beta
+      const cplx ic2 = mkc(-c2.y * beta, c2.x * beta);
+      wr[0] = cmul(ic1, G4);
+      wr[ts] = cmul(ic1, G3);
+      wr[2 * ts] = cmul(ic2, G2);
+      wr[3 * ts] = cmul(ic2, G1);
+    }
+  }
+}
+
+// zero A-side / B-side entries (padding and nodes past ngauss)
+__device__ __forceinline__ void zero_side(cplx *f, int ts, int nt) {
+  for (int t = 0; t < nt; ++t) {
+    f[t * ts] = mkc(0., 0.);
+  }
+}
+
 template <int TC>
 __device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
                             int m, int ng, int g0, const double *__restrict__ T,
@@ -47,29 +131,12 @@ __device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
     const int pr = u % L.NRp;
     const int g = g0 + gl;
     const int a = padded_member(D, pr);
-    cplx f1 = mkc(0., 0.), f2 = f1, f3 = f1, f4 = f1;
+    cplx *fp = Fs + (int64_t)(4 * gl) * L.NRp + pr;
     if (a >= 0 && g < ng) {
-      int i, n;
-      member(D, a, i, n);
-      const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
-      const double j = t[TMX_Q_J], dj = t[TMX_Q_DJ];
-      const double y = t[TMX_Q_Y], dy = t[TMX_Q_DY];
-      const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
-      const double d = w[0], dd = w[1];
-      const double *s = S + (int64_t)g * TMX_NS;
-      const double an = a_n(n);
-      const double nn = n * (n + 1.);
-      const double q = nn * s[TMX_NS_DRR] * s[TMX_NS_KRINV] * d;
-      f1 = mkc(an * d * j, an * d * y);
-      f2 = mkc(an * dd * j, an * dd * y);
-      f3 = mkc(an * d * dj, an * d * dy);
-      f4 = mkc(an * (dd * dj + q * j), an * (dd * dy + q * y));
+      a_side(D, a, N, g, T, S, Wg, fp, L.NRp);
+    } else {
+      zero_side(fp, L.NRp, 4);
     }
-    cplx *f = Fs + (int64_t)(4 * gl) * L.NRp + pr;
-    f[0] = f1;
-    f[L.NRp] = f2;
-    f[2 * L.NRp] = f3;
-    f[3 * L.NRp] = f4;
   }
   // B side
   const int ncolp = L.CT * TC;
@@ -77,60 +144,14 @@ __device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
     const int gl = u / ncolp;
     const int b = u % ncolp;
     const int g = g0 + gl;
-    cplx w1[2], w2[2], w3[2], w4[2];
-    for (int rg = 0; rg < 2; ++rg) {
-      w1[rg] = w2[rg] = w3[rg] = w4[rg] = mkc(0., 0.);
-    }
+    cplx *wp = Ws + (int64_t)(4 * gl) * ncolp + b;
+    const int gs = 4 * G * ncolp;
     if (b < D.nb && g < ng) {
-      int ib, n;
-      member(D, b, ib, n);
-      const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
-      const cplx jm = mkc(t[TMX_Q_JM_RE], t[TMX_Q_JM_IM]);
-      const cplx djm = mkc(t[TMX_Q_DJM_RE], t[TMX_Q_DJM_IM]);
-      const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
-      const double d = w[0], dd = w[1];
-      const double *s = S + (int64_t)g * TMX_NS;
-      const double an = a_n(n);
-      const double nn = n * (n + 1.);
-      const cplx kmi = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
-      const cplx G1 = cscale(djm, an * d);
-      const cplx G2 = cscale(
-          cadd(cscale(djm, dd), cscale(cmul(kmi, jm), s[TMX_NS_DRR] * nn * d)),
-          an);
-      const cplx G3 = cscale(jm, an * d);
-      const cplx G4 = cscale(jm, an * dd);
-      const double wr2 = s[TMX_NS_W] * s[TMX_NS_R2];
-      const double mu = (double)(m * m) * s[TMX_NS_SIN2INV];
-      const double beta = s[TMX_NS_SININV] * m * wr2;
+      b_side(D, b, N, m, g, L.ngroups, T, S, Wg, k2, k2mr, wp, ncolp, gs);
+    } else {
       for (int rg = 0; rg < L.ngroups; ++rg) {
-        const int ia = (rg == 0) ? D.iA : D.iB;
-        if (ia == ib) {
-          // diagonal-type block: Q11 (i = 0) or Q22 (i = 1)
-          const cplx chi = (ia == 0) ? k2mr : mkc(k2, 0.);
-          const cplx clo = (ia == 0) ? mkc(-k2, 0.) : mkc(-k2mr.x, -k2mr.y);
-          w1[rg] = cmul(chi, cscale(G1, wr2 * mu));
-          w2[rg] = cmul(chi, cscale(G2, wr2));
-          w3[rg] = cmul(clo, cscale(G3, wr2 * mu));
-          w4[rg] = cmul(clo, cscale(G4, wr2));
-        } else {
-          // off-diagonal block: Q12 (ia = 0, ib = 1) or Q21 (ia = 1, ib = 0)
-          const cplx c1 = (ia == 0) ? k2mr : mkc(k2, 0.);
-          const cplx c2 = (ia == 0) ? mkc(k2, 0.) : k2mr;
-          const cplx ic1 = mkc(-c1.y * beta, c1.x * beta); // i c1 beta
-          const cplx ic2 = mkc(-c2.y * beta, c2.x * beta);
-          w1[rg] = cmul(ic1, G4);
-          w2[rg] = cmul(ic1, G3);
-          w3[rg] = cmul(ic2, G2);
-          w4[rg] = cmul(ic2, G1);
-        }
+        zero_side(wp + rg * gs, ncolp, 4);
       }
-    }
-    for (int rg = 0; rg < L.ngroups; ++rg) {
-      cplx *wp = Ws + ((int64_t)rg * 4 * G + 4 * gl) * ncolp + b;
-      wp[0] = w1[rg];
-      wp[ncolp] = w2[rg];
-      wp[2 * ncolp] = w3[rg];
-      wp[3 * ncolp] = w4[rg];
     }
   }
 }
@@ -414,6 +435,271 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+// ------------------------------------------------- warp-per-item variant --
+//
+// Classes of at most 16 members (nearly every item of grains up to order 32)
+// are too small for a CTA: one warp owns one item from assembly to write-out
+// and synchronises with __syncwarp only, so four independent items share a
+// CTA. Assembly: lane (rt, ct) = (lane / 4, lane % 4) accumulates rows
+// rt * TR .. rt * TR + TR - 1 and columns ct, ct + 4, .. of the class matrix
+// over warp-private chunks of WG nodes. LU: lane r updates row r; the pivot
+// column's maximum is a shuffle reduction (first maximum wins, as
+// in Matrix::plu_inverse) and the factors stay in warp-private shared
+// memory. Solve: lane r owns row r of -RgQ_c and runs both triangular solves
+// on it against the factors, so no lane waits on another.
+
+#define TMX_WG 4 // quadrature nodes per warp chunk
+
+template <int NBM>
+__host__ __device__ constexpr int warp_elems() {
+  // chunk buffers F[WG][4][NBM] + W[2][WG][4][NBM]; the LU phase reuses them
+  // for Q, RgQ ([NBM][NBM + 1] each), 1/U_jj and the pivot/gather indices
+  return 12 * TMX_WG * NBM;
+}
+
+template <int TR, int TC, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    k_blocks_warp(TmxBlockArgs A) {
+  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  constexpr int LD = NBM + 1;
+  static_assert(2 * NBM * LD + 2 * NBM <= warp_elems<NBM>(), "warp smem");
+  extern __shared__ __align__(16) unsigned char tmx_wsmem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  cplx *base = reinterpret_cast<cplx *>(tmx_wsmem) + wib * warp_elems<NBM>();
+  cplx *Fs = base;                      // [WG][4][NBM]
+  cplx *Ws = Fs + TMX_WG * 4 * NBM;     // [2][WG][4][NBM]
+  cplx *Qm = base;                      // [NBM][LD]  (after the assembly)
+  cplx *Rm = Qm + NBM * LD;             // [NBM][LD]
+  cplx *uinv = Rm + NBM * LD;           // [NBM]
+  int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
+  int *piv = perm + NBM;                           // [NBM]
+  const int rt = lane >> 2;
+  const int ct = lane & 3;
+  for (int it = blockIdx.x * 4 + wib; it < A.nitems; it += gridDim.x * 4) {
+    const TmxItem item = A.items[it];
+    const TmxSlot sl = A.slots[item.slot];
+    const TmxGrain Gr = A.grains[sl.grain];
+    const int N = sl.nmax;
+    const int ng = sl.ngauss;
+    const int m = item.m;
+    const ClassDesc D = describe<1>(N, m, item.cls);
+    const int nb = D.nb;
+    if (nb <= 0) {
+      continue;
+    }
+    if (nb > NBM) {
+      if (lane == 0) {
+        atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
+      }
+      continue;
+    }
+    const double *T = A.tab + sl.tab;
+    const double *S = A.nsc + sl.nsc;
+    const double *Wg = A.wig + A.wig_off[sl.wig_n] + (int64_t)m * ng * N * 2;
+    const double k2 = Gr.k * Gr.k;
+    const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
+    const int ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
+    const int tstep = (m == 0) ? 2 : 1; // m = 0: mu = 0 kills t = 0, 2
+    const int t0 = (m == 0) ? 1 : 0;
+
+    // ---------------------------------------------------------- assembly
+    double aj[TR][TC][2], ay[TR][TC][2];
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        aj[r][c][0] = aj[r][c][1] = ay[r][c][0] = ay[r][c][1] = 0.;
+      }
+    }
+    int rgr[TR];
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+      rgr[r] = (rt * TR + r < D.R0) ? 0 : 1;
+    }
+    for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
+      __syncwarp();
+      for (int u = lane; u < TMX_WG * nb; u += 32) {
+        const int gl = u / nb;
+        const int a = u - gl * nb;
+        cplx *fp = Fs + gl * 4 * NBM + a;
+        cplx *wp = Ws + gl * 4 * NBM + a;
+        if (g0 + gl < ng) {
+          a_side(D, a, N, g0 + gl, T, S, Wg, fp, NBM);
+          b_side(D, a, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
+                 TMX_WG * 4 * NBM);
+        } else {
+          zero_side(fp, NBM, 4);
+          for (int rg = 0; rg < ngroups; ++rg) {
+            zero_side(wp + rg * TMX_WG * 4 * NBM, NBM, 4);
+          }
+        }
+      }
+      __syncwarp();
+      const int gmax = min(TMX_WG, ng - g0);
+      for (int gl = 0; gl < gmax; ++gl) {
+        for (int t = t0; t < 4; t += tstep) {
+          const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
+          const cplx *w0 = Ws + (gl * 4 + t) * NBM + ct;
+#pragma unroll
+          for (int r = 0; r < TR; ++r) {
+            const cplx f = fr[r];
+            const cplx *wr = w0 + rgr[r] * (TMX_WG * 4 * NBM);
+#pragma unroll
+            for (int c = 0; c < TC; ++c) {
+              const cplx w = wr[4 * c];
+              aj[r][c][0] = fma(f.x, w.x, aj[r][c][0]);
+              aj[r][c][1] = fma(f.x, w.y, aj[r][c][1]);
+              ay[r][c][0] = fma(f.y, w.x, ay[r][c][0]);
+              ay[r][c][1] = fma(f.y, w.y, ay[r][c][1]);
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // Q = G^j + i G^y, RgQ = G^j, into the (reused) chunk buffers
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+      const int a = rt * TR + r;
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        const int b = ct + 4 * c;
+        if (a < nb && b < nb) {
+          Qm[a * LD + b] = mkc(aj[r][c][0] - ay[r][c][1], aj[r][c][1] + ay[r][c][0]);
+          Rm[a * LD + b] = mkc(aj[r][c][0], aj[r][c][1]);
+        }
+      }
+    }
+    __syncwarp();
+
+    // ---------------------------------------------------------------- LU
+    // in place in Qm; lane r updates row r
+    bool singular = false;
+    for (int i = 0; i < nb; ++i) {
+      // pivot: first row r >= i with the largest |Q_ri|
+      double best = (lane >= i && lane < nb) ? cabs_dev(Qm[lane * LD + i]) : -1.;
+      int bi = lane;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) {
+          best = ov;
+          bi = oi;
+        }
+      }
+      singular = singular || !(best > 0.);
+      if (lane == 0) {
+        piv[i] = bi;
+      }
+      if (bi != i) {
+        for (int k = lane; k < nb; k += 32) {
+          const cplx t = Qm[i * LD + k];
+          Qm[i * LD + k] = Qm[bi * LD + k];
+          Qm[bi * LD + k] = t;
+        }
+      }
+      __syncwarp();
+      if (lane > i && lane < nb) {
+        const cplx pinv = cinv(Qm[i * LD + i]);
+        const cplx l = cmul(Qm[lane * LD + i], pinv);
+        Qm[lane * LD + i] = l;
+        for (int k = i + 1; k < nb; ++k) {
+          Qm[lane * LD + k] = csub(Qm[lane * LD + k], cmul(l, Qm[i * LD + k]));
+        }
+      }
+      __syncwarp();
+    }
+    if (lane < nb) {
+      uinv[lane] = cinv(Qm[lane * LD + lane]);
+    }
+    if (lane == 0) {
+      // column exchanges of Matrix::plu_inverse step 4, as a gather index
+      for (int j = 0; j < nb; ++j) {
+        perm[j] = j;
+      }
+      for (int j = nb - 1; j >= 0; --j) {
+        const int p = piv[j];
+        const int t = perm[j];
+        perm[j] = perm[p];
+        perm[p] = t;
+      }
+      if (singular) {
+        atomicOr(&A.status[sl.grain], TMX_ST_SINGULAR);
+      }
+    }
+    __syncwarp();
+    if (A.lu) {
+      cplx *Ls = A.lu + item.scratch;
+      for (int u = lane; u < nb * nb; u += 32) {
+        Ls[u] = Qm[(u / nb) * LD + (u % nb)];
+      }
+      int *ps = reinterpret_cast<int *>(Ls + (int64_t)nb * nb);
+      for (int j = lane; j < nb; j += 32) {
+        ps[j] = perm[j];
+      }
+    }
+
+    // ------------------------------------------ solve T_c Q_c = -RgQ_c
+    // lane r solves row r of -RgQ_c in place in Rm
+    if (lane < nb) {
+      cplx *x = Rm + lane * LD;
+      for (int k = 0; k < nb; ++k) {
+        x[k] = mkc(-x[k].x, -x[k].y);
+      }
+      // Z U = X (forward over columns)
+      for (int j = 0; j < nb; ++j) {
+        const cplx xj = cmul(x[j], uinv[j]);
+        x[j] = xj;
+        for (int k = j + 1; k < nb; ++k) {
+          x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
+        }
+      }
+      // Y L = Z (backward over columns, L unit lower)
+      for (int j = nb - 1; j >= 1; --j) {
+        const cplx xj = x[j];
+        for (int k = 0; k < j; ++k) {
+          x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
+        }
+      }
+    }
+    __syncwarp();
+    // write out: T_c[a][b] = Y[a][perm[b]]
+    if (sl.tout < 0) {
+      if (lane < nb) {
+        int ia, na;
+        member(D, lane, ia, na);
+        A.diag[sl.diag + ia * N + (na - 1)] = Rm[lane * LD + perm[lane]];
+      }
+    } else {
+      cplx *Tb = A.tout + sl.tout + block_offset(N, m);
+      const int w2 = 2 * D.nbb;
+      for (int u = lane; u < nb * nb; u += 32) {
+        const int a = u / nb;
+        const int b = u - a * nb;
+        int ia, na, ib, nbn;
+        member(D, a, ia, na);
+        member(D, b, ib, nbn);
+        const int rowi = ia * D.nbb + (na - D.nmin);
+        const int col = ib * D.nbb + (nbn - D.nmin);
+        Tb[(int64_t)rowi * w2 + col] = Rm[a * LD + perm[b]];
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <int TR, int TC, int MINB>
+static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
+  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  const size_t smem = (size_t)4 * warp_elems<NBM>() * sizeof(cplx);
+  cudaFuncSetAttribute(k_blocks_warp<TR, TC, MINB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (int)std::min<int64_t>((a.nitems + 3) / 4, 148 * 16);
+  k_blocks_warp<TR, TC, MINB><<<blocks, 128, smem, stream>>>(a);
+}
+
 // shared memory of one block: the larger of the assembly chunk buffers and
 // the LU phase (factors, pivots and a right-hand-side chunk)
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
@@ -456,10 +742,16 @@ void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
   if (a.nitems <= 0) {
     return;
   }
-  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
+  if (a.max_nb <= 8) {
+    launch_warp_variant<1, 2, 4>(a, stream);
+    return;
+  }
   if (a.max_nb <= 16) {
-    launch_variant<2, 2, 64, 8>(a, smem, stream);
-  } else if (a.max_nb <= 32) {
+    launch_warp_variant<2, 4, 3>(a, stream);
+    return;
+  }
+  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
+  if (a.max_nb <= 32) {
     launch_variant<2, 4, 128, 4>(a, smem, stream);
   } else {
     launch_variant<4, 4, 256, 1>(a, smem, stream);

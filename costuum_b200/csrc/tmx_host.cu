@@ -424,12 +424,32 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
   for (int s = 0; s < np2; ++s) {
     slots[s].wig_n = full_sets[key_idx[std::make_pair(slots[s].nmax, slots[s].ngauss)]];
   }
-  // items, bucketed by class size (largest first)
-  struct HItem {
-    int nb;
-    TmxItem it;
-  };
-  std::vector<HItem> hitems;
+  // items, ordered by class size (largest first; a counting sort, stable in
+  // (slot, m, class) order)
+  std::vector<int64_t> cnt(TMX_MAX_NB + 2, 0);
+  int64_t nitems = 0;
+  for (int s = 0; s < np2; ++s) {
+    const int N = slots[s].nmax;
+    for (int m = 0; m <= N; ++m) {
+      const int ncls = (m == 0) ? 4 : 2;
+      for (int c = 0; c < ncls; ++c) {
+        const int nb = tmx_host_class_size(N, m, c);
+        if (nb > 0) {
+          cnt[std::min(nb, TMX_MAX_NB + 1)] += 1;
+          ++nitems;
+        }
+      }
+    }
+  }
+  std::vector<int64_t> pos(TMX_MAX_NB + 2, 0);
+  for (int nb = TMX_MAX_NB + 1, acc = 0; nb >= 1; --nb) {
+    pos[nb] = acc;
+    acc += (int)cnt[nb];
+  }
+  std::vector<TmxItem> &items = ctx->p2_items;
+  std::vector<int> &inb = ctx->p2_nb;
+  items.resize(nitems);
+  inb.resize(nitems);
   for (int s = 0; s < np2; ++s) {
     const int N = slots[s].nmax;
     for (int m = 0; m <= N; ++m) {
@@ -439,29 +459,19 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
         if (nb <= 0) {
           continue;
         }
-        HItem h;
-        h.nb = nb;
-        h.it.slot = s;
-        h.it.m = (int16_t)m;
-        h.it.cls = (int16_t)c;
-        h.it.scratch = 0;
-        hitems.push_back(h);
+        const int64_t i = pos[std::min(nb, TMX_MAX_NB + 1)]++;
+        items[i].slot = s;
+        items[i].m = (int16_t)m;
+        items[i].cls = (int16_t)c;
+        inb[i] = nb;
       }
     }
   }
-  std::stable_sort(hitems.begin(), hitems.end(),
-                   [](const HItem &a, const HItem &b) { return a.nb > b.nb; });
   ctx->p2_slots = slots;
-  ctx->p2_items.resize(hitems.size());
-  ctx->p2_nb.resize(hitems.size());
-  std::vector<TmxItem> items(hitems.size());
   int64_t scr_total = 0;
-  for (size_t i = 0; i < hitems.size(); ++i) {
-    items[i] = hitems[i].it;
+  for (int64_t i = 0; i < nitems; ++i) {
     items[i].scratch = scr_total;
-    ctx->p2_items[i] = items[i];
-    ctx->p2_nb[i] = hitems[i].nb;
-    scr_total += 2 * (int64_t)hitems[i].nb * hitems[i].nb;
+    scr_total += 2 * (int64_t)inb[i] * inb[i];
   }
   ctx->p2_scr_total = scr_total;
   ctx->p2_t_total = t_total;
@@ -470,7 +480,7 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
       (rc = ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->slots, std::max(1, np2) * sizeof(TmxSlot))) ||
-      (rc = ensure(ctx, ctx->items, std::max<size_t>(1, items.size()) * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->items, std::max<int64_t>(1, nitems) * sizeof(TmxItem))) ||
       (rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
@@ -479,7 +489,7 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
   if (np2 > 0) {
     CK(cudaMemcpyAsync(ctx->slots.p, slots.data(), np2 * sizeof(TmxSlot),
                        cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(TmxItem),
+    CK(cudaMemcpyAsync(ctx->items.p, items.data(), nitems * sizeof(TmxItem),
                        cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->T.p, 0, t_total * sizeof(cplx), st));
     cudaEvent_t pe = nullptr;
@@ -496,11 +506,11 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
       return rc;
     }
     // buckets by class size
-    const int edges[] = {128, 64, 32, 16, 0};
-    size_t i0 = 0;
+    const int edges[] = {1 << 30, 64, 32, 16, 0};
+    int64_t i0 = 0;
     for (int b = 0; b < 4; ++b) {
-      size_t i1 = i0;
-      while (i1 < hitems.size() && hitems[i1].nb > edges[b + 1]) {
+      int64_t i1 = i0;
+      while (i1 < nitems && inb[i1] > edges[b + 1]) {
         ++i1;
       }
       if (i1 > i0) {
@@ -517,12 +527,13 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
         B.tout = (cplx *)ctx->T.p;
         B.diag = nullptr;
         B.status = (int32_t *)ctx->status.p;
-        B.max_nb = hitems[i0].nb;
+        B.max_nb = inb[i0];
         B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
         double fl = 0.;
-        for (size_t q = i0; q < i1; ++q) {
-          fl += item_flops(hitems[q].nb, hitems[q].it.m,
-                           slots[hitems[q].it.slot].ngauss);
+        if (ctx->profiling) {
+          for (int64_t q = i0; q < i1; ++q) {
+            fl += item_flops(inb[q], items[q].m, slots[items[q].slot].ngauss);
+          }
         }
         if ((rc = prof_begin(ctx, 0, &pe))) {
           return rc;
@@ -564,7 +575,7 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
   }
   // survey-model flops (per grain: every order of the m = 0 chain on the
   // unreduced 2k x 2k block, then every m >= 1 block on 2nm x 2nm)
-  for (int64_t i = 0; i < n; ++i) {
+  for (int64_t i = 0; ctx->profiling && i < n; ++i) {
     const int N = ctx->nmax_h[i];
     if (N <= 0) {
       continue;

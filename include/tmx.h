@@ -139,7 +139,8 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
                      double *flops);
 
 /* FP64 flops of the last batch counted with the unreduced per-grain model
- * (every chain order and every m block as a full 2nb x 2nb LU + solve). */
+ * (every chain order and every m block as a full 2nb x 2nb LU + solve);
+ * counted only for batches computed while profiling is enabled, else 0. */
 double tmx_batch_flops_survey(const tmx_ctx *ctx);
 
 /* ------------------------------------------------ averaged observables ---

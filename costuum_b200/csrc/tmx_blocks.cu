@@ -483,12 +483,12 @@ __global__ void __launch_bounds__(128, MINB)
     const int N = sl.nmax;
     const int ng = sl.ngauss;
     const int m = item.m;
-    const ClassDesc D = describe<1>(N, m, item.cls);
+    const ClassDesc D = describe<TR>(N, m, item.cls);
     const int nb = D.nb;
     if (nb <= 0) {
       continue;
     }
-    if (nb > NBM) {
+    if (nb > NBM || D.NRp > NBM) {
       if (lane == 0) {
         atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
       }
@@ -512,26 +512,32 @@ __global__ void __launch_bounds__(128, MINB)
         aj[r][c][0] = aj[r][c][1] = ay[r][c][0] = ay[r][c][1] = 0.;
       }
     }
-    int rgr[TR];
-#pragma unroll
-    for (int r = 0; r < TR; ++r) {
-      rgr[r] = (rt * TR + r < D.R0) ? 0 : 1;
-    }
+    // rows are padded per group to a multiple of TR (describe<TR>), so the
+    // TR rows of a lane share one row group and one set of B-side vectors
+    const int rgl = (rt * TR < D.R0p) ? 0 : 1;
     for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
       __syncwarp();
-      for (int u = lane; u < TMX_WG * nb; u += 32) {
-        const int gl = u / nb;
-        const int a = u - gl * nb;
-        cplx *fp = Fs + gl * 4 * NBM + a;
-        cplx *wp = Ws + gl * 4 * NBM + a;
-        if (g0 + gl < ng) {
+      for (int u = lane; u < TMX_WG * D.NRp; u += 32) {
+        const int gl = u / D.NRp;
+        const int pr = u - gl * D.NRp;
+        const int a = padded_member(D, pr);
+        cplx *fp = Fs + gl * 4 * NBM + pr;
+        if (a >= 0 && g0 + gl < ng) {
           a_side(D, a, N, g0 + gl, T, S, Wg, fp, NBM);
-          b_side(D, a, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
-                 TMX_WG * 4 * NBM);
         } else {
           zero_side(fp, NBM, 4);
-          for (int rg = 0; rg < ngroups; ++rg) {
-            zero_side(wp + rg * TMX_WG * 4 * NBM, NBM, 4);
+        }
+      }
+      for (int u = lane; u < TMX_WG * nb; u += 32) {
+        const int gl = u / nb;
+        const int b = u - gl * nb;
+        cplx *wp = Ws + gl * 4 * NBM + b;
+        if (g0 + gl < ng) {
+          b_side(D, b, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
+                 TMX_WG * 4 * NBM);
+        } else {
+          for (int q = 0; q < ngroups; ++q) {
+            zero_side(wp + q * TMX_WG * 4 * NBM, NBM, 4);
           }
         }
       }
@@ -540,18 +546,21 @@ __global__ void __launch_bounds__(128, MINB)
       for (int gl = 0; gl < gmax; ++gl) {
         for (int t = t0; t < 4; t += tstep) {
           const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
-          const cplx *w0 = Ws + (gl * 4 + t) * NBM + ct;
+          const cplx *wr = Ws + (rgl * TMX_WG * 4 + gl * 4 + t) * NBM + ct;
+          cplx w[TC];
+#pragma unroll
+          for (int c = 0; c < TC; ++c) {
+            w[c] = wr[4 * c];
+          }
 #pragma unroll
           for (int r = 0; r < TR; ++r) {
             const cplx f = fr[r];
-            const cplx *wr = w0 + rgr[r] * (TMX_WG * 4 * NBM);
 #pragma unroll
             for (int c = 0; c < TC; ++c) {
-              const cplx w = wr[4 * c];
-              aj[r][c][0] = fma(f.x, w.x, aj[r][c][0]);
-              aj[r][c][1] = fma(f.x, w.y, aj[r][c][1]);
-              ay[r][c][0] = fma(f.y, w.x, ay[r][c][0]);
-              ay[r][c][1] = fma(f.y, w.y, ay[r][c][1]);
+              aj[r][c][0] = fma(f.x, w[c].x, aj[r][c][0]);
+              aj[r][c][1] = fma(f.x, w[c].y, aj[r][c][1]);
+              ay[r][c][0] = fma(f.y, w[c].x, ay[r][c][0]);
+              ay[r][c][1] = fma(f.y, w[c].y, ay[r][c][1]);
             }
           }
         }
@@ -561,11 +570,11 @@ __global__ void __launch_bounds__(128, MINB)
     // Q = G^j + i G^y, RgQ = G^j, into the (reused) chunk buffers
 #pragma unroll
     for (int r = 0; r < TR; ++r) {
-      const int a = rt * TR + r;
+      const int a = padded_member(D, rt * TR + r);
 #pragma unroll
       for (int c = 0; c < TC; ++c) {
         const int b = ct + 4 * c;
-        if (a < nb && b < nb) {
+        if (a >= 0 && b < nb) {
           Qm[a * LD + b] = mkc(aj[r][c][0] - ay[r][c][1], aj[r][c][1] + ay[r][c][0]);
           Rm[a * LD + b] = mkc(aj[r][c][0], aj[r][c][1]);
         }

@@ -506,9 +506,10 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
       return rc;
     }
     // buckets by class size
-    const int edges[] = {1 << 30, 64, 32, 16, 0};
+    // class-size buckets, one launch each (largest first)
+    const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
     int64_t i0 = 0;
-    for (int b = 0; b < 4; ++b) {
+    for (int b = 0; b < 5; ++b) {
       int64_t i1 = i0;
       while (i1 < nitems && inb[i1] > edges[b + 1]) {
         ++i1;

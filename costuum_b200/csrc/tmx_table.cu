@@ -918,9 +918,9 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
     CK(cudaMemsetAsync(ctx->dT.p, 0, 3 * tt * sizeof(cplx), st));
     // forward blocks again, now keeping the LU factors, then the tangents;
     // both in the class-size buckets of the forward schedule
-    const int edges[] = {128, 64, 32, 16, 0};
+    const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
     int64_t i0 = 0;
-    for (int b = 0; b < 4; ++b) {
+    for (int b = 0; b < 5; ++b) {
       int64_t i1 = i0;
       while (i1 < nitems && ctx->p2_nb[i1] > edges[b + 1]) {
         ++i1;

@@ -36,12 +36,15 @@
 // This is the expansion of the J11, J12, J21, J22 terms of
 // TMatrixResource.hpp:993-1097 into products of one n1 factor and one n2
 // factor per node.
-// A-side vectors (F^j, F^y) of row member a at node g, stored to f[t * ts]
+// A-side vectors (F^j, F^y) of row member a at node g, stored to f[t * ts].
+// LEAN: without the factor a_n (the caller scales the finished entries by
+// a_n1 a_n2) and, for m = 0, only the terms 1 and 3 that survive mu = 0.
+template <bool LEAN = false>
 __device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
                                        const double *__restrict__ T,
                                        const double *__restrict__ S,
                                        const double *__restrict__ Wg, cplx *f,
-                                       int ts) {
+                                       int ts, int m = 1) {
   int i, n;
   member(D, a, i, n);
   const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
@@ -50,9 +53,18 @@ __device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
   const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
   const double d = w[0], dd = w[1];
   const double *s = S + (int64_t)g * TMX_NS;
-  const double an = a_n(n);
   const double nn = n * (n + 1.);
   const double q = nn * s[TMX_NS_DRR] * s[TMX_NS_KRINV] * d;
+  if (LEAN) {
+    if (m != 0) {
+      f[0] = mkc(d * j, d * y);
+      f[2 * ts] = mkc(d * dj, d * dy);
+    }
+    f[ts] = mkc(dd * j, dd * y);
+    f[3 * ts] = mkc(dd * dj + q * j, dd * dy + q * y);
+    return;
+  }
+  const double an = a_n(n);
   f[0] = mkc(an * d * j, an * d * y);
   f[ts] = mkc(an * dd * j, an * dd * y);
   f[2 * ts] = mkc(an * d * dj, an * d * dy);
@@ -60,7 +72,9 @@ __device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
 }
 
 // B-side vectors of column member b at node g for each row group, stored to
-// w[rg * gs + t * ts] (rg = 0 rows of block index D.iA, rg = 1 rows of D.iB)
+// w[rg * gs + t * ts] (rg = 0 rows of block index D.iA, rg = 1 rows of D.iB).
+// LEAN as for a_side.
+template <bool LEAN = false>
 __device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
                                        int g, int ngroups,
                                        const double *__restrict__ T,
@@ -75,7 +89,7 @@ __device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
   const double *wg = Wg + ((int64_t)g * N + (n - 1)) * 2;
   const double d = wg[0], dd = wg[1];
   const double *s = S + (int64_t)g * TMX_NS;
-  const double an = a_n(n);
+  const double an = LEAN ? 1. : a_n(n);
   const double nn = n * (n + 1.);
   const cplx kmi = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
   const cplx G1 = cscale(djm, an * d);
@@ -93,9 +107,11 @@ __device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
       // diagonal-type block: Q11 (i = 0) or Q22 (i = 1)
       const cplx chi = (ia == 0) ? k2mr : mkc(k2, 0.);
       const cplx clo = (ia == 0) ? mkc(-k2, 0.) : mkc(-k2mr.x, -k2mr.y);
-      wr[0] = cmul(chi, cscale(G1, wr2 * mu));
+      if (!LEAN || m != 0) {
+        wr[0] = cmul(chi, cscale(G1, wr2 * mu));
+        wr[2 * ts] = cmul(clo, cscale(G3, wr2 * mu));
+      }
       wr[ts] = cmul(chi, cscale(G2, wr2));
-      wr[2 * ts] = cmul(clo, cscale(G3, wr2 * mu));
       wr[3 * ts] = cmul(clo, cscale(G4, wr2));
     } else {
       // off-diagonal block: Q12 (ia = 0, ib = 1) or Q21 (ia = 1, ib = 0)
@@ -457,10 +473,20 @@ __host__ __device__ constexpr int warp_elems() {
   return 12 * TMX_WG * NBM;
 }
 
-template <int TR, int TC, int MINB>
+// D += A B for one m8n8k4 FP64 tensor-core tile: lane l holds A[l / 4][l % 4],
+// B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}]
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, "
+      "{%0, %1};\n"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
+
+template <int TR, int TC, int MINB, bool MMA>
 __global__ void __launch_bounds__(128, MINB)
     k_blocks_warp(TmxBlockArgs A) {
-  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  constexpr int NBM = MMA ? 16 : ((8 * TR > 4 * TC) ? 8 * TR : 4 * TC);
+  constexpr int PR = MMA ? 1 : TR; // row padding unit of the class rows
   constexpr int LD = NBM + 1;
   static_assert(2 * NBM * LD + 2 * NBM <= warp_elems<NBM>(), "warp smem");
   extern __shared__ __align__(16) unsigned char tmx_wsmem[];
@@ -483,7 +509,7 @@ __global__ void __launch_bounds__(128, MINB)
     const int N = sl.nmax;
     const int ng = sl.ngauss;
     const int m = item.m;
-    const ClassDesc D = describe<TR>(N, m, item.cls);
+    const ClassDesc D = describe<PR>(N, m, item.cls);
     const int nb = D.nb;
     if (nb <= 0) {
       continue;
@@ -504,7 +530,10 @@ __global__ void __launch_bounds__(128, MINB)
     const int t0 = (m == 0) ? 1 : 0;
 
     // ---------------------------------------------------------- assembly
+    // DFMA path: aj/ay[TR][TC]; tensor path: acc[row tile][col tile][jr, ji,
+    // yr, yi] as m8n8 accumulator fragments
     double aj[TR][TC][2], ay[TR][TC][2];
+    double acc[2][2][4][2];
 #pragma unroll
     for (int r = 0; r < TR; ++r) {
 #pragma unroll
@@ -512,28 +541,40 @@ __global__ void __launch_bounds__(128, MINB)
         aj[r][c][0] = aj[r][c][1] = ay[r][c][0] = ay[r][c][1] = 0.;
       }
     }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          acc[r][c][p][0] = acc[r][c][p][1] = 0.;
+        }
+      }
+    }
     // rows are padded per group to a multiple of TR (describe<TR>), so the
     // TR rows of a lane share one row group and one set of B-side vectors
     const int rgl = (rt * TR < D.R0p) ? 0 : 1;
     for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
       __syncwarp();
+#pragma unroll 1
       for (int u = lane; u < TMX_WG * D.NRp; u += 32) {
         const int gl = u / D.NRp;
         const int pr = u - gl * D.NRp;
         const int a = padded_member(D, pr);
         cplx *fp = Fs + gl * 4 * NBM + pr;
         if (a >= 0 && g0 + gl < ng) {
-          a_side(D, a, N, g0 + gl, T, S, Wg, fp, NBM);
+          a_side<true>(D, a, N, g0 + gl, T, S, Wg, fp, NBM, m);
         } else {
           zero_side(fp, NBM, 4);
         }
       }
+#pragma unroll 1
       for (int u = lane; u < TMX_WG * nb; u += 32) {
         const int gl = u / nb;
         const int b = u - gl * nb;
         cplx *wp = Ws + gl * 4 * NBM + b;
         if (g0 + gl < ng) {
-          b_side(D, b, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
+          b_side<true>(D, b, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
                  TMX_WG * 4 * NBM);
         } else {
           for (int q = 0; q < ngroups; ++q) {
@@ -543,24 +584,68 @@ __global__ void __launch_bounds__(128, MINB)
       }
       __syncwarp();
       const int gmax = min(TMX_WG, ng - g0);
-      for (int gl = 0; gl < gmax; ++gl) {
-        for (int t = t0; t < 4; t += tstep) {
-          const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
-          const cplx *wr = Ws + (rgl * TMX_WG * 4 + gl * 4 + t) * NBM + ct;
-          cplx w[TC];
+      if constexpr (MMA) {
+        // K slices of 4: the four terms of one node (m >= 1), or terms 1 and
+        // 3 of two nodes (m = 0, where terms 0 and 2 vanish)
+        const int q = lane & 3;
+        const int rr = lane >> 2;
+        const int nrt = (nb + 7) >> 3;
+        const int nsl = (m == 0) ? (gmax + 1) >> 1 : gmax;
+        for (int sx = 0; sx < nsl; ++sx) {
+          const int gl = (m == 0) ? 2 * sx + (q >> 1) : sx;
+          const int t = (m == 0) ? 1 + 2 * (q & 1) : q;
 #pragma unroll
-          for (int c = 0; c < TC; ++c) {
-            w[c] = wr[4 * c];
+          for (int rti = 0; rti < 2; ++rti) {
+            if (rti < nrt) {
+              const int row = rti * 8 + rr;
+              const cplx f = (row < nb) ? Fs[(gl * 4 + t) * NBM + row] : mkc(0., 0.);
+              const int grp = (row < D.R0) ? 0 : 1;
+              const int lo = rti * 8, hi = min(rti * 8 + 8, nb);
+#pragma unroll
+              for (int g = 0; g < 2; ++g) {
+                const bool present = (g == 0) ? (lo < D.R0) : (ngroups == 2 && hi > D.R0);
+                if (present) {
+                  const double fj = (grp == g) ? f.x : 0.;
+                  const double fy = (grp == g) ? f.y : 0.;
+#pragma unroll
+                  for (int cti = 0; cti < 2; ++cti) {
+                    if (cti < nrt) {
+                      const int col = cti * 8 + rr;
+                      const cplx w = (col < nb)
+                          ? Ws[((g * TMX_WG + gl) * 4 + t) * NBM + col]
+                          : mkc(0., 0.);
+                      double *a4 = &acc[rti][cti][0][0];
+                      dmma(a4[0], a4[1], fj, w.x); // jr
+                      dmma(a4[2], a4[3], fj, w.y); // ji
+                      dmma(a4[4], a4[5], fy, w.x); // yr
+                      dmma(a4[6], a4[7], fy, w.y); // yi
+                    }
+                  }
+                }
+              }
+            }
           }
-#pragma unroll
-          for (int r = 0; r < TR; ++r) {
-            const cplx f = fr[r];
+        }
+      } else {
+        for (int gl = 0; gl < gmax; ++gl) {
+          for (int t = t0; t < 4; t += tstep) {
+            const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
+            const cplx *wr = Ws + (rgl * TMX_WG * 4 + gl * 4 + t) * NBM + ct;
+            cplx w[TC];
 #pragma unroll
             for (int c = 0; c < TC; ++c) {
-              aj[r][c][0] = fma(f.x, w[c].x, aj[r][c][0]);
-              aj[r][c][1] = fma(f.x, w[c].y, aj[r][c][1]);
-              ay[r][c][0] = fma(f.y, w[c].x, ay[r][c][0]);
-              ay[r][c][1] = fma(f.y, w[c].y, ay[r][c][1]);
+              w[c] = wr[4 * c];
+            }
+#pragma unroll
+            for (int r = 0; r < TR; ++r) {
+              const cplx f = fr[r];
+#pragma unroll
+              for (int c = 0; c < TC; ++c) {
+                aj[r][c][0] = fma(f.x, w[c].x, aj[r][c][0]);
+                aj[r][c][1] = fma(f.x, w[c].y, aj[r][c][1]);
+                ay[r][c][0] = fma(f.y, w[c].x, ay[r][c][0]);
+                ay[r][c][1] = fma(f.y, w[c].y, ay[r][c][1]);
+              }
             }
           }
         }
@@ -568,15 +653,46 @@ __global__ void __launch_bounds__(128, MINB)
     }
     __syncwarp();
     // Q = G^j + i G^y, RgQ = G^j, into the (reused) chunk buffers
+    if constexpr (MMA) {
+      const int rr = lane >> 2;
+      const int q = lane & 3;
 #pragma unroll
-    for (int r = 0; r < TR; ++r) {
-      const int a = padded_member(D, rt * TR + r);
+      for (int rti = 0; rti < 2; ++rti) {
 #pragma unroll
-      for (int c = 0; c < TC; ++c) {
-        const int b = ct + 4 * c;
-        if (a >= 0 && b < nb) {
-          Qm[a * LD + b] = mkc(aj[r][c][0] - ay[r][c][1], aj[r][c][1] + ay[r][c][0]);
-          Rm[a * LD + b] = mkc(aj[r][c][0], aj[r][c][1]);
+        for (int cti = 0; cti < 2; ++cti) {
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int a = rti * 8 + rr;
+            const int b = cti * 8 + 2 * q + i;
+            if (a < nb && b < nb) {
+              int ia, na, ib, nbn;
+              member(D, a, ia, na);
+              member(D, b, ib, nbn);
+              const double sc = a_n(na) * a_n(nbn);
+              const double jr = acc[rti][cti][0][i], ji = acc[rti][cti][1][i];
+              const double yr = acc[rti][cti][2][i], yi = acc[rti][cti][3][i];
+              Qm[a * LD + b] = mkc((jr - yi) * sc, (ji + yr) * sc);
+              Rm[a * LD + b] = mkc(jr * sc, ji * sc);
+            }
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < TR; ++r) {
+        const int a = padded_member(D, rt * TR + r);
+#pragma unroll
+        for (int c = 0; c < TC; ++c) {
+          const int b = ct + 4 * c;
+          if (a >= 0 && b < nb) {
+            int ia, na, ib, nbn;
+            member(D, a, ia, na);
+            member(D, b, ib, nbn);
+            const double sc = a_n(na) * a_n(nbn);
+            Qm[a * LD + b] = mkc((aj[r][c][0] - ay[r][c][1]) * sc,
+                                 (aj[r][c][1] + ay[r][c][0]) * sc);
+            Rm[a * LD + b] = mkc(aj[r][c][0] * sc, aj[r][c][1] * sc);
+          }
         }
       }
     }
@@ -699,14 +815,14 @@ __global__ void __launch_bounds__(128, MINB)
   }
 }
 
-template <int TR, int TC, int MINB>
+template <int TR, int TC, int MINB, bool MMA>
 static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
-  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  constexpr int NBM = MMA ? 16 : ((8 * TR > 4 * TC) ? 8 * TR : 4 * TC);
   const size_t smem = (size_t)4 * warp_elems<NBM>() * sizeof(cplx);
-  cudaFuncSetAttribute(k_blocks_warp<TR, TC, MINB>,
+  cudaFuncSetAttribute(k_blocks_warp<TR, TC, MINB, MMA>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (int)std::min<int64_t>((a.nitems + 3) / 4, 148 * 16);
-  k_blocks_warp<TR, TC, MINB><<<blocks, 128, smem, stream>>>(a);
+  k_blocks_warp<TR, TC, MINB, MMA><<<blocks, 128, smem, stream>>>(a);
 }
 
 // shared memory of one block: the larger of the assembly chunk buffers and
@@ -752,11 +868,11 @@ void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
     return;
   }
   if (a.max_nb <= 8) {
-    launch_warp_variant<1, 2, 4>(a, stream);
+    launch_warp_variant<1, 2, 4, false>(a, stream);
     return;
   }
   if (a.max_nb <= 16) {
-    launch_warp_variant<2, 4, 3>(a, stream);
+    launch_warp_variant<1, 1, 3, true>(a, stream);
     return;
   }
   const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);

@@ -30,7 +30,9 @@ struct DevBuf {
 
 struct tmx_ctx {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;  // every launch unless noted (high priority)
+  cudaStream_t stream2 = nullptr; // blocks of grains that converged while the
+                                  // order loop continues (low priority)
   std::string err;
   int64_t launches = 0;
   // Gauss-Legendre cache: lower-half nodes of the 2 * ngauss rule
@@ -78,7 +80,11 @@ struct tmx_ctx {
   std::vector<int32_t> nmax_h, ngauss_h, status_h;
   std::vector<double> q_h;
   std::vector<int64_t> t_off_h;
-  // block schedule of the last batch (phase 2), reused by the tangents
+  // block schedule of the last batch (phase 2), reused by the tangents; its
+  // tables, slots, items and scratch live in the p2 buffers. p2_rounds > 1:
+  // the blocks ran in two rounds and the buffers hold the last round only.
+  DevBuf p2tab, p2nsc, p2scratch, p2slots, p2items;
+  int p2_rounds = 0;
   std::vector<TmxSlot> p2_slots;
   std::vector<TmxItem> p2_items;
   std::vector<int> p2_nb;
@@ -111,23 +117,25 @@ static inline double item_flops(int nb, int m, int ng) {
   return 8. * terms * b * b * ng + (8. / 3.) * b * b * b + 8. * b * b * b;
 }
 
-static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a) {
+static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a,
+                             cudaStream_t st = nullptr) {
   if (!ctx->profiling) {
     return 0;
   }
   CK(cudaEventCreate(a));
-  CK(cudaEventRecord(*a, ctx->stream));
+  CK(cudaEventRecord(*a, st ? st : ctx->stream));
   (void)k;
   return 0;
 }
 
-static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops) {
+static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
+                           cudaStream_t st = nullptr) {
   if (!ctx->profiling) {
     return 0;
   }
   cudaEvent_t b;
   CK(cudaEventCreate(&b));
-  CK(cudaEventRecord(b, ctx->stream));
+  CK(cudaEventRecord(b, st ? st : ctx->stream));
   ctx->prof[k].pending.push_back({a, b});
   ctx->prof[k].launches += 1;
   ctx->prof[k].flops += flops;
@@ -210,3 +218,7 @@ static inline int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep
 
 // Clebsch-Gordan table for all (n1, n2) <= nmax (tmx_table.cu)
 int tmx_ensure_cg(tmx_ctx *ctx, int nmax);
+
+// Blocks of the last batch again in one round (tmx_host.cu), so that the p2
+// buffers hold the whole schedule for the tangent kernels.
+extern "C" __attribute__((visibility("hidden"))) int tmx_rerun_blocks(tmx_ctx *ctx);

@@ -224,9 +224,13 @@ int tmx_create(tmx_ctx **out, int device) {
   }
   tmx_ctx *ctx = new tmx_ctx();
   ctx->device = device;
+  int prio_lo = 0, prio_hi = 0;
   if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) !=
-          cudaSuccess ||
+      cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking,
+                                   prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->pinned, 64) != cudaSuccess) {
     cudaGetLastError();
     delete ctx;
@@ -242,6 +246,9 @@ void tmx_destroy(tmx_ctx *ctx) {
   }
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->stream2) {
+    cudaStreamSynchronize(ctx->stream2);
+  }
   if (ctx->t0) {
     cudaEventDestroy(ctx->t0);
     cudaEventDestroy(ctx->t1);
@@ -252,6 +259,8 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->o_og, &ctx->o_work, &ctx->o_sj, &ctx->o_qj, &ctx->o_S,
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
                     &ctx->o_pairs, &ctx->o_grp, &ctx->o_x,
+                    &ctx->p2tab, &ctx->p2nsc, &ctx->p2scratch, &ctx->p2slots,
+                    &ctx->p2items,
                     &ctx->state0, &ctx->actinit,
                     &ctx->gl_x,  &ctx->gl_w,   &ctx->gl_off,  &ctx->wig,
                     &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,
@@ -269,6 +278,9 @@ void tmx_destroy(tmx_ctx *ctx) {
     cudaFreeHost(ctx->pinned);
   }
   cudaStreamDestroy(ctx->stream);
+  if (ctx->stream2) {
+    cudaStreamDestroy(ctx->stream2);
+  }
   delete ctx;
 }
 
@@ -380,22 +392,22 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   return TMX_OK;
 }
 
-// Phase 2 of a batch: every (grain, m, class) block at the grain's order in
-// ctx->nmax_h / ctx->ngauss_h (grains listed in p2), then the full Q sums.
-// The block schedule is kept in the context for the tangent kernels.
-static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
-  cudaStream_t st = ctx->stream;
-  const int64_t n = ctx->n;
-  const tmx_schedule S = ctx->up_sched;
-  const int glf = S.gauss_legendre_factor;
+// One round of phase 2: every (grain, m, class) block of the grains in p2 at
+// their orders (ctx->nmax_h / ctx->ngauss_h), launched on stream `st`, with
+// T-matrices from complex offset t_base on (keep_T: T already holds earlier
+// rounds below t_base). The schedule is kept in the context (p2 buffers and
+// ctx->p2_*) for the tangent kernels. Host-side setup runs on ctx->stream
+// (Wigner tables), which the round then waits for.
+static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
+                            cudaStream_t st, int64_t t_base, bool keep_T,
+                            int64_t *t_end) {
   int rc;
-  // ---- 2. all blocks at the converged orders
   NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
   std::vector<TmxSlot> slots(np2);
   std::vector<std::pair<int, int>> keys;
   std::map<std::pair<int, int>, int> key_idx;
-  int64_t tab_total = 0, nsc_total = 0, t_total = 0;
+  int64_t tab_total = 0, nsc_total = 0, t_total = t_base;
   for (int s = 0; s < np2; ++s) {
     const int g = p2[s];
     const int N = ctx->nmax_h[g], ng = ctx->ngauss_h[g];
@@ -417,6 +429,7 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
     nsc_total += (int64_t)ng * TMX_NS;
     t_total += tmx_tmatrix_size(N);
   }
+  *t_end = t_total;
   std::vector<int> full_sets;
   if ((rc = ensure_wigner(ctx, keys, true, full_sets))) {
     return rc;
@@ -474,80 +487,105 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
     scr_total += 2 * (int64_t)inb[i] * inb[i];
   }
   ctx->p2_scr_total = scr_total;
-  ctx->p2_t_total = t_total;
-  if ((rc = ensure(ctx, ctx->tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->slots, std::max(1, np2) * sizeof(TmxSlot))) ||
-      (rc = ensure(ctx, ctx->items, std::max<int64_t>(1, nitems) * sizeof(TmxItem))) ||
-      (rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
-      (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
-      (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
+  if ((rc = ensure(ctx, ctx->p2tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->p2nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
+      (rc = (keep_T ? ensure_keep(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx),
+                                  t_base * sizeof(cplx))
+                    : ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx)))) ||
+      (rc = ensure(ctx, ctx->p2scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->p2slots, std::max(1, np2) * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->p2items, std::max<int64_t>(1, nitems) * sizeof(TmxItem)))) {
     return rc;
   }
-  if (np2 > 0) {
-    CK(cudaMemcpyAsync(ctx->slots.p, slots.data(), np2 * sizeof(TmxSlot),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->items.p, items.data(), nitems * sizeof(TmxItem),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(ctx->T.p, 0, t_total * sizeof(cplx), st));
-    cudaEvent_t pe = nullptr;
-    if ((rc = prof_begin(ctx, 1, &pe))) {
+  if (np2 == 0) {
+    return TMX_OK;
+  }
+  if (st != ctx->stream) {
+    // the allocations and Wigner tables above are ordered on ctx->stream
+    cudaEvent_t ready;
+    CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    CK(cudaEventRecord(ready, ctx->stream));
+    CK(cudaStreamWaitEvent(st, ready, 0));
+    CK(cudaEventDestroy(ready));
+  }
+  CK(cudaMemcpyAsync(ctx->p2slots.p, slots.data(), np2 * sizeof(TmxSlot),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->p2items.p, items.data(), nitems * sizeof(TmxItem),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync((cplx *)ctx->T.p + t_base, 0, (t_total - t_base) * sizeof(cplx), st));
+  cudaEvent_t pe = nullptr;
+  if ((rc = prof_begin(ctx, 1, &pe, st))) {
+    return rc;
+  }
+  tmx_launch_tables((const TmxSlot *)ctx->p2slots.p, np2,
+                    (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
+                    (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
+                    (double *)ctx->p2tab.p, (double *)ctx->p2nsc.p,
+                    ctx->up_sched.bessel_start, st);
+  LAUNCHED();
+  if ((rc = prof_end(ctx, 1, pe, 0., st))) {
+    return rc;
+  }
+  // class-size buckets, one launch each (largest first)
+  const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
+  int64_t i0 = 0;
+  for (int b = 0; b < 5; ++b) {
+    int64_t i1 = i0;
+    while (i1 < nitems && inb[i1] > edges[b + 1]) {
+      ++i1;
+    }
+    if (i1 > i0) {
+      TmxBlockArgs B;
+      B.items = (const TmxItem *)ctx->p2items.p + i0;
+      B.nitems = (int)(i1 - i0);
+      B.slots = (const TmxSlot *)ctx->p2slots.p;
+      B.grains = (const TmxGrain *)ctx->grains.p;
+      B.tab = (const double *)ctx->p2tab.p;
+      B.nsc = (const double *)ctx->p2nsc.p;
+      B.wig = (const double *)ctx->wig.p;
+      B.wig_off = (const int64_t *)ctx->wig_off.p;
+      B.scratch = (cplx *)ctx->p2scratch.p;
+      B.tout = (cplx *)ctx->T.p;
+      B.diag = nullptr;
+      B.status = (int32_t *)ctx->status.p;
+      B.max_nb = inb[i0];
+      B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+      double fl = 0.;
+      if (ctx->profiling) {
+        for (int64_t q = i0; q < i1; ++q) {
+          fl += item_flops(inb[q], items[q].m, slots[items[q].slot].ngauss);
+        }
+      }
+      if ((rc = prof_begin(ctx, 0, &pe, st))) {
+        return rc;
+      }
+      tmx_launch_blocks(B, st);
+      LAUNCHED();
+      if ((rc = prof_end(ctx, 0, pe, fl, st))) {
+        return rc;
+      }
+    }
+    i0 = i1;
+  }
+  return TMX_OK;
+}
+
+// End of a batch: full Q sums of every grain (TMatrixQTask) on ctx->stream
+// after all block rounds, per-grain results to the host.
+static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  const tmx_schedule S = ctx->up_sched;
+  const int glf = S.gauss_legendre_factor;
+  int rc;
+  ctx->p2_t_total = t_total;
+  ctx->p2_rounds = rounds;
+  if (t_total > 0) {
+    if ((rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
+        (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
+        (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
       return rc;
     }
-    tmx_launch_tables((const TmxSlot *)ctx->slots.p, np2,
-                      (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
-                      (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
-                      (double *)ctx->tab.p, (double *)ctx->nsc.p, S.bessel_start,
-                      st);
-    LAUNCHED();
-    if ((rc = prof_end(ctx, 1, pe, 0.))) {
-      return rc;
-    }
-    // buckets by class size
-    // class-size buckets, one launch each (largest first)
-    const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
-    int64_t i0 = 0;
-    for (int b = 0; b < 5; ++b) {
-      int64_t i1 = i0;
-      while (i1 < nitems && inb[i1] > edges[b + 1]) {
-        ++i1;
-      }
-      if (i1 > i0) {
-        TmxBlockArgs B;
-        B.items = (const TmxItem *)ctx->items.p + i0;
-        B.nitems = (int)(i1 - i0);
-        B.slots = (const TmxSlot *)ctx->slots.p;
-        B.grains = (const TmxGrain *)ctx->grains.p;
-        B.tab = (const double *)ctx->tab.p;
-        B.nsc = (const double *)ctx->nsc.p;
-        B.wig = (const double *)ctx->wig.p;
-        B.wig_off = (const int64_t *)ctx->wig_off.p;
-        B.scratch = (cplx *)ctx->scratch.p;
-        B.tout = (cplx *)ctx->T.p;
-        B.diag = nullptr;
-        B.status = (int32_t *)ctx->status.p;
-        B.max_nb = inb[i0];
-        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
-        double fl = 0.;
-        if (ctx->profiling) {
-          for (int64_t q = i0; q < i1; ++q) {
-            fl += item_flops(inb[q], items[q].m, slots[items[q].slot].ngauss);
-          }
-        }
-        if ((rc = prof_begin(ctx, 0, &pe))) {
-          return rc;
-        }
-        tmx_launch_blocks(B, st);
-        LAUNCHED();
-        if ((rc = prof_end(ctx, 0, pe, fl))) {
-          return rc;
-        }
-      }
-      i0 = i1;
-    }
-    // ---- 3. full Q sums
     std::vector<int32_t> nmv(n);
     for (int64_t i = 0; i < n; ++i) {
       nmv[i] = ctx->nmax_h[i];
@@ -594,6 +632,36 @@ static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
     return rc;
   }
   ctx->have_batch = true;
+  return TMX_OK;
+}
+
+// Phase 2 in one round for the grains in p2 (all grains with an order).
+static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
+  int64_t t_end = 0;
+  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end);
+  if (rc) {
+    return rc;
+  }
+  return finish_blocks(ctx, t_end, 1);
+}
+
+// Phase 2 again in one round for the last batch, so that the p2 buffers hold
+// the whole schedule (after a batch whose blocks ran in two rounds).
+int tmx_rerun_blocks(tmx_ctx *ctx) {
+  std::vector<int32_t> p2;
+  for (int64_t i = 0; i < ctx->n; ++i) {
+    if (ctx->nmax_h[i] > 0) {
+      p2.push_back((int32_t)i);
+    }
+  }
+  int64_t t_end = 0;
+  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end);
+  if (rc) {
+    return rc;
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->p2_t_total = t_end;
+  ctx->p2_rounds = 1;
   return TMX_OK;
 }
 
@@ -650,6 +718,10 @@ int tmx_batch_compute(tmx_ctx *ctx) {
 
   // ---- 1. order loop
   int nact = ctx->up_nact;
+  bool early = false;            // first block round started
+  std::vector<int32_t> round1;   // its grains
+  std::vector<char> in_round1(n, 0);
+  int64_t t_round1 = 0;
   DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
   const size_t budget = (size_t)8 << 30; // table bytes per chunk
   std::unique_ptr<NvtxRange> chain_range(new NvtxRange("tmx_chain"));
@@ -730,6 +802,29 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     CK(cudaStreamSynchronize(st));
     nact = ctx->pinned[0];
     std::swap(cur, nxt);
+    if (!early && nact > 0 && 4 * (int64_t)nact < ctx->up_nact &&
+        ctx->up_nact - nact >= 256) {
+      // Most grains have their order: their blocks start now on the second
+      // (lower-priority) stream and fill the GPU while the few remaining
+      // grains run the latency-bound tail of the order loop.
+      CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      for (int64_t i = 0; i < n; ++i) {
+        const bool done = st0[i].converged ||
+                          (st0[i].status & (TMX_ST_NAN | TMX_ST_NOT_CONVERGED));
+        if (st0[i].nmax > 0 && done) {
+          ctx->nmax_h[i] = st0[i].nmax;
+          ctx->ngauss_h[i] = st0[i].ngauss;
+          round1.push_back((int32_t)i);
+          in_round1[i] = 1;
+        }
+      }
+      if ((rc = run_blocks_round(ctx, round1, ctx->stream2, 0, false, &t_round1))) {
+        return rc;
+      }
+      early = true;
+    }
   }
 
   chain_range.reset();
@@ -738,7 +833,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  std::vector<int32_t> p2; // grains that get blocks
+  std::vector<int32_t> p2; // grains that get blocks (in this round)
   for (int64_t i = 0; i < n; ++i) {
     ctx->nmax_h[i] = st0[i].nmax;
     ctx->ngauss_h[i] = st0[i].ngauss;
@@ -747,12 +842,20 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     ctx->q_h[6 * i + 1] = st0[i].qext;
     ctx->q_h[6 * i + 4] = st0[i].dqs;
     ctx->q_h[6 * i + 5] = st0[i].dqe;
-    if (st0[i].nmax > 0) {
+    if (st0[i].nmax > 0 && !in_round1[i]) {
       p2.push_back((int32_t)i);
     }
   }
-
-  return run_blocks(ctx, p2);
+  if (!early) {
+    return run_blocks(ctx, p2);
+  }
+  // the first round still owns the p2 buffers: wait for it, then the rest
+  CK(cudaStreamSynchronize(ctx->stream2));
+  int64_t t_end = t_round1;
+  if ((rc = run_blocks_round(ctx, p2, st, t_round1, true, &t_end))) {
+    return rc;
+  }
+  return finish_blocks(ctx, t_end, 2);
 }
 
 int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,

@@ -901,10 +901,13 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const int64_t n = ctx->n;
+  int rc;
+  if (ctx->p2_rounds > 1 && (rc = tmx_rerun_blocks(ctx))) {
+    return rc;
+  }
   const int64_t nitems = (int64_t)ctx->p2_items.size();
   const int64_t scr = ctx->p2_scr_total;
   const int64_t tt = ctx->p2_t_total;
-  int rc;
   NvtxRange range("tmx_gradients");
   if ((rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, scr) * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->tscr, std::max<int64_t>(1, 3 * scr) * sizeof(cplx))) ||
@@ -928,15 +931,15 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
       if (i1 > i0) {
         const int max_nb = ctx->p2_nb[i0];
         TmxBlockArgs B;
-        B.items = (const TmxItem *)ctx->items.p + i0;
+        B.items = (const TmxItem *)ctx->p2items.p + i0;
         B.nitems = (int)(i1 - i0);
-        B.slots = (const TmxSlot *)ctx->slots.p;
+        B.slots = (const TmxSlot *)ctx->p2slots.p;
         B.grains = (const TmxGrain *)ctx->grains.p;
-        B.tab = (const double *)ctx->tab.p;
-        B.nsc = (const double *)ctx->nsc.p;
+        B.tab = (const double *)ctx->p2tab.p;
+        B.nsc = (const double *)ctx->p2nsc.p;
         B.wig = (const double *)ctx->wig.p;
         B.wig_off = (const int64_t *)ctx->wig_off.p;
-        B.scratch = (cplx *)ctx->scratch.p;
+        B.scratch = (cplx *)ctx->p2scratch.p;
         B.tout = (cplx *)ctx->T.p;
         B.diag = nullptr;
         B.status = (int32_t *)ctx->status.p;

@@ -92,3 +92,31 @@ def test_bessel_start_automatic_equals_800(ctx):
     assert np.array_equal(na, b.nmax)
     for i in range(len(r)):
         assert np.array_equal(Ta[i], b.tmatrix(i)), i
+
+
+def test_two_block_rounds_match_one_round(ctx):
+    # 1024 grains: most converge early, so the blocks of the converged grains
+    # run while the order loop continues (two rounds on two streams); the
+    # same blocks in one round (fixed orders) must give the same doubles
+    r, lam, m, d = H.config2_sample(1024, 5)
+    res = ctx.tmatrix_batch(r, lam, m, d)
+    nm, ng, q = res.nmax.copy(), res.ngauss.copy(), res.q.copy()
+    T2 = [res.tmatrix(i) for i in range(0, 1024, 7)]
+    assert (res.status == 0).all()
+    fix = ctx.tmatrix_batch_fixed(r, lam, m, d, nm, ng)
+    assert np.array_equal(fix.q[:, 2:4], q[:, 2:4])
+    for k, i in enumerate(range(0, 1024, 7)):
+        assert np.array_equal(fix.tmatrix(i), T2[k]), i
+
+
+def test_gradients_after_two_rounds(ctx):
+    # gradients right after a two-round batch equal those after a fixed batch
+    r, lam, m, d = H.config2_sample(1024, 6)
+    th = np.array([0.3, 1.1, 2.0])
+    res = ctx.tmatrix_batch(r, lam, m, d)
+    nm, ng = res.nmax.copy(), res.ngauss.copy()
+    q1, dq1 = ctx.gradients(th)
+    ctx.tmatrix_batch_fixed(r, lam, m, d, nm, ng)
+    q2, dq2 = ctx.gradients(th)
+    assert np.array_equal(q1, q2)
+    assert np.array_equal(dq1, dq2)

@@ -719,6 +719,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   // ---- 1. order loop
   int nact = ctx->up_nact;
   bool early = false;            // first block round started
+  bool pending = false;          // first block round due with the next order
   std::vector<int32_t> round1;   // its grains
   std::vector<char> in_round1(n, 0);
   int64_t t_round1 = 0;
@@ -799,14 +800,22 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
     CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
+    if (pending) {
+      // the first block round: its host set-up overlaps this order on the GPU
+      if ((rc = run_blocks_round(ctx, round1, ctx->stream2, 0, false, &t_round1))) {
+        return rc;
+      }
+      pending = false;
+      early = true;
+    }
     CK(cudaStreamSynchronize(st));
     nact = ctx->pinned[0];
     std::swap(cur, nxt);
-    if (!early && nact > 0 && 4 * (int64_t)nact < ctx->up_nact &&
+    if (!early && !pending && nact > 0 && 4 * (int64_t)nact < ctx->up_nact &&
         ctx->up_nact - nact >= 256) {
-      // Most grains have their order: their blocks start now on the second
-      // (lower-priority) stream and fill the GPU while the few remaining
-      // grains run the latency-bound tail of the order loop.
+      // Most grains have their order: their blocks start with the next order
+      // on the second (lower-priority) stream and fill the GPU while the few
+      // remaining grains run the latency-bound tail of the order loop.
       CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                          cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
@@ -820,11 +829,13 @@ int tmx_batch_compute(tmx_ctx *ctx) {
           in_round1[i] = 1;
         }
       }
-      if ((rc = run_blocks_round(ctx, round1, ctx->stream2, 0, false, &t_round1))) {
-        return rc;
-      }
-      early = true;
+      pending = true;
     }
+  }
+  if (pending) {
+    // the order loop ended first: one round for every grain
+    round1.clear();
+    std::fill(in_round1.begin(), in_round1.end(), 0);
   }
 
   chain_range.reset();

@@ -892,7 +892,8 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
                            const TmxSlot *__restrict__ slots,
                            const cplx *__restrict__ diag, TmxChainState *state,
                            double tolerance, int order, int last_order,
-                           int32_t *next_active, int32_t *next_count) {
+                           int32_t *next_active, int32_t *next_count,
+                           int32_t *done_list, int32_t *done_count) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive) {
     return;
@@ -933,28 +934,35 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
   if (!finite) {
     st.status |= TMX_ST_NAN;
   }
+  bool stays = false;
   if (!st.converged && finite) {
     if (order < last_order) {
       const int q = atomicAdd(next_count, 1);
       next_active[q] = g;
+      stays = true;
     } else {
       st.status |= TMX_ST_NOT_CONVERGED;
     }
   }
   state[g] = st;
+  if (!stays) {
+    // the grain's order is final: its blocks may start
+    done_list[atomicAdd(done_count, 1)] = g;
+  }
 }
 
 void tmx_launch_converge(const int32_t *active, int nactive,
                          const TmxSlot *slots, const double2 *diag,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
-                         int32_t *next_count, cudaStream_t stream) {
+                         int32_t *next_count, int32_t *done_list,
+                         int32_t *done_count, cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
       active, nactive, slots, diag, state, tolerance, order, last_order,
-      next_active, next_count);
+      next_active, next_count, done_list, done_count);
 }
 
 // ------------------------------------------------------------- Q sums ------

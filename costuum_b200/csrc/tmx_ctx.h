@@ -33,6 +33,8 @@ struct tmx_ctx {
   cudaStream_t stream = nullptr;  // every launch unless noted (high priority)
   cudaStream_t stream2 = nullptr; // blocks of grains that converged while the
                                   // order loop continues (low priority)
+  cudaMemPool_t pool = nullptr;   // device memory of this context; keeps
+                                  // freed blocks for reuse (no release)
   std::string err;
   int64_t launches = 0;
   // Gauss-Legendre cache: lower-half nodes of the 2 * ngauss rule
@@ -63,7 +65,10 @@ struct tmx_ctx {
   // plan of the observable kernels (first pair of each grain, job groups)
   int64_t o_ngrains = 0, o_npairs = 0;
   int o_nbmax = 1, o_ngrp = 0;
-  int32_t *pinned = nullptr;
+  int32_t *pinned = nullptr;     // [0] active count, [1] done count
+  DevBuf done;                    // grains whose order became final, in order
+  int32_t *pinned_done = nullptr; // host copy of new done-list entries
+  int64_t pinned_done_cap = 0;
   // timing: events on the library stream
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   bool profiling = false;
@@ -178,10 +183,10 @@ static inline int ensure(tmx_ctx *ctx, DevBuf &b, size_t bytes) {
     b.cap = 0;
   }
   size_t want = bytes + bytes / 4;
-  cudaError_t e = cudaMallocAsync(&b.p, want, ctx->stream);
+  cudaError_t e = cudaMallocFromPoolAsync(&b.p, want, ctx->pool, ctx->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    e = cudaMallocAsync(&b.p, bytes, ctx->stream);
+    e = cudaMallocFromPoolAsync(&b.p, bytes, ctx->pool, ctx->stream);
     want = bytes;
   }
   if (e != cudaSuccess) {
@@ -200,7 +205,7 @@ static inline int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep
   }
   DevBuf nb;
   size_t want = std::max(bytes, b.cap * 2);
-  if (cudaMallocAsync(&nb.p, want, ctx->stream) != cudaSuccess) {
+  if (cudaMallocFromPoolAsync(&nb.p, want, ctx->pool, ctx->stream) != cudaSuccess) {
     cudaGetLastError();
     return fail(ctx, TMX_ERR_NOMEM, "device allocation failed (table cache)");
   }

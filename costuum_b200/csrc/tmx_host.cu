@@ -152,8 +152,8 @@ static int ensure_wigner(tmx_ctx *ctx,
                      ctx->wig_off_h.size() * sizeof(int64_t),
                      cudaMemcpyHostToDevice, ctx->stream));
   TmxWigJob *djobs = nullptr;
-  CK(cudaMallocAsync((void **)&djobs, jobs.size() * sizeof(TmxWigJob),
-                     ctx->stream));
+  CK(cudaMallocFromPoolAsync((void **)&djobs, jobs.size() * sizeof(TmxWigJob),
+                             ctx->pool, ctx->stream));
   CK(cudaMemcpyAsync(djobs, jobs.data(), jobs.size() * sizeof(TmxWigJob),
                      cudaMemcpyHostToDevice, ctx->stream));
   tmx_launch_wigner(djobs, (int)jobs.size(), max_work,
@@ -236,6 +236,27 @@ int tmx_create(tmx_ctx **out, int device) {
     delete ctx;
     return TMX_ERR_CUDA;
   }
+  // a memory pool of this context: stream-ordered allocations of repeated
+  // batches reuse its blocks instead of mapping new memory each time
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  // (no reuse that would make one stream wait for the other)
+  uint64_t keep_all = UINT64_MAX;
+  int no_deps = 0;
+  if (cudaMemPoolCreate(&ctx->pool, &props) != cudaSuccess ||
+      cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold,
+                              &keep_all) != cudaSuccess ||
+      cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolReuseAllowInternalDependencies,
+                              &no_deps) != cudaSuccess) {
+    cudaGetLastError();
+    cudaStreamDestroy(ctx->stream);
+    cudaStreamDestroy(ctx->stream2);
+    cudaFreeHost(ctx->pinned);
+    delete ctx;
+    return TMX_ERR_CUDA;
+  }
   *out = ctx;
   return TMX_OK;
 }
@@ -260,7 +281,7 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
                     &ctx->o_pairs, &ctx->o_grp, &ctx->o_x,
                     &ctx->p2tab, &ctx->p2nsc, &ctx->p2scratch, &ctx->p2slots,
-                    &ctx->p2items,
+                    &ctx->p2items, &ctx->done,
                     &ctx->state0, &ctx->actinit,
                     &ctx->gl_x,  &ctx->gl_w,   &ctx->gl_off,  &ctx->wig,
                     &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,
@@ -274,12 +295,18 @@ void tmx_destroy(tmx_ctx *ctx) {
     }
   }
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->pinned_done) {
+    cudaFreeHost(ctx->pinned_done);
+  }
   if (ctx->pinned) {
     cudaFreeHost(ctx->pinned);
   }
   cudaStreamDestroy(ctx->stream);
   if (ctx->stream2) {
     cudaStreamDestroy(ctx->stream2);
+  }
+  if (ctx->pool) {
+    cudaMemPoolDestroy(ctx->pool);
   }
   delete ctx;
 }
@@ -400,7 +427,7 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
 // (Wigner tables), which the round then waits for.
 static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
                             cudaStream_t st, int64_t t_base, bool keep_T,
-                            int64_t *t_end) {
+                            int64_t *t_end, bool temp = false) {
   int rc;
   NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
@@ -487,14 +514,21 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     scr_total += 2 * (int64_t)inb[i] * inb[i];
   }
   ctx->p2_scr_total = scr_total;
-  if ((rc = ensure(ctx, ctx->p2tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->p2nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
-      (rc = (keep_T ? ensure_keep(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx),
+  if (keep_T && (size_t)t_total * sizeof(cplx) > ctx->T.cap) {
+    // growing T moves it: earlier rounds on the second stream must be done
+    CK(cudaStreamSynchronize(ctx->stream2));
+  }
+  if ((rc = (keep_T ? ensure_keep(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx),
                                   t_base * sizeof(cplx))
-                    : ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx)))) ||
-      (rc = ensure(ctx, ctx->p2scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->p2slots, std::max(1, np2) * sizeof(TmxSlot))) ||
-      (rc = ensure(ctx, ctx->p2items, std::max<int64_t>(1, nitems) * sizeof(TmxItem)))) {
+                    : ensure(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx))))) {
+    return rc;
+  }
+  if (!temp &&
+      ((rc = ensure(ctx, ctx->p2tab, std::max<int64_t>(1, tab_total) * sizeof(double))) ||
+       (rc = ensure(ctx, ctx->p2nsc, std::max<int64_t>(1, nsc_total) * sizeof(double))) ||
+       (rc = ensure(ctx, ctx->p2scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx))) ||
+       (rc = ensure(ctx, ctx->p2slots, std::max(1, np2) * sizeof(TmxSlot))) ||
+       (rc = ensure(ctx, ctx->p2items, std::max<int64_t>(1, nitems) * sizeof(TmxItem))))) {
     return rc;
   }
   if (np2 == 0) {
@@ -508,19 +542,31 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     CK(cudaStreamWaitEvent(st, ready, 0));
     CK(cudaEventDestroy(ready));
   }
-  CK(cudaMemcpyAsync(ctx->p2slots.p, slots.data(), np2 * sizeof(TmxSlot),
+  // buffers of this round: the persistent p2 set, or (temp) stream-ordered
+  // allocations on `st` that are released after the round's launches
+  double *tab = (double *)ctx->p2tab.p, *nsc = (double *)ctx->p2nsc.p;
+  cplx *scratch = (cplx *)ctx->p2scratch.p;
+  TmxSlot *dslots = (TmxSlot *)ctx->p2slots.p;
+  TmxItem *ditems = (TmxItem *)ctx->p2items.p;
+  if (temp) {
+    CK(cudaMallocFromPoolAsync((void **)&tab, std::max<int64_t>(1, tab_total) * sizeof(double), ctx->pool, st));
+    CK(cudaMallocFromPoolAsync((void **)&nsc, std::max<int64_t>(1, nsc_total) * sizeof(double), ctx->pool, st));
+    CK(cudaMallocFromPoolAsync((void **)&scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx), ctx->pool, st));
+    CK(cudaMallocFromPoolAsync((void **)&dslots, np2 * sizeof(TmxSlot), ctx->pool, st));
+    CK(cudaMallocFromPoolAsync((void **)&ditems, std::max<int64_t>(1, nitems) * sizeof(TmxItem), ctx->pool, st));
+  }
+  CK(cudaMemcpyAsync(dslots, slots.data(), np2 * sizeof(TmxSlot),
                      cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(ctx->p2items.p, items.data(), nitems * sizeof(TmxItem),
+  CK(cudaMemcpyAsync(ditems, items.data(), nitems * sizeof(TmxItem),
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync((cplx *)ctx->T.p + t_base, 0, (t_total - t_base) * sizeof(cplx), st));
   cudaEvent_t pe = nullptr;
   if ((rc = prof_begin(ctx, 1, &pe, st))) {
     return rc;
   }
-  tmx_launch_tables((const TmxSlot *)ctx->p2slots.p, np2,
-                    (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
-                    (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
-                    (double *)ctx->p2tab.p, (double *)ctx->p2nsc.p,
+  tmx_launch_tables(dslots, np2, (const TmxGrain *)ctx->grains.p,
+                    (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
+                    (const int64_t *)ctx->gl_off.p, tab, nsc,
                     ctx->up_sched.bessel_start, st);
   LAUNCHED();
   if ((rc = prof_end(ctx, 1, pe, 0., st))) {
@@ -536,15 +582,15 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     }
     if (i1 > i0) {
       TmxBlockArgs B;
-      B.items = (const TmxItem *)ctx->p2items.p + i0;
+      B.items = ditems + i0;
       B.nitems = (int)(i1 - i0);
-      B.slots = (const TmxSlot *)ctx->p2slots.p;
+      B.slots = dslots;
       B.grains = (const TmxGrain *)ctx->grains.p;
-      B.tab = (const double *)ctx->p2tab.p;
-      B.nsc = (const double *)ctx->p2nsc.p;
+      B.tab = tab;
+      B.nsc = nsc;
       B.wig = (const double *)ctx->wig.p;
       B.wig_off = (const int64_t *)ctx->wig_off.p;
-      B.scratch = (cplx *)ctx->p2scratch.p;
+      B.scratch = scratch;
       B.tout = (cplx *)ctx->T.p;
       B.diag = nullptr;
       B.status = (int32_t *)ctx->status.p;
@@ -566,6 +612,13 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       }
     }
     i0 = i1;
+  }
+  if (temp) {
+    CK(cudaFreeAsync(tab, st));
+    CK(cudaFreeAsync(nsc, st));
+    CK(cudaFreeAsync(scratch, st));
+    CK(cudaFreeAsync(dslots, st));
+    CK(cudaFreeAsync(ditems, st));
   }
   return TMX_OK;
 }
@@ -717,12 +770,32 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   }
 
   // ---- 1. order loop
+  // Grains whose order became final are collected from the done list after
+  // every order; once enough are ready, their blocks run as a round on the
+  // second (lower-priority) stream while the order loop continues, so the
+  // blocks fill the GPU during the latency-bound tail of the loop. A round's
+  // host set-up is issued after the next order's launches, so it overlaps
+  // that order on the GPU.
   int nact = ctx->up_nact;
-  bool early = false;            // first block round started
-  bool pending = false;          // first block round due with the next order
-  std::vector<int32_t> round1;   // its grains
-  std::vector<char> in_round1(n, 0);
-  int64_t t_round1 = 0;
+  if ((rc = ensure(ctx, ctx->done, std::max<int64_t>(1, n) * sizeof(int32_t)))) {
+    return rc;
+  }
+  if (ctx->pinned_done_cap < n) {
+    if (ctx->pinned_done) {
+      CK(cudaFreeHost(ctx->pinned_done));
+      ctx->pinned_done = nullptr;
+      ctx->pinned_done_cap = 0;
+    }
+    CK(cudaMallocHost((void **)&ctx->pinned_done, n * sizeof(int32_t)));
+    ctx->pinned_done_cap = n;
+  }
+  CK(cudaMemsetAsync(ctx->count.p, 0, 2 * sizeof(int32_t), st));
+  const int64_t round_min = std::max<int64_t>(256, ctx->up_nact / 16);
+  int64_t done_seen = 0;
+  std::vector<int32_t> ready, pending;
+  std::vector<char> launched(n, 0);
+  int rounds = 0;
+  int64_t t_next = 0;
   DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
   const size_t budget = (size_t)8 << 30; // table bytes per chunk
   std::unique_ptr<NvtxRange> chain_range(new NvtxRange("tmx_chain"));
@@ -795,56 +868,54 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       tmx_launch_converge(a, cn, (const TmxSlot *)ctx->slots.p,
                           (const cplx *)ctx->diag.p,
                           (TmxChainState *)ctx->state.p, S.tolerance, k, last,
-                          (int32_t *)nxt->p, (int32_t *)ctx->count.p, st);
+                          (int32_t *)nxt->p, (int32_t *)ctx->count.p,
+                          (int32_t *)ctx->done.p, (int32_t *)ctx->count.p + 1,
+                          st);
       LAUNCHED();
     }
-    CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, sizeof(int32_t),
+    // active count, done count, and the done-list entries this order can add
+    CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, 2 * sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
-    if (pending) {
-      // the first block round: its host set-up overlaps this order on the GPU
-      if ((rc = run_blocks_round(ctx, round1, ctx->stream2, 0, false, &t_round1))) {
+    CK(cudaMemcpyAsync(ctx->pinned_done + done_seen, (int32_t *)ctx->done.p + done_seen,
+                       nact * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (!pending.empty()) {
+      if ((rc = run_blocks_round(ctx, pending, ctx->stream2, t_next, rounds > 0,
+                                 &t_next, true))) {
         return rc;
       }
-      pending = false;
-      early = true;
+      ++rounds;
+      pending.clear();
     }
     CK(cudaStreamSynchronize(st));
+    const int prev = nact;
     nact = ctx->pinned[0];
+    const int64_t done_now = ctx->pinned[1];
     std::swap(cur, nxt);
-    if (!early && !pending && nact > 0 && 4 * (int64_t)nact < ctx->up_nact &&
-        ctx->up_nact - nact >= 256) {
-      // Most grains have their order: their blocks start with the next order
-      // on the second (lower-priority) stream and fill the GPU while the few
-      // remaining grains run the latency-bound tail of the order loop.
-      CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
-                         cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      for (int64_t i = 0; i < n; ++i) {
-        const bool done = st0[i].converged ||
-                          (st0[i].status & (TMX_ST_NAN | TMX_ST_NOT_CONVERGED));
-        if (st0[i].nmax > 0 && done) {
-          ctx->nmax_h[i] = st0[i].nmax;
-          ctx->ngauss_h[i] = st0[i].ngauss;
-          round1.push_back((int32_t)i);
-          in_round1[i] = 1;
-        }
+    if (done_now > done_seen + prev) {
+      return fail(ctx, TMX_ERR_CUDA, "order loop: inconsistent done list");
+    }
+    for (int64_t j = done_seen; j < done_now; ++j) {
+      const int32_t g = ctx->pinned_done[j];
+      ctx->nmax_h[g] = k;
+      ctx->ngauss_h[g] = ng;
+      ready.push_back(g);
+    }
+    done_seen = done_now;
+    if (nact > 0 && (int64_t)ready.size() >= round_min) {
+      for (int32_t g : ready) {
+        launched[g] = 1;
       }
-      pending = true;
+      pending.swap(ready);
+      ready.clear();
     }
   }
-  if (pending) {
-    // the order loop ended first: one round for every grain
-    round1.clear();
-    std::fill(in_round1.begin(), in_round1.end(), 0);
-  }
-
   chain_range.reset();
 
   // ---- per-grain outcome of the order loop
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
-  std::vector<int32_t> p2; // grains that get blocks (in this round)
+  std::vector<int32_t> p2; // grains whose blocks have not been launched
   for (int64_t i = 0; i < n; ++i) {
     ctx->nmax_h[i] = st0[i].nmax;
     ctx->ngauss_h[i] = st0[i].ngauss;
@@ -853,20 +924,23 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     ctx->q_h[6 * i + 1] = st0[i].qext;
     ctx->q_h[6 * i + 4] = st0[i].dqs;
     ctx->q_h[6 * i + 5] = st0[i].dqe;
-    if (st0[i].nmax > 0 && !in_round1[i]) {
+    if (st0[i].nmax > 0 && !launched[i]) {
       p2.push_back((int32_t)i);
     }
   }
-  if (!early) {
+  if (rounds == 0) {
     return run_blocks(ctx, p2);
   }
-  // the first round still owns the p2 buffers: wait for it, then the rest
-  CK(cudaStreamSynchronize(ctx->stream2));
-  int64_t t_end = t_round1;
-  if ((rc = run_blocks_round(ctx, p2, st, t_round1, true, &t_end))) {
+  // the last round on this stream, then wait for the second stream's rounds
+  if ((rc = run_blocks_round(ctx, p2, st, t_next, true, &t_next, true))) {
     return rc;
   }
-  return finish_blocks(ctx, t_end, 2);
+  cudaEvent_t rounds_done;
+  CK(cudaEventCreateWithFlags(&rounds_done, cudaEventDisableTiming));
+  CK(cudaEventRecord(rounds_done, ctx->stream2));
+  CK(cudaStreamWaitEvent(st, rounds_done, 0));
+  CK(cudaEventDestroy(rounds_done));
+  return finish_blocks(ctx, t_next, rounds + 1);
 }
 
 int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,

@@ -66,11 +66,14 @@ void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
                            cudaStream_t stream);
 
 // convergence step for the active slots of one order
+// m = 0 sums and the convergence test of one order; grains that continue go
+// to next_active, grains whose order is final are appended to done_list
 void tmx_launch_converge(const int32_t *active, int nactive,
                          const TmxSlot *slots, const double2 *diag,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
-                         int32_t *next_count, cudaStream_t stream);
+                         int32_t *next_count, int32_t *done_list,
+                         int32_t *done_count, cudaStream_t stream);
 
 // full Q sums over all m blocks (TMatrixQTask)
 void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,

@@ -3,7 +3,9 @@
 //
 // This translation unit is compiled with --fmad=false: the recurrences below
 // follow the reference's operation order (src/SpecialFunctions.hpp) and, with
-// no fused multiply-add, round the way the reference's x86-64 build rounds.
+// no fused multiply-add, round the way the reference's x86-64 build rounds,
+// except for the complex reciprocal of the downward j_n(m k r) recurrence
+// (see bessel_j_complex).
 // Transcendentals (sin, cos, cosh, sinh) come from CUDA's libdevice and may
 // differ from the C library by an ulp.
 #include "tmx_common.cuh"
@@ -94,7 +96,11 @@ __device__ static cplx csin_dev(cplx z) {
 // Complex-argument version of bessel_j_real: every constant enters as a
 // complex number in the reference (std::complex arithmetic); multiplying by a
 // complex number with zero imaginary part equals scaling by its real part
-// bit for bit, which is what is done here.
+// bit for bit, which is what is done here. The reciprocal in the downward
+// recurrence is conj(w) / |w|^2 (one real division; |w| ~ (2n + 1) / |z|
+// is far from overflow and underflow), where the reference's complex
+// division takes three (Smith's algorithm): the ratios agree to the last
+// few bits.
 // out[(n-1) * stride + {0,1,2,3}] = (Re j, Im j, Re dj, Im dj)
 __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
                                         double *out, int stride) {
@@ -102,7 +108,9 @@ __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
   cplx cur = cdiv(z, mkc(2. * nstart + 1., 0.));
   for (int index = nstart - 1; index >= 1; --index) {
     const double twoip1 = 2. * index + 1.;
-    const cplx nxt = cinv(csub(cscale(zinv, twoip1), cur));
+    const cplx w = csub(cscale(zinv, twoip1), cur);
+    const double inv = 1. / (w.x * w.x + w.y * w.y);
+    const cplx nxt = mkc(w.x * inv, -w.y * inv);
     if (index - 1 < nmax) {
       out[(index - 1) * stride] = nxt.x;
       out[(index - 1) * stride + 1] = nxt.y;
@@ -128,8 +136,9 @@ __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
   }
 }
 
-// One block per slot; threads 0..ng-1 do the real-argument tables and node
-// scalars of node g, threads ng..2ng-1 the complex-argument tables.
+// Grid (slot, node chunk, kind): kind 0 threads do the real-argument tables
+// and node scalars of node g, kind 1 threads the complex-argument tables, so
+// every warp runs one recurrence type.
 // Node scalars follow GaussBasedResources::execute (GaussBasedResources.hpp:
 // 132-152), get_r_dr_spheroid (SpecialFunctions.hpp:872-893) and
 // InteractionTask::execute (InteractionResource.hpp:478-527).
@@ -149,9 +158,12 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
   const int ng = sl.ngauss;
   const double *x = gl_x + gl_off[ng];
   const double *w = gl_w + gl_off[ng];
-  for (int u = threadIdx.x; u < 2 * ng; u += blockDim.x) {
-    const int g = u % ng;
-    const int kind = u / ng;
+  const int kind = blockIdx.z;
+  {
+    const int g = blockIdx.y * blockDim.x + threadIdx.x;
+    if (g >= ng) {
+      return;
+    }
     const double c = x[g];
     const double s2 = (1. - c) * (1. + c);
     const double sn = sqrt(s2);
@@ -294,12 +306,14 @@ __global__ void k_wigner(const TmxWigJob *__restrict__ jobs, int njobs,
 void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
                        const double *gl_x, const double *gl_w,
                        const int64_t *gl_off, double *tab, double *nsc,
-                       int bessel_start, cudaStream_t stream) {
-  if (nslots <= 0) {
+                       int bessel_start, int ngmax, cudaStream_t stream) {
+  if (nslots <= 0 || ngmax <= 0) {
     return;
   }
-  k_tables<<<nslots, 128, 0, stream>>>(slots, nslots, grains, gl_x, gl_w,
-                                       gl_off, tab, nsc, bessel_start);
+  const int threads = 64;
+  dim3 grid(nslots, (ngmax + threads - 1) / threads, 2);
+  k_tables<<<grid, threads, 0, stream>>>(slots, nslots, grains, gl_x, gl_w,
+                                         gl_off, tab, nsc, bessel_start);
 }
 
 void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,

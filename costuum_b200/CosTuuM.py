@@ -340,3 +340,89 @@ def get_table(types, sizes, wavelengths, thetas, shape_distribution,
     if len(res) == 1:
         return res[0]
     return tuple(res)
+
+
+# ----------------------------------------------------------- plain path --
+
+class TMatrix:
+    """One particle's T-matrix on the plain path (CosTuuM.TMatrix,
+    PyTMatrix.hpp:118-227): converged with the calculator schedule
+    (TMatrixCalculator::calculate_TMatrix), then, for cos2beta >= 0,
+    averaged over the orientation distribution with expansion order
+    2 nmax: Davis-Greenstein for cos2beta 0 or 1, random orientation for
+    1/3, Mishchenko otherwise. Each object keeps its T-matrix on the GPU in
+    a context of its own. Angles are in radians, lengths in metres.
+    """
+
+    def __init__(self, particle_radius, axis_ratio, wavelength, refractive_index,
+                 cos2beta=1.0 / 3.0, tolerance=1e-4, maximum_order=200,
+                 gauss_legendre_factor=2, maximum_ngauss=500,
+                 is_equal_volume_radius=True):
+        from .tmatrix import Context
+        r = float(particle_radius)
+        if not is_equal_volume_radius:
+            r = get_equal_volume_radius(r, axis_ratio)
+        self._ctx = Context(0)
+        res = self._ctx.tmatrix_batch_calculator(
+            [r], float(wavelength), complex(refractive_index), float(axis_ratio),
+            maximum_order=maximum_order, tolerance=tolerance,
+            gauss_legendre_factor=gauss_legendre_factor,
+            maximum_ngauss=maximum_ngauss)
+        self._status = int(res.status[0])
+        if self._status & ~1:
+            raise RuntimeError("T-matrix calculation failed (status %d)" % self._status)
+        self._nmax = int(res.nmax[0])
+        self._ngauss = int(res.ngauss[0])
+        self._q = res.q[0].copy()
+        if cos2beta >= 0.0:
+            order = 2 * self._nmax
+            if cos2beta == 0.0 or cos2beta == 1.0:
+                od = DavisGreensteinOrientationDistribution(axis_ratio, order)
+            elif cos2beta == 1.0 / 3.0:
+                od = RandomOrientationDistribution(order)
+            else:
+                od = MishchenkoOrientationDistribution(cos2beta, order)
+            self._ctx.orientation_average(od.coefficients, [0])
+
+    @property
+    def converged(self):
+        """False where the reference would have aborted ("Unable to
+        converge!"): the order or quadrature limit was reached."""
+        return self._status == 0
+
+    def get_nmax(self):
+        return self._nmax
+
+    def get_ngauss(self):
+        return self._ngauss
+
+    def get_extinction_matrix(self, theta, phi, alpha=0.0, beta=0.0):
+        """K[theta, phi, 4, 4], squeezed."""
+        th = np.atleast_1d(np.asarray(theta, np.float64)).ravel()
+        ph = np.atleast_1d(np.asarray(phi, np.float64)).ravel()
+        T, P = np.meshgrid(th, ph, indexing="ij")
+        K = self._ctx.extinction_matrix(0, T, P, alpha, beta)
+        return np.squeeze(K)
+
+    def get_scattering_matrix(self, theta_in, phi_in, theta_out, phi_out,
+                              alpha=0.0, beta=0.0):
+        """Z[theta_in, phi_in, theta_out, phi_out, 4, 4], squeezed."""
+        a = [np.atleast_1d(np.asarray(x, np.float64)).ravel()
+             for x in (theta_in, phi_in, theta_out, phi_out)]
+        grids = np.meshgrid(*a, indexing="ij")
+        Z = self._ctx.scattering_matrix(0, grids[0], grids[1], grids[2], grids[3],
+                                        alpha, beta)
+        return np.squeeze(Z)
+
+    def get_absorption_cross_section(self, theta, ngauss=100):
+        """Cabs for each zenith angle (1D array)."""
+        th = np.atleast_1d(np.asarray(theta, np.float64)).ravel()
+        return self._ctx.absorption_cross_sections(0, th, ngauss)[:, 0].copy()
+
+    def get_absorption_cross_sections(self, theta, ngauss=100):
+        """(Cabs, Cabspol) for each zenith angle, squeezed."""
+        th = np.atleast_1d(np.asarray(theta, np.float64)).ravel()
+        return np.squeeze(self._ctx.absorption_cross_sections(0, th, ngauss))
+
+    def get_average_absorption_cross_section(self):
+        return self._ctx.average_absorption_cross_section(0, 20)

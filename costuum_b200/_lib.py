@@ -11,6 +11,7 @@ LIB_PATH = os.path.join(HERE, "libtmx.so")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I32 = ctypes.POINTER(ctypes.c_int32)
+_I64 = ctypes.POINTER(ctypes.c_int64)
 _VP = ctypes.c_void_p
 
 
@@ -35,6 +36,21 @@ SIGNATURES = {
     "tmx_batch_compute": (ctypes.c_int, [_VP]),
     "tmx_tmatrix_batch_fixed": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D,
                                                _D, _D, _I32, _I32]),
+    "tmx_tmatrix_batch_calculator": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D,
+                                                    _D, _D, ctypes.c_int32,
+                                                    ctypes.c_double, ctypes.c_int32,
+                                                    ctypes.c_int32]),
+    "tmx_batch_orientation_average": (ctypes.c_int, [_VP, _D, ctypes.c_int32,
+                                                     ctypes.c_int32, _I32]),
+    "tmx_batch_scattering_matrix": (ctypes.c_int, [_VP, ctypes.c_int64, _I64, _D, _D,
+                                                   _D, _D, _D, _D, _D, _D]),
+    "tmx_batch_extinction_matrix": (ctypes.c_int, [_VP, ctypes.c_int64, _I64, _D, _D,
+                                                   _D, _D, _D]),
+    "tmx_batch_absorption_cross_sections": (ctypes.c_int, [_VP, ctypes.c_int64,
+                                                           ctypes.c_int32, _D,
+                                                           ctypes.c_int32, _D]),
+    "tmx_batch_average_absorption_cross_section": (ctypes.c_int, [_VP, ctypes.c_int64,
+                                                                  ctypes.c_int32, _D]),
     "tmx_batch_results": (ctypes.c_int, [_VP, _I32, _I32, _I32, _D]),
     "tmx_batch_observables": (ctypes.c_int, [_VP, ctypes.c_int32, _D, _D,
                                              ctypes.c_int32, _D]),
@@ -92,6 +108,10 @@ def ptr(a):
 
 def iptr(a):
     return a.ctypes.data_as(_I32)
+
+
+def lptr(a):
+    return a.ctypes.data_as(_I64)
 
 
 # p(beta) callback of a custom orientation distribution

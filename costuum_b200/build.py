@@ -22,6 +22,7 @@ SOURCES = [
     ("tmx_host.cu", []),
     ("tmx_table.cu", []),
     ("tmx_noalloc.cu", []),
+    ("tmx_plain.cu", []),
 ]
 
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -82,6 +82,7 @@ struct tmx_ctx {
   // last batch
   int64_t n = 0;
   bool have_batch = false;
+  bool t_averaged = false; // T holds orientation averages (no gradients)
   std::vector<int32_t> nmax_h, ngauss_h, status_h;
   std::vector<double> q_h;
   std::vector<int64_t> t_off_h;
@@ -223,6 +224,16 @@ static inline int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep
 
 // Clebsch-Gordan table for all (n1, n2) <= nmax (tmx_table.cu)
 int tmx_ensure_cg(tmx_ctx *ctx, int nmax);
+
+// Host helpers of tmx_host.cu shared with the other host units: quadrature
+// and Wigner table caches, and every block of the given grains at their
+// orders in ctx->nmax_h / ctx->ngauss_h (one round, then the Q sums).
+#define TMX_HIDDEN __attribute__((visibility("hidden")))
+TMX_HIDDEN int tmx_ensure_gl(tmx_ctx *ctx, const std::vector<int> &ngs);
+TMX_HIDDEN int tmx_ensure_wigner(tmx_ctx *ctx,
+                                 const std::vector<std::pair<int, int>> &keys,
+                                 bool all_m, std::vector<int> &set_ids);
+TMX_HIDDEN int tmx_run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &grains);
 
 // Blocks of the last batch again in one round (tmx_host.cu), so that the p2
 // buffers hold the whole schedule for the tangent kernels.

@@ -637,6 +637,7 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   int rc;
   ctx->p2_t_total = t_total;
   ctx->p2_rounds = rounds;
+  ctx->t_averaged = false;
   if (t_total > 0) {
     if ((rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
         (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
@@ -1158,3 +1159,18 @@ int tmx_probe_fp64(tmx_ctx *ctx, int kind, double *tflops) {
 }
 
 } // extern "C"
+
+// ------------------------------------------- helpers for other host units --
+
+int tmx_ensure_gl(tmx_ctx *ctx, const std::vector<int> &ngs) {
+  return ensure_gl(ctx, ngs);
+}
+
+int tmx_ensure_wigner(tmx_ctx *ctx, const std::vector<std::pair<int, int>> &keys,
+                      bool all_m, std::vector<int> &set_ids) {
+  return ensure_wigner(ctx, keys, all_m, set_ids);
+}
+
+int tmx_run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &grains) {
+  return run_blocks(ctx, grains);
+}

@@ -136,14 +136,16 @@ struct TmxQJob {
 
 void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
                    int blocks, cudaStream_t stream);
-// orientation average (coef_set >= 0) or copy of every grain's T-matrix
-// with the amplitude factors c_{n' n} folded in; pair_base[g] = first
-// (n1, n2) pair of grain g (nmax^2 pairs per grain), mmax >= every nmax
+// orientation average (coef_set >= 0) or copy of every grain's T-matrix,
+// with the amplitude factors c_{n' n} folded in when fold != 0;
+// pair_base[g] = first (n1, n2) pair of grain g (nmax^2 pairs per grain),
+// mmax >= every nmax
 void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
                              int ngrains, int64_t npairs, const double2 *T,
                              double2 *Ta, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
-                             int cg_nmax, int mmax, cudaStream_t stream);
+                             int cg_nmax, int mmax, int fold,
+                             cudaStream_t stream);
 // CTAs of the amplitude kernel at full occupancy for nbmax (its work slots:
 // grid x 32 x (nbmax + 1) x 4 complex)
 int tmx_amp_grid(int nbmax);

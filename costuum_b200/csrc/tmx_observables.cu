@@ -173,7 +173,8 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
                int64_t npairs, const cplx *__restrict__ T,
                cplx *__restrict__ Ta, const double *__restrict__ coeffs,
                int ncoef, const int64_t *__restrict__ cg_off,
-               const double *__restrict__ cg, int cg_nmax, int wcap) {
+               const double *__restrict__ cg, int cg_nmax, int wcap,
+               int fold) {
   extern __shared__ cplx osh[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -199,13 +200,15 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
     const int M = min(n1, n2);
     const cplx *Tg = T + G.t_off;
     cplx *Tag = Ta + G.t_off;
-    const double afold = a_fac(n1) * a_fac(n2);
+    // fold = 0: the plain averaged T-matrix (c = 1: i^0 times 1)
+    const double afold = fold ? a_fac(n1) * a_fac(n2) : 1.;
+    const int nfold = fold ? n1 : n2 - 1;
     if (G.coef_set < 0) {
       for (int m = lane; m <= M; m += 32) {
         for (int q = 0; q < 4; ++q) {
           const int i1 = q >> 1, i2 = q & 1;
           const int64_t e = telem(N, m, i1, n1, i2, n2);
-          Tag[e] = c_fold(n2, n1, afold, Tg[e]);
+          Tag[e] = c_fold(n2, nfold, afold, Tg[e]);
         }
       }
       continue;
@@ -255,10 +258,10 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
         cfma(e01, S[2 * j], f);
         cfma(e10, S[2 * j + 1], f);
       }
-      Tag[telem(N, m, 0, n1, 0, n2)] = c_fold(n2, n1, afold, e00);
-      Tag[telem(N, m, 1, n1, 1, n2)] = c_fold(n2, n1, afold, e11);
-      Tag[telem(N, m, 0, n1, 1, n2)] = c_fold(n2, n1, afold, e01);
-      Tag[telem(N, m, 1, n1, 0, n2)] = c_fold(n2, n1, afold, e10);
+      Tag[telem(N, m, 0, n1, 0, n2)] = c_fold(n2, nfold, afold, e00);
+      Tag[telem(N, m, 1, n1, 1, n2)] = c_fold(n2, nfold, afold, e11);
+      Tag[telem(N, m, 0, n1, 1, n2)] = c_fold(n2, nfold, afold, e01);
+      Tag[telem(N, m, 1, n1, 0, n2)] = c_fold(n2, nfold, afold, e10);
     }
     __syncwarp();
   }
@@ -636,7 +639,8 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
                              int ngrains, int64_t npairs, const double2 *T,
                              double2 *Ta, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
-                             int cg_nmax, int mmax, cudaStream_t stream) {
+                             int cg_nmax, int mmax, int fold,
+                             cudaStream_t stream) {
   if (npairs <= 0) {
     return;
   }
@@ -648,7 +652,7 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
   const int blocks = (int)std::min<int64_t>(want, 148 * 8);
   k_orient_pairs<<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs, T,
                                                 Ta, coeffs, ncoef, cg_off, cg,
-                                                cg_nmax, wcap);
+                                                cg_nmax, wcap, fold);
 }
 
 static size_t amp_smem(int nbmax) {

@@ -8,6 +8,7 @@
 // DavisGreensteinOrientationDistribution.hpp:81-102,
 // ShapeDistribution.hpp:95-106, DraineHensleyShapeDistribution.hpp.
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <vector>
 
@@ -398,7 +399,7 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int64_t t_total, int ncoef,
                           ctx->o_npairs, Tsrc, (cplx *)ctx->Ta.p,
                           (const double *)ctx->o_coef.p, ncoef,
                           (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
-                          ctx->cg_nmax, ctx->o_nbmax, st);
+                          ctx->cg_nmax, ctx->o_nbmax, 1, st);
   LAUNCHED();
   const int grid = tmx_amp_grid(ctx->o_nbmax);
   if ((rc = ensure(ctx, ctx->o_x,
@@ -902,6 +903,10 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   cudaStream_t st = ctx->stream;
   const int64_t n = ctx->n;
   int rc;
+  if (ctx->t_averaged) {
+    return fail(ctx, TMX_ERR_STATE,
+                "gradients need the batch's own T-matrices, not orientation averages");
+  }
   if (ctx->p2_rounds > 1 && (rc = tmx_rerun_blocks(ctx))) {
     return rc;
   }
@@ -1003,5 +1008,510 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   CK(cudaMemcpyAsync(dq, ctx->o_gz.p, n * ntheta * 12 * sizeof(double),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  return TMX_OK;
+}
+
+// ------------------------------------------ plain-path observables (A25) --
+
+namespace {
+
+// Lab-frame direction (theta, phi) in the frame of a particle whose symmetry
+// axis points at (beta, alpha), and the 2 x 2 amplitude rotation between the
+// frames (TMatrix::get_forward_scattering_matrix, TMatrix.hpp:1306-1420).
+struct PDir {
+  TmxAngle a;        // cos, sin, 1/sin (or 9000) of the particle zenith
+  double cphi, sphi; // particle azimuth
+  double R[2][2];    // AP B AL
+};
+
+PDir particle_dir(double cosalpha, double sinalpha, double cosbeta,
+                  double sinbeta, double theta, double phi) {
+  PDir d;
+  const double ct = cos(theta), st = sin(theta);
+  const double cp = cos(phi), sp = sin(phi);
+  const double cosphirel = cp * cosalpha + sp * sinalpha;
+  const double sinphirel = sp * cosalpha - cp * sinalpha;
+  const double ctp = ct * cosbeta + st * sinbeta * cosphirel;
+  const double stp = sin(acos(ctp));
+  double cphi, sphi, sinv;
+  if (stp != 0.) {
+    sinv = 1. / stp;
+    cphi = (cosbeta * st * cosphirel - sinbeta * ct) * sinv;
+    sphi = st * sinphirel * sinv;
+  } else {
+    cphi = 1.;
+    sphi = 0.;
+    sinv = 9000.;
+  }
+  d.a.c = ctp;
+  d.a.s = stp;
+  d.a.si = sinv;
+  d.cphi = cphi;
+  d.sphi = sphi;
+  const double B[3][3] = {{cosalpha * cosbeta, sinalpha * cosbeta, -sinbeta},
+                          {-sinalpha, cosalpha, 0.},
+                          {cosalpha * sinbeta, sinalpha * sinbeta, cosbeta}};
+  const double AL[3][2] = {{ct * cp, -sp}, {ct * sp, cp}, {-st, 0.}};
+  const double AP[2][3] = {{ctp * cphi, ctp * sphi, -stp}, {-sphi, cphi, 0.}};
+  double C[3][2];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 2; ++j) {
+      C[i][j] = 0.;
+      for (int k = 0; k < 3; ++k) {
+        C[i][j] += B[i][k] * AL[k][j];
+      }
+    }
+  }
+  for (int i = 0; i < 2; ++i) {
+    for (int j = 0; j < 2; ++j) {
+      d.R[i][j] = 0.;
+      for (int k = 0; k < 3; ++k) {
+        d.R[i][j] += AP[i][k] * C[k][j];
+      }
+    }
+  }
+  return d;
+}
+
+// direction of a particle-frame zenith angle without rotation (the
+// four-angle form of get_forward_scattering_matrix, TMatrix.hpp:1245-1290)
+TmxAngle plain_angle(double theta) {
+  TmxAngle a;
+  a.c = cos(theta);
+  a.s = sin(theta);
+  a.si = (a.s != 0.) ? 1. / a.s : 9000.;
+  return a;
+}
+
+typedef std::complex<double> zc;
+
+// Z from the 2 x 2 amplitude matrix S (TMatrix.hpp:1896-1948), row major
+void z_from_s(const zc S[2][2], double *Z) {
+  const zc ic(0., 1.);
+  const double half(0.5);
+  Z[0] = (half * (S[0][0] * conj(S[0][0]) + S[0][1] * conj(S[0][1]) +
+                  S[1][0] * conj(S[1][0]) + S[1][1] * conj(S[1][1])))
+             .real();
+  Z[1] = (half * (S[0][0] * conj(S[0][0]) - S[0][1] * conj(S[0][1]) +
+                  S[1][0] * conj(S[1][0]) - S[1][1] * conj(S[1][1])))
+             .real();
+  Z[2] = (-S[0][0] * conj(S[0][1]) - S[1][1] * conj(S[1][0])).real();
+  Z[3] = (ic * (S[0][0] * conj(S[0][1]) - S[1][1] * conj(S[1][0]))).real();
+  Z[4] = (half * (S[0][0] * conj(S[0][0]) + S[0][1] * conj(S[0][1]) -
+                  S[1][0] * conj(S[1][0]) - S[1][1] * conj(S[1][1])))
+             .real();
+  Z[5] = (half * (S[0][0] * conj(S[0][0]) - S[0][1] * conj(S[0][1]) -
+                  S[1][0] * conj(S[1][0]) + S[1][1] * conj(S[1][1])))
+             .real();
+  Z[6] = (-S[0][0] * conj(S[0][1]) + S[1][1] * conj(S[1][0])).real();
+  Z[7] = (ic * (S[0][0] * conj(S[0][1]) + S[1][1] * conj(S[1][0]))).real();
+  Z[8] = (-S[0][0] * conj(S[1][0]) - S[1][1] * conj(S[0][1])).real();
+  Z[9] = (-S[0][0] * conj(S[1][0]) + S[1][1] * conj(S[0][1])).real();
+  Z[10] = (S[0][0] * conj(S[1][1]) + S[0][1] * conj(S[1][0])).real();
+  Z[11] = (-ic * (S[0][0] * conj(S[1][1]) + S[1][0] * conj(S[0][1]))).real();
+  Z[12] = (ic * (S[1][0] * conj(S[0][0]) + S[1][1] * conj(S[0][1]))).real();
+  Z[13] = (ic * (S[1][0] * conj(S[0][0]) - S[1][1] * conj(S[0][1]))).real();
+  Z[14] = (-ic * (S[1][1] * conj(S[0][0]) - S[0][1] * conj(S[1][0]))).real();
+  Z[15] = (S[1][1] * conj(S[0][0]) - S[0][1] * conj(S[1][0])).real();
+}
+
+// K from the forward amplitude matrix (TMatrix.hpp:1972-2010), row major
+void k_from_s(double k, const zc S[2][2], double *K) {
+  const double pf = 2. * M_PI / k;
+  for (int i = 0; i < 16; ++i) {
+    K[i] = 0.;
+  }
+  K[0] = pf * (S[0][0] + S[1][1]).imag();
+  K[5] = K[0];
+  K[10] = K[0];
+  K[15] = K[0];
+  K[1] = pf * (S[0][0] - S[1][1]).imag();
+  K[4] = K[1];
+  K[2] = -pf * (S[0][1] + S[1][0]).imag();
+  K[8] = K[2];
+  K[3] = pf * (S[1][0] - S[0][1]).real();
+  K[12] = K[3];
+  K[6] = pf * (S[1][0] - S[0][1]).imag();
+  K[9] = -K[6];
+  K[7] = -pf * (S[0][1] + S[1][0]).real();
+  K[13] = -K[7];
+  K[11] = pf * (S[1][1] - S[0][0]).real();
+  K[14] = -K[11];
+}
+
+// Amplitude matrices S^P of jobs (grain, incoming angle index, outgoing
+// angle index, e^{i(phi_out - phi_in)}) for the T-matrices of the last batch
+// (plain or averaged): sorted by grain for the amplitude kernel's groups,
+// results in job order.
+int plain_amplitudes(tmx_ctx *ctx, const std::vector<int32_t> &grain,
+                     const std::vector<TmxAngle> &ang,
+                     const std::vector<int32_t> &ain,
+                     const std::vector<int32_t> &aout,
+                     const std::vector<cplx> &e1, std::vector<zc> &S) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  const int64_t nj = (int64_t)grain.size();
+  int rc;
+  std::vector<TmxObsGrain> og(n);
+  for (int64_t g = 0; g < n; ++g) {
+    og[g].nmax = ctx->nmax_h[g];
+    og[g].coef_set = -1;
+    og[g].t_off = ctx->t_off_h[g];
+    og[g].k = ctx->up_grains[g].k;
+    og[g].r_ev = ctx->up_grains[g].r_ev;
+  }
+  std::vector<int64_t> order(nj);
+  for (int64_t j = 0; j < nj; ++j) {
+    order[j] = j;
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int64_t a, int64_t b) { return grain[a] < grain[b]; });
+  std::vector<TmxSJob> sj;
+  sj.reserve(nj);
+  for (int64_t q = 0; q < nj; ++q) {
+    const int64_t j = order[q];
+    if (og[grain[j]].nmax <= 0) {
+      continue;
+    }
+    TmxSJob J;
+    J.grain = grain[j];
+    J.angle_in = ain[j];
+    J.angle_out = aout[j];
+    J.nphi = 1;
+    J.phi0 = j;
+    J.out = j;
+    sj.push_back(J);
+  }
+  if ((rc = ensure(ctx, ctx->o_og, std::max<int64_t>(1, n) * sizeof(TmxObsGrain))) ||
+      (rc = ensure(ctx, ctx->o_angles, std::max<size_t>(1, ang.size()) * sizeof(TmxAngle))) ||
+      (rc = ensure(ctx, ctx->o_phis, std::max<size_t>(1, e1.size()) * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->o_sj, std::max<size_t>(1, sj.size()) * sizeof(TmxSJob))) ||
+      (rc = ensure(ctx, ctx->o_S, std::max<int64_t>(1, nj) * 4 * sizeof(cplx)))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->o_phis.p, e1.data(), e1.size() * sizeof(cplx),
+                     cudaMemcpyHostToDevice, st));
+  if (!sj.empty()) {
+    CK(cudaMemcpyAsync(ctx->o_sj.p, sj.data(), sj.size() * sizeof(TmxSJob),
+                       cudaMemcpyHostToDevice, st));
+  }
+  if ((rc = upload_obs_plan(ctx, og, sj)) ||
+      (rc = run_amplitudes(ctx, (const cplx *)ctx->T.p, ctx->p2_t_total, 1,
+                           (cplx *)ctx->o_S.p, nj))) {
+    return rc;
+  }
+  std::vector<cplx> Sh(4 * nj);
+  CK(cudaMemcpyAsync(Sh.data(), ctx->o_S.p, 4 * nj * sizeof(cplx),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  S.resize(4 * nj);
+  for (int64_t i = 0; i < 4 * nj; ++i) {
+    S[i] = zc(Sh[i].x, Sh[i].y);
+  }
+  return TMX_OK;
+}
+
+int check_jobs(tmx_ctx *ctx, int64_t njobs, const int64_t *grain) {
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  for (int64_t j = 0; j < njobs; ++j) {
+    if (grain[j] < 0 || grain[j] >= ctx->n) {
+      return fail(ctx, TMX_ERR_INVALID, "grain index out of range");
+    }
+  }
+  return TMX_OK;
+}
+
+// lab-frame S for jobs at particle orientations: S^L = R_out^-1 S^P R_in
+// (TMatrix.hpp:1420-1460)
+int lab_amplitudes(tmx_ctx *ctx, int64_t njobs, const int64_t *grain,
+                   const double *alpha, const double *beta,
+                   const double *theta_in, const double *phi_in,
+                   const double *theta_out, const double *phi_out,
+                   std::vector<zc> &SL) {
+  std::vector<int32_t> g(njobs), ain(njobs), aout(njobs);
+  std::vector<TmxAngle> ang(2 * njobs);
+  std::vector<cplx> e1(njobs);
+  std::vector<PDir> din(njobs), dout(njobs);
+  for (int64_t j = 0; j < njobs; ++j) {
+    const double ca = cos(alpha[j]), sa = sin(alpha[j]);
+    const double cb = cos(beta[j]), sb = sin(beta[j]);
+    din[j] = particle_dir(ca, sa, cb, sb, theta_in[j], phi_in[j]);
+    dout[j] = particle_dir(ca, sa, cb, sb, theta_out[j], phi_out[j]);
+    g[j] = (int32_t)grain[j];
+    ang[2 * j] = din[j].a;
+    ang[2 * j + 1] = dout[j].a;
+    ain[j] = (int32_t)(2 * j);
+    aout[j] = (int32_t)(2 * j + 1);
+    e1[j] = mkc(dout[j].cphi * din[j].cphi + dout[j].sphi * din[j].sphi,
+                dout[j].sphi * din[j].cphi - dout[j].cphi * din[j].sphi);
+  }
+  std::vector<zc> SP;
+  int rc = plain_amplitudes(ctx, g, ang, ain, aout, e1, SP);
+  if (rc) {
+    return rc;
+  }
+  SL.resize(4 * njobs);
+  for (int64_t j = 0; j < njobs; ++j) {
+    const zc *S = SP.data() + 4 * j;
+    const double(&Ri)[2][2] = din[j].R;
+    double Ro[2][2];
+    const double det = 1. / (dout[j].R[0][0] * dout[j].R[1][1] -
+                             dout[j].R[0][1] * dout[j].R[1][0]);
+    Ro[0][0] = dout[j].R[1][1] * det;
+    Ro[0][1] = -dout[j].R[0][1] * det;
+    Ro[1][0] = -dout[j].R[1][0] * det;
+    Ro[1][1] = dout[j].R[0][0] * det;
+    const zc cS11 = S[0] * Ri[0][0] + S[1] * Ri[1][0];
+    const zc cS12 = S[0] * Ri[0][1] + S[1] * Ri[1][1];
+    const zc cS21 = S[2] * Ri[0][0] + S[3] * Ri[1][0];
+    const zc cS22 = S[2] * Ri[0][1] + S[3] * Ri[1][1];
+    SL[4 * j + 0] = Ro[0][0] * cS11 + Ro[0][1] * cS21;
+    SL[4 * j + 1] = Ro[0][0] * cS12 + Ro[0][1] * cS22;
+    SL[4 * j + 2] = Ro[1][0] * cS11 + Ro[1][1] * cS21;
+    SL[4 * j + 3] = Ro[1][0] * cS12 + Ro[1][1] * cS22;
+  }
+  return TMX_OK;
+}
+
+// absorption cross sections (Cabs, Cabspol) of one grain at zenith angles
+// th: per angle the forward amplitude and ngauss^2 incoming directions
+// (TMatrix.hpp:2133-2200)
+int absorption(tmx_ctx *ctx, int32_t grain, int32_t ntheta, const double *th,
+               int32_t ngauss, double *out) {
+  std::vector<double> ct(ngauss), wt(ngauss), ph(ngauss), wp(ngauss), tg(ngauss);
+  tmx_host_gauss_legendre(ngauss, ct.data(), wt.data());
+  gl_ab(ngauss, 0., 2. * M_PI, ph.data(), wp.data());
+  for (int i = 0; i < ngauss; ++i) {
+    tg[i] = acos(ct[i]);
+  }
+  std::vector<TmxAngle> ang;
+  for (int i = 0; i < ngauss; ++i) {
+    ang.push_back(plain_angle(tg[i]));
+  }
+  const int a0 = (int)ang.size();
+  for (int t = 0; t < ntheta; ++t) {
+    ang.push_back(plain_angle(th[t]));
+  }
+  std::vector<int32_t> g, ain, aout;
+  std::vector<cplx> e1;
+  for (int t = 0; t < ntheta; ++t) {
+    g.push_back(grain);
+    ain.push_back(a0 + t);
+    aout.push_back(a0 + t);
+    e1.push_back(mkc(1., 0.));
+    for (int it = 0; it < ngauss; ++it) {
+      for (int ip = 0; ip < ngauss; ++ip) {
+        // e^{i(0 - phi_in)} as the reference forms it
+        const double cp = cos(ph[ip]), sp = sin(ph[ip]);
+        g.push_back(grain);
+        ain.push_back(it);
+        aout.push_back(a0 + t);
+        e1.push_back(mkc(1. * cp + 0. * sp, 0. * cp - 1. * sp));
+      }
+    }
+  }
+  std::vector<zc> S;
+  int rc = plain_amplitudes(ctx, g, ang, ain, aout, e1, S);
+  if (rc) {
+    return rc;
+  }
+  const double pf = 2. * M_PI / ctx->up_grains[grain].k;
+  const double half(0.5);
+  int64_t j = 0;
+  for (int t = 0; t < ntheta; ++t) {
+    const zc *s = S.data() + 4 * j++;
+    double c0 = pf * (s[0] + s[3]).imag();
+    double c1 = pf * (s[0] - s[3]).imag();
+    for (int it = 0; it < ngauss; ++it) {
+      for (int ip = 0; ip < ngauss; ++ip) {
+        const zc *q = S.data() + 4 * j++;
+        const double w = wt[it] * wp[ip];
+        const double z00 = (half * (q[0] * conj(q[0]) + q[1] * conj(q[1]) +
+                                    q[2] * conj(q[2]) + q[3] * conj(q[3])))
+                               .real();
+        const double z10 = (half * (q[0] * conj(q[0]) + q[1] * conj(q[1]) -
+                                    q[2] * conj(q[2]) - q[3] * conj(q[3])))
+                               .real();
+        c0 -= z00 * w;
+        c1 -= z10 * w;
+      }
+    }
+    out[2 * t] = c0;
+    out[2 * t + 1] = c1;
+  }
+  return TMX_OK;
+}
+
+} // namespace
+
+extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
+                                             int32_t nsets, int32_t ncoef,
+                                             const int32_t *coef_set) {
+  if (!ctx || nsets < 0 || (nsets > 0 && (!coeffs || ncoef < 1))) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  CK(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->n;
+  int rc;
+  std::vector<TmxObsGrain> og(n);
+  int nmax_b = 1;
+  for (int64_t g = 0; g < n; ++g) {
+    og[g].nmax = ctx->nmax_h[g];
+    og[g].coef_set = coef_set ? coef_set[g] : -1;
+    og[g].t_off = ctx->t_off_h[g];
+    og[g].k = ctx->up_grains[g].k;
+    og[g].r_ev = ctx->up_grains[g].r_ev;
+    if (og[g].coef_set >= nsets) {
+      return fail(ctx, TMX_ERR_INVALID, "orientation set index");
+    }
+    if (og[g].coef_set >= 0 && og[g].nmax > 0 && 2 * og[g].nmax + 1 > ncoef) {
+      return fail(ctx, TMX_ERR_INVALID,
+                  "orientation coefficients shorter than 2 nmax + 1");
+    }
+    nmax_b = std::max(nmax_b, og[g].nmax);
+  }
+  const int64_t t_total = ctx->p2_t_total;
+  if ((rc = ensure(ctx, ctx->o_og, std::max<int64_t>(1, n) * sizeof(TmxObsGrain))) ||
+      (rc = ensure(ctx, ctx->o_coef, std::max<int64_t>(1, (int64_t)nsets * ncoef) * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->Ta, std::max<int64_t>(1, t_total) * sizeof(cplx))) ||
+      (rc = tmx_ensure_cg(ctx, nmax_b))) {
+    return rc;
+  }
+  CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
+                     cudaMemcpyHostToDevice, st));
+  if (nsets > 0) {
+    CK(cudaMemcpyAsync(ctx->o_coef.p, coeffs, (int64_t)nsets * ncoef * sizeof(double),
+                       cudaMemcpyHostToDevice, st));
+  }
+  if ((rc = upload_obs_plan(ctx, og, std::vector<TmxSJob>()))) {
+    return rc;
+  }
+  if (t_total > 0 && ctx->o_npairs > 0) {
+    tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
+                            (const int64_t *)ctx->o_pairs.p, (int)n, ctx->o_npairs,
+                            (const cplx *)ctx->T.p, (cplx *)ctx->Ta.p,
+                            (const double *)ctx->o_coef.p, ncoef,
+                            (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
+                            ctx->cg_nmax, ctx->o_nbmax, 0, st);
+    LAUNCHED();
+    std::swap(ctx->T, ctx->Ta);
+  }
+  CK(cudaStreamSynchronize(st));
+  ctx->t_averaged = true;
+  return TMX_OK;
+}
+
+extern "C" int tmx_batch_scattering_matrix(
+    tmx_ctx *ctx, int64_t njobs, const int64_t *grain, const double *alpha,
+    const double *beta, const double *theta_in, const double *phi_in,
+    const double *theta_out, const double *phi_out, double *Z, double *S) {
+  if (!ctx || njobs < 0 || (njobs > 0 && (!grain || !alpha || !beta || !theta_in ||
+                                          !phi_in || !theta_out || !phi_out ||
+                                          (!Z && !S)))) {
+    return TMX_ERR_INVALID;
+  }
+  int rc;
+  if ((rc = check_jobs(ctx, njobs, grain))) {
+    return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  std::vector<zc> SL;
+  if ((rc = lab_amplitudes(ctx, njobs, grain, alpha, beta, theta_in, phi_in,
+                           theta_out, phi_out, SL))) {
+    return rc;
+  }
+  for (int64_t j = 0; j < njobs; ++j) {
+    const zc M[2][2] = {{SL[4 * j], SL[4 * j + 1]}, {SL[4 * j + 2], SL[4 * j + 3]}};
+    if (Z) {
+      z_from_s(M, Z + 16 * j);
+    }
+    if (S) {
+      for (int q = 0; q < 4; ++q) {
+        S[8 * j + 2 * q] = SL[4 * j + q].real();
+        S[8 * j + 2 * q + 1] = SL[4 * j + q].imag();
+      }
+    }
+  }
+  return TMX_OK;
+}
+
+extern "C" int tmx_batch_extinction_matrix(tmx_ctx *ctx, int64_t njobs,
+                                           const int64_t *grain,
+                                           const double *alpha,
+                                           const double *beta,
+                                           const double *theta,
+                                           const double *phi, double *K) {
+  if (!ctx || njobs < 0 ||
+      (njobs > 0 && (!grain || !alpha || !beta || !theta || !phi || !K))) {
+    return TMX_ERR_INVALID;
+  }
+  int rc;
+  if ((rc = check_jobs(ctx, njobs, grain))) {
+    return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  std::vector<zc> SL;
+  if ((rc = lab_amplitudes(ctx, njobs, grain, alpha, beta, theta, phi, theta,
+                           phi, SL))) {
+    return rc;
+  }
+  for (int64_t j = 0; j < njobs; ++j) {
+    const zc M[2][2] = {{SL[4 * j], SL[4 * j + 1]}, {SL[4 * j + 2], SL[4 * j + 3]}};
+    k_from_s(ctx->up_grains[grain[j]].k, M, K + 16 * j);
+  }
+  return TMX_OK;
+}
+
+extern "C" int tmx_batch_absorption_cross_sections(tmx_ctx *ctx, int64_t grain,
+                                                   int32_t ntheta,
+                                                   const double *theta,
+                                                   int32_t ngauss, double *out) {
+  if (!ctx || ntheta < 0 || ngauss < 1 || (ntheta > 0 && (!theta || !out))) {
+    return TMX_ERR_INVALID;
+  }
+  int rc;
+  if ((rc = check_jobs(ctx, 1, &grain))) {
+    return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  return absorption(ctx, (int32_t)grain, ntheta, theta, ngauss, out);
+}
+
+extern "C" int tmx_batch_average_absorption_cross_section(tmx_ctx *ctx,
+                                                          int64_t grain,
+                                                          int32_t ngauss,
+                                                          double *out) {
+  if (!ctx || ngauss < 1 || !out) {
+    return TMX_ERR_INVALID;
+  }
+  int rc;
+  if ((rc = check_jobs(ctx, 1, &grain))) {
+    return rc;
+  }
+  CK(cudaSetDevice(ctx->device));
+  // TMatrix::get_average_absorption_cross_section (TMatrix.hpp:2260-2287)
+  std::vector<double> ct(ngauss), wt(ngauss), tg(ngauss), cabs(2 * ngauss);
+  tmx_host_gauss_legendre(ngauss, ct.data(), wt.data());
+  for (int i = 0; i < ngauss; ++i) {
+    tg[i] = acos(ct[i]);
+  }
+  if ((rc = absorption(ctx, (int32_t)grain, ngauss, tg.data(), ngauss, cabs.data()))) {
+    return rc;
+  }
+  double result = 0.;
+  for (int i = 0; i < ngauss; ++i) {
+    result += cabs[2 * i] * wt[i];
+  }
+  *out = 0.5 * result;
   return TMX_OK;
 }

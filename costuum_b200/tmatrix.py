@@ -148,6 +148,95 @@ class Context:
             _lib.check(self._h, rc, "tmx_tmatrix_batch_fixed")
             return self._results(n)
 
+    def tmatrix_batch_calculator(self, r_ev, wavelength, m, axis_ratio,
+                                 maximum_order=200, tolerance=1e-4,
+                                 gauss_legendre_factor=2, maximum_ngauss=500):
+        """Converged T-matrices on the plain path's schedule (order loop, then
+        quadrature loop; TMatrixCalculator::calculate_TMatrix)."""
+        r_ev = np.ascontiguousarray(r_ev, np.float64).ravel()
+        n = r_ev.size
+        wl = np.ascontiguousarray(np.broadcast_to(wavelength, (n,)), np.float64)
+        mm = np.broadcast_to(np.asarray(m, np.complex128), (n,))
+        mr = np.ascontiguousarray(mm.real)
+        mi = np.ascontiguousarray(mm.imag)
+        d = np.ascontiguousarray(np.broadcast_to(axis_ratio, (n,)), np.float64)
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_tmatrix_batch_calculator(
+                self._h, n, _lib.ptr(r_ev), _lib.ptr(wl), _lib.ptr(mr), _lib.ptr(mi),
+                _lib.ptr(d), int(maximum_order), float(tolerance),
+                int(gauss_legendre_factor), int(maximum_ngauss))
+            _lib.check(self._h, rc, "tmx_tmatrix_batch_calculator")
+            return self._results(n)
+
+    def orientation_average(self, coefficient_sets, coef_set):
+        """Replace the last batch's T-matrices by orientation averages:
+        coef_set[i] indexes a row of coefficient_sets, -1 keeps grain i."""
+        c = np.ascontiguousarray(np.atleast_2d(coefficient_sets), np.float64)
+        idx = np.ascontiguousarray(coef_set, np.int32)
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_batch_orientation_average(self._h, _lib.ptr(c), c.shape[0],
+                                                   c.shape[1], _lib.iptr(idx))
+            _lib.check(self._h, rc, "tmx_batch_orientation_average")
+
+    @staticmethod
+    def _jobs(grain, *angles):
+        arrs = np.broadcast_arrays(np.asarray(grain, np.int64),
+                                   *[np.asarray(a, np.float64) for a in angles])
+        shape = arrs[0].shape
+        return shape, [np.ascontiguousarray(a.ravel()) for a in arrs]
+
+    def scattering_matrix(self, grain, theta_in, phi_in, theta_out, phi_out,
+                          alpha=0.0, beta=0.0):
+        """Z (..., 4, 4) for lab-frame directions at particle orientation
+        (alpha, beta); arguments broadcast against each other."""
+        shape, (g, a, b, ti, pi, to, po) = self._jobs(grain, alpha, beta, theta_in,
+                                                       phi_in, theta_out, phi_out)
+        Z = np.zeros((g.size, 16))
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_batch_scattering_matrix(self._h, g.size, _lib.lptr(g),
+                                                 _lib.ptr(a), _lib.ptr(b), _lib.ptr(ti),
+                                                 _lib.ptr(pi), _lib.ptr(to),
+                                                 _lib.ptr(po), _lib.ptr(Z), None)
+            _lib.check(self._h, rc, "tmx_batch_scattering_matrix")
+        return Z.reshape(shape + (4, 4))
+
+    def extinction_matrix(self, grain, theta, phi, alpha=0.0, beta=0.0):
+        """K (..., 4, 4) for the lab-frame direction (theta, phi)."""
+        shape, (g, a, b, t, p) = self._jobs(grain, alpha, beta, theta, phi)
+        K = np.zeros((g.size, 16))
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_batch_extinction_matrix(self._h, g.size, _lib.lptr(g),
+                                                 _lib.ptr(a), _lib.ptr(b), _lib.ptr(t),
+                                                 _lib.ptr(p), _lib.ptr(K))
+            _lib.check(self._h, rc, "tmx_batch_extinction_matrix")
+        return K.reshape(shape + (4, 4))
+
+    def absorption_cross_sections(self, grain, theta, ngauss=100):
+        """(ntheta, 2) array of (Cabs, Cabspol) of one grain."""
+        th = np.ascontiguousarray(np.atleast_1d(theta), np.float64)
+        out = np.zeros((th.size, 2))
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_batch_absorption_cross_sections(self._h, int(grain), th.size,
+                                                         _lib.ptr(th), int(ngauss),
+                                                         _lib.ptr(out))
+            _lib.check(self._h, rc, "tmx_batch_absorption_cross_sections")
+        return out
+
+    def average_absorption_cross_section(self, grain, ngauss=20):
+        out = np.zeros(1)
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_batch_average_absorption_cross_section(self._h, int(grain),
+                                                                int(ngauss),
+                                                                _lib.ptr(out))
+            _lib.check(self._h, rc, "tmx_batch_average_absorption_cross_section")
+        return float(out[0])
+
     def _results(self, n):
         self._n = n
         lib = _lib.load()

@@ -108,6 +108,24 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
                             const double *mi, const double *axis_ratio,
                             const int32_t *nmax, const int32_t *ngauss);
 
+/* Converged T-matrices on the plain path's schedule
+ * (TMatrixCalculator::calculate_TMatrix, src/TMatrixCalculator.hpp:64-213,
+ * which the reference runs one grain at a time): starting at
+ * nmax = int(max(4, x + 4.05 x^(1/3))), raise nmax until the m = 0 Qsca and
+ * Qext change by <= tolerance (ngauss = ndgs nmax), then raise ngauss from
+ * ndgs nmax + 1 until they change by <= tolerance; then every m block at the
+ * final (nmax, ngauss). r_ev is the equal-volume radius. A grain that reaches
+ * maximum_order or maximum_ngauss (the reference aborts) gets
+ * TMX_GRAIN_NOT_CONVERGED and keeps its last order; one that needs an order
+ * above 128 gets TMX_GRAIN_TOO_LARGE. Results as for tmx_tmatrix_batch;
+ * q[6 i + 0], q[6 i + 1] hold the m = 0 sums of the last step and
+ * q[6 i + 4], q[6 i + 5] their relative changes. */
+int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                                 const double *wavelength, const double *mr,
+                                 const double *mi, const double *axis_ratio,
+                                 int32_t maximum_order, double tolerance,
+                                 int32_t ndgs, int32_t maximum_ngauss);
+
 /* Per-grain results of the last batch (any pointer may be NULL):
  * nmax, ngauss, status bits, and q[6 * i + {0..5}] =
  * {m=0 Qsca, m=0 Qext of the converged order, full Qsca, full Qext
@@ -219,6 +237,53 @@ int tmx_batch_observables(tmx_ctx *ctx, int32_t ntheta, const double *thetas,
 int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta, const double *thetas,
                         const double *coeffs, int32_t ncoef, double *q,
                         double *dq);
+
+/* ------------------------------------------- plain-path observables ---
+ *
+ * The per-particle queries of the reference's TMatrix object
+ * (src/PyTMatrix.hpp, src/TMatrix.hpp), for any grain of the last batch.
+ *
+ * Replace every grain's T-matrix by its orientation average
+ * (TMatrixCalculator::apply_orientation_distribution,
+ * src/TMatrixCalculator.hpp:229-307): coef_set[i] selects row coef_set[i] of
+ * coeffs (nsets x ncoef expansion coefficients p_0..), -1 keeps grain i.
+ * Gradients are unavailable afterwards. */
+int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
+                                  int32_t nsets, int32_t ncoef,
+                                  const int32_t *coef_set);
+
+/* Scattering matrices Z (row-major 4 x 4 per job) and, if S is not NULL,
+ * the amplitude matrices S (2 x 2 complex per job) for incoming
+ * (theta_in, phi_in) and outgoing (theta_out, phi_out) lab-frame directions
+ * at a particle whose symmetry axis has azimuth alpha and zenith beta
+ * (TMatrix::get_scattering_matrix, src/TMatrix.hpp:1891-1952, with the frame
+ * rotation of :1306-1482). Angles in radians; grain[j] indexes the batch. */
+int tmx_batch_scattering_matrix(tmx_ctx *ctx, int64_t njobs,
+                                const int64_t *grain, const double *alpha,
+                                const double *beta, const double *theta_in,
+                                const double *phi_in, const double *theta_out,
+                                const double *phi_out, double *Z, double *S);
+
+/* Extinction matrices K (row-major 4 x 4 per job) for the direction
+ * (theta, phi) (TMatrix::get_extinction_matrix, src/TMatrix.hpp:1972-2010). */
+int tmx_batch_extinction_matrix(tmx_ctx *ctx, int64_t njobs,
+                                const int64_t *grain, const double *alpha,
+                                const double *beta, const double *theta,
+                                const double *phi, double *K);
+
+/* Absorption cross sections (Cabs, Cabspol) at zenith angles theta: the
+ * forward-amplitude extinction minus the scattering integral over ngauss x
+ * ngauss incoming directions (TMatrix::get_absorption_cross_sections,
+ * src/TMatrix.hpp:2133-2225); out[2 t], out[2 t + 1]. */
+int tmx_batch_absorption_cross_sections(tmx_ctx *ctx, int64_t grain,
+                                        int32_t ntheta, const double *theta,
+                                        int32_t ngauss, double *out);
+
+/* Orientation-averaged absorption cross section: the Cabs of the ngauss
+ * Gauss-Legendre zenith angles, weighted and halved
+ * (TMatrix::get_average_absorption_cross_section, src/TMatrix.hpp:2260-2287). */
+int tmx_batch_average_absorption_cross_section(tmx_ctx *ctx, int64_t grain,
+                                               int32_t ngauss, double *out);
 
 /* T-matrix of one grain at a fixed (nmax, ngauss), all m blocks, for callers
  * that cannot allocate device memory -- e.g. a host application whose device

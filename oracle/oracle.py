@@ -84,6 +84,13 @@ def lib():
                                     ctypes.c_int, ctypes.c_int, _D]
         L.or_scattering_matrix.argtypes = [ctypes.c_int, _D, ctypes.c_double,
                                            ctypes.c_int, _D]
+        L.or_calculator_orders.argtypes = ([ctypes.c_double] * 5 + [ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, _I, _I])
+        L.or_calculator_orders.restype = ctypes.c_int
+        L.or_amplitude_lab.argtypes = [ctypes.c_int, _D] + [ctypes.c_double] * 7 + [_D]
+        L.or_z_from_s.argtypes = [_D, _D]
+        L.or_k_from_s.argtypes = [ctypes.c_double, _D, _D]
         _lib = L
     return _lib
 
@@ -250,6 +257,49 @@ def absorption(T, nmax, wavelength, r_ev, theta, ngauss=20,
     lib().or_absorption(nmax, _p(_cplx(T)), wavelength, r_ev, len(theta),
                         _p(theta), ngauss, int(account_for_scattering), _p(out))
     return out
+
+
+def calculator_orders(r_ev, wavelength, m, d, maximum_order=200, tolerance=1e-4,
+                      ndgs=2, maximum_ngauss=500):
+    """Plain-path (TMatrixCalculator) orders: (nmax, ngauss, status)."""
+    nm = ctypes.c_int(0)
+    ng = ctypes.c_int(0)
+    st = lib().or_calculator_orders(r_ev, wavelength, m.real, m.imag, d,
+                                    maximum_order, tolerance, ndgs, maximum_ngauss,
+                                    ctypes.byref(nm), ctypes.byref(ng))
+    return nm.value, ng.value, st
+
+
+def full_tmatrix(r_ev, wavelength, m, d, nmax, ngauss):
+    """Every block at (nmax, ngauss), flat complex in the block layout."""
+    T = np.zeros(tmatrix_size(nmax), np.complex128)
+    T0, _, _ = tmatrix_m0(r_ev, wavelength, m, d, nmax, ngauss)
+    T[:4 * nmax * nmax] = T0.ravel()
+    for mm in range(1, nmax + 1):
+        o = block_offset(nmax, mm)
+        blk = tmatrix_mblock(r_ev, wavelength, m, d, nmax, ngauss, mm)
+        T[o:o + blk.size] = blk.ravel()
+    return T
+
+
+def amplitude_lab(T, nmax, wavelength, alpha, beta, theta_in, phi_in, theta_out,
+                  phi_out):
+    S = np.zeros((2, 2), np.complex128)
+    lib().or_amplitude_lab(nmax, _p(_cplx(T)), wavelength, alpha, beta, theta_in,
+                           phi_in, theta_out, phi_out, _p(S))
+    return S
+
+
+def z_from_s(S):
+    Z = np.zeros((4, 4))
+    lib().or_z_from_s(_p(np.ascontiguousarray(S, np.complex128)), _p(Z))
+    return Z
+
+
+def k_from_s(wavelength, S):
+    K = np.zeros((4, 4))
+    lib().or_k_from_s(wavelength, _p(np.ascontiguousarray(S, np.complex128)), _p(K))
+    return K
 
 
 def scattering_matrix(T, nmax, wavelength, ntheta):

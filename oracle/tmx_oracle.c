@@ -1378,3 +1378,189 @@ void or_scattering_matrix(int nmax, const double *Td, double wavelength,
   free(phi);
   free(wphi);
 }
+
+/* ------------------------------------------------------------ plain path --- */
+
+/* TMatrixCalculator::calculate_TMatrix (TMatrixCalculator.hpp:64-213): the
+ * order loop (ngauss = ndgs nmax) and then the quadrature loop on the m = 0
+ * sums. Returns 0, or 1 where the reference aborts ("Unable to converge!"). */
+int or_calculator_orders(double r_ev, double wavelength, double mr, double mi,
+                         double axis_ratio, int maximum_order, double tolerance,
+                         int ndgs, int maximum_ngauss, int *nmax_out,
+                         int *ngauss_out) {
+  const double xev = 2. * M_PI * r_ev / wavelength;
+  int nmax = (int)fmax(4., xev + 4.05 * cbrt(xev));
+  double old_qext = 0., old_qsca = 0., dext = 1., dsca = 1.;
+  int status = 0;
+  while (nmax < maximum_order && (dext > tolerance || dsca > tolerance)) {
+    const int ngauss = ndgs * nmax;
+    double *T0 = (double *)malloc(sizeof(double) * 8 * nmax * nmax);
+    double qsca, qext;
+    or_tmatrix_m0(r_ev, wavelength, mr, mi, axis_ratio, nmax, ngauss, T0, &qsca,
+                  &qext);
+    free(T0);
+    dsca = fabs((old_qsca - qsca) / qsca);
+    dext = fabs((old_qext - qext) / qext);
+    old_qext = qext;
+    old_qsca = qsca;
+    ++nmax;
+  }
+  if (nmax == maximum_order) {
+    *nmax_out = nmax - 1;
+    *ngauss_out = ndgs * (nmax - 1);
+    return 1;
+  }
+  --nmax;
+  int ngauss = nmax * ndgs + 1;
+  dext = tolerance + 1.;
+  dsca = tolerance + 1.;
+  while (ngauss < maximum_ngauss && (dext > tolerance || dsca > tolerance)) {
+    double *T0 = (double *)malloc(sizeof(double) * 8 * nmax * nmax);
+    double qsca, qext;
+    or_tmatrix_m0(r_ev, wavelength, mr, mi, axis_ratio, nmax, ngauss, T0, &qsca,
+                  &qext);
+    free(T0);
+    dsca = fabs((old_qsca - qsca) / qsca);
+    dext = fabs((old_qext - qext) / qext);
+    old_qext = qext;
+    old_qsca = qsca;
+    ++ngauss;
+  }
+  if (ngauss == maximum_ngauss) {
+    status = 1;
+  }
+  --ngauss;
+  *nmax_out = nmax;
+  *ngauss_out = ngauss;
+  return status;
+}
+
+/* particle-frame direction and amplitude rotation of a lab direction
+ * (TMatrix::get_forward_scattering_matrix, TMatrix.hpp:1306-1420) */
+struct pdir {
+  double c, s, si, cphi, sphi;
+  double R[2][2];
+};
+
+static void particle_dir(double ca, double sa, double cb, double sb,
+                         double theta, double phi, struct pdir *d) {
+  const double ct = cos(theta), st = sin(theta);
+  const double cp = cos(phi), sp = sin(phi);
+  const double cosphirel = cp * ca + sp * sa;
+  const double sinphirel = sp * ca - cp * sa;
+  const double ctp = ct * cb + st * sb * cosphirel;
+  const double stp = sin(acos(ctp));
+  if (stp != 0.) {
+    d->si = 1. / stp;
+    d->cphi = (cb * st * cosphirel - sb * ct) * d->si;
+    d->sphi = st * sinphirel * d->si;
+  } else {
+    d->cphi = 1.;
+    d->sphi = 0.;
+    d->si = 9000.;
+  }
+  d->c = ctp;
+  d->s = stp;
+  const double B[3][3] = {{ca * cb, sa * cb, -sb}, {-sa, ca, 0.}, {ca * sb, sa * sb, cb}};
+  const double AL[3][2] = {{ct * cp, -sp}, {ct * sp, cp}, {-st, 0.}};
+  const double AP[2][3] = {{ctp * d->cphi, ctp * d->sphi, -stp}, {-d->sphi, d->cphi, 0.}};
+  double C[3][2];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 2; ++j) {
+      C[i][j] = 0.;
+      for (int k = 0; k < 3; ++k) {
+        C[i][j] += B[i][k] * AL[k][j];
+      }
+    }
+  }
+  for (int i = 0; i < 2; ++i) {
+    for (int j = 0; j < 2; ++j) {
+      d->R[i][j] = 0.;
+      for (int k = 0; k < 3; ++k) {
+        d->R[i][j] += AP[i][k] * C[k][j];
+      }
+    }
+  }
+}
+
+void or_amplitude_lab(int nmax, const double *Td, double wavelength, double alpha,
+                      double beta, double theta_in, double phi_in,
+                      double theta_out, double phi_out, double *Sout) {
+  const cplx *T = (const cplx *)Td;
+  const double k = 2. * M_PI / wavelength;
+  const double ca = cos(alpha), sa = sin(alpha), cb = cos(beta), sb = sin(beta);
+  struct pdir din, dout;
+  particle_dir(ca, sa, cb, sb, theta_in, phi_in, &din);
+  particle_dir(ca, sa, cb, sb, theta_out, phi_out, &dout);
+  struct angle_tab ain, aout;
+  angle_tab_build(&ain, nmax, din.c, din.s, din.si);
+  angle_tab_build(&aout, nmax, dout.c, dout.s, dout.si);
+  const cplx e1 = CX(dout.cphi * din.cphi + dout.sphi * din.sphi,
+                     dout.sphi * din.cphi - dout.cphi * din.sphi);
+  cplx S[4];
+  forward_s(nmax, T, k, &ain, &aout, e1, S);
+  angle_tab_free(&ain);
+  angle_tab_free(&aout);
+  /* S^L = R_out^-1 S^P R_in (TMatrix.hpp:1420-1460) */
+  double Ro[2][2];
+  const double det = 1. / (dout.R[0][0] * dout.R[1][1] - dout.R[0][1] * dout.R[1][0]);
+  Ro[0][0] = dout.R[1][1] * det;
+  Ro[0][1] = -dout.R[0][1] * det;
+  Ro[1][0] = -dout.R[1][0] * det;
+  Ro[1][1] = dout.R[0][0] * det;
+  const cplx cS11 = S[0] * din.R[0][0] + S[1] * din.R[1][0];
+  const cplx cS12 = S[0] * din.R[0][1] + S[1] * din.R[1][1];
+  const cplx cS21 = S[2] * din.R[0][0] + S[3] * din.R[1][0];
+  const cplx cS22 = S[2] * din.R[0][1] + S[3] * din.R[1][1];
+  const cplx L[4] = {Ro[0][0] * cS11 + Ro[0][1] * cS21, Ro[0][0] * cS12 + Ro[0][1] * cS22,
+                     Ro[1][0] * cS11 + Ro[1][1] * cS21, Ro[1][0] * cS12 + Ro[1][1] * cS22};
+  for (int q = 0; q < 4; ++q) {
+    Sout[2 * q] = creal(L[q]);
+    Sout[2 * q + 1] = cimag(L[q]);
+  }
+}
+
+/* Z (TMatrix.hpp:1896-1948) and K (:1972-2010) from S, row major */
+void or_z_from_s(const double *Sd, double *Z) {
+  const cplx *S = (const cplx *)Sd;
+  const cplx I1 = CX(0., 1.);
+  Z[0] = creal(0.5 * (S[0] * conj(S[0]) + S[1] * conj(S[1]) + S[2] * conj(S[2]) +
+                      S[3] * conj(S[3])));
+  Z[1] = creal(0.5 * (S[0] * conj(S[0]) - S[1] * conj(S[1]) + S[2] * conj(S[2]) -
+                      S[3] * conj(S[3])));
+  Z[2] = creal(-S[0] * conj(S[1]) - S[3] * conj(S[2]));
+  Z[3] = creal(I1 * (S[0] * conj(S[1]) - S[3] * conj(S[2])));
+  Z[4] = creal(0.5 * (S[0] * conj(S[0]) + S[1] * conj(S[1]) - S[2] * conj(S[2]) -
+                      S[3] * conj(S[3])));
+  Z[5] = creal(0.5 * (S[0] * conj(S[0]) - S[1] * conj(S[1]) - S[2] * conj(S[2]) +
+                      S[3] * conj(S[3])));
+  Z[6] = creal(-S[0] * conj(S[1]) + S[3] * conj(S[2]));
+  Z[7] = creal(I1 * (S[0] * conj(S[1]) + S[3] * conj(S[2])));
+  Z[8] = creal(-S[0] * conj(S[2]) - S[3] * conj(S[1]));
+  Z[9] = creal(-S[0] * conj(S[2]) + S[3] * conj(S[1]));
+  Z[10] = creal(S[0] * conj(S[3]) + S[1] * conj(S[2]));
+  Z[11] = creal(-I1 * (S[0] * conj(S[3]) + S[2] * conj(S[1])));
+  Z[12] = creal(I1 * (S[2] * conj(S[0]) + S[3] * conj(S[1])));
+  Z[13] = creal(I1 * (S[2] * conj(S[0]) - S[3] * conj(S[1])));
+  Z[14] = creal(-I1 * (S[3] * conj(S[0]) - S[1] * conj(S[2])));
+  Z[15] = creal(S[3] * conj(S[0]) - S[1] * conj(S[2]));
+}
+
+void or_k_from_s(double wavelength, const double *Sd, double *K) {
+  const cplx *S = (const cplx *)Sd;
+  const double pf = 2. * M_PI / (2. * M_PI / wavelength);
+  for (int i = 0; i < 16; ++i) {
+    K[i] = 0.;
+  }
+  K[0] = pf * cimag(S[0] + S[3]);
+  K[5] = K[10] = K[15] = K[0];
+  K[1] = K[4] = pf * cimag(S[0] - S[3]);
+  K[2] = K[8] = -pf * cimag(S[1] + S[2]);
+  K[3] = K[12] = pf * creal(S[2] - S[1]);
+  K[6] = pf * cimag(S[2] - S[1]);
+  K[9] = -K[6];
+  K[7] = -pf * creal(S[1] + S[2]);
+  K[13] = -K[7];
+  K[11] = pf * creal(S[3] - S[0]);
+  K[14] = -K[11];
+}

@@ -93,6 +93,22 @@ void or_absorption(int nmax, const double *T, double wavelength, double r_ev,
 void or_scattering_matrix(int nmax, const double *T, double wavelength,
                           int ntheta, double *out);
 
+/* plain path: TMatrixCalculator::calculate_TMatrix orders
+ * (TMatrixCalculator.hpp:64-213); returns 1 where the reference aborts */
+int or_calculator_orders(double r_ev, double wavelength, double mr, double mi,
+                         double axis_ratio, int maximum_order, double tolerance,
+                         int ndgs, int maximum_ngauss, int *nmax, int *ngauss);
+
+/* lab-frame amplitude matrix S (2 x 2 complex, interleaved) at particle
+ * orientation (alpha, beta) (TMatrix.hpp:1109-1460) */
+void or_amplitude_lab(int nmax, const double *T, double wavelength, double alpha,
+                      double beta, double theta_in, double phi_in,
+                      double theta_out, double phi_out, double *S);
+
+/* Z (TMatrix.hpp:1896-1948) and K (:1972-2010) from S, row major 4 x 4 */
+void or_z_from_s(const double *S, double *Z);
+void or_k_from_s(double wavelength, const double *S, double *K);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the unmodified reference.
 
 Run in a container where the reference has been built (oracle/build_ref.sh):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [stages tmatrices tables plain]
 It imports the reference's own CPython module (oracle/_ref/CosTuuM*.so) and
 its task objects (oracle/_ref/libref_driver.so) and stores their outputs.
 The fixtures pin the C restatement in oracle/ (tests/test_oracle_golden.py).
@@ -12,6 +12,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = os.environ.get("COSTUUM_REFERENCE", "/root/reference")
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 from oracle import _p  # noqa: E402
@@ -173,8 +174,53 @@ def tables():
     return out
 
 
+# plain-path cases: (radius, axis ratio, wavelength, m, cos2beta,
+# is_equal_volume_radius)
+PLAIN = [
+    (0.2e-6, 2.0, 1e-6, 1.5 + 0.02j, -1.0, True),
+    (0.2e-6, 2.0, 1e-6, 1.5 + 0.02j, 1.0 / 3.0, True),
+    (0.5e-6, 0.6, 1.2e-6, 1.7 + 0.1j, 0.6, False),
+    (0.3e-6, 1.5, 0.9e-6, 1.4 + 0.05j, 1.0, True),
+    (1.9e-6, 0.5, 1e-6, 1.5 + 0.02j, 1.0 / 3.0, True),
+]
+
+
+def plain():
+    """Outputs of the reference module's TMatrix object (the plain path) and
+    the Mishchenko-code fixture of the reference's calculator test."""
+    C = O.ref_module()
+    out = {}
+    rows = []
+    with open(os.path.join(REFERENCE, "test", "test_tmatrixcalculator.txt")) as f:
+        for line in f:
+            if line.startswith("#") or not line.strip():
+                continue
+            rows.append([float(v) for v in line.split()])
+    out["mish_rows"] = np.array(rows)
+    th = np.array([0.3, 1.2])
+    ph = np.array([0.0, 0.7])
+    for i, (r, d, lam, m, c2b, ev) in enumerate(PLAIN):
+        T = C.TMatrix(r, d, lam, m, cos2beta=c2b, is_equal_volume_radius=ev)
+        out["p%d_nmax" % i] = np.array([T.get_nmax()])
+        out["p%d_K" % i] = T.get_extinction_matrix(th, ph, alpha=0.4, beta=0.9)
+        out["p%d_Z" % i] = T.get_scattering_matrix(0.5, 0.1, 1.7, 2.2,
+                                                   alpha=0.3, beta=1.1)
+        if i < 4:
+            out["p%d_cabs" % i] = T.get_absorption_cross_sections(
+                np.array([0.4, 1.3]), ngauss=10)
+            out["p%d_avg" % i] = np.array([T.get_average_absorption_cross_section()])
+        if i == 4:
+            tout = np.radians(np.arange(181.0))
+            out["p4_z181"] = T.get_scattering_matrix(0.0, 0.0, tout, 0.0)
+    out["plain_args"] = np.array([[r, d, lam, m.real, m.imag, c2b, float(ev)]
+                                  for (r, d, lam, m, c2b, ev) in PLAIN])
+    return out
+
+
 if __name__ == "__main__":
-    np.savez_compressed(os.path.join(HERE, "stages.npz"), **stages())
-    np.savez_compressed(os.path.join(HERE, "tmatrices.npz"), **tmatrices())
-    np.savez_compressed(os.path.join(HERE, "tables.npz"), **tables())
+    # python make_golden.py [stages tmatrices tables plain]: the named sets
+    # (default all)
+    which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain"]
+    for name in which:
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **globals()[name]())
     print("golden fixtures written to", HERE)

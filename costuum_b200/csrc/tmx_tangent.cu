@@ -16,6 +16,8 @@
 // dw/dR_V = w/R_V, dz/dd = z (dln r^2/dd)/2; the quadrature weights w r^2
 // (and m w r^2 / sin) scale with r^2, so d/dd multiplies them by dln r^2/dd;
 // r'/r also depends on d.
+#include <algorithm>
+
 #include "tmx_blocks_common.cuh"
 
 extern __shared__ __align__(16) unsigned char tmx_tsmem[];
@@ -25,17 +27,20 @@ enum { P_M = 0, P_R = 1, P_D = 2 };
 // Tangent chunk: per node 8 slots, slot t (t < 4) pairs F_t with dW_t and
 // slot 4 + t pairs dF_t with W_t. For p = m the F side does not depend on
 // the parameter and only slots 0..3 are used.
-template <int TC>
+// Threads tid = 0..nth-1 of the caller share the work; rows are stored with
+// stride L.NRp, columns with stride ncolp.
 __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
-                                    int N, int m, int ng, int g0, int param,
-                                    double R, const double *__restrict__ T,
+                                    int ncolp, int N, int m, int ng, int g0,
+                                    int param, double R,
+                                    const double *__restrict__ T,
                                     const double *__restrict__ S,
                                     const double *__restrict__ Wg, double k2,
-                                    cplx k2mr, cplx *Fs, cplx *Ws) {
+                                    cplx k2mr, cplx *Fs, cplx *Ws, int tid,
+                                    int nth) {
   const int G = L.G;
   const int slots = 8;
   // ---- A side: F_t (slots 0..3) and dF_t (slots 4..7), (F^j, F^y) pairs
-  for (int u = threadIdx.x; u < G * L.NRp; u += blockDim.x) {
+  for (int u = tid; u < G * L.NRp; u += nth) {
     const int gl = u / L.NRp;
     const int pr = u % L.NRp;
     const int g = g0 + gl;
@@ -89,8 +94,7 @@ __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
     }
   }
   // ---- B side: dW_t (slots 0..3) and W_t (slots 4..7) for each row group
-  const int ncolp = L.CT * TC;
-  for (int u = threadIdx.x; u < G * ncolp; u += blockDim.x) {
+  for (int u = tid; u < G * ncolp; u += nth) {
     const int gl = u / ncolp;
     const int b = u % ncolp;
     const int g = g0 + gl;
@@ -250,8 +254,8 @@ __global__ void __launch_bounds__(NT, MINB)
     }
     for (int g0 = 0; g0 < ng; g0 += L.G) {
       __syncthreads();
-      build_chunk_tangent<TC>(D, L, N, m, ng, g0, param, Gr.r_ev, T, S, Wg, k2,
-                              k2mr, Fs, Ws);
+      build_chunk_tangent(D, L, L.CT * TC, N, m, ng, g0, param, Gr.r_ev, T, S,
+                          Wg, k2, k2mr, Fs, Ws, threadIdx.x, blockDim.x);
       __syncthreads();
       if (active) {
         const int gmax = min(L.G, ng - g0);
@@ -384,6 +388,199 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+// ------------------------------------------------- warp-per-item variant --
+//
+// (item, parameter) pairs of classes with at most 16 members: one warp each,
+// four per CTA, synchronised by __syncwarp only (as the forward warp kernel).
+// Assembly: lane (rt, ct) accumulates rows rt * TR.. and columns ct, ct + 4,
+// .. over chunks of TMX_TWG nodes. Solve: lane r forms row r of
+// X = -(dRgQ + T_c dQ) and runs both triangular solves with the saved
+// factors on it.
+
+#define TMX_TWG 2 // quadrature nodes per warp chunk
+
+template <int NBM>
+__host__ __device__ constexpr int tangent_warp_elems() {
+  // chunk buffers F[WG][8][NBM] + W[2][WG][8][NBM], or in the solve phase
+  // dQ, X, LU ([NBM][NBM + 1] each), 1/U_jj and the gather index
+  return (24 * TMX_TWG * NBM > 3 * NBM * (NBM + 1) + 2 * NBM)
+             ? 24 * TMX_TWG * NBM
+             : 3 * NBM * (NBM + 1) + 2 * NBM;
+}
+
+template <int TR, int TC, int MINB>
+__global__ void __launch_bounds__(128, MINB)
+    k_tangent_warp(TmxTangentArgs A) {
+  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  constexpr int LD = NBM + 1;
+  extern __shared__ __align__(16) unsigned char tmx_twsmem[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  cplx *base = reinterpret_cast<cplx *>(tmx_twsmem) + wib * tangent_warp_elems<NBM>();
+  cplx *Fs = base;                       // [WG][8][NBM]
+  cplx *Ws = Fs + 8 * TMX_TWG * NBM;     // [2][WG][8][NBM]
+  cplx *dQm = base;                      // [NBM][LD]  (after the assembly)
+  cplx *Xm = dQm + NBM * LD;             // [NBM][LD]
+  cplx *LUm = Xm + NBM * LD;             // [NBM][LD]
+  cplx *uinv = LUm + NBM * LD;           // [NBM]
+  int *perm = reinterpret_cast<int *>(uinv + NBM);
+  const int rt = lane >> 2;
+  const int ct = lane & 3;
+  const int64_t nwork = (int64_t)A.nitems * A.nparams;
+  for (int64_t w = (int64_t)blockIdx.x * 4 + wib; w < nwork;
+       w += (int64_t)gridDim.x * 4) {
+    const int it = (int)(w / A.nparams);
+    const int param = (int)(w % A.nparams);
+    const TmxItem item = A.items[it];
+    const TmxSlot sl = A.slots[item.slot];
+    const TmxGrain Gr = A.grains[sl.grain];
+    const int N = sl.nmax;
+    const int ng = sl.ngauss;
+    const int m = item.m;
+    const ClassDesc D = describe<TR>(N, m, item.cls);
+    const int nb = D.nb;
+    if (nb <= 0 || nb > NBM || D.NRp > NBM) {
+      continue;
+    }
+    const double *T = A.tab + sl.tab;
+    const double *S = A.nsc + sl.nsc;
+    const double *Wg = A.wig + A.wig_off[sl.wig_n] + (int64_t)m * ng * N * 2;
+    const double k2 = Gr.k * Gr.k;
+    const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
+    AsmLayout L;
+    L.G = TMX_TWG;
+    L.NRp = NBM;
+    L.CT = 0;
+    L.ncol = NBM;
+    L.ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
+    const int tstep = (m == 0) ? 2 : 1;
+    const int t0 = (m == 0) ? 1 : 0;
+    const int per_node = (param == P_M) ? 4 : 8;
+    const int rgl = (rt * TR < D.R0p) ? 0 : 1;
+
+    // -------------------------------------------------- tangent assembly
+    double aj[TR][TC][2], ay[TR][TC][2];
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        aj[r][c][0] = aj[r][c][1] = ay[r][c][0] = ay[r][c][1] = 0.;
+      }
+    }
+    for (int g0 = 0; g0 < ng; g0 += TMX_TWG) {
+      __syncwarp();
+      build_chunk_tangent(D, L, NBM, N, m, ng, g0, param, Gr.r_ev, T, S, Wg, k2,
+                          k2mr, Fs, Ws, lane, 32);
+      __syncwarp();
+      const int gmax = min(TMX_TWG, ng - g0);
+      for (int gl = 0; gl < gmax; ++gl) {
+        for (int ts = t0; ts < per_node; ts += tstep) {
+          const int kk = 8 * gl + ts;
+          const cplx *fr = Fs + kk * NBM + rt * TR;
+          const cplx *wr = Ws + (rgl * 8 * TMX_TWG + kk) * NBM + ct;
+          cplx wv[TC];
+#pragma unroll
+          for (int c = 0; c < TC; ++c) {
+            wv[c] = wr[4 * c];
+          }
+#pragma unroll
+          for (int r = 0; r < TR; ++r) {
+            const cplx f = fr[r];
+#pragma unroll
+            for (int c = 0; c < TC; ++c) {
+              aj[r][c][0] = fma(f.x, wv[c].x, aj[r][c][0]);
+              aj[r][c][1] = fma(f.x, wv[c].y, aj[r][c][1]);
+              ay[r][c][0] = fma(f.y, wv[c].x, ay[r][c][0]);
+              ay[r][c][1] = fma(f.y, wv[c].y, ay[r][c][1]);
+            }
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // dQ = dG^j + i dG^y into dQm, dRgQ = dG^j into Xm
+#pragma unroll
+    for (int r = 0; r < TR; ++r) {
+      const int a = padded_member(D, rt * TR + r);
+#pragma unroll
+      for (int c = 0; c < TC; ++c) {
+        const int b = ct + 4 * c;
+        if (a >= 0 && b < nb) {
+          dQm[a * LD + b] = mkc(aj[r][c][0] - ay[r][c][1], aj[r][c][1] + ay[r][c][0]);
+          Xm[a * LD + b] = mkc(aj[r][c][0], aj[r][c][1]);
+        }
+      }
+    }
+    // saved factors and gather index of the forward solve
+    const cplx *Ls = A.lu + item.scratch;
+    const int *ps = reinterpret_cast<const int *>(Ls + (int64_t)nb * nb);
+    for (int u = lane; u < nb * nb; u += 32) {
+      LUm[(u / nb) * LD + (u % nb)] = Ls[u];
+    }
+    for (int j = lane; j < nb; j += 32) {
+      perm[j] = ps[j];
+      uinv[j] = cinv(Ls[(int64_t)j * nb + j]);
+    }
+    __syncwarp();
+    // --------------------------------- X = -(dRgQ + T_c dQ), then solve
+    const cplx *Tb = A.T + sl.tout + block_offset(N, m);
+    const int w2 = 2 * D.nbb;
+    if (lane < nb) {
+      int ia, na;
+      member(D, lane, ia, na);
+      const cplx *trow = Tb + (int64_t)(ia * D.nbb + (na - D.nmin)) * w2;
+      cplx *x = Xm + lane * LD;
+      for (int b = 0; b < nb; ++b) {
+        cplx acc = x[b];
+        for (int k = 0; k < nb; ++k) {
+          int ik, nk;
+          member(D, k, ik, nk);
+          acc = cadd(acc, cmul(trow[ik * D.nbb + (nk - D.nmin)], dQm[k * LD + b]));
+        }
+        x[b] = mkc(-acc.x, -acc.y);
+      }
+      // Z U = X (forward over columns)
+      for (int j = 0; j < nb; ++j) {
+        const cplx xj = cmul(x[j], uinv[j]);
+        x[j] = xj;
+        for (int k = j + 1; k < nb; ++k) {
+          x[k] = csub(x[k], cmul(xj, LUm[j * LD + k]));
+        }
+      }
+      // Y L = Z (backward over columns, L unit lower)
+      for (int j = nb - 1; j >= 1; --j) {
+        const cplx xj = x[j];
+        for (int k = 0; k < j; ++k) {
+          x[k] = csub(x[k], cmul(xj, LUm[j * LD + k]));
+        }
+      }
+    }
+    __syncwarp();
+    cplx *dTb = A.dT + param * A.dT_stride + sl.tout + block_offset(N, m);
+    for (int u = lane; u < nb * nb; u += 32) {
+      const int a = u / nb;
+      const int b = u - a * nb;
+      int ia, na, ib, nbn;
+      member(D, a, ia, na);
+      member(D, b, ib, nbn);
+      dTb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ib * D.nbb + (nbn - D.nmin)] =
+          Xm[a * LD + perm[b]];
+    }
+    __syncwarp();
+  }
+}
+
+template <int TR, int TC, int MINB>
+static void launch_tangent_warp(const TmxTangentArgs &a, cudaStream_t stream) {
+  constexpr int NBM = (8 * TR > 4 * TC) ? 8 * TR : 4 * TC;
+  const size_t smem = (size_t)4 * tangent_warp_elems<NBM>() * sizeof(cplx);
+  cudaFuncSetAttribute(k_tangent_warp<TR, TC, MINB>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int64_t work = (int64_t)a.nitems * a.nparams;
+  const int blocks = (int)std::min<int64_t>((work + 3) / 4, 148 * 16);
+  k_tangent_warp<TR, TC, MINB><<<blocks, 128, smem, stream>>>(a);
+}
+
 size_t tmx_tangent_smem_bytes(int max_nb, int chunk_nodes) {
   const int nrp = (max_nb + 3) / 4 * 4 + 4;
   const int ncol = (max_nb + 3) / 4 * 4;
@@ -421,10 +618,12 @@ void tmx_launch_tangents(const TmxTangentArgs &a, cudaStream_t stream) {
   if (a.nitems <= 0 || a.nparams <= 0) {
     return;
   }
-  const size_t smem = tmx_tangent_smem_bytes(a.max_nb, a.chunk_nodes);
   if (a.max_nb <= 16) {
-    launch_tangent<2, 2, 64, 8>(a, smem, stream);
-  } else if (a.max_nb <= 32) {
+    launch_tangent_warp<2, 4, 2>(a, stream);
+    return;
+  }
+  const size_t smem = tmx_tangent_smem_bytes(a.max_nb, a.chunk_nodes);
+  if (a.max_nb <= 32) {
     launch_tangent<2, 4, 128, 4>(a, smem, stream);
   } else {
     launch_tangent<4, 4, 256, 1>(a, smem, stream);

@@ -46,6 +46,11 @@ def grains(n, seed):
     return r, np.full(n, lam), mr + 1j * mi, d
 
 
+def rank_seed(rank):
+    """Each rank computes its own independent grains (weak scaling)."""
+    return 1 + rank
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -54,18 +59,21 @@ def dist_env():
 
 
 class Dist:
-    """Barrier and max-reduction across ranks (NCCL when world > 1)."""
+    """Barrier and max-reduction across ranks (NCCL when world > 1; gloo on
+    CPU for the multi-process tests)."""
 
-    def __init__(self, world, local):
+    def __init__(self, world, local, backend="nccl"):
         self.world = world
         self.pg = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
         if world > 1:
             import datetime
 
             import torch
             import torch.distributed as td
-            torch.cuda.set_device(local)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            td.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.td = td
             self.torch = torch
 
@@ -76,7 +84,7 @@ class Dist:
     def max(self, v):
         if self.world == 1:
             return v
-        t = self.torch.tensor([v], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=self.device)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
@@ -219,7 +227,7 @@ def run_ours(args):
     dfma = ctx.probe_fp64(0)
     dmma = ctx.probe_fp64(1)
 
-    r, lam, m, d = grains(N_GRAINS, 1 + rank)
+    r, lam, m, d = grains(N_GRAINS, rank_seed(rank))
     mr = np.ascontiguousarray(m.real)
     mi = np.ascontiguousarray(m.imag)
     sched = _lib.TmxSchedule(SCHEDULE["min_order"], SCHEDULE["max_order"],

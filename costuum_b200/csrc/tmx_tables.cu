@@ -32,28 +32,30 @@ __device__ __forceinline__ int bessel_nstart(int bessel_start, int nmax,
 // downward ratio recurrence rho_n = j_n / j_{n-1} started at n = nstart with
 // rho ~ z / (2 nstart + 1), then j_n = rho_n j_{n-1} upward
 // (SpecialFunctions::spherical_j_jdj_array, SpecialFunctions.hpp:201-240).
-// out[(n-1) * stride + 0] = j_n, [+1] = [z j_n]'/z
+// The ratios go to rho[(n-1) * rs] (shared memory, or the output slots
+// themselves); out[(n-1) * stride + {0, 1}] = (j_n, [z j_n]'/z), stored as
+// one 16-byte pair.
 __device__ static void bessel_j_real(int nmax, int nstart, double z,
-                                     double *out, int stride) {
+                                     double *out, int stride, double *rho,
+                                     int rs) {
   const double zinv = 1. / z;
   double cur = z / (2. * nstart + 1.);
   for (int index = nstart - 1; index >= 1; --index) {
     const double twoip1 = 2. * index + 1.;
     const double nxt = 1. / (twoip1 * zinv - cur);
     if (index - 1 < nmax) {
-      out[(index - 1) * stride] = nxt; // rho_{index-1} (0-based), kept
+      rho[(index - 1) * rs] = nxt; // rho_{index-1} (0-based), kept
     }
     cur = nxt;
   }
   const double j0 = sin(z) * zinv;
-  double jprev = out[0] * j0;
-  out[0] = jprev;
-  out[1] = j0 - jprev * zinv;
+  double jprev = rho[0] * j0;
+  *reinterpret_cast<double2 *>(out) = make_double2(jprev, j0 - jprev * zinv);
   for (int i = 1; i < nmax; ++i) {
-    const double ji = out[i * stride] * jprev;
+    const double ji = rho[i * rs] * jprev;
     const double ip1 = i + 1.;
-    out[i * stride] = ji;
-    out[i * stride + 1] = jprev - ip1 * zinv * ji;
+    *reinterpret_cast<double2 *>(out + i * stride) =
+        make_double2(ji, jprev - ip1 * zinv * ji);
     jprev = ji;
   }
 }
@@ -69,18 +71,17 @@ __device__ static void bessel_y_real(int nmax, double z, double *out,
   const double zinv3 = zinv2 * zinv;
   double y0 = -cosz * zinv2 - sinz * zinv;
   double y1 = (-3. * zinv3 + zinv) * cosz - 3. * zinv2 * sinz;
-  out[0] = y0;
-  out[1] = -zinv * (cosz + y0);
+  *reinterpret_cast<double2 *>(out) = make_double2(y0, -zinv * (cosz + y0));
   if (nmax > 1) {
-    out[stride] = y1;
-    out[stride + 1] = y0 - 2. * zinv * y1;
+    *reinterpret_cast<double2 *>(out + stride) =
+        make_double2(y1, y0 - 2. * zinv * y1);
   }
   for (int i = 2; i < nmax; ++i) {
     const double twoip1 = 2. * i + 1.;
     const double ip1 = i + 1.;
     const double yi = twoip1 * zinv * y1 - y0;
-    out[i * stride] = yi;
-    out[i * stride + 1] = y1 - ip1 * zinv * yi;
+    *reinterpret_cast<double2 *>(out + i * stride) =
+        make_double2(yi, y1 - ip1 * zinv * yi);
     y0 = y1;
     y1 = yi;
   }
@@ -101,9 +102,11 @@ __device__ static cplx csin_dev(cplx z) {
 // is far from overflow and underflow), where the reference's complex
 // division takes three (Smith's algorithm): the ratios agree to the last
 // few bits.
-// out[(n-1) * stride + {0,1,2,3}] = (Re j, Im j, Re dj, Im dj)
+// out[(n-1) * stride + {0,1,2,3}] = (Re j, Im j, Re dj, Im dj), stored as
+// two 16-byte pairs; the ratios go to rho[(n-1) * rs].
 __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
-                                        double *out, int stride) {
+                                        double *out, int stride, cplx *rho,
+                                        int rs) {
   const cplx zinv = cinv(z);
   cplx cur = cdiv(z, mkc(2. * nstart + 1., 0.));
   for (int index = nstart - 1; index >= 1; --index) {
@@ -112,26 +115,21 @@ __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
     const double inv = 1. / (w.x * w.x + w.y * w.y);
     const cplx nxt = mkc(w.x * inv, -w.y * inv);
     if (index - 1 < nmax) {
-      out[(index - 1) * stride] = nxt.x;
-      out[(index - 1) * stride + 1] = nxt.y;
+      rho[(index - 1) * rs] = nxt;
     }
     cur = nxt;
   }
   const cplx j0 = cmul(csin_dev(z), zinv);
-  cplx jprev = cmul(mkc(out[0], out[1]), j0);
-  out[0] = jprev.x;
-  out[1] = jprev.y;
-  const cplx dj0 = csub(j0, cmul(jprev, zinv));
-  out[2] = dj0.x;
-  out[3] = dj0.y;
+  cplx jprev = cmul(rho[0], j0);
+  cplx *o = reinterpret_cast<cplx *>(out);
+  o[0] = jprev;
+  o[1] = csub(j0, cmul(jprev, zinv));
   for (int i = 1; i < nmax; ++i) {
-    const cplx rho = mkc(out[i * stride], out[i * stride + 1]);
-    const cplx ji = cmul(rho, jprev);
+    const cplx ji = cmul(rho[i * rs], jprev);
     const cplx dji = csub(jprev, cmul(cscale(zinv, i + 1.), ji));
-    out[i * stride] = ji.x;
-    out[i * stride + 1] = ji.y;
-    out[i * stride + 2] = dji.x;
-    out[i * stride + 3] = dji.y;
+    cplx *oi = reinterpret_cast<cplx *>(out + i * stride);
+    oi[0] = ji;
+    oi[1] = dji;
     jprev = ji;
   }
 }
@@ -147,7 +145,10 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
                          const double *__restrict__ gl_x,
                          const double *__restrict__ gl_w,
                          const int64_t *__restrict__ gl_off, double *tab,
-                         double *nsc, int bessel_start) {
+                         double *nsc, int bessel_start, int rho_smem) {
+  // ratio buffers: a shared-memory column per thread (rho_smem rows), or
+  // the output slots themselves when the orders exceed rho_smem
+  extern __shared__ cplx trho[];
   const int s = blockIdx.x;
   if (s >= nslots) {
     return;
@@ -203,13 +204,25 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       S[TMX_NS_DDRR_DD] =
           2. * dd * c * sn * r2oa2 * (1. - (c * c) * r2oa2 * d2m1);
       S[TMX_NS_PAD] = 0.;
-      bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
-                    TMX_NQ);
+      if (N <= rho_smem) {
+        bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
+                      TMX_NQ, reinterpret_cast<double *>(trho) + threadIdx.x,
+                      blockDim.x);
+      } else {
+        bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
+                      TMX_NQ, T + TMX_Q_J, TMX_NQ);
+      }
       bessel_y_real(N, kr, T + TMX_Q_Y, TMX_NQ);
     } else {
       const cplx krmr = mkc(G.mr * G.k * r * G.r_ev, G.mi * G.k * r * G.r_ev);
-      bessel_j_complex(N, bessel_nstart(bessel_start, N, hypot(krmr.x, krmr.y)),
-                       krmr, T + TMX_Q_JM_RE, TMX_NQ);
+      const int ns = bessel_nstart(bessel_start, N, hypot(krmr.x, krmr.y));
+      if (N <= rho_smem) {
+        bessel_j_complex(N, ns, krmr, T + TMX_Q_JM_RE, TMX_NQ,
+                         trho + threadIdx.x, blockDim.x);
+      } else {
+        bessel_j_complex(N, ns, krmr, T + TMX_Q_JM_RE, TMX_NQ,
+                         reinterpret_cast<cplx *>(T + TMX_Q_JM_RE), TMX_NQ / 2);
+      }
     }
   }
 }
@@ -311,9 +324,21 @@ void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
     return;
   }
   const int threads = 64;
+  // ratios in shared memory for orders up to 48 (48 KB per CTA)
+  const int rho_smem = 48;
+  const size_t smem = (size_t)threads * rho_smem * sizeof(cplx);
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    attr_dev = dev;
+  }
   dim3 grid(nslots, (ngmax + threads - 1) / threads, 2);
-  k_tables<<<grid, threads, 0, stream>>>(slots, nslots, grains, gl_x, gl_w,
-                                         gl_off, tab, nsc, bessel_start);
+  k_tables<<<grid, threads, smem, stream>>>(slots, nslots, grains, gl_x, gl_w,
+                                            gl_off, tab, nsc, bessel_start,
+                                            rho_smem);
 }
 
 void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,

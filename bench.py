@@ -446,6 +446,77 @@ def run_ours(args):
     return 0
 
 
+def dielectric_m(lam):
+    """Seeded-style refractive index model of the averaged-grid workload:
+    eps = eps_inf + sum_j f_j w_j^2 / (w_j^2 - w^2 - i g_j w) - wp^2 / (w^2 +
+    i gD w) with resonances at 9.7, 18 and 25 um (w = 1 / lambda[um]),
+    m = sqrt(eps) on the branch with Im m >= 0."""
+    w = 1.0 / (lam * 1e6)
+    eps = 2.5 + 0j
+    for lj, f in ((9.7, 0.8), (18.0, 0.4), (25.0, 0.2)):
+        wj = 1.0 / lj
+        eps += f * wj * wj / (wj * wj - w * w - 1j * 0.1 * wj * w)
+    eps -= 0.05 ** 2 / (w * w + 1j * 0.01 * w)
+    m = np.sqrt(eps)
+    return complex(m if m.imag >= 0 else -m)
+
+
+def run_config3(args):
+    """The averaged-grid workload: 64 radii (0.01-2 um) x wavelengths
+    logspace(0.1, 100 um, 200) with x = 2 pi r / lambda <= 50 at the largest
+    radius (the 27 shortest wavelengths dropped, maximum_order 100) x the
+    20-node Draine-Hensley shape distribution, Davis-Greenstein alignment
+    above 0.1 um, Qabs and Qext at 32 zenith angles, through get_table. CPU:
+    the reference module's get_table on a 2 x 2-cell sub-grid of small size
+    parameters (cells with larger ones take the reference minutes each)."""
+    from costuum_b200 import CosTuuM as C
+    sizes = np.logspace(np.log10(0.01e-6), np.log10(2e-6), 64)
+    lams = np.logspace(-7, -4, 200)
+    lams = lams[2 * np.pi * sizes[-1] / lams <= 50.0]
+    th = np.arccos(np.linspace(-1, 1, 32))
+    kw = dict(thetas=th, do_absorption=True, do_extinction=True)
+
+    def run(mod, sz, lm, nthreads):
+        return mod.get_table(
+            types=np.array([0]), sizes=sz, wavelengths=lm,
+            shape_distribution=mod.DraineHensleyShapeDistribution(20),
+            alignment_distribution=mod.SizeBasedAlignmentDistribution(
+                1e-7, mod.DAVIS_GREENSTEIN_ALIGNMENT, maximum_order=100),
+            dust_properties=mod.CustomDustProperties(
+                lambda w, s, t: dielectric_m(w)),
+            maximum_order=100, number_of_threads=nthreads, **kw)
+
+    run(C, sizes[:4], lams[:4], 1)  # warm-up (tables, contexts)
+    t0 = time.perf_counter()
+    out = run(C, sizes, lams, 1)
+    gpu_s = time.perf_counter() - t0
+    ncell = len(sizes) * len(lams)
+    line = {"metric": "grains/s (averaged get_table grid)",
+            "value": ncell * 20 / gpu_s, "unit": "grains/s",
+            "cells": ncell, "grains": ncell * 20, "seconds": gpu_s,
+            "finite": bool(np.isfinite(out).all())}
+    if not args.skip_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        R = O.ref_module()
+        sub_s = sizes[[10, 30]]
+        sub_l = lams[[100, 150]]
+        t0 = time.perf_counter()
+        run(R, sub_s, sub_l, os.cpu_count() or 1)
+        cpu_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        run(C, sub_s, sub_l, 1)
+        gpu_sub = time.perf_counter() - t0
+        line["cpu_reference"] = {"value": 4 * 20 / cpu_s, "unit": "grains/s",
+                                 "cores": os.cpu_count(),
+                                 "sample": "2 sizes x 2 wavelengths x 20 shapes "
+                                           "(small-x cells) of the same grid, "
+                                           "reference get_table",
+                                 "gpu_same_sample": 4 * 20 / gpu_sub}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     global N_GRAINS
     ap = argparse.ArgumentParser()
@@ -459,10 +530,14 @@ def main():
                     help="omit the plain-path and gradient measurements")
     ap.add_argument("--grains", type=int, default=N_GRAINS,
                     help="grains per GPU (smaller cases for profiling)")
+    ap.add_argument("--config3", action="store_true",
+                    help="measure the averaged get_table grid instead")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     N_GRAINS = args.grains
+    if args.config3:
+        return run_config3(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

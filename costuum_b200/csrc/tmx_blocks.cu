@@ -893,12 +893,21 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
                            const cplx *__restrict__ diag, TmxChainState *state,
                            double tolerance, int order, int last_order,
                            int32_t *next_active, int32_t *next_count,
-                           int32_t *done_list, int32_t *done_count) {
+                           int32_t *done_list, int32_t *done_ord,
+                           int32_t *done_count) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive) {
     return;
   }
   const int g = active[p];
+  {
+    // speculative orders: a grain whose order became final at an earlier
+    // order of the same group is not touched again
+    const TmxChainState s0 = state[g];
+    if (s0.converged || (s0.status & (TMX_ST_NAN | TMX_ST_NOT_CONVERGED))) {
+      return;
+    }
+  }
   const TmxSlot sl = slots[p];
   const cplx *dg = diag + sl.diag;
   const int N = order;
@@ -947,7 +956,9 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
   state[g] = st;
   if (!stays) {
     // the grain's order is final: its blocks may start
-    done_list[atomicAdd(done_count, 1)] = g;
+    const int q = atomicAdd(done_count, 1);
+    done_list[q] = g;
+    done_ord[q] = order;
   }
 }
 
@@ -956,13 +967,14 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
-                         int32_t *done_count, cudaStream_t stream) {
+                         int32_t *done_ord, int32_t *done_count,
+                         cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
       active, nactive, slots, diag, state, tolerance, order, last_order,
-      next_active, next_count, done_list, done_count);
+      next_active, next_count, done_list, done_ord, done_count);
 }
 
 // ------------------------------------------------------------- Q sums ------
@@ -1036,9 +1048,7 @@ void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
 // Slots and items of one order step: active position p gets the tables at
 // p * strides and the four m = 0 classes as items 4p .. 4p + 3.
 __global__ void k_chain_prep(const int32_t *__restrict__ active, int nactive,
-                             int order, int ngauss, int wig_n,
-                             int64_t tab_stride, int64_t nsc_stride,
-                             int64_t diag_stride, int64_t scr_stride,
+                             int order, int ngauss, int wig_n, TmxChainBase b,
                              TmxSlot *slots, TmxItem *items) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive) {
@@ -1049,30 +1059,27 @@ __global__ void k_chain_prep(const int32_t *__restrict__ active, int nactive,
   s.nmax = order;
   s.ngauss = ngauss;
   s.wig_n = wig_n;
-  s.tab = p * tab_stride;
-  s.nsc = p * nsc_stride;
+  s.tab = b.tab + p * b.tab_stride;
+  s.nsc = b.nsc + p * b.nsc_stride;
   s.tout = -1;
-  s.diag = p * diag_stride;
-  slots[p] = s;
+  s.diag = b.diag + p * b.diag_stride;
+  slots[b.slot + p] = s;
   for (int c = 0; c < 4; ++c) {
     TmxItem it;
-    it.slot = p;
+    it.slot = b.slot + p;
     it.m = 0;
     it.cls = (int16_t)c;
-    it.scratch = (4 * (int64_t)p + c) * scr_stride;
-    items[4 * p + c] = it;
+    it.scratch = b.scr + (4 * (int64_t)p + c) * b.scr_stride;
+    items[4 * (b.slot + p) + c] = it;
   }
 }
 
 void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
-                           int ngauss, int wig_n, int64_t tab_stride,
-                           int64_t nsc_stride, int64_t diag_stride,
-                           int64_t scr_stride, TmxSlot *slots, TmxItem *items,
-                           cudaStream_t stream) {
+                           int ngauss, int wig_n, const TmxChainBase &b,
+                           TmxSlot *slots, TmxItem *items, cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_chain_prep<<<(nactive + 127) / 128, 128, 0, stream>>>(
-      active, nactive, order, ngauss, wig_n, tab_stride, nsc_stride,
-      diag_stride, scr_stride, slots, items);
+      active, nactive, order, ngauss, wig_n, b, slots, items);
 }

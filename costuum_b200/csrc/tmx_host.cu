@@ -782,17 +782,18 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   // host set-up is issued after the next order's launches, so it overlaps
   // that order on the GPU.
   int nact = ctx->up_nact;
-  if ((rc = ensure(ctx, ctx->done, std::max<int64_t>(1, n) * sizeof(int32_t)))) {
+  // done list: grains [0, n) and their final orders [n, 2n)
+  if ((rc = ensure(ctx, ctx->done, std::max<int64_t>(1, 2 * n) * sizeof(int32_t)))) {
     return rc;
   }
-  if (ctx->pinned_done_cap < n) {
+  if (ctx->pinned_done_cap < 2 * n) {
     if (ctx->pinned_done) {
       CK(cudaFreeHost(ctx->pinned_done));
       ctx->pinned_done = nullptr;
       ctx->pinned_done_cap = 0;
     }
-    CK(cudaMallocHost((void **)&ctx->pinned_done, n * sizeof(int32_t)));
-    ctx->pinned_done_cap = n;
+    CK(cudaMallocHost((void **)&ctx->pinned_done, 2 * n * sizeof(int32_t)));
+    ctx->pinned_done_cap = 2 * n;
   }
   CK(cudaMemsetAsync(ctx->count.p, 0, 2 * sizeof(int32_t), st));
   const int64_t round_min = std::max<int64_t>(256, ctx->up_nact / 16);
@@ -804,48 +805,76 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
   const size_t budget = (size_t)8 << 30; // table bytes per chunk
   std::unique_ptr<NvtxRange> chain_range(new NvtxRange("tmx_chain"));
-  for (int k = S.min_order; k < S.max_order && nact > 0; ++k) {
-    const int ng = glf * k;
-    const int64_t tab_stride = (int64_t)ng * k * TMX_NQ;
-    const int64_t nsc_stride = (int64_t)ng * TMX_NS;
-    const int cmax = (k + 1) / 2;
-    const int64_t scr_stride = 2 * (int64_t)cmax * cmax;
-    const size_t per_slot = (tab_stride + nsc_stride) * sizeof(double) +
-                            (4 * scr_stride + 2 * k) * sizeof(cplx);
-    const int chunk = (int)std::max<size_t>(1, std::min<size_t>(nact, budget / per_slot));
-    if ((rc = ensure(ctx, ctx->tab, chunk * tab_stride * sizeof(double))) ||
-        (rc = ensure(ctx, ctx->nsc, chunk * nsc_stride * sizeof(double))) ||
-        (rc = ensure(ctx, ctx->scratch, chunk * 4 * scr_stride * sizeof(cplx))) ||
-        (rc = ensure(ctx, ctx->diag, (size_t)chunk * 2 * k * sizeof(cplx))) ||
-        (rc = ensure(ctx, ctx->slots, chunk * sizeof(TmxSlot))) ||
-        (rc = ensure(ctx, ctx->items, 4 * (size_t)chunk * sizeof(TmxItem)))) {
+  const int last = S.max_order - 1;
+  for (int k = S.min_order; k < S.max_order && nact > 0;) {
+    // Few grains left: evaluate the next G orders of every active grain at
+    // once (the convergence rule is then applied order by order), which
+    // cuts the latency-bound tail of the loop at the cost of orders past
+    // convergence.
+    const int G = std::min(S.max_order - k, nact <= 32 ? 8 : (nact <= 128 ? 4 : 1));
+    std::vector<TmxChainBase> base(G);
+    int64_t tab_t = 0, nsc_t = 0, diag_t = 0, scr_t = 0;
+    int chunk = nact;
+    for (int s = 0; s < G; ++s) {
+      const int ks = k + s;
+      const int cm = (ks + 1) / 2;
+      TmxChainBase &b = base[s];
+      b.tab_stride = (int64_t)glf * ks * ks * TMX_NQ;
+      b.nsc_stride = (int64_t)glf * ks * TMX_NS;
+      b.diag_stride = 2 * (int64_t)ks;
+      b.scr_stride = 2 * (int64_t)cm * cm;
+      if (G == 1) {
+        const size_t per_slot = (b.tab_stride + b.nsc_stride) * sizeof(double) +
+                                (4 * b.scr_stride + b.diag_stride) * sizeof(cplx);
+        chunk = (int)std::max<size_t>(1, std::min<size_t>(nact, budget / per_slot));
+      }
+      b.slot = s * chunk;
+      b.tab = tab_t;
+      b.nsc = nsc_t;
+      b.diag = diag_t;
+      b.scr = scr_t;
+      tab_t += chunk * b.tab_stride;
+      nsc_t += chunk * b.nsc_stride;
+      diag_t += chunk * b.diag_stride;
+      scr_t += 4 * chunk * b.scr_stride;
+    }
+    if ((rc = ensure(ctx, ctx->tab, tab_t * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->nsc, nsc_t * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->scratch, scr_t * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->diag, diag_t * sizeof(cplx))) ||
+        (rc = ensure(ctx, ctx->slots, (size_t)G * chunk * sizeof(TmxSlot))) ||
+        (rc = ensure(ctx, ctx->items, 4 * (size_t)G * chunk * sizeof(TmxItem)))) {
       return rc;
     }
     CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(int32_t), st));
-    const int last = S.max_order - 1;
+    const int kl = k + G - 1;
     for (int c0 = 0; c0 < nact; c0 += chunk) {
       const int cn = std::min(chunk, nact - c0);
       const int32_t *a = (const int32_t *)cur->p + c0;
-      tmx_launch_chain_prep(a, cn, k, ng, chain_sets[k - S.min_order],
-                            tab_stride, nsc_stride, 2 * k, scr_stride,
-                            (TmxSlot *)ctx->slots.p, (TmxItem *)ctx->items.p, st);
-      LAUNCHED();
+      for (int s = 0; s < G; ++s) {
+        tmx_launch_chain_prep(a, cn, k + s, glf * (k + s), chain_sets[k + s - S.min_order],
+                              base[s], (TmxSlot *)ctx->slots.p,
+                              (TmxItem *)ctx->items.p, st);
+        LAUNCHED();
+      }
+      // slots and items of the group are contiguous: [s][p]
+      const int nsl = (G == 1) ? cn : G * chunk;
       cudaEvent_t pe = nullptr;
       if ((rc = prof_begin(ctx, 1, &pe))) {
         return rc;
       }
-      tmx_launch_tables((const TmxSlot *)ctx->slots.p, cn,
+      tmx_launch_tables((const TmxSlot *)ctx->slots.p, nsl,
                         (const TmxGrain *)ctx->grains.p,
                         (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
                         (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
-                        (double *)ctx->nsc.p, S.bessel_start, ng, st);
+                        (double *)ctx->nsc.p, S.bessel_start, glf * kl, st);
       LAUNCHED();
       if ((rc = prof_end(ctx, 1, pe, 0.))) {
         return rc;
       }
       TmxBlockArgs B;
       B.items = (const TmxItem *)ctx->items.p;
-      B.nitems = 4 * cn;
+      B.nitems = 4 * nsl;
       B.slots = (const TmxSlot *)ctx->slots.p;
       B.grains = (const TmxGrain *)ctx->grains.p;
       B.tab = (const double *)ctx->tab.p;
@@ -856,33 +885,45 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       B.tout = nullptr;
       B.diag = (cplx *)ctx->diag.p;
       B.status = (int32_t *)ctx->status.p;
-      B.max_nb = cmax;
-      B.chunk_nodes = tmx_host_chunk_nodes(cmax);
+      B.max_nb = (kl + 1) / 2;
+      B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
       double fl = 0.;
-      for (int c = 0; c < 4; ++c) {
-        fl += item_flops(tmx_host_class_size(k, 0, c), 0, ng);
+      for (int s = 0; s < G; ++s) {
+        for (int c = 0; c < 4; ++c) {
+          fl += item_flops(tmx_host_class_size(k + s, 0, c), 0, glf * (k + s)) * cn;
+        }
       }
       if ((rc = prof_begin(ctx, 0, &pe))) {
         return rc;
       }
       tmx_launch_blocks(B, st);
       LAUNCHED();
-      if ((rc = prof_end(ctx, 0, pe, fl * cn))) {
+      if ((rc = prof_end(ctx, 0, pe, fl))) {
         return rc;
       }
-      tmx_launch_converge(a, cn, (const TmxSlot *)ctx->slots.p,
-                          (const cplx *)ctx->diag.p,
-                          (TmxChainState *)ctx->state.p, S.tolerance, k, last,
-                          (int32_t *)nxt->p, (int32_t *)ctx->count.p,
-                          (int32_t *)ctx->done.p, (int32_t *)ctx->count.p + 1,
-                          st);
-      LAUNCHED();
+      for (int s = 0; s < G; ++s) {
+        if (G > 1) {
+          // the active list after the group is the one of its last order
+          CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(int32_t), st));
+        }
+        tmx_launch_converge(a, cn, (const TmxSlot *)ctx->slots.p + base[s].slot,
+                            (const cplx *)ctx->diag.p,
+                            (TmxChainState *)ctx->state.p, S.tolerance, k + s, last,
+                            (int32_t *)nxt->p, (int32_t *)ctx->count.p,
+                            (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
+                            (int32_t *)ctx->count.p + 1, st);
+        LAUNCHED();
+      }
     }
-    // active count, done count, and the done-list entries this order can add
+    // active count, done count, and the done-list entries (grain, order)
+    // this group can add
     CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, 2 * sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(ctx->pinned_done + done_seen, (int32_t *)ctx->done.p + done_seen,
                        nact * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->pinned_done + n + done_seen,
+                       (int32_t *)ctx->done.p + n + done_seen, nact * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
     if (!pending.empty()) {
       if ((rc = run_blocks_round(ctx, pending, ctx->stream2, t_next, rounds > 0,
                                  &t_next, true))) {
@@ -901,11 +942,13 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
     for (int64_t j = done_seen; j < done_now; ++j) {
       const int32_t g = ctx->pinned_done[j];
-      ctx->nmax_h[g] = k;
-      ctx->ngauss_h[g] = ng;
+      const int32_t ko = ctx->pinned_done[n + j];
+      ctx->nmax_h[g] = ko;
+      ctx->ngauss_h[g] = glf * ko;
       ready.push_back(g);
     }
     done_seen = done_now;
+    k += G;
     if (nact > 0 && (int64_t)ready.size() >= round_min) {
       for (int32_t g : ready) {
         launched[g] = 1;

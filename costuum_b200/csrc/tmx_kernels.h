@@ -60,21 +60,30 @@ size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes);
 void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream);
 
 // slots and m = 0 items of one order step from the active list
+// buffer offsets of one order's slots in a (possibly speculative) group of
+// orders: slot index, table/scalar/diagonal/scratch bases and strides
+struct TmxChainBase {
+  int32_t slot;
+  int64_t tab, tab_stride;
+  int64_t nsc, nsc_stride;
+  int64_t diag, diag_stride;
+  int64_t scr, scr_stride;
+};
 void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
-                           int ngauss, int wig_n, int64_t tab_stride,
-                           int64_t nsc_stride, int64_t diag_stride,
-                           int64_t scr_stride, TmxSlot *slots, TmxItem *items,
-                           cudaStream_t stream);
+                           int ngauss, int wig_n, const TmxChainBase &b,
+                           TmxSlot *slots, TmxItem *items, cudaStream_t stream);
 
 // convergence step for the active slots of one order
 // m = 0 sums and the convergence test of one order; grains that continue go
 // to next_active, grains whose order is final are appended to done_list
+// (with that order in done_ord); grains already final are skipped
 void tmx_launch_converge(const int32_t *active, int nactive,
                          const TmxSlot *slots, const double2 *diag,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
-                         int32_t *done_count, cudaStream_t stream);
+                         int32_t *done_ord, int32_t *done_count,
+                         cudaStream_t stream);
 
 // full Q sums over all m blocks (TMatrixQTask)
 void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,

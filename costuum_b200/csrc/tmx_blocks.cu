@@ -825,6 +825,270 @@ static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
   k_blocks_warp<TR, TC, MINB, MMA><<<blocks, 128, smem, stream>>>(a);
 }
 
+// ------------------------------------------ four warps per item (<= 32) --
+//
+// Classes of 17..32 members: one CTA of four warps per item. The warps
+// build each chunk of TMX_WG32 nodes together (one barrier), warp w then
+// accumulates column tile w (columns 8w..8w+7) over all four row tiles on
+// the FP64 tensor pipe (as in k_blocks_warp's tensor path), and warp 0
+// factors and solves with one lane per row (no barriers inside the LU).
+
+#define TMX_WG32 4
+
+__host__ __device__ constexpr int cta32_elems() {
+  // F[WG][4][32] + W[2][WG][4][32], or Q, RgQ [32][33], 1/U_jj, indices
+  return (12 * TMX_WG32 * 32 > 2 * 32 * 33 + 3 * 32) ? 12 * TMX_WG32 * 32
+                                                      : 2 * 32 * 33 + 3 * 32;
+}
+
+__global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
+  constexpr int NBM = 32;
+  constexpr int LD = NBM + 1;
+  extern __shared__ __align__(16) unsigned char tmx_c32smem[];
+  cplx *base = reinterpret_cast<cplx *>(tmx_c32smem);
+  cplx *Fs = base;                   // [WG][4][NBM]
+  cplx *Ws = Fs + TMX_WG32 * 4 * NBM; // [2][WG][4][NBM]
+  cplx *Qm = base;                   // [NBM][LD]  (after the assembly)
+  cplx *Rm = Qm + NBM * LD;          // [NBM][LD]
+  cplx *uinv = Rm + NBM * LD;        // [NBM]
+  int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
+  int *piv = perm + NBM;                           // [NBM]
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wib = tid >> 5;
+  const int q = lane & 3;
+  const int rr = lane >> 2;
+  for (int it = blockIdx.x; it < A.nitems; it += gridDim.x) {
+    const TmxItem item = A.items[it];
+    const TmxSlot sl = A.slots[item.slot];
+    const TmxGrain Gr = A.grains[sl.grain];
+    const int N = sl.nmax;
+    const int ng = sl.ngauss;
+    const int m = item.m;
+    const ClassDesc D = describe<1>(N, m, item.cls);
+    const int nb = D.nb;
+    if (nb <= 0) {
+      continue;
+    }
+    if (nb > NBM) {
+      if (tid == 0) {
+        atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
+      }
+      continue;
+    }
+    const double *T = A.tab + sl.tab;
+    const double *S = A.nsc + sl.nsc;
+    const double *Wg = A.wig + A.wig_off[sl.wig_n] + (int64_t)m * ng * N * 2;
+    const double k2 = Gr.k * Gr.k;
+    const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
+    const int ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
+    const int nrt = (nb + 7) >> 3;
+    const int col = wib * 8 + rr; // B-fragment column of this lane
+    double acc[4][4][2];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        acc[r][p][0] = acc[r][p][1] = 0.;
+      }
+    }
+    for (int g0 = 0; g0 < ng; g0 += TMX_WG32) {
+      __syncthreads();
+      for (int u = tid; u < TMX_WG32 * nb; u += 128) {
+        const int gl = u / nb;
+        const int a = u - gl * nb;
+        cplx *fp = Fs + gl * 4 * NBM + a;
+        cplx *wp = Ws + gl * 4 * NBM + a;
+        if (g0 + gl < ng) {
+          a_side<true>(D, a, N, g0 + gl, T, S, Wg, fp, NBM, m);
+          b_side<true>(D, a, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
+                       TMX_WG32 * 4 * NBM);
+        } else {
+          zero_side(fp, NBM, 4);
+          for (int g = 0; g < ngroups; ++g) {
+            zero_side(wp + g * TMX_WG32 * 4 * NBM, NBM, 4);
+          }
+        }
+      }
+      __syncthreads();
+      if (wib * 8 < nb) {
+        const int gmax = min(TMX_WG32, ng - g0);
+        const int nsl = (m == 0) ? (gmax + 1) >> 1 : gmax;
+        for (int sx = 0; sx < nsl; ++sx) {
+          const int gl = (m == 0) ? 2 * sx + (q >> 1) : sx;
+          const int t = (m == 0) ? 1 + 2 * (q & 1) : q;
+          cplx w[2];
+#pragma unroll
+          for (int g = 0; g < 2; ++g) {
+            w[g] = (col < nb && g < ngroups)
+                       ? Ws[((g * TMX_WG32 + gl) * 4 + t) * NBM + col]
+                       : mkc(0., 0.);
+          }
+#pragma unroll
+          for (int rti = 0; rti < 4; ++rti) {
+            if (rti < nrt) {
+              const int row = rti * 8 + rr;
+              const cplx f = (row < nb) ? Fs[(gl * 4 + t) * NBM + row] : mkc(0., 0.);
+              const int grp = (row < D.R0) ? 0 : 1;
+              const int lo = rti * 8, hi = min(rti * 8 + 8, nb);
+#pragma unroll
+              for (int g = 0; g < 2; ++g) {
+                const bool present = (g == 0) ? (lo < D.R0) : (ngroups == 2 && hi > D.R0);
+                if (present) {
+                  const double fj = (grp == g) ? f.x : 0.;
+                  const double fy = (grp == g) ? f.y : 0.;
+                  double *a4 = &acc[rti][0][0];
+                  dmma(a4[0], a4[1], fj, w[g].x);
+                  dmma(a4[2], a4[3], fj, w[g].y);
+                  dmma(a4[4], a4[5], fy, w[g].x);
+                  dmma(a4[6], a4[7], fy, w[g].y);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+    // Q = G^j + i G^y, RgQ = G^j (times a_n1 a_n2), into the chunk buffers
+#pragma unroll
+    for (int rti = 0; rti < 4; ++rti) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int a = rti * 8 + rr;
+        const int b = wib * 8 + 2 * q + i;
+        if (a < nb && b < nb) {
+          int ia, na, ib, nbn;
+          member(D, a, ia, na);
+          member(D, b, ib, nbn);
+          const double sc = a_n(na) * a_n(nbn);
+          const double jr = acc[rti][0][i], ji = acc[rti][1][i];
+          const double yr = acc[rti][2][i], yi = acc[rti][3][i];
+          Qm[a * LD + b] = mkc((jr - yi) * sc, (ji + yr) * sc);
+          Rm[a * LD + b] = mkc(jr * sc, ji * sc);
+        }
+      }
+    }
+    __syncthreads();
+    if (wib == 0) {
+      // LU in place in Qm, lane r updates row r
+      bool singular = false;
+      for (int i = 0; i < nb; ++i) {
+        double best = (lane >= i && lane < nb) ? cabs_dev(Qm[lane * LD + i]) : -1.;
+        int bi = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ov > best || (ov == best && oi < bi)) {
+            best = ov;
+            bi = oi;
+          }
+        }
+        singular = singular || !(best > 0.);
+        if (lane == 0) {
+          piv[i] = bi;
+        }
+        if (bi != i) {
+          for (int k = lane; k < nb; k += 32) {
+            const cplx t = Qm[i * LD + k];
+            Qm[i * LD + k] = Qm[bi * LD + k];
+            Qm[bi * LD + k] = t;
+          }
+        }
+        __syncwarp();
+        if (lane > i && lane < nb) {
+          const cplx pinv = cinv(Qm[i * LD + i]);
+          const cplx l = cmul(Qm[lane * LD + i], pinv);
+          Qm[lane * LD + i] = l;
+          for (int k = i + 1; k < nb; ++k) {
+            Qm[lane * LD + k] = csub(Qm[lane * LD + k], cmul(l, Qm[i * LD + k]));
+          }
+        }
+        __syncwarp();
+      }
+      if (lane < nb) {
+        uinv[lane] = cinv(Qm[lane * LD + lane]);
+      }
+      if (lane == 0) {
+        // column exchanges of Matrix::plu_inverse step 4, as a gather index
+        for (int j = 0; j < nb; ++j) {
+          perm[j] = j;
+        }
+        for (int j = nb - 1; j >= 0; --j) {
+          const int p = piv[j];
+          const int t = perm[j];
+          perm[j] = perm[p];
+          perm[p] = t;
+        }
+        if (singular) {
+          atomicOr(&A.status[sl.grain], TMX_ST_SINGULAR);
+        }
+      }
+      __syncwarp();
+      // solve T_c Q_c = -RgQ_c, lane r on row r of Rm
+      if (lane < nb) {
+        cplx *x = Rm + lane * LD;
+        for (int k = 0; k < nb; ++k) {
+          x[k] = mkc(-x[k].x, -x[k].y);
+        }
+        for (int j = 0; j < nb; ++j) {
+          const cplx xj = cmul(x[j], uinv[j]);
+          x[j] = xj;
+          for (int k = j + 1; k < nb; ++k) {
+            x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
+          }
+        }
+        for (int j = nb - 1; j >= 1; --j) {
+          const cplx xj = x[j];
+          for (int k = 0; k < j; ++k) {
+            x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (A.lu) {
+      cplx *Ls = A.lu + item.scratch;
+      for (int u = tid; u < nb * nb; u += 128) {
+        Ls[u] = Qm[(u / nb) * LD + (u % nb)];
+      }
+      int *ps = reinterpret_cast<int *>(Ls + (int64_t)nb * nb);
+      for (int j = tid; j < nb; j += 128) {
+        ps[j] = perm[j];
+      }
+    }
+    // write out: T_c[a][b] = Y[a][perm[b]]
+    if (sl.tout < 0) {
+      if (tid < nb) {
+        int ia, na;
+        member(D, tid, ia, na);
+        A.diag[sl.diag + ia * N + (na - 1)] = Rm[tid * LD + perm[tid]];
+      }
+    } else {
+      cplx *Tb = A.tout + sl.tout + block_offset(N, m);
+      const int w2 = 2 * D.nbb;
+      for (int u = tid; u < nb * nb; u += 128) {
+        const int a = u / nb;
+        const int b = u - a * nb;
+        int ia, na, ib, nbn;
+        member(D, a, ia, na);
+        member(D, b, ib, nbn);
+        Tb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ib * D.nbb + (nbn - D.nmin)] =
+            Rm[a * LD + perm[b]];
+      }
+    }
+  }
+}
+
+static void launch_cta32(const TmxBlockArgs &a, cudaStream_t stream) {
+  const size_t smem = (size_t)cta32_elems() * sizeof(cplx);
+  cudaFuncSetAttribute(k_blocks_cta32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int blocks = (int)std::min<int64_t>(a.nitems, 148 * 12);
+  k_blocks_cta32<<<blocks, 128, smem, stream>>>(a);
+}
+
 // shared memory of one block: the larger of the assembly chunk buffers and
 // the LU phase (factors, pivots and a right-hand-side chunk)
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
@@ -875,12 +1139,12 @@ void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
     launch_warp_variant<1, 1, 3, true>(a, stream);
     return;
   }
-  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
   if (a.max_nb <= 32) {
-    launch_variant<2, 4, 128, 4>(a, smem, stream);
-  } else {
-    launch_variant<4, 4, 256, 1>(a, smem, stream);
+    launch_cta32(a, stream);
+    return;
   }
+  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
+  launch_variant<4, 4, 256, 1>(a, smem, stream);
 }
 
 // ----------------------------------------------------------- convergence --

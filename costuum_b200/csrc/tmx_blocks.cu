@@ -40,19 +40,10 @@
 // LEAN: without the factor a_n (the caller scales the finished entries by
 // a_n1 a_n2) and, for m = 0, only the terms 1 and 3 that survive mu = 0.
 template <bool LEAN = false>
-__device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
-                                       const double *__restrict__ T,
-                                       const double *__restrict__ S,
-                                       const double *__restrict__ Wg, cplx *f,
-                                       int ts, int m = 1) {
-  int i, n;
-  member(D, a, i, n);
-  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
-  const double j = t[TMX_Q_J], dj = t[TMX_Q_DJ];
-  const double y = t[TMX_Q_Y], dy = t[TMX_Q_DY];
-  const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
-  const double d = w[0], dd = w[1];
-  const double *s = S + (int64_t)g * TMX_NS;
+__device__ __forceinline__ void a_side_row(double j, double dj, double y,
+                                           double dy, double d, double dd,
+                                           const double *s, int n, cplx *f,
+                                           int ts, int m) {
   const double nn = n * (n + 1.);
   const double q = nn * s[TMX_NS_DRR] * s[TMX_NS_KRINV] * d;
   if (LEAN) {
@@ -71,24 +62,29 @@ __device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
   f[3 * ts] = mkc(an * (dd * dj + q * j), an * (dd * dy + q * y));
 }
 
+template <bool LEAN = false>
+__device__ __forceinline__ void a_side(const ClassDesc &D, int a, int N, int g,
+                                       const double *__restrict__ T,
+                                       const double *__restrict__ S,
+                                       const double *__restrict__ Wg, cplx *f,
+                                       int ts, int m = 1) {
+  int i, n;
+  member(D, a, i, n);
+  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+  const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
+  a_side_row<LEAN>(t[TMX_Q_J], t[TMX_Q_DJ], t[TMX_Q_Y], t[TMX_Q_DY], w[0], w[1],
+                   S + (int64_t)g * TMX_NS, n, f, ts, m);
+}
+
 // B-side vectors of column member b at node g for each row group, stored to
 // w[rg * gs + t * ts] (rg = 0 rows of block index D.iA, rg = 1 rows of D.iB).
 // LEAN as for a_side.
 template <bool LEAN = false>
-__device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
-                                       int g, int ngroups,
-                                       const double *__restrict__ T,
-                                       const double *__restrict__ S,
-                                       const double *__restrict__ Wg, double k2,
-                                       cplx k2mr, cplx *w, int ts, int gs) {
-  int ib, n;
-  member(D, b, ib, n);
-  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
-  const cplx jm = mkc(t[TMX_Q_JM_RE], t[TMX_Q_JM_IM]);
-  const cplx djm = mkc(t[TMX_Q_DJM_RE], t[TMX_Q_DJM_IM]);
-  const double *wg = Wg + ((int64_t)g * N + (n - 1)) * 2;
-  const double d = wg[0], dd = wg[1];
-  const double *s = S + (int64_t)g * TMX_NS;
+__device__ __forceinline__ void b_side_row(const ClassDesc &D, int ib, int n,
+                                           int m, cplx jm, cplx djm, double d,
+                                           double dd, const double *s,
+                                           int ngroups, double k2, cplx k2mr,
+                                           cplx *w, int ts, int gs) {
   const double an = LEAN ? 1. : a_n(n);
   const double nn = n * (n + 1.);
   const cplx kmi = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
@@ -125,6 +121,22 @@ __device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
       wr[3 * ts] = cmul(ic2, G1);
     }
   }
+}
+
+template <bool LEAN = false>
+__device__ __forceinline__ void b_side(const ClassDesc &D, int b, int N, int m,
+                                       int g, int ngroups,
+                                       const double *__restrict__ T,
+                                       const double *__restrict__ S,
+                                       const double *__restrict__ Wg, double k2,
+                                       cplx k2mr, cplx *w, int ts, int gs) {
+  int ib, n;
+  member(D, b, ib, n);
+  const double *t = T + ((int64_t)g * N + (n - 1)) * TMX_NQ;
+  const double *wg = Wg + ((int64_t)g * N + (n - 1)) * 2;
+  b_side_row<LEAN>(D, ib, n, m, mkc(t[TMX_Q_JM_RE], t[TMX_Q_JM_IM]),
+                   mkc(t[TMX_Q_DJM_RE], t[TMX_Q_DJM_IM]), wg[0], wg[1],
+                   S + (int64_t)g * TMX_NS, ngroups, k2, k2mr, w, ts, gs);
 }
 
 // zero A-side / B-side entries (padding and nodes past ngauss)
@@ -473,6 +485,66 @@ __host__ __device__ constexpr int warp_elems() {
   return 12 * TMX_WG * NBM;
 }
 
+// Staging area of the next chunk's table rows (complex units): per node and
+// class member one row of TMX_ROW doubles (the Bessel row j, j', y, y', j~,
+// j~' and the Wigner pair d, d'; 80 bytes, so 16-byte reads of consecutive
+// members hit distinct banks), and the node's scalar row (TMX_NS doubles).
+#define TMX_ROW 10
+template <int NBM>
+__host__ __device__ constexpr int warp_stage_elems() {
+  return TMX_WG * (NBM * TMX_ROW + TMX_NS) / 2;
+}
+
+// 16-byte asynchronous global -> shared copies (L2 only)
+__device__ __forceinline__ void cp16(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Issue the copies of the rows of nodes [g0, g0 + TMX_WG) for members
+// [0, nb) of class D into the staging area (one commit group per lane).
+// Rows start on 16-byte boundaries: table offsets are multiples of TMX_NQ
+// (8) doubles, Wigner offsets of 2 and node-scalar offsets of TMX_NS (16).
+template <int NBM>
+__device__ __forceinline__ void stage_rows(double *st, const ClassDesc &D,
+                                           int N, int g0, int ng,
+                                           const double *__restrict__ T,
+                                           const double *__restrict__ S,
+                                           const double *__restrict__ Wg,
+                                           int lane) {
+  double *ss = st + TMX_WG * NBM * TMX_ROW;
+  for (int q = lane; q < D.nb * 5; q += 32) {
+    const int a = q / 5;
+    const int p = q - 5 * a;
+    int ia, n;
+    member(D, a, ia, n);
+#pragma unroll
+    for (int gl = 0; gl < TMX_WG; ++gl) {
+      const int g = g0 + gl;
+      if (g < ng) {
+        const int64_t r = (int64_t)g * N + (n - 1);
+        const double *src = (p < 4) ? T + r * TMX_NQ + 2 * p : Wg + r * 2;
+        cp16(st + (gl * NBM + a) * TMX_ROW + 2 * p, src);
+      }
+    }
+  }
+  for (int q = lane; q < TMX_WG * (TMX_NS / 2); q += 32) {
+    const int gl = q / (TMX_NS / 2);
+    const int p = q - gl * (TMX_NS / 2);
+    if (g0 + gl < ng) {
+      cp16(ss + gl * TMX_NS + 2 * p, S + (int64_t)(g0 + gl) * TMX_NS + 2 * p);
+    }
+  }
+  cp_commit();
+}
+
 // D += A B for one m8n8k4 FP64 tensor-core tile: lane l holds A[l / 4][l % 4],
 // B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}]
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
@@ -482,11 +554,185 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
       : "d"(a), "d"(b));
 }
 
+// ------------------------------------------ LU and solves in registers --
+//
+// Row r of a class matrix lives in the registers of the C lanes
+// [C r, C r + C) of a warp: lane c of the group holds the columns
+// k = c + C t (t < NBM / C). Both routines perform the operations of the
+// one-row-per-lane versions in the same order.
+
+// Pivot of one elimination step: the candidate with the largest key (the
+// bits of |Q_ri| with the top bit set, which order like the non-negative
+// doubles; 0 for lanes that are no candidate), ties to the smallest position.
+__device__ __forceinline__ void warp_argmax(unsigned long long key, int pos,
+                                            int &best_pos, int &best_lane) {
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, (hi == mh) ? lo : 0u);
+  const bool top = (hi == mh) && (lo == ml) && key != 0ull;
+  const unsigned mp = __reduce_min_sync(0xffffffffu, top ? (unsigned)pos : 0xffffffffu);
+  const unsigned bal = __ballot_sync(0xffffffffu, top && (unsigned)pos == mp);
+  best_pos = (int)mp;
+  best_lane = __ffs(bal) - 1;
+}
+
+// In-place LU with partial pivoting of the nb x nb matrix Q (row stride LD,
+// shared memory) by one warp: the pivot of step i is the first row (by
+// position) at or below i with the largest |Q_ri| (Matrix::plu_inverse,
+// src/Matrix.hpp:261-384); rows stay in their lanes and carry a position.
+// prow: NBM complex of scratch. Returns true if a pivot was zero.
+template <int NBM, int C>
+__device__ __forceinline__ bool lu_rows(cplx *Qm, int LD, cplx *prow, int *piv,
+                                        int nb, int lane) {
+  constexpr int NT = NBM / C;
+  const int row = lane / C;
+  const int c = lane % C;
+  cplx q[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int k = c + C * t;
+    q[t] = (row < nb && k < nb) ? Qm[row * LD + k] : mkc(0., 0.);
+  }
+  int pos = row;
+  bool singular = false;
+#pragma unroll
+  for (int i = 0; i < NBM; ++i) {
+    if (i >= nb) {
+      break;
+    }
+    const bool own = (c == i % C);
+    double av = 0.;
+    unsigned long long key = 0ull;
+    if (own && row < nb && pos >= i) {
+      av = cabs_dev(q[i / C]);
+      key = (unsigned long long)__double_as_longlong(av) | (1ull << 63);
+    }
+    int bi, wl;
+    warp_argmax(key, pos, bi, wl);
+    const double best = __shfl_sync(0xffffffffu, av, wl);
+    singular = singular || !(best > 0.);
+    if (lane == 0) {
+      piv[i] = bi;
+    }
+    const int wrow = wl / C;
+    if (pos == i) {
+      pos = bi;
+    }
+    if (row == wrow) {
+      pos = i;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int k = c + C * t;
+        if (k >= i && k < nb) {
+          prow[k] = q[t];
+        }
+      }
+    }
+    __syncwarp();
+    const bool elim = row < nb && pos > i;
+    cplx l = mkc(0., 0.);
+    if (elim && own) {
+      const cplx pinv = cinv(prow[i]);
+      l = cmul(q[i / C], pinv);
+      q[i / C] = l;
+    }
+    l.x = __shfl_sync(0xffffffffu, l.x, i % C, C);
+    l.y = __shfl_sync(0xffffffffu, l.y, i % C, C);
+    if (elim) {
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int k = c + C * t;
+        if (k > i && k < nb) {
+          q[t] = csub(q[t], cmul(l, prow[k]));
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (row < nb) {
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int k = c + C * t;
+      if (k < nb) {
+        Qm[pos * LD + k] = q[t];
+      }
+    }
+  }
+  return singular;
+}
+
+// Solve X U = -B, then Y L = X (L unit lower) for row `row` of B (in Rm,
+// overwritten by Y) with the factors in Qm and 1/U_jj in uinv; C lanes per
+// row (a group of C consecutive lanes), lane c of the group on columns
+// c + C t.
+template <int NBM, int C>
+__device__ __forceinline__ void solve_rows(cplx *Rm, const cplx *Qm, int LD,
+                                           const cplx *uinv, int nb, int row,
+                                           int c) {
+  constexpr int NT = NBM / C;
+  const bool act = row < nb;
+  cplx x[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int k = c + C * t;
+    const cplx v = (act && k < nb) ? Rm[row * LD + k] : mkc(0., 0.);
+    x[t] = mkc(-v.x, -v.y);
+  }
+  // Z U = X (forward over columns)
+#pragma unroll
+  for (int j = 0; j < NBM; ++j) {
+    if (j >= nb) {
+      break;
+    }
+    cplx xj = mkc(0., 0.);
+    if (c == j % C) {
+      xj = cmul(x[j / C], uinv[j]);
+      x[j / C] = xj;
+    }
+    xj.x = __shfl_sync(0xffffffffu, xj.x, j % C, C);
+    xj.y = __shfl_sync(0xffffffffu, xj.y, j % C, C);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int k = c + C * t;
+      if (k > j && k < nb) {
+        x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
+      }
+    }
+  }
+  // Y L = Z (backward over columns)
+#pragma unroll
+  for (int j = NBM - 1; j >= 1; --j) {
+    if (j < nb) {
+      cplx xj;
+      xj.x = __shfl_sync(0xffffffffu, x[j / C].x, j % C, C);
+      xj.y = __shfl_sync(0xffffffffu, x[j / C].y, j % C, C);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int k = c + C * t;
+        if (k < j) {
+          x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
+        }
+      }
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int k = c + C * t;
+      if (k < nb) {
+        Rm[row * LD + k] = x[t];
+      }
+    }
+  }
+}
+
 template <int TR, int TC, int MINB, bool MMA>
 __global__ void __launch_bounds__(128, MINB)
     k_blocks_warp(TmxBlockArgs A) {
   constexpr int NBM = MMA ? 16 : ((8 * TR > 4 * TC) ? 8 * TR : 4 * TC);
-  constexpr int PR = MMA ? 1 : TR; // row padding unit of the class rows
+  // row padding unit of the class rows: a tensor row tile of 8 holds one
+  // row group only
+  constexpr int PR = MMA ? 8 : TR;
   constexpr int LD = NBM + 1;
   static_assert(2 * NBM * LD + 2 * NBM <= warp_elems<NBM>(), "warp smem");
   extern __shared__ __align__(16) unsigned char tmx_wsmem[];
@@ -500,6 +746,10 @@ __global__ void __launch_bounds__(128, MINB)
   cplx *uinv = Rm + NBM * LD;           // [NBM]
   int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
   int *piv = perm + NBM;                           // [NBM]
+  double *stg = reinterpret_cast<double *>(
+      reinterpret_cast<cplx *>(tmx_wsmem) + 4 * warp_elems<NBM>() +
+      wib * warp_stage_elems<NBM>());
+  const double *stgS = stg + TMX_WG * NBM * TMX_ROW;
   const int rt = lane >> 2;
   const int ct = lane & 3;
   for (int it = blockIdx.x * 4 + wib; it < A.nitems; it += gridDim.x * 4) {
@@ -554,28 +804,56 @@ __global__ void __launch_bounds__(128, MINB)
     // rows are padded per group to a multiple of TR (describe<TR>), so the
     // TR rows of a lane share one row group and one set of B-side vectors
     const int rgl = (rt * TR < D.R0p) ? 0 : 1;
+    // the table rows of each chunk are staged in shared memory while the
+    // previous chunk is contracted
+    stage_rows<NBM>(stg, D, N, 0, ng, T, S, Wg, lane);
     for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
+      cp_wait_all();
       __syncwarp();
-#pragma unroll 1
-      for (int u = lane; u < TMX_WG * D.NRp; u += 32) {
+      // at most (TMX_WG NBM) / 32 entries per lane on each side, unrolled so
+      // that the entries' shared-memory reads and arithmetic interleave
+      constexpr int NIT = (TMX_WG * NBM + 31) / 32;
+#pragma unroll
+      for (int j = 0; j < NIT; ++j) {
+        const int u = lane + 32 * j;
+        if (u >= TMX_WG * D.NRp) {
+          break;
+        }
         const int gl = u / D.NRp;
         const int pr = u - gl * D.NRp;
         const int a = padded_member(D, pr);
         cplx *fp = Fs + gl * 4 * NBM + pr;
         if (a >= 0 && g0 + gl < ng) {
-          a_side<true>(D, a, N, g0 + gl, T, S, Wg, fp, NBM, m);
+          int ia, n;
+          member(D, a, ia, n);
+          const double *r = stg + (gl * NBM + a) * TMX_ROW;
+          const double2 jd = *reinterpret_cast<const double2 *>(r + TMX_Q_J);
+          const double2 yd = *reinterpret_cast<const double2 *>(r + TMX_Q_Y);
+          const double2 wd = *reinterpret_cast<const double2 *>(r + TMX_NQ);
+          a_side_row<true>(jd.x, jd.y, yd.x, yd.y, wd.x, wd.y, stgS + gl * TMX_NS,
+                           n, fp, NBM, m);
         } else {
           zero_side(fp, NBM, 4);
         }
       }
-#pragma unroll 1
-      for (int u = lane; u < TMX_WG * nb; u += 32) {
+#pragma unroll
+      for (int j = 0; j < NIT; ++j) {
+        const int u = lane + 32 * j;
+        if (u >= TMX_WG * nb) {
+          break;
+        }
         const int gl = u / nb;
         const int b = u - gl * nb;
         cplx *wp = Ws + gl * 4 * NBM + b;
         if (g0 + gl < ng) {
-          b_side<true>(D, b, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
-                 TMX_WG * 4 * NBM);
+          int ib, n;
+          member(D, b, ib, n);
+          const double *r = stg + (gl * NBM + b) * TMX_ROW;
+          const double2 jm = *reinterpret_cast<const double2 *>(r + TMX_Q_JM_RE);
+          const double2 djm = *reinterpret_cast<const double2 *>(r + TMX_Q_DJM_RE);
+          const double2 wd = *reinterpret_cast<const double2 *>(r + TMX_NQ);
+          b_side_row<true>(D, ib, n, m, jm, djm, wd.x, wd.y, stgS + gl * TMX_NS,
+                           ngroups, k2, k2mr, wp, NBM, TMX_WG * 4 * NBM);
         } else {
           for (int q = 0; q < ngroups; ++q) {
             zero_side(wp + q * TMX_WG * 4 * NBM, NBM, 4);
@@ -583,13 +861,18 @@ __global__ void __launch_bounds__(128, MINB)
         }
       }
       __syncwarp();
+      if (g0 + TMX_WG < ng) {
+        stage_rows<NBM>(stg, D, N, g0 + TMX_WG, ng, T, S, Wg, lane);
+      }
       const int gmax = min(TMX_WG, ng - g0);
       if constexpr (MMA) {
         // K slices of 4: the four terms of one node (m >= 1), or terms 1 and
         // 3 of two nodes (m = 0, where terms 0 and 2 vanish)
+        // padded row tile rti holds row group (rti * 8 < R0p ? 0 : 1) only
         const int q = lane & 3;
         const int rr = lane >> 2;
-        const int nrt = (nb + 7) >> 3;
+        const int nrt = D.NRp >> 3;
+        const int nct = (nb + 7) >> 3;
         const int nsl = (m == 0) ? (gmax + 1) >> 1 : gmax;
         for (int sx = 0; sx < nsl; ++sx) {
           const int gl = (m == 0) ? 2 * sx + (q >> 1) : sx;
@@ -597,30 +880,20 @@ __global__ void __launch_bounds__(128, MINB)
 #pragma unroll
           for (int rti = 0; rti < 2; ++rti) {
             if (rti < nrt) {
-              const int row = rti * 8 + rr;
-              const cplx f = (row < nb) ? Fs[(gl * 4 + t) * NBM + row] : mkc(0., 0.);
-              const int grp = (row < D.R0) ? 0 : 1;
-              const int lo = rti * 8, hi = min(rti * 8 + 8, nb);
+              const cplx f = Fs[(gl * 4 + t) * NBM + rti * 8 + rr];
+              const int g = (rti * 8 < D.R0p) ? 0 : 1;
 #pragma unroll
-              for (int g = 0; g < 2; ++g) {
-                const bool present = (g == 0) ? (lo < D.R0) : (ngroups == 2 && hi > D.R0);
-                if (present) {
-                  const double fj = (grp == g) ? f.x : 0.;
-                  const double fy = (grp == g) ? f.y : 0.;
-#pragma unroll
-                  for (int cti = 0; cti < 2; ++cti) {
-                    if (cti < nrt) {
-                      const int col = cti * 8 + rr;
-                      const cplx w = (col < nb)
-                          ? Ws[((g * TMX_WG + gl) * 4 + t) * NBM + col]
-                          : mkc(0., 0.);
-                      double *a4 = &acc[rti][cti][0][0];
-                      dmma(a4[0], a4[1], fj, w.x); // jr
-                      dmma(a4[2], a4[3], fj, w.y); // ji
-                      dmma(a4[4], a4[5], fy, w.x); // yr
-                      dmma(a4[6], a4[7], fy, w.y); // yi
-                    }
-                  }
+              for (int cti = 0; cti < 2; ++cti) {
+                if (cti < nct) {
+                  const int col = cti * 8 + rr;
+                  const cplx w = (col < nb)
+                      ? Ws[((g * TMX_WG + gl) * 4 + t) * NBM + col]
+                      : mkc(0., 0.);
+                  double *a4 = &acc[rti][cti][0][0];
+                  dmma(a4[0], a4[1], f.x, w.x); // jr
+                  dmma(a4[2], a4[3], f.x, w.y); // ji
+                  dmma(a4[4], a4[5], f.y, w.x); // yr
+                  dmma(a4[6], a4[7], f.y, w.y); // yi
                 }
               }
             }
@@ -662,9 +935,9 @@ __global__ void __launch_bounds__(128, MINB)
         for (int cti = 0; cti < 2; ++cti) {
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
-            const int a = rti * 8 + rr;
+            const int a = padded_member(D, rti * 8 + rr);
             const int b = cti * 8 + 2 * q + i;
-            if (a < nb && b < nb) {
+            if (a >= 0 && b < nb) {
               int ia, na, ib, nbn;
               member(D, a, ia, na);
               member(D, b, ib, nbn);
@@ -699,43 +972,10 @@ __global__ void __launch_bounds__(128, MINB)
     __syncwarp();
 
     // ---------------------------------------------------------------- LU
-    // in place in Qm; lane r updates row r
-    bool singular = false;
-    for (int i = 0; i < nb; ++i) {
-      // pivot: first row r >= i with the largest |Q_ri|
-      double best = (lane >= i && lane < nb) ? cabs_dev(Qm[lane * LD + i]) : -1.;
-      int bi = lane;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) {
-          best = ov;
-          bi = oi;
-        }
-      }
-      singular = singular || !(best > 0.);
-      if (lane == 0) {
-        piv[i] = bi;
-      }
-      if (bi != i) {
-        for (int k = lane; k < nb; k += 32) {
-          const cplx t = Qm[i * LD + k];
-          Qm[i * LD + k] = Qm[bi * LD + k];
-          Qm[bi * LD + k] = t;
-        }
-      }
-      __syncwarp();
-      if (lane > i && lane < nb) {
-        const cplx pinv = cinv(Qm[i * LD + i]);
-        const cplx l = cmul(Qm[lane * LD + i], pinv);
-        Qm[lane * LD + i] = l;
-        for (int k = i + 1; k < nb; ++k) {
-          Qm[lane * LD + k] = csub(Qm[lane * LD + k], cmul(l, Qm[i * LD + k]));
-        }
-      }
-      __syncwarp();
-    }
+    // in registers, 32 / NBM lanes per row; the pivot row goes through uinv
+    constexpr int CL = 32 / NBM;
+    const bool singular = lu_rows<NBM, CL>(Qm, LD, uinv, piv, nb, lane);
+    __syncwarp();
     if (lane < nb) {
       uinv[lane] = cinv(Qm[lane * LD + lane]);
     }
@@ -767,28 +1007,7 @@ __global__ void __launch_bounds__(128, MINB)
     }
 
     // ------------------------------------------ solve T_c Q_c = -RgQ_c
-    // lane r solves row r of -RgQ_c in place in Rm
-    if (lane < nb) {
-      cplx *x = Rm + lane * LD;
-      for (int k = 0; k < nb; ++k) {
-        x[k] = mkc(-x[k].x, -x[k].y);
-      }
-      // Z U = X (forward over columns)
-      for (int j = 0; j < nb; ++j) {
-        const cplx xj = cmul(x[j], uinv[j]);
-        x[j] = xj;
-        for (int k = j + 1; k < nb; ++k) {
-          x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
-        }
-      }
-      // Y L = Z (backward over columns, L unit lower)
-      for (int j = nb - 1; j >= 1; --j) {
-        const cplx xj = x[j];
-        for (int k = 0; k < j; ++k) {
-          x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
-        }
-      }
-    }
+    solve_rows<NBM, CL>(Rm, Qm, LD, uinv, nb, lane / CL, lane % CL);
     __syncwarp();
     // write out: T_c[a][b] = Y[a][perm[b]]
     if (sl.tout < 0) {
@@ -818,7 +1037,8 @@ __global__ void __launch_bounds__(128, MINB)
 template <int TR, int TC, int MINB, bool MMA>
 static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
   constexpr int NBM = MMA ? 16 : ((8 * TR > 4 * TC) ? 8 * TR : 4 * TC);
-  const size_t smem = (size_t)4 * warp_elems<NBM>() * sizeof(cplx);
+  const size_t smem =
+      (size_t)4 * (warp_elems<NBM>() + warp_stage_elems<NBM>()) * sizeof(cplx);
   cudaFuncSetAttribute(k_blocks_warp<TR, TC, MINB, MMA>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   const int blocks = (int)std::min<int64_t>((a.nitems + 3) / 4, 148 * 16);
@@ -1025,28 +1245,10 @@ __global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
           atomicOr(&A.status[sl.grain], TMX_ST_SINGULAR);
         }
       }
-      __syncwarp();
-      // solve T_c Q_c = -RgQ_c, lane r on row r of Rm
-      if (lane < nb) {
-        cplx *x = Rm + lane * LD;
-        for (int k = 0; k < nb; ++k) {
-          x[k] = mkc(-x[k].x, -x[k].y);
-        }
-        for (int j = 0; j < nb; ++j) {
-          const cplx xj = cmul(x[j], uinv[j]);
-          x[j] = xj;
-          for (int k = j + 1; k < nb; ++k) {
-            x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
-          }
-        }
-        for (int j = nb - 1; j >= 1; --j) {
-          const cplx xj = x[j];
-          for (int k = 0; k < j; ++k) {
-            x[k] = csub(x[k], cmul(xj, Qm[j * LD + k]));
-          }
-        }
-      }
     }
+    __syncthreads();
+    // solve T_c Q_c = -RgQ_c: four lanes per row, row 8 w + lane / 4
+    solve_rows<NBM, 4>(Rm, Qm, LD, uinv, nb, wib * 8 + (lane >> 2), lane & 3);
     __syncthreads();
     if (A.lu) {
       cplx *Ls = A.lu + item.scratch;

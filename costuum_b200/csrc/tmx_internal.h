@@ -32,9 +32,11 @@ enum {
   TMX_NS_KRMR_IM,
   TMX_NS_DLNR2_DD,  // d ln(r^2) / d(axis ratio)
   TMX_NS_DDRR_DD,   // d (r'/r) / d(axis ratio)
-  TMX_NS_PAD,
+  TMX_NS_PAD,       // two pads: a node's row is 128 bytes, so rows are
+  TMX_NS_PAD2,      // 16-byte aligned for asynchronous copies
   TMX_NS
 };
+static_assert(TMX_NS == 16, "node-scalar rows of 16 doubles");
 enum {
   TMX_Q_J = 0, // j_n(kr)
   TMX_Q_DJ,    // [kr j_n(kr)]' / kr

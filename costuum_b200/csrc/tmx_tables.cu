@@ -204,6 +204,7 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       S[TMX_NS_DDRR_DD] =
           2. * dd * c * sn * r2oa2 * (1. - (c * c) * r2oa2 * d2m1);
       S[TMX_NS_PAD] = 0.;
+      S[TMX_NS_PAD2] = 0.;
       if (N <= rho_smem) {
         bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
                       TMX_NQ, reinterpret_cast<double *>(trho) + threadIdx.x,

@@ -24,6 +24,20 @@
 
 #include "tmx_blocks_common.cuh"
 
+// 1 / z for the LU pivots and diagonals: conj(z) / |z|^2 on z scaled by the
+// power of two 2^-e, e the exponent of max(|Re z|, |Im z|) (exact scaling,
+// so |z|^2 lies in [1, 8) and neither overflows nor underflows); one real
+// division where Smith's quotient takes two in sequence.
+__device__ __forceinline__ cplx cinv_lu(cplx z) {
+  const double mx = fmax(fabs(z.x), fabs(z.y));
+  const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
+  const int be = min(max(1023 - e, 1), 2046);
+  const double s = __hiloint2double(be << 20, 0); // 2^-e
+  const double a = z.x * s, b = z.y * s;
+  const double r = 1. / (a * a + b * b);
+  return mkc((a * r) * s, (-b * r) * s);
+}
+
 // Build the A-side (F) and B-side (W) vectors of nodes [g0, g0 + G).
 //   F1 = a d h, F2 = a dd h, F3 = a d dh, F4 = a (dd dh + n(n+1) drr/kr d h)
 //   G1 = a d dj~, G2 = a (dd dj~ + drr/(m k r) n(n+1) d j~), G3 = a d j~,
@@ -359,7 +373,7 @@ __global__ void __launch_bounds__(NT, MINB)
       }
       __syncthreads();
     }
-    const cplx pinv = cinv(Am[i * lda + i]);
+    const cplx pinv = cinv_lu(Am[i * lda + i]);
     for (int j = i + 1 + threadIdx.x; j < nb; j += blockDim.x) {
       Am[j * lda + i] = cmul(Am[j * lda + i], pinv);
     }
@@ -373,7 +387,7 @@ __global__ void __launch_bounds__(NT, MINB)
     __syncthreads();
   }
   for (int j = threadIdx.x; j < nb; j += blockDim.x) {
-    uinv[j] = cinv(Am[j * lda + j]);
+    uinv[j] = cinv_lu(Am[j * lda + j]);
   }
   if (threadIdx.x == 0) {
     // column exchanges of Matrix::plu_inverse step 4, as a gather index
@@ -632,7 +646,7 @@ __device__ __forceinline__ bool lu_rows(cplx *Qm, int LD, cplx *prow, int *piv,
     const bool elim = row < nb && pos > i;
     cplx l = mkc(0., 0.);
     if (elim && own) {
-      const cplx pinv = cinv(prow[i]);
+      const cplx pinv = cinv_lu(prow[i]);
       l = cmul(q[i / C], pinv);
       q[i / C] = l;
     }
@@ -776,8 +790,6 @@ __global__ void __launch_bounds__(128, MINB)
     const double k2 = Gr.k * Gr.k;
     const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
     const int ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
-    const int tstep = (m == 0) ? 2 : 1; // m = 0: mu = 0 kills t = 0, 2
-    const int t0 = (m == 0) ? 1 : 0;
 
     // ---------------------------------------------------------- assembly
     // DFMA path: aj/ay[TR][TC]; tensor path: acc[row tile][col tile][jr, ji,
@@ -900,29 +912,51 @@ __global__ void __launch_bounds__(128, MINB)
           }
         }
       } else {
-        for (int gl = 0; gl < gmax; ++gl) {
-          for (int t = t0; t < 4; t += tstep) {
-            const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
-            const cplx *wr = Ws + (rgl * TMX_WG * 4 + gl * 4 + t) * NBM + ct;
-            cplx w[TC];
+        // one term t of node gl; the terms of a node are unrolled (t = 1, 3
+        // for m = 0, where mu = 0 removes t = 0, 2) so their reads overlap
+        auto term = [&](int gl, int t) {
+          const cplx *fr = Fs + (gl * 4 + t) * NBM + rt * TR;
+          const cplx *wr = Ws + (rgl * TMX_WG * 4 + gl * 4 + t) * NBM + ct;
+          cplx w[TC];
+#pragma unroll
+          for (int c = 0; c < TC; ++c) {
+            w[c] = wr[4 * c];
+          }
+#pragma unroll
+          for (int r = 0; r < TR; ++r) {
+            const cplx f = fr[r];
 #pragma unroll
             for (int c = 0; c < TC; ++c) {
-              w[c] = wr[4 * c];
+              aj[r][c][0] = fma(f.x, w[c].x, aj[r][c][0]);
+              aj[r][c][1] = fma(f.x, w[c].y, aj[r][c][1]);
+              ay[r][c][0] = fma(f.y, w[c].x, ay[r][c][0]);
+              ay[r][c][1] = fma(f.y, w[c].y, ay[r][c][1]);
             }
+          }
+        };
+        if (m == 0) {
+          for (int gl = 0; gl < gmax; ++gl) {
+            term(gl, 1);
+            term(gl, 3);
+          }
+        } else {
+          for (int gl = 0; gl < gmax; ++gl) {
 #pragma unroll
-            for (int r = 0; r < TR; ++r) {
-              const cplx f = fr[r];
-#pragma unroll
-              for (int c = 0; c < TC; ++c) {
-                aj[r][c][0] = fma(f.x, w[c].x, aj[r][c][0]);
-                aj[r][c][1] = fma(f.x, w[c].y, aj[r][c][1]);
-                ay[r][c][0] = fma(f.y, w[c].x, ay[r][c][0]);
-                ay[r][c][1] = fma(f.y, w[c].y, ay[r][c][1]);
-              }
+            for (int t = 0; t < 4; ++t) {
+              term(gl, t);
             }
           }
         }
       }
+    }
+    __syncwarp();
+    // a_n of each member once per item (in the 1/U_jj slots, free until the
+    // LU); entry (a, b) is scaled by a_n(n_a) a_n(n_b)
+    double *an_s = reinterpret_cast<double *>(uinv);
+    if (lane < nb) {
+      int ia, na;
+      member(D, lane, ia, na);
+      an_s[lane] = a_n(na);
     }
     __syncwarp();
     // Q = G^j + i G^y, RgQ = G^j, into the (reused) chunk buffers
@@ -938,10 +972,7 @@ __global__ void __launch_bounds__(128, MINB)
             const int a = padded_member(D, rti * 8 + rr);
             const int b = cti * 8 + 2 * q + i;
             if (a >= 0 && b < nb) {
-              int ia, na, ib, nbn;
-              member(D, a, ia, na);
-              member(D, b, ib, nbn);
-              const double sc = a_n(na) * a_n(nbn);
+              const double sc = an_s[a] * an_s[b];
               const double jr = acc[rti][cti][0][i], ji = acc[rti][cti][1][i];
               const double yr = acc[rti][cti][2][i], yi = acc[rti][cti][3][i];
               Qm[a * LD + b] = mkc((jr - yi) * sc, (ji + yr) * sc);
@@ -958,10 +989,7 @@ __global__ void __launch_bounds__(128, MINB)
         for (int c = 0; c < TC; ++c) {
           const int b = ct + 4 * c;
           if (a >= 0 && b < nb) {
-            int ia, na, ib, nbn;
-            member(D, a, ia, na);
-            member(D, b, ib, nbn);
-            const double sc = a_n(na) * a_n(nbn);
+            const double sc = an_s[a] * an_s[b];
             Qm[a * LD + b] = mkc((aj[r][c][0] - ay[r][c][1]) * sc,
                                  (aj[r][c][1] + ay[r][c][0]) * sc);
             Rm[a * LD + b] = mkc(aj[r][c][0] * sc, aj[r][c][1] * sc);
@@ -977,7 +1005,7 @@ __global__ void __launch_bounds__(128, MINB)
     const bool singular = lu_rows<NBM, CL>(Qm, LD, uinv, piv, nb, lane);
     __syncwarp();
     if (lane < nb) {
-      uinv[lane] = cinv(Qm[lane * LD + lane]);
+      uinv[lane] = cinv_lu(Qm[lane * LD + lane]);
     }
     if (lane == 0) {
       // column exchanges of Matrix::plu_inverse step 4, as a gather index
@@ -1169,6 +1197,14 @@ __global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
         }
       }
     }
+    // a_n of each member once per item (in the 1/U_jj slots, free until the
+    // LU)
+    double *an_s = reinterpret_cast<double *>(uinv);
+    if (tid < nb) {
+      int ia, na;
+      member(D, tid, ia, na);
+      an_s[tid] = a_n(na);
+    }
     __syncthreads();
     // Q = G^j + i G^y, RgQ = G^j (times a_n1 a_n2), into the chunk buffers
 #pragma unroll
@@ -1178,10 +1214,7 @@ __global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
         const int a = rti * 8 + rr;
         const int b = wib * 8 + 2 * q + i;
         if (a < nb && b < nb) {
-          int ia, na, ib, nbn;
-          member(D, a, ia, na);
-          member(D, b, ib, nbn);
-          const double sc = a_n(na) * a_n(nbn);
+          const double sc = an_s[a] * an_s[b];
           const double jr = acc[rti][0][i], ji = acc[rti][1][i];
           const double yr = acc[rti][2][i], yi = acc[rti][3][i];
           Qm[a * LD + b] = mkc((jr - yi) * sc, (ji + yr) * sc);
@@ -1218,7 +1251,7 @@ __global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
         }
         __syncwarp();
         if (lane > i && lane < nb) {
-          const cplx pinv = cinv(Qm[i * LD + i]);
+          const cplx pinv = cinv_lu(Qm[i * LD + i]);
           const cplx l = cmul(Qm[lane * LD + i], pinv);
           Qm[lane * LD + i] = l;
           for (int k = i + 1; k < nb; ++k) {
@@ -1228,7 +1261,7 @@ __global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
         __syncwarp();
       }
       if (lane < nb) {
-        uinv[lane] = cinv(Qm[lane * LD + lane]);
+        uinv[lane] = cinv_lu(Qm[lane * LD + lane]);
       }
       if (lane == 0) {
         // column exchanges of Matrix::plu_inverse step 4, as a gather index

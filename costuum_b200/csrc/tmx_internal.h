@@ -85,4 +85,4 @@ enum {
 
 // orders above max(nmax, |z|) at which the Bessel ratio recurrence starts
 // when no fixed start is requested
-#define TMX_BESSEL_MARGIN 64
+#define TMX_BESSEL_MARGIN 48

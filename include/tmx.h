@@ -61,7 +61,7 @@ typedef struct tmx_schedule {
   int32_t gauss_legendre_factor; /* default 2 */
   int32_t bessel_start;          /* start index of the downward j_n ratio
                                     recurrence: 0 = automatic,
-                                    max(nmax, |z|) + 64 capped at 800 (same
+                                    max(nmax, |z|) + 48 capped at 800 (same
                                     doubles as the reference's fixed start
                                     SPECIALFUNCTIONS_BESSEL_NMAX = 800);
                                     > 0 = that fixed start */

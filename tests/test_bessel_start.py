@@ -2,7 +2,7 @@
 
 The reference starts the recurrence for j_n at n = 800 for every argument
 (SpecialFunctions.hpp:40, :201-240). The CUDA table kernel starts it at
-max(nmax, ceil|z|) + 64 (capped at 800). Above max(nmax, |z|) the recurrence
+max(nmax, ceil|z|) + 48 (capped at 800). Above max(nmax, |z|) the recurrence
 contracts the start error by about (|z| / 2n)^2 per step, so both starts end
 on the same doubles. This test checks bit-equality with the oracle's
 restatement of the reference arithmetic over the argument ranges of every
@@ -11,7 +11,7 @@ import numpy as np
 
 import oracle as O
 
-MARGIN = 64
+MARGIN = 48
 
 
 def rule(nmax, absz):

@@ -822,17 +822,19 @@ __global__ void __launch_bounds__(128, MINB)
     for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
       cp_wait_all();
       __syncwarp();
-      // at most (TMX_WG NBM) / 32 entries per lane on each side, unrolled so
-      // that the entries' shared-memory reads and arithmetic interleave
-      constexpr int NIT = (TMX_WG * NBM + 31) / 32;
+      // slots (node gl, row or column) = (u / NBM, u % NBM): TMX_WG NBM / 32
+      // per lane on each side, unrolled so that their shared-memory reads and
+      // arithmetic interleave
+      constexpr int NIT = TMX_WG * NBM / 32;
+      static_assert(NIT * 32 == TMX_WG * NBM, "build slots");
 #pragma unroll
       for (int j = 0; j < NIT; ++j) {
         const int u = lane + 32 * j;
-        if (u >= TMX_WG * D.NRp) {
-          break;
+        const int gl = u / NBM;
+        const int pr = u % NBM;
+        if (pr >= D.NRp) {
+          continue;
         }
-        const int gl = u / D.NRp;
-        const int pr = u - gl * D.NRp;
         const int a = padded_member(D, pr);
         cplx *fp = Fs + gl * 4 * NBM + pr;
         if (a >= 0 && g0 + gl < ng) {
@@ -851,11 +853,11 @@ __global__ void __launch_bounds__(128, MINB)
 #pragma unroll
       for (int j = 0; j < NIT; ++j) {
         const int u = lane + 32 * j;
-        if (u >= TMX_WG * nb) {
-          break;
+        const int gl = u / NBM;
+        const int b = u % NBM;
+        if (b >= nb) {
+          continue;
         }
-        const int gl = u / nb;
-        const int b = u - gl * nb;
         cplx *wp = Ws + gl * 4 * NBM + b;
         if (g0 + gl < ng) {
           int ib, n;
@@ -1485,27 +1487,43 @@ void tmx_launch_converge(const int32_t *active, int nactive,
 // T_m[(1,n),(0,n)] + T_m[(1,n),(1,n)]), f_0 = 1, f_m = 2. One block per
 // grain reads each (contiguous) block coalesced; the reduction order is fixed.
 #define QS_THREADS 256
+// Qsca and Qext sums of the grains of one block round (TMatrixQTask,
+// TMatrixResource.hpp:1136-1210): one CTA per slot, thread t adds the
+// entries t, t + 256, ... of every m block in order (|T|^2, and Re T on the
+// block diagonals), then a warp tree and the warp partial sums in order.
+// Row and column of an entry advance incrementally (no division per entry).
 __global__ void __launch_bounds__(QS_THREADS)
-    k_qsums(const int64_t *__restrict__ t_off, const int32_t *__restrict__ nmaxv,
-            int n, const cplx *__restrict__ T, double *q_out) {
-  const int g = blockIdx.x;
-  if (g >= n) {
+    k_qsums(const TmxSlot *__restrict__ slots, int ns,
+            const cplx *__restrict__ T, double *q_out) {
+  const int s = blockIdx.x;
+  if (s >= ns) {
     return;
   }
-  const int N = nmaxv[g];
-  const cplx *Tg = T + t_off[g];
+  const TmxSlot sl = slots[s];
+  const int N = sl.nmax;
+  const cplx *Tg = T + sl.tout;
   double qs = 0., qe = 0.;
   for (int m = 0; m <= N && N > 0; ++m) {
     const int nb = (m == 0) ? N : N + 1 - m;
     const int w = 2 * nb;
     const double f = (m > 0) ? 2. : 1.;
     const cplx *B = Tg + block_offset(N, m);
+    const int dq = QS_THREADS / w, dr = QS_THREADS % w;
+    int row = threadIdx.x / w, col = threadIdx.x % w;
     double bs = 0., be = 0.;
     for (int u = threadIdx.x; u < w * w; u += QS_THREADS) {
       const cplx v = B[u];
       bs += cnorm2(v);
-      if ((u / w) % nb == (u % w) % nb) {
+      const int rm = (row >= nb) ? row - nb : row;
+      const int cm = (col >= nb) ? col - nb : col;
+      if (rm == cm) {
         be += v.x;
+      }
+      row += dq;
+      col += dr;
+      if (col >= w) {
+        col -= w;
+        ++row;
       }
     }
     qs += f * bs;
@@ -1529,17 +1547,17 @@ __global__ void __launch_bounds__(QS_THREADS)
       a += red[0][i];
       b += red[1][i];
     }
-    q_out[2 * g] = a;
-    q_out[2 * g + 1] = b;
+    q_out[2 * sl.grain] = a;
+    q_out[2 * sl.grain + 1] = b;
   }
 }
 
-void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
-                      const double2 *T, double *q_out, cudaStream_t stream) {
-  if (n <= 0) {
+void tmx_launch_qsums(const TmxSlot *slots, int ns, const cplx *T,
+                      double *q_out, cudaStream_t stream) {
+  if (ns <= 0) {
     return;
   }
-  k_qsums<<<n, QS_THREADS, 0, stream>>>(t_off, nmax, n, T, q_out);
+  k_qsums<<<ns, QS_THREADS, 0, stream>>>(slots, ns, T, q_out);
 }
 
 // ------------------------------------------------------------ chain prep --

@@ -33,6 +33,9 @@ struct tmx_ctx {
   cudaStream_t stream = nullptr;  // every launch unless noted (high priority)
   cudaStream_t stream2 = nullptr; // blocks of grains that converged while the
                                   // order loop continues (low priority)
+  cudaStream_t aux[4] = {};       // further class-size buckets of a block
+                                  // round: [0, 1] beside stream, [2, 3]
+                                  // beside stream2
   cudaMemPool_t pool = nullptr;   // device memory of this context; keeps
                                   // freed blocks for reuse (no release)
   std::string err;
@@ -49,7 +52,7 @@ struct tmx_ctx {
   DevBuf wig, wig_off;
   // batch buffers
   DevBuf grains, state, state0, act0, act1, actinit, count, slots, items, tab,
-      nsc, scratch, diag, T, t_off, nmaxv, q, status, probe;
+      nsc, scratch, diag, T, q, status, probe;
   // uploaded batch (device-resident inputs)
   bool uploaded = false;
   int64_t up_n = 0;

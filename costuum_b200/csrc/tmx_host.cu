@@ -231,8 +231,22 @@ int tmx_create(tmx_ctx **out, int device) {
                                    prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking,
                                    prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[0], cudaStreamNonBlocking,
+                                   prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[1], cudaStreamNonBlocking,
+                                   prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[2], cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[3], cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->pinned, 64) != cudaSuccess) {
     cudaGetLastError();
+    for (cudaStream_t x : {ctx->stream, ctx->stream2, ctx->aux[0], ctx->aux[1],
+                           ctx->aux[2], ctx->aux[3]}) {
+      if (x) {
+        cudaStreamDestroy(x);
+      }
+    }
     delete ctx;
     return TMX_ERR_CUDA;
   }
@@ -253,6 +267,9 @@ int tmx_create(tmx_ctx **out, int device) {
     cudaGetLastError();
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->stream2);
+    for (cudaStream_t x : ctx->aux) {
+      cudaStreamDestroy(x);
+    }
     cudaFreeHost(ctx->pinned);
     delete ctx;
     return TMX_ERR_CUDA;
@@ -269,6 +286,11 @@ void tmx_destroy(tmx_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->stream2) {
     cudaStreamSynchronize(ctx->stream2);
+  }
+  for (cudaStream_t x : ctx->aux) {
+    if (x) {
+      cudaStreamSynchronize(x);
+    }
   }
   if (ctx->t0) {
     cudaEventDestroy(ctx->t0);
@@ -287,7 +309,7 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,
                     &ctx->act1,  &ctx->count,  &ctx->slots,   &ctx->items,
                     &ctx->tab,   &ctx->nsc,    &ctx->scratch, &ctx->diag,
-                    &ctx->T,     &ctx->t_off,  &ctx->nmaxv,   &ctx->q,
+                    &ctx->T,     &ctx->q,
                     &ctx->status, &ctx->probe};
   for (DevBuf *b : bufs) {
     if (b->p) {
@@ -304,6 +326,11 @@ void tmx_destroy(tmx_ctx *ctx) {
   cudaStreamDestroy(ctx->stream);
   if (ctx->stream2) {
     cudaStreamDestroy(ctx->stream2);
+  }
+  for (cudaStream_t x : ctx->aux) {
+    if (x) {
+      cudaStreamDestroy(x);
+    }
   }
   if (ctx->pool) {
     cudaMemPoolDestroy(ctx->pool);
@@ -531,6 +558,14 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
        (rc = ensure(ctx, ctx->p2items, std::max<int64_t>(1, nitems) * sizeof(TmxItem))))) {
     return rc;
   }
+  if (ctx->q.cap < (size_t)2 * ctx->n * sizeof(double)) {
+    // Q sums of every grain of the batch; rounds on the second stream may
+    // still write the old buffer
+    CK(cudaStreamSynchronize(ctx->stream2));
+    if ((rc = ensure(ctx, ctx->q, std::max<int64_t>(1, 2 * ctx->n) * sizeof(double)))) {
+      return rc;
+    }
+  }
   if (np2 == 0) {
     return TMX_OK;
   }
@@ -576,7 +611,14 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   if ((rc = prof_end(ctx, 1, pe, 0., st))) {
     return rc;
   }
-  // class-size buckets, one launch each (largest first)
+  // class-size buckets, one launch each (largest first): the first on `st`,
+  // the others on the two auxiliary streams beside it, so that the smaller
+  // buckets fill the SMs that the tail of the larger one leaves idle; the
+  // round ends (Q sums, buffer release) when all of them are done
+  cudaStream_t *aux = (st == ctx->stream) ? &ctx->aux[0] : &ctx->aux[2];
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  int nbuckets = 0;
   const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
   int64_t i0 = 0;
   for (int b = 0; b < 5; ++b) {
@@ -585,6 +627,16 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       ++i1;
     }
     if (i1 > i0) {
+      cudaStream_t bs = st;
+      if (nbuckets > 0) {
+        bs = aux[(nbuckets - 1) & 1];
+        if (!fork) {
+          CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+          CK(cudaEventRecord(fork, st));
+        }
+        CK(cudaStreamWaitEvent(bs, fork, 0));
+      }
+      ++nbuckets;
       TmxBlockArgs B;
       B.items = ditems + i0;
       B.nitems = (int)(i1 - i0);
@@ -606,17 +658,32 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
           fl += item_flops(inb[q], items[q].m, slots[items[q].slot].ngauss);
         }
       }
-      if ((rc = prof_begin(ctx, 0, &pe, st))) {
+      if ((rc = prof_begin(ctx, 0, &pe, bs))) {
         return rc;
       }
-      tmx_launch_blocks(B, st);
+      tmx_launch_blocks(B, bs);
       LAUNCHED();
-      if ((rc = prof_end(ctx, 0, pe, fl, st))) {
+      if ((rc = prof_end(ctx, 0, pe, fl, bs))) {
         return rc;
+      }
+      if (bs != st) {
+        cudaEvent_t j;
+        CK(cudaEventCreateWithFlags(&j, cudaEventDisableTiming));
+        CK(cudaEventRecord(j, bs));
+        joins.push_back(j);
       }
     }
     i0 = i1;
   }
+  for (cudaEvent_t j : joins) {
+    CK(cudaStreamWaitEvent(st, j, 0));
+    CK(cudaEventDestroy(j));
+  }
+  if (fork) {
+    CK(cudaEventDestroy(fork));
+  }
+  tmx_launch_qsums(dslots, np2, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
+  LAUNCHED();
   if (temp) {
     CK(cudaFreeAsync(tab, st));
     CK(cudaFreeAsync(nsc, st));
@@ -639,22 +706,6 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   ctx->p2_rounds = rounds;
   ctx->t_averaged = false;
   if (t_total > 0) {
-    if ((rc = ensure(ctx, ctx->t_off, n * sizeof(int64_t))) ||
-        (rc = ensure(ctx, ctx->nmaxv, n * sizeof(int32_t))) ||
-        (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
-      return rc;
-    }
-    std::vector<int32_t> nmv(n);
-    for (int64_t i = 0; i < n; ++i) {
-      nmv[i] = ctx->nmax_h[i];
-    }
-    CK(cudaMemcpyAsync(ctx->t_off.p, ctx->t_off_h.data(), n * sizeof(int64_t),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->nmaxv.p, nmv.data(), n * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, st));
-    tmx_launch_qsums((const int64_t *)ctx->t_off.p, (const int32_t *)ctx->nmaxv.p,
-                     (int)n, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
-    LAUNCHED();
     std::vector<double> q2(2 * n);
     std::vector<int32_t> stb(n);
     CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),

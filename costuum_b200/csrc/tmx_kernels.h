@@ -85,9 +85,10 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          int32_t *done_ord, int32_t *done_count,
                          cudaStream_t stream);
 
-// full Q sums over all m blocks (TMatrixQTask)
-void tmx_launch_qsums(const int64_t *t_off, const int32_t *nmax, int n,
-                      const double2 *T, double *q_out, cudaStream_t stream);
+// full Q sums over all m blocks (TMatrixQTask) of the grains of a block round: q_out[2 g], q_out[2 g + 1]
+// for g = slots[s].grain
+void tmx_launch_qsums(const TmxSlot *slots, int ns, const double2 *T,
+                      double *q_out, cudaStream_t stream);
 
 // FP64 throughput probes (DFMA pipe and DMMA tensor pipe)
 void tmx_launch_probe_dfma(double *out, int iters, int blocks,

@@ -320,7 +320,12 @@ def run_ours(args):
         res = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
         nm, ng = res.nmax.copy(), res.ngauss.copy()
         fwd, bwd = [], []
-        for _ in range(2):
+        # one untimed pass of both sequences (buffers and table caches of the
+        # observable and gradient paths), then the best of three
+        ctx.observables(th, co)
+        ctx.tmatrix_batch_fixed(r, lam, m, d, nm, ng)
+        ctx.gradients(th, co)
+        for _ in range(3):
             flush_l2(flush)
             torch.cuda.synchronize()
             lib.tmx_timer_start(h)

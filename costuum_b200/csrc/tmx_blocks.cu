@@ -24,19 +24,6 @@
 
 #include "tmx_blocks_common.cuh"
 
-// 1 / z for the LU pivots and diagonals: conj(z) / |z|^2 on z scaled by the
-// power of two 2^-e, e the exponent of max(|Re z|, |Im z|) (exact scaling,
-// so |z|^2 lies in [1, 8) and neither overflows nor underflows); one real
-// division where Smith's quotient takes two in sequence.
-__device__ __forceinline__ cplx cinv_lu(cplx z) {
-  const double mx = fmax(fabs(z.x), fabs(z.y));
-  const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
-  const int be = min(max(1023 - e, 1), 2046);
-  const double s = __hiloint2double(be << 20, 0); // 2^-e
-  const double a = z.x * s, b = z.y * s;
-  const double r = 1. / (a * a + b * b);
-  return mkc((a * r) * s, (-b * r) * s);
-}
 
 // Build the A-side (F) and B-side (W) vectors of nodes [g0, g0 + G).
 //   F1 = a d h, F2 = a dd h, F3 = a d dh, F4 = a (dd dh + n(n+1) drr/kr d h)
@@ -522,42 +509,73 @@ __device__ __forceinline__ void cp_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
-// Issue the copies of the rows of nodes [g0, g0 + TMX_WG) for members
-// [0, nb) of class D into the staging area (one commit group per lane).
+// Copies of one item's table rows into the staging area. Each lane owns up
+// to SL_MAX 16-byte pieces of the member rows (piece p < 4 of the Bessel row
+// of member a, or p = 4: its Wigner pair) and one piece of the node scalars;
+// their source addresses at node 0 and their per-node strides are set up
+// once per item, so a chunk costs one add and one copy per piece and node.
 // Rows start on 16-byte boundaries: table offsets are multiples of TMX_NQ
 // (8) doubles, Wigner offsets of 2 and node-scalar offsets of TMX_NS (16).
 template <int NBM>
-__device__ __forceinline__ void stage_rows(double *st, const ClassDesc &D,
-                                           int N, int g0, int ng,
-                                           const double *__restrict__ T,
-                                           const double *__restrict__ S,
-                                           const double *__restrict__ Wg,
-                                           int lane) {
-  double *ss = st + TMX_WG * NBM * TMX_ROW;
-  for (int q = lane; q < D.nb * 5; q += 32) {
-    const int a = q / 5;
-    const int p = q - 5 * a;
-    int ia, n;
-    member(D, a, ia, n);
+struct StagePlan {
+  static constexpr int SL_MAX = (NBM * 5 + 31) / 32;
+  const double *src[SL_MAX]; // piece at node 0
+  int stride[SL_MAX];        // doubles per node
+  int dst[SL_MAX];           // double offset in the stage (node 0); -1: none
+  const double *ssrc;        // node-scalar piece at node 0
+  int sdst;                  // -1: none
+
+  __device__ __forceinline__ void init(const ClassDesc &D, int N,
+                                       const double *__restrict__ T,
+                                       const double *__restrict__ S,
+                                       const double *__restrict__ Wg,
+                                       int lane) {
 #pragma unroll
-    for (int gl = 0; gl < TMX_WG; ++gl) {
-      const int g = g0 + gl;
-      if (g < ng) {
-        const int64_t r = (int64_t)g * N + (n - 1);
-        const double *src = (p < 4) ? T + r * TMX_NQ + 2 * p : Wg + r * 2;
-        cp16(st + (gl * NBM + a) * TMX_ROW + 2 * p, src);
+    for (int j = 0; j < SL_MAX; ++j) {
+      const int q = lane + 32 * j;
+      dst[j] = -1;
+      src[j] = T;
+      stride[j] = 0;
+      if (q < D.nb * 5) {
+        const int a = q / 5;
+        const int p = q - 5 * a;
+        int ia, n;
+        member(D, a, ia, n);
+        src[j] = (p < 4) ? T + (int64_t)(n - 1) * TMX_NQ + 2 * p
+                         : Wg + (int64_t)(n - 1) * 2;
+        stride[j] = (p < 4) ? N * TMX_NQ : 2 * N;
+        dst[j] = a * TMX_ROW + 2 * p;
       }
     }
+    // TMX_WG nodes x TMX_NS / 2 pieces of node scalars = 32
+    static_assert(TMX_WG * (TMX_NS / 2) == 32, "one node-scalar piece per lane");
+    const int gl = lane / (TMX_NS / 2);
+    const int p = lane - gl * (TMX_NS / 2);
+    ssrc = S + (int64_t)gl * TMX_NS + 2 * p;
+    sdst = TMX_WG * NBM * TMX_ROW + gl * TMX_NS + 2 * p;
   }
-  for (int q = lane; q < TMX_WG * (TMX_NS / 2); q += 32) {
-    const int gl = q / (TMX_NS / 2);
-    const int p = q - gl * (TMX_NS / 2);
-    if (g0 + gl < ng) {
-      cp16(ss + gl * TMX_NS + 2 * p, S + (int64_t)(g0 + gl) * TMX_NS + 2 * p);
+
+  // copies of nodes [g0, g0 + TMX_WG) (one commit group per lane)
+  __device__ __forceinline__ void issue(double *st, int g0, int ng) const {
+#pragma unroll
+    for (int j = 0; j < SL_MAX; ++j) {
+      if (dst[j] >= 0) {
+        const double *sp = src[j] + (int64_t)g0 * stride[j];
+#pragma unroll
+        for (int gl = 0; gl < TMX_WG; ++gl) {
+          if (g0 + gl < ng) {
+            cp16(st + dst[j] + gl * NBM * TMX_ROW, sp);
+          }
+          sp += stride[j];
+        }
+      }
     }
+    if (g0 + (sdst - TMX_WG * NBM * TMX_ROW) / TMX_NS < ng) {
+      cp16(st + sdst, ssrc + (int64_t)g0 * TMX_NS);
+    }
+    cp_commit();
   }
-  cp_commit();
-}
+};
 
 // D += A B for one m8n8k4 FP64 tensor-core tile: lane l holds A[l / 4][l % 4],
 // B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}]
@@ -675,71 +693,6 @@ __device__ __forceinline__ bool lu_rows(cplx *Qm, int LD, cplx *prow, int *piv,
   return singular;
 }
 
-// Solve X U = -B, then Y L = X (L unit lower) for row `row` of B (in Rm,
-// overwritten by Y) with the factors in Qm and 1/U_jj in uinv; C lanes per
-// row (a group of C consecutive lanes), lane c of the group on columns
-// c + C t.
-template <int NBM, int C>
-__device__ __forceinline__ void solve_rows(cplx *Rm, const cplx *Qm, int LD,
-                                           const cplx *uinv, int nb, int row,
-                                           int c) {
-  constexpr int NT = NBM / C;
-  const bool act = row < nb;
-  cplx x[NT];
-#pragma unroll
-  for (int t = 0; t < NT; ++t) {
-    const int k = c + C * t;
-    const cplx v = (act && k < nb) ? Rm[row * LD + k] : mkc(0., 0.);
-    x[t] = mkc(-v.x, -v.y);
-  }
-  // Z U = X (forward over columns)
-#pragma unroll
-  for (int j = 0; j < NBM; ++j) {
-    if (j >= nb) {
-      break;
-    }
-    cplx xj = mkc(0., 0.);
-    if (c == j % C) {
-      xj = cmul(x[j / C], uinv[j]);
-      x[j / C] = xj;
-    }
-    xj.x = __shfl_sync(0xffffffffu, xj.x, j % C, C);
-    xj.y = __shfl_sync(0xffffffffu, xj.y, j % C, C);
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      const int k = c + C * t;
-      if (k > j && k < nb) {
-        x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
-      }
-    }
-  }
-  // Y L = Z (backward over columns)
-#pragma unroll
-  for (int j = NBM - 1; j >= 1; --j) {
-    if (j < nb) {
-      cplx xj;
-      xj.x = __shfl_sync(0xffffffffu, x[j / C].x, j % C, C);
-      xj.y = __shfl_sync(0xffffffffu, x[j / C].y, j % C, C);
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        const int k = c + C * t;
-        if (k < j) {
-          x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
-        }
-      }
-    }
-  }
-  if (act) {
-#pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      const int k = c + C * t;
-      if (k < nb) {
-        Rm[row * LD + k] = x[t];
-      }
-    }
-  }
-}
-
 template <int TR, int TC, int MINB, bool MMA>
 __global__ void __launch_bounds__(128, MINB)
     k_blocks_warp(TmxBlockArgs A) {
@@ -818,7 +771,9 @@ __global__ void __launch_bounds__(128, MINB)
     const int rgl = (rt * TR < D.R0p) ? 0 : 1;
     // the table rows of each chunk are staged in shared memory while the
     // previous chunk is contracted
-    stage_rows<NBM>(stg, D, N, 0, ng, T, S, Wg, lane);
+    StagePlan<NBM> plan;
+    plan.init(D, N, T, S, Wg, lane);
+    plan.issue(stg, 0, ng);
     for (int g0 = 0; g0 < ng; g0 += TMX_WG) {
       cp_wait_all();
       __syncwarp();
@@ -876,7 +831,7 @@ __global__ void __launch_bounds__(128, MINB)
       }
       __syncwarp();
       if (g0 + TMX_WG < ng) {
-        stage_rows<NBM>(stg, D, N, g0 + TMX_WG, ng, T, S, Wg, lane);
+        plan.issue(stg, g0 + TMX_WG, ng);
       }
       const int gmax = min(TMX_WG, ng - g0);
       if constexpr (MMA) {

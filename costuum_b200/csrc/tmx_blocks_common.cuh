@@ -95,3 +95,82 @@ struct AsmLayout {
 // hypot without the libm scaling path; the magnitudes here are far from
 // overflow/underflow
 __device__ __forceinline__ double cabs_dev(cplx a) { return hypot(a.x, a.y); }
+
+// 1 / z for the LU pivots and diagonals: conj(z) / |z|^2 on z scaled by the
+// power of two 2^-e, e the exponent of max(|Re z|, |Im z|) (exact scaling,
+// so |z|^2 lies in [1, 8) and neither overflows nor underflows); one real
+// division where Smith's quotient takes two in sequence.
+__device__ __forceinline__ cplx cinv_lu(cplx z) {
+  const double mx = fmax(fabs(z.x), fabs(z.y));
+  const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
+  const int be = min(max(1023 - e, 1), 2046);
+  const double s = __hiloint2double(be << 20, 0); // 2^-e
+  const double a = z.x * s, b = z.y * s;
+  const double r = 1. / (a * a + b * b);
+  return mkc((a * r) * s, (-b * r) * s);
+}
+
+// Solve X U = -B, then Y L = X (L unit lower) for row `row` of B (in Rm,
+// overwritten by Y) with the factors in Qm and 1/U_jj in uinv; C lanes per
+// row (a group of C consecutive lanes), lane c of the group on columns
+// c + C t.
+template <int NBM, int C>
+__device__ __forceinline__ void solve_rows(cplx *Rm, const cplx *Qm, int LD,
+                                           const cplx *uinv, int nb, int row,
+                                           int c) {
+  constexpr int NT = NBM / C;
+  const bool act = row < nb;
+  cplx x[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int k = c + C * t;
+    const cplx v = (act && k < nb) ? Rm[row * LD + k] : mkc(0., 0.);
+    x[t] = mkc(-v.x, -v.y);
+  }
+  // Z U = X (forward over columns)
+#pragma unroll
+  for (int j = 0; j < NBM; ++j) {
+    if (j >= nb) {
+      break;
+    }
+    cplx xj = mkc(0., 0.);
+    if (c == j % C) {
+      xj = cmul(x[j / C], uinv[j]);
+      x[j / C] = xj;
+    }
+    xj.x = __shfl_sync(0xffffffffu, xj.x, j % C, C);
+    xj.y = __shfl_sync(0xffffffffu, xj.y, j % C, C);
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int k = c + C * t;
+      if (k > j && k < nb) {
+        x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
+      }
+    }
+  }
+  // Y L = Z (backward over columns)
+#pragma unroll
+  for (int j = NBM - 1; j >= 1; --j) {
+    if (j < nb) {
+      cplx xj;
+      xj.x = __shfl_sync(0xffffffffu, x[j / C].x, j % C, C);
+      xj.y = __shfl_sync(0xffffffffu, x[j / C].y, j % C, C);
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const int k = c + C * t;
+        if (k < j) {
+          x[t] = csub(x[t], cmul(xj, Qm[j * LD + k]));
+        }
+      }
+    }
+  }
+  if (act) {
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int k = c + C * t;
+      if (k < nb) {
+        Rm[row * LD + k] = x[t];
+      }
+    }
+  }
+}

@@ -146,23 +146,30 @@ struct TmxQJob {
 
 void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
                    int blocks, cudaStream_t stream);
+// source and destination arrays of up to four matrix sets processed by one
+// launch (a T-matrix set and its tangents)
+struct TmxMatSet {
+  const double2 *src[4];
+  double2 *dst[4];
+};
 // orientation average (coef_set >= 0) or copy of every grain's T-matrix,
 // with the amplitude factors c_{n' n} folded in when fold != 0;
 // pair_base[g] = first (n1, n2) pair of grain g (nmax^2 pairs per grain),
-// mmax >= every nmax
+// mmax >= every nmax; nmat (1 or 4) sets src[k] -> dst[k]
 void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
-                             int ngrains, int64_t npairs, const double2 *T,
-                             double2 *Ta, const double *coeffs, int ncoef,
+                             int ngrains, int64_t npairs, const TmxMatSet &mats,
+                             int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,
                              cudaStream_t stream);
-// CTAs of the amplitude kernel at full occupancy for nbmax (its work slots:
-// grid x 32 x (nbmax + 1) x 4 complex)
-int tmx_amp_grid(int nbmax);
+// CTAs of the amplitude kernel at full occupancy for nbmax and nmat (its
+// work slots: grid x nmat x 32 x (nbmax + 1) x 4 complex)
+int tmx_amp_grid(int nbmax, int nmat);
+// amplitudes of nmat (1 or 4) averaged sets: src[k] -> S at dst[k]
 void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
-                    const TmxObsGrain *og, const double2 *Ta,
-                    const TmxAngle *angles, const double2 *phis, double2 *S,
-                    double2 *xslot, int nbmax, int grid, cudaStream_t stream);
+                    const TmxObsGrain *og, const TmxMatSet &mats, int nmat,
+                    const TmxAngle *angles, const double2 *phis, double2 *xslot,
+                    int nbmax, int grid, cudaStream_t stream);
 void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,
                            const double2 *S, const double *wts, int nacc,
                            double *qout, int qstride, int do_abs, int do_ext,

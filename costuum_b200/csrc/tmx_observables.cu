@@ -166,20 +166,21 @@ __device__ __forceinline__ cplx c_fold(int nin, int nout, double a, cplx z) {
 // without an orientation distribution (coef_set < 0) are copied. Either way
 // the output carries the factor c_{n2 n1} of the amplitude sums, so that
 // the amplitude kernel contracts Ta with real vectors only.
-// Shared memory per warp: t[4][M + 1] and S[2][2M + 1] complex.
+// Shared memory per warp and matrix: t[4][M + 1] and S[2][2M + 1] complex.
+// NMAT matrices (a T-matrix and its tangents) share the Clebsch-Gordan
+// reads and the loops; each is summed in the same order as alone.
+template <int NMAT>
 __global__ void __launch_bounds__(256)
 k_orient_pairs(const TmxObsGrain *__restrict__ og,
                const int64_t *__restrict__ pair_base, int ngrains,
-               int64_t npairs, const cplx *__restrict__ T,
-               cplx *__restrict__ Ta, const double *__restrict__ coeffs,
+               int64_t npairs, TmxMatSet mats, const double *__restrict__ coeffs,
                int ncoef, const int64_t *__restrict__ cg_off,
-               const double *__restrict__ cg, int cg_nmax, int wcap,
-               int fold) {
+               const double *__restrict__ cg, int cg_nmax, int wcap, int fold) {
   extern __shared__ cplx osh[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
-  cplx *tv = osh + (int64_t)warp * wcap;
+  cplx *tv = osh + (int64_t)warp * wcap * NMAT;
   for (int64_t w = (int64_t)blockIdx.x * nwarps + warp; w < npairs;
        w += (int64_t)gridDim.x * nwarps) {
     // grain of pair w: the last g with pair_base[g] <= w
@@ -198,8 +199,6 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
     const int n1 = pair / N + 1;
     const int n2 = pair % N + 1;
     const int M = min(n1, n2);
-    const cplx *Tg = T + G.t_off;
-    cplx *Tag = Ta + G.t_off;
     // fold = 0: the plain averaged T-matrix (c = 1: i^0 times 1)
     const double afold = fold ? a_fac(n1) * a_fac(n2) : 1.;
     const int nfold = fold ? n1 : n2 - 1;
@@ -208,7 +207,10 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
         for (int q = 0; q < 4; ++q) {
           const int i1 = q >> 1, i2 = q & 1;
           const int64_t e = telem(N, m, i1, n1, i2, n2);
-          Tag[e] = c_fold(n2, nfold, afold, Tg[e]);
+#pragma unroll
+          for (int k = 0; k < NMAT; ++k) {
+            mats.dst[k][G.t_off + e] = c_fold(n2, nfold, afold, mats.src[k][G.t_off + e]);
+          }
         }
       }
       continue;
@@ -217,51 +219,79 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
     const int nN = 2 * M + 1;
     const int Nlo = abs(n1 - n2);
     const double *C = cg + cg_off[(n1 - 1) * cg_nmax + (n2 - 1)];
-    cplx *t00 = tv, *t11 = tv + (M + 1), *t01 = tv + 2 * (M + 1),
-         *t10 = tv + 3 * (M + 1);
-    cplx *S = tv + 4 * (M + 1);
+    // per matrix k: t00, t11, t01, t10 [M + 1] and S [2 (2M + 1)] at tv + k wcap
+    const int o11 = M + 1, o01 = 2 * (M + 1), o10 = 3 * (M + 1), oS = 4 * (M + 1);
     for (int m1 = lane; m1 <= M; m1 += 32) {
       // f(m1) (-1)^m1 is a power of two with a sign: the product is exact
       const double f = ((m1 == 0) ? 1. : 2.) * ((m1 & 1) ? -1. : 1.);
-      t00[m1] = cscale(Tg[telem(N, m1, 0, n1, 0, n2)], f);
-      t11[m1] = cscale(Tg[telem(N, m1, 1, n1, 1, n2)], f);
-      t01[m1] = cscale(Tg[telem(N, m1, 0, n1, 1, n2)], f);
-      t10[m1] = cscale(Tg[telem(N, m1, 1, n1, 0, n2)], f);
+#pragma unroll
+      for (int k = 0; k < NMAT; ++k) {
+        const cplx *Tg = mats.src[k] + G.t_off;
+        cplx *t = tv + k * wcap;
+        t[m1] = cscale(Tg[telem(N, m1, 0, n1, 0, n2)], f);
+        t[o11 + m1] = cscale(Tg[telem(N, m1, 1, n1, 1, n2)], f);
+        t[o01 + m1] = cscale(Tg[telem(N, m1, 0, n1, 1, n2)], f);
+        t[o10 + m1] = cscale(Tg[telem(N, m1, 1, n1, 0, n2)], f);
+      }
     }
     __syncwarp();
     // pass 1: S(N') for the two sub-blocks of its parity
     for (int j = lane; j < nN; j += 32) {
       const double *Cr = C + (int64_t)j * (M + 1);
-      const cplx *ta = (j & 1) ? t01 : t00;
-      const cplx *tb = (j & 1) ? t10 : t11;
-      cplx sa = mkc(0., 0.), sb = sa;
+      const int oa = (j & 1) ? o01 : 0;
+      const int ob = (j & 1) ? o10 : o11;
+      cplx sa[NMAT], sb[NMAT];
+#pragma unroll
+      for (int k = 0; k < NMAT; ++k) {
+        sa[k] = sb[k] = mkc(0., 0.);
+      }
       for (int m1 = 0; m1 <= M; ++m1) {
         const double c = Cr[m1];
-        cfma(sa, ta[m1], c);
-        cfma(sb, tb[m1], c);
+#pragma unroll
+        for (int k = 0; k < NMAT; ++k) {
+          cfma(sa[k], tv[k * wcap + oa + m1], c);
+          cfma(sb[k], tv[k * wcap + ob + m1], c);
+        }
       }
-      S[2 * j] = sa;
-      S[2 * j + 1] = sb;
+#pragma unroll
+      for (int k = 0; k < NMAT; ++k) {
+        tv[k * wcap + oS + 2 * j] = sa[k];
+        tv[k * wcap + oS + 2 * j + 1] = sb[k];
+      }
     }
     __syncwarp();
     // pass 2: Ta_m = sum_N' p_N' (-1)^m CG(m) S(N')
     for (int m = lane; m <= M; m += 32) {
-      cplx e00 = mkc(0., 0.), e11 = e00, e01 = e00, e10 = e00;
+      cplx e00[NMAT], e11[NMAT], e01[NMAT], e10[NMAT];
+#pragma unroll
+      for (int k = 0; k < NMAT; ++k) {
+        e00[k] = e11[k] = e01[k] = e10[k] = mkc(0., 0.);
+      }
       const double ms = (m & 1) ? -1. : 1.;
       for (int j = 0; j < nN; j += 2) {
         const double f = ms * p[Nlo + j] * C[(int64_t)j * (M + 1) + m];
-        cfma(e00, S[2 * j], f);
-        cfma(e11, S[2 * j + 1], f);
+#pragma unroll
+        for (int k = 0; k < NMAT; ++k) {
+          cfma(e00[k], tv[k * wcap + oS + 2 * j], f);
+          cfma(e11[k], tv[k * wcap + oS + 2 * j + 1], f);
+        }
       }
       for (int j = 1; j < nN; j += 2) {
         const double f = ms * p[Nlo + j] * C[(int64_t)j * (M + 1) + m];
-        cfma(e01, S[2 * j], f);
-        cfma(e10, S[2 * j + 1], f);
+#pragma unroll
+        for (int k = 0; k < NMAT; ++k) {
+          cfma(e01[k], tv[k * wcap + oS + 2 * j], f);
+          cfma(e10[k], tv[k * wcap + oS + 2 * j + 1], f);
+        }
       }
-      Tag[telem(N, m, 0, n1, 0, n2)] = c_fold(n2, nfold, afold, e00);
-      Tag[telem(N, m, 1, n1, 1, n2)] = c_fold(n2, nfold, afold, e11);
-      Tag[telem(N, m, 0, n1, 1, n2)] = c_fold(n2, nfold, afold, e01);
-      Tag[telem(N, m, 1, n1, 0, n2)] = c_fold(n2, nfold, afold, e10);
+#pragma unroll
+      for (int k = 0; k < NMAT; ++k) {
+        cplx *Tag = mats.dst[k] + G.t_off;
+        Tag[telem(N, m, 0, n1, 0, n2)] = c_fold(n2, nfold, afold, e00[k]);
+        Tag[telem(N, m, 1, n1, 1, n2)] = c_fold(n2, nfold, afold, e11[k]);
+        Tag[telem(N, m, 0, n1, 1, n2)] = c_fold(n2, nfold, afold, e01[k]);
+        Tag[telem(N, m, 1, n1, 0, n2)] = c_fold(n2, nfold, afold, e10[k]);
+      }
     }
     __syncwarp();
   }
@@ -349,30 +379,29 @@ __device__ static void wigner_col(double cosx, double sinx, double sinx_inv,
 // kept in this CTA's global slot; the azimuth pass then forms
 //   S = (1/k) sum_m (2 cos m phi, 2 sin m phi) X_m
 // with e^{i m phi} built by repeated multiplication as in the reference.
-__global__ void __launch_bounds__(256)
+template <int NMAT>
+__global__ void __launch_bounds__(256, (NMAT > 1) ? 2 : 1)
 k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const TmxSJob *__restrict__ jobs, const TmxObsGrain *__restrict__ og,
-      const cplx *__restrict__ Ta, const TmxAngle *__restrict__ angles,
-      const cplx *__restrict__ phis, cplx *__restrict__ S_out,
-      cplx *__restrict__ xslot, int nbmax) {
+      TmxMatSet mats, const TmxAngle *__restrict__ angles,
+      const cplx *__restrict__ phis, cplx *__restrict__ xslot, int nbmax) {
   extern __shared__ double ash[];
   double *po = ash;
   double *to = po + nbmax * 32;
   double *pi = to + nbmax * 32;
   double *ti = pi + nbmax * 32;
-  cplx *red = (cplx *)(ti + nbmax * 32); // [8 warps][4][32 lanes]
+  cplx *red = (cplx *)(ti + nbmax * 32); // [NMAT][8 warps][4][32 lanes]
   __shared__ TmxSJob sj[32];
   __shared__ int pref[33];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  cplx *X = xslot + (int64_t)blockIdx.x * 32 * (nbmax + 1) * 4;
+  cplx *X = xslot + (int64_t)blockIdx.x * 32 * (nbmax + 1) * 4 * NMAT;
   for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
     const TmxAmpGroup grp = groups[gi];
     const TmxObsGrain G = og[grp.grain];
     const int N = G.nmax;
     const int nj = grp.njobs;
-    const cplx *Tg = Ta + G.t_off;
     if (tid < nj) {
       sj[tid] = jobs[grp.job0 + tid];
     }
@@ -402,43 +431,63 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
         }
       }
       __syncthreads();
-      cplx x0 = mkc(0., 0.), x1 = x0, x2 = x0, x3 = x0;
-      const cplx *Tm = Tg + tblock(N, m);
+      cplx x0[NMAT], x1[NMAT], x2[NMAT], x3[NMAT];
+#pragma unroll
+      for (int q = 0; q < NMAT; ++q) {
+        x0[q] = x1[q] = x2[q] = x3[q] = mkc(0., 0.);
+      }
+      const int64_t tb = G.t_off + tblock(N, m);
       for (int r = warp; r < 2 * nb; r += 8) {
-        const cplx *Tr = Tm + (int64_t)r * 2 * nb;
-        cplx y0 = mkc(0., 0.), y1 = y0;
+        cplx y0[NMAT], y1[NMAT];
+#pragma unroll
+        for (int q = 0; q < NMAT; ++q) {
+          y0[q] = y1[q] = mkc(0., 0.);
+        }
 #pragma unroll 4
         for (int k = 0; k < nb; ++k) {
           const double a = pi[k * 32 + lane];
           const double b = ti[k * 32 + lane];
-          const cplx t0 = Tr[k];
-          const cplx t1 = Tr[nb + k];
-          cfma(y0, t0, a);
-          cfma(y0, t1, b);
-          cfma(y1, t0, b);
-          cfma(y1, t1, a);
+#pragma unroll
+          for (int q = 0; q < NMAT; ++q) {
+            const cplx *Tr = mats.src[q] + tb + (int64_t)r * 2 * nb;
+            const cplx t0 = Tr[k];
+            const cplx t1 = Tr[nb + k];
+            cfma(y0[q], t0, a);
+            cfma(y0[q], t1, b);
+            cfma(y1[q], t0, b);
+            cfma(y1[q], t1, a);
+          }
         }
         const int kr = (r < nb) ? r : r - nb;
         const double u = (r < nb) ? po[kr * 32 + lane] : to[kr * 32 + lane];
         const double up = (r < nb) ? to[kr * 32 + lane] : po[kr * 32 + lane];
-        cfma(x0, y0, u);
-        cfma(x1, y1, u);
-        cfma(x2, y0, up);
-        cfma(x3, y1, up);
+#pragma unroll
+        for (int q = 0; q < NMAT; ++q) {
+          cfma(x0[q], y0[q], u);
+          cfma(x1[q], y1[q], u);
+          cfma(x2[q], y0[q], up);
+          cfma(x3[q], y1[q], up);
+        }
       }
-      red[(warp * 4 + 0) * 32 + lane] = x0;
-      red[(warp * 4 + 1) * 32 + lane] = x1;
-      red[(warp * 4 + 2) * 32 + lane] = x2;
-      red[(warp * 4 + 3) * 32 + lane] = x3;
+#pragma unroll
+      for (int q = 0; q < NMAT; ++q) {
+        cplx *rq = red + q * 8 * 4 * 32;
+        rq[(warp * 4 + 0) * 32 + lane] = x0[q];
+        rq[(warp * 4 + 1) * 32 + lane] = x1[q];
+        rq[(warp * 4 + 2) * 32 + lane] = x2[q];
+        rq[(warp * 4 + 3) * 32 + lane] = x3[q];
+      }
       __syncthreads();
-      if (tid < 128) {
-        const int k = tid >> 5;
-        cplx s = red[k * 32 + lane];
+      for (int v = tid; v < 128 * NMAT; v += blockDim.x) {
+        const int q = v >> 7;
+        const int k = (v >> 5) & 3;
+        const cplx *rq = red + q * 8 * 4 * 32;
+        cplx s = rq[k * 32 + lane];
         for (int w = 1; w < 8; ++w) {
-          s = cadd(s, red[(w * 4 + k) * 32 + lane]);
+          s = cadd(s, rq[(w * 4 + k) * 32 + lane]);
         }
         if (lane < nj) {
-          X[((int64_t)lane * (N + 1) + m) * 4 + k] = s;
+          X[(((int64_t)q * 32 + lane) * (N + 1) + m) * 4 + k] = s;
         }
       }
     }
@@ -452,28 +501,31 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const TmxSJob J = sj[p];
       const int f = item - pref[p];
       const cplx e1 = phis[J.phi0 + f];
-      const cplx *Xp = X + (int64_t)p * (N + 1) * 4;
-      cplx e = mkc(1., 0.);
-      cplx s0 = mkc(0., 0.), s1 = s0, s2 = s0, s3 = s0;
-      for (int m = 0; m <= N; ++m) {
-        const double fcos = 2. * e.x;
-        const double fsin = 2. * e.y;
-        e = cmul(e, e1);
-        if (m == 0) {
-          s0 = cadd(s0, Xp[0]);
-          s3 = cadd(s3, Xp[3]);
-        } else {
-          s0 = cadd(s0, cscale(Xp[m * 4 + 0], fcos));
-          s1 = cadd(s1, cscale(Xp[m * 4 + 1], fsin));
-          s2 = csub(s2, cscale(Xp[m * 4 + 2], fsin));
-          s3 = cadd(s3, cscale(Xp[m * 4 + 3], fcos));
+#pragma unroll
+      for (int q = 0; q < NMAT; ++q) {
+        const cplx *Xp = X + ((int64_t)q * 32 + p) * (N + 1) * 4;
+        cplx e = mkc(1., 0.);
+        cplx s0 = mkc(0., 0.), s1 = s0, s2 = s0, s3 = s0;
+        for (int m = 0; m <= N; ++m) {
+          const double fcos = 2. * e.x;
+          const double fsin = 2. * e.y;
+          e = cmul(e, e1);
+          if (m == 0) {
+            s0 = cadd(s0, Xp[0]);
+            s3 = cadd(s3, Xp[3]);
+          } else {
+            s0 = cadd(s0, cscale(Xp[m * 4 + 0], fcos));
+            s1 = cadd(s1, cscale(Xp[m * 4 + 1], fsin));
+            s2 = csub(s2, cscale(Xp[m * 4 + 2], fsin));
+            s3 = cadd(s3, cscale(Xp[m * 4 + 3], fcos));
+          }
         }
+        cplx *o = mats.dst[q] + (J.out + f) * 4;
+        o[0] = cscale(s0, kinv);
+        o[1] = cscale(s1, kinv);
+        o[2] = cscale(s2, kinv);
+        o[3] = cscale(s3, kinv);
       }
-      cplx *o = S_out + (J.out + f) * 4;
-      o[0] = cscale(s0, kinv);
-      o[1] = cscale(s1, kinv);
-      o[2] = cscale(s2, kinv);
-      o[3] = cscale(s3, kinv);
     }
     __syncthreads();
   }
@@ -636,8 +688,8 @@ void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
 }
 
 void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
-                             int ngrains, int64_t npairs, const double2 *T,
-                             double2 *Ta, const double *coeffs, int ncoef,
+                             int ngrains, int64_t npairs, const TmxMatSet &mats,
+                             int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,
                              cudaStream_t stream) {
@@ -645,40 +697,64 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
     return;
   }
   const int wcap = 4 * (mmax + 1) + 2 * (2 * mmax + 1);
-  const size_t smem = (size_t)8 * wcap * sizeof(double2);
-  cudaFuncSetAttribute(k_orient_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
+  const size_t smem = (size_t)8 * wcap * nmat * sizeof(double2);
   const int64_t want = (npairs + 7) / 8;
   const int blocks = (int)std::min<int64_t>(want, 148 * 8);
-  k_orient_pairs<<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs, T,
-                                                Ta, coeffs, ncoef, cg_off, cg,
-                                                cg_nmax, wcap, fold);
+  if (nmat == 4) {
+    cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    k_orient_pairs<4><<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs,
+                                                     mats, coeffs, ncoef, cg_off, cg,
+                                                     cg_nmax, wcap, fold);
+  } else {
+    cudaFuncSetAttribute(k_orient_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    k_orient_pairs<1><<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs,
+                                                     mats, coeffs, ncoef, cg_off, cg,
+                                                     cg_nmax, wcap, fold);
+  }
 }
 
-static size_t amp_smem(int nbmax) {
-  return (size_t)4 * nbmax * 32 * sizeof(double) + 8 * 4 * 32 * sizeof(double2);
+static size_t amp_smem(int nbmax, int nmat) {
+  return (size_t)4 * nbmax * 32 * sizeof(double) +
+         (size_t)nmat * 8 * 4 * 32 * sizeof(double2);
 }
 
-int tmx_amp_grid(int nbmax) {
-  cudaFuncSetAttribute(k_amp, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)amp_smem(TMX_MAX_NB));
+int tmx_amp_grid(int nbmax, int nmat) {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp, 256, amp_smem(nbmax));
+  if (nmat == 4) {
+    cudaFuncSetAttribute(k_amp<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)amp_smem(TMX_MAX_NB, 4));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<4>, 256,
+                                                  amp_smem(nbmax, 4));
+  } else {
+    cudaFuncSetAttribute(k_amp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)amp_smem(TMX_MAX_NB, 1));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<1>, 256,
+                                                  amp_smem(nbmax, 1));
+  }
   return std::max(1, sms * std::max(1, per_sm));
 }
 
 void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
-                    const TmxObsGrain *og, const double2 *Ta,
-                    const TmxAngle *angles, const double2 *phis, double2 *S,
-                    double2 *xslot, int nbmax, int grid, cudaStream_t stream) {
+                    const TmxObsGrain *og, const TmxMatSet &mats, int nmat,
+                    const TmxAngle *angles, const double2 *phis, double2 *xslot,
+                    int nbmax, int grid, cudaStream_t stream) {
   if (ngroups <= 0) {
     return;
   }
   const int blocks = std::min(grid, ngroups);
-  k_amp<<<blocks, 256, amp_smem(nbmax), stream>>>(groups, ngroups, jobs, og, Ta,
-                                                  angles, phis, S, xslot, nbmax);
+  if (nmat == 4) {
+    k_amp<4><<<blocks, 256, amp_smem(nbmax, 4), stream>>>(groups, ngroups, jobs, og,
+                                                          mats, angles, phis, xslot,
+                                                          nbmax);
+  } else {
+    k_amp<1><<<blocks, 256, amp_smem(nbmax, 1), stream>>>(groups, ngroups, jobs, og,
+                                                          mats, angles, phis, xslot,
+                                                          nbmax);
+  }
 }
 
 void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,

@@ -383,36 +383,52 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
 // Ta = orientation average (or copy) of Tsrc with the amplitude factors
 // folded in, then the amplitudes S of every job (zeroed first: grains with
 // nmax 0 have no jobs)
-int run_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int64_t t_total, int ncoef,
-                   cplx *S_out, int64_t s_total) {
+int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
+                   int64_t t_total, int ncoef, cplx *const *S_out,
+                   int64_t s_total) {
   cudaStream_t st = ctx->stream;
   int rc;
-  if ((rc = ensure(ctx, ctx->Ta, std::max<int64_t>(1, t_total) * sizeof(cplx)))) {
+  if ((rc = ensure(ctx, ctx->Ta,
+                   std::max<int64_t>(1, nmat * t_total) * sizeof(cplx)))) {
     return rc;
   }
-  CK(cudaMemsetAsync(S_out, 0, std::max<int64_t>(0, s_total) * 4 * sizeof(cplx), st));
+  for (int k = 0; k < nmat; ++k) {
+    CK(cudaMemsetAsync(S_out[k], 0, std::max<int64_t>(0, s_total) * 4 * sizeof(cplx),
+                       st));
+  }
   if (t_total <= 0 || ctx->o_npairs <= 0) {
     return TMX_OK;
   }
+  TmxMatSet avg = {}, amp = {};
+  for (int k = 0; k < nmat; ++k) {
+    avg.src[k] = Tsrc[k];
+    avg.dst[k] = (cplx *)ctx->Ta.p + k * t_total;
+    amp.src[k] = avg.dst[k];
+    amp.dst[k] = S_out[k];
+  }
   tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
                           (const int64_t *)ctx->o_pairs.p, (int)ctx->o_ngrains,
-                          ctx->o_npairs, Tsrc, (cplx *)ctx->Ta.p,
-                          (const double *)ctx->o_coef.p, ncoef,
-                          (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
-                          ctx->cg_nmax, ctx->o_nbmax, 1, st);
+                          ctx->o_npairs, avg, nmat, (const double *)ctx->o_coef.p,
+                          ncoef, (const int64_t *)ctx->cg_off.p,
+                          (const double *)ctx->cg.p, ctx->cg_nmax, ctx->o_nbmax, 1,
+                          st);
   LAUNCHED();
-  const int grid = tmx_amp_grid(ctx->o_nbmax);
+  const int grid = tmx_amp_grid(ctx->o_nbmax, nmat);
   if ((rc = ensure(ctx, ctx->o_x,
-                   (size_t)grid * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
+                   (size_t)grid * nmat * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
     return rc;
   }
   tmx_launch_amp((const TmxAmpGroup *)ctx->o_grp.p, ctx->o_ngrp,
-                 (const TmxSJob *)ctx->o_sj.p, (const TmxObsGrain *)ctx->o_og.p,
-                 (const cplx *)ctx->Ta.p, (const TmxAngle *)ctx->o_angles.p,
-                 (const cplx *)ctx->o_phis.p, S_out, (cplx *)ctx->o_x.p,
-                 ctx->o_nbmax, grid, st);
+                 (const TmxSJob *)ctx->o_sj.p, (const TmxObsGrain *)ctx->o_og.p, amp,
+                 nmat, (const TmxAngle *)ctx->o_angles.p, (const cplx *)ctx->o_phis.p,
+                 (cplx *)ctx->o_x.p, ctx->o_nbmax, grid, st);
   LAUNCHED();
   return TMX_OK;
+}
+
+int run_amplitudes(tmx_ctx *ctx, const cplx *Tsrc, int64_t t_total, int ncoef,
+                   cplx *S_out, int64_t s_total) {
+  return run_amplitudes(ctx, &Tsrc, 1, t_total, ncoef, &S_out, s_total);
 }
 
 } // namespace
@@ -982,12 +998,12 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   }
   cplx *S = (cplx *)ctx->dS.p;
   const int64_t sz = n * ntheta * 4;
-  if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, ncoef, S))) {
-    return rc;
-  }
-  for (int p = 0; p < 3; ++p) {
-    if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->dT.p + p * tt, ntheta,
-                               ncoef, S + (1 + p) * sz))) {
+  {
+    // T and its three tangents in one pass (shared angle and coupling work)
+    const cplx *src[4] = {(const cplx *)ctx->T.p, (const cplx *)ctx->dT.p,
+                          (const cplx *)ctx->dT.p + tt, (const cplx *)ctx->dT.p + 2 * tt};
+    cplx *dst[4] = {S, S + sz, S + 2 * sz, S + 3 * sz};
+    if ((rc = run_amplitudes(ctx, src, 4, ctx->p2_t_total, ncoef, dst, n * ntheta))) {
       return rc;
     }
   }
@@ -1397,10 +1413,12 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
     return rc;
   }
   if (t_total > 0 && ctx->o_npairs > 0) {
+    TmxMatSet avg = {};
+    avg.src[0] = (const cplx *)ctx->T.p;
+    avg.dst[0] = (cplx *)ctx->Ta.p;
     tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
                             (const int64_t *)ctx->o_pairs.p, (int)n, ctx->o_npairs,
-                            (const cplx *)ctx->T.p, (cplx *)ctx->Ta.p,
-                            (const double *)ctx->o_coef.p, ncoef,
+                            avg, 1, (const double *)ctx->o_coef.p, ncoef,
                             (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
                             ctx->cg_nmax, ctx->o_nbmax, 0, st);
     LAUNCHED();

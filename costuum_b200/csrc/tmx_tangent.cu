@@ -28,7 +28,7 @@ enum { P_M = 0, P_R = 1, P_D = 2 };
 // slot 4 + t pairs dF_t with W_t. For p = m the F side does not depend on
 // the parameter and only slots 0..3 are used.
 // Threads tid = 0..nth-1 of the caller share the work; rows are stored with
-// stride L.NRp, columns with stride ncolp.
+// stride L.NRp, columns with stride ncolp. an_tab[a] = a_n of member a.
 __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
                                     int ncolp, int N, int m, int ng, int g0,
                                     int param, double R,
@@ -36,7 +36,7 @@ __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
                                     const double *__restrict__ S,
                                     const double *__restrict__ Wg, double k2,
                                     cplx k2mr, cplx *Fs, cplx *Ws, int tid,
-                                    int nth) {
+                                    int nth, const double *an_tab) {
   const int G = L.G;
   const int slots = 8;
   // ---- A side: F_t (slots 0..3) and dF_t (slots 4..7), (F^j, F^y) pairs
@@ -56,7 +56,7 @@ __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
       const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
       const double *s = S + (int64_t)g * TMX_NS;
       const double d = w[0], dd = w[1];
-      const double an = a_n(n);
+      const double an = an_tab[a];
       const double nn = n * (n + 1.);
       const double iz = s[TMX_NS_KRINV];
       const double drr = s[TMX_NS_DRR];
@@ -113,7 +113,7 @@ __device__ void build_chunk_tangent(const ClassDesc &D, const AsmLayout &L,
       const double *w = Wg + ((int64_t)g * N + (n - 1)) * 2;
       const double *s = S + (int64_t)g * TMX_NS;
       const double d = w[0], dd = w[1];
-      const double an = a_n(n);
+      const double an = an_tab[b];
       const double nn = n * (n + 1.);
       const cplx iw = mkc(s[TMX_NS_KRMRINV_RE], s[TMX_NS_KRMRINV_IM]);
       const double drr = s[TMX_NS_DRR];
@@ -223,6 +223,12 @@ __global__ void __launch_bounds__(NT, MINB)
   const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
   cplx *dQ = A.scratch + param * A.scratch_stride + item.scratch;
   cplx *dR = dQ + (int64_t)nb * nb;
+  __shared__ double an_tab[TMX_MAX_NB];
+  for (int a = threadIdx.x; a < nb; a += blockDim.x) {
+    int ia, na;
+    member(D, a, ia, na);
+    an_tab[a] = a_n(na);
+  }
 
   // ---------------------------------------------------- tangent assembly
   AsmLayout L;
@@ -255,7 +261,7 @@ __global__ void __launch_bounds__(NT, MINB)
     for (int g0 = 0; g0 < ng; g0 += L.G) {
       __syncthreads();
       build_chunk_tangent(D, L, L.CT * TC, N, m, ng, g0, param, Gr.r_ev, T, S,
-                          Wg, k2, k2mr, Fs, Ws, threadIdx.x, blockDim.x);
+                          Wg, k2, k2mr, Fs, Ws, threadIdx.x, blockDim.x, an_tab);
       __syncthreads();
       if (active) {
         const int gmax = min(L.G, ng - g0);
@@ -310,6 +316,61 @@ __global__ void __launch_bounds__(NT, MINB)
   __syncthreads();
 
   // ---------------------------------------- solve with the saved factors
+  if constexpr (NT == 128) {
+    // classes of up to 32 members: T_c and the factors in shared memory,
+    // B = dRgQ + T_c dQ by all threads, then the register solve with four
+    // lanes per row (row tid / 4)
+    constexpr int LF = 33;
+    if (nb <= 32) {
+      cplx *Am = reinterpret_cast<cplx *>(tmx_tsmem);
+      cplx *Tc = Am + 32 * LF;
+      cplx *Xs = Tc + 32 * LF;
+      cplx *uinv = Xs + 32 * LF;
+      int *perm = reinterpret_cast<int *>(uinv + 32);
+      const cplx *Ls = A.lu + item.scratch;
+      const int *ps = reinterpret_cast<const int *>(Ls + (int64_t)nb * nb);
+      const cplx *Tb = A.T + sl.tout + block_offset(N, m);
+      const int w2 = 2 * D.nbb;
+      for (int u = threadIdx.x; u < nb * nb; u += NT) {
+        const int a = u / nb;
+        const int k = u - a * nb;
+        Am[a * LF + k] = Ls[u];
+        int ia, na, ik, nk;
+        member(D, a, ia, na);
+        member(D, k, ik, nk);
+        Tc[a * LF + k] = Tb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ik * D.nbb +
+                            (nk - D.nmin)];
+      }
+      for (int j = threadIdx.x; j < nb; j += NT) {
+        perm[j] = ps[j];
+        uinv[j] = cinv_lu(Ls[(int64_t)j * nb + j]);
+      }
+      __syncthreads();
+      for (int u = threadIdx.x; u < nb * nb; u += NT) {
+        const int a = u / nb;
+        const int b = u - a * nb;
+        cplx acc = dR[u];
+        for (int k = 0; k < nb; ++k) {
+          acc = cadd(acc, cmul(Tc[a * LF + k], dQ[(int64_t)k * nb + b]));
+        }
+        Xs[a * LF + b] = acc;
+      }
+      __syncthreads();
+      solve_rows<32, 4>(Xs, Am, LF, uinv, nb, threadIdx.x >> 2, threadIdx.x & 3);
+      __syncthreads();
+      cplx *dTb = A.dT + param * A.dT_stride + sl.tout + block_offset(N, m);
+      for (int u = threadIdx.x; u < nb * nb; u += NT) {
+        const int a = u / nb;
+        const int b = u - a * nb;
+        int ia, na, ib, nbn;
+        member(D, a, ia, na);
+        member(D, b, ib, nbn);
+        dTb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ib * D.nbb + (nbn - D.nmin)] =
+            Xs[a * LF + perm[b]];
+      }
+      return;
+    }
+  }
   const int lda = nb | 1;
   cplx *Am = reinterpret_cast<cplx *>(tmx_tsmem);
   cplx *uinv = Am + (int64_t)nb * lda;
@@ -402,10 +463,10 @@ __global__ void __launch_bounds__(NT, MINB)
 template <int NBM>
 __host__ __device__ constexpr int tangent_warp_elems() {
   // chunk buffers F[WG][8][NBM] + W[2][WG][8][NBM], or in the solve phase
-  // dQ, X, LU ([NBM][NBM + 1] each), 1/U_jj and the gather index
-  return (24 * TMX_TWG * NBM > 3 * NBM * (NBM + 1) + 2 * NBM)
+  // dQ, X, LU, T_c ([NBM][NBM + 1] each), 1/U_jj and the gather index
+  return (24 * TMX_TWG * NBM > 4 * NBM * (NBM + 1) + 2 * NBM)
              ? 24 * TMX_TWG * NBM
-             : 3 * NBM * (NBM + 1) + 2 * NBM;
+             : 4 * NBM * (NBM + 1) + 2 * NBM;
 }
 
 template <int TR, int TC, int MINB>
@@ -422,8 +483,11 @@ __global__ void __launch_bounds__(128, MINB)
   cplx *dQm = base;                      // [NBM][LD]  (after the assembly)
   cplx *Xm = dQm + NBM * LD;             // [NBM][LD]
   cplx *LUm = Xm + NBM * LD;             // [NBM][LD]
-  cplx *uinv = LUm + NBM * LD;           // [NBM]
+  cplx *Tcm = LUm + NBM * LD;            // [NBM][LD]
+  cplx *uinv = Tcm + NBM * LD;           // [NBM]
   int *perm = reinterpret_cast<int *>(uinv + NBM);
+  __shared__ double an_w[4][NBM];
+  double *an_tab = an_w[wib];
   const int rt = lane >> 2;
   const int ct = lane & 3;
   const int64_t nwork = (int64_t)A.nitems * A.nparams;
@@ -457,6 +521,12 @@ __global__ void __launch_bounds__(128, MINB)
     const int t0 = (m == 0) ? 1 : 0;
     const int per_node = (param == P_M) ? 4 : 8;
     const int rgl = (rt * TR < D.R0p) ? 0 : 1;
+    __syncwarp();
+    if (lane < nb) {
+      int ia, na;
+      member(D, lane, ia, na);
+      an_tab[lane] = a_n(na);
+    }
 
     // -------------------------------------------------- tangent assembly
     double aj[TR][TC][2], ay[TR][TC][2];
@@ -470,7 +540,7 @@ __global__ void __launch_bounds__(128, MINB)
     for (int g0 = 0; g0 < ng; g0 += TMX_TWG) {
       __syncwarp();
       build_chunk_tangent(D, L, NBM, N, m, ng, g0, param, Gr.r_ev, T, S, Wg, k2,
-                          k2mr, Fs, Ws, lane, 32);
+                          k2mr, Fs, Ws, lane, 32, an_tab);
       __syncwarp();
       const int gmax = min(TMX_TWG, ng - g0);
       for (int gl = 0; gl < gmax; ++gl) {
@@ -511,50 +581,40 @@ __global__ void __launch_bounds__(128, MINB)
         }
       }
     }
-    // saved factors and gather index of the forward solve
+    // saved factors, gather index and T_c (class order) of the forward solve
     const cplx *Ls = A.lu + item.scratch;
     const int *ps = reinterpret_cast<const int *>(Ls + (int64_t)nb * nb);
+    const cplx *Tb = A.T + sl.tout + block_offset(N, m);
+    const int w2 = 2 * D.nbb;
     for (int u = lane; u < nb * nb; u += 32) {
-      LUm[(u / nb) * LD + (u % nb)] = Ls[u];
+      const int a = u / nb;
+      const int k = u - a * nb;
+      LUm[a * LD + k] = Ls[u];
+      int ia, na, ik, nk;
+      member(D, a, ia, na);
+      member(D, k, ik, nk);
+      Tcm[a * LD + k] = Tb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ik * D.nbb +
+                           (nk - D.nmin)];
     }
     for (int j = lane; j < nb; j += 32) {
       perm[j] = ps[j];
-      uinv[j] = cinv(Ls[(int64_t)j * nb + j]);
+      uinv[j] = cinv_lu(Ls[(int64_t)j * nb + j]);
     }
     __syncwarp();
-    // --------------------------------- X = -(dRgQ + T_c dQ), then solve
-    const cplx *Tb = A.T + sl.tout + block_offset(N, m);
-    const int w2 = 2 * D.nbb;
-    if (lane < nb) {
-      int ia, na;
-      member(D, lane, ia, na);
-      const cplx *trow = Tb + (int64_t)(ia * D.nbb + (na - D.nmin)) * w2;
-      cplx *x = Xm + lane * LD;
-      for (int b = 0; b < nb; ++b) {
-        cplx acc = x[b];
-        for (int k = 0; k < nb; ++k) {
-          int ik, nk;
-          member(D, k, ik, nk);
-          acc = cadd(acc, cmul(trow[ik * D.nbb + (nk - D.nmin)], dQm[k * LD + b]));
-        }
-        x[b] = mkc(-acc.x, -acc.y);
+    // ------------------- B = dRgQ + T_c dQ; the solve takes X = -B and
+    // solves X U = -B, then Y L = X
+    for (int u = lane; u < nb * nb; u += 32) {
+      const int a = u / nb;
+      const int b = u - a * nb;
+      cplx acc = Xm[a * LD + b];
+      for (int k = 0; k < nb; ++k) {
+        acc = cadd(acc, cmul(Tcm[a * LD + k], dQm[k * LD + b]));
       }
-      // Z U = X (forward over columns)
-      for (int j = 0; j < nb; ++j) {
-        const cplx xj = cmul(x[j], uinv[j]);
-        x[j] = xj;
-        for (int k = j + 1; k < nb; ++k) {
-          x[k] = csub(x[k], cmul(xj, LUm[j * LD + k]));
-        }
-      }
-      // Y L = Z (backward over columns, L unit lower)
-      for (int j = nb - 1; j >= 1; --j) {
-        const cplx xj = x[j];
-        for (int k = 0; k < j; ++k) {
-          x[k] = csub(x[k], cmul(xj, LUm[j * LD + k]));
-        }
-      }
+      Xm[a * LD + b] = acc;
     }
+    __syncwarp();
+    solve_rows<NBM, 32 / NBM>(Xm, LUm, LD, uinv, nb, lane / (32 / NBM),
+                              lane % (32 / NBM));
     __syncwarp();
     cplx *dTb = A.dT + param * A.dT_stride + sl.tout + block_offset(N, m);
     for (int u = lane; u < nb * nb; u += 32) {
@@ -596,6 +656,12 @@ size_t tmx_tangent_smem_bytes(int max_nb, int chunk_nodes) {
   if (full <= 200 * 1024) {
     lu_total = full;
   }
+  if (max_nb <= 32) {
+    // solve of the 128-thread kernel: factors, T_c and B (32 x 33 each),
+    // 1/U_jj and the gather index
+    const size_t small = (size_t)(3 * 32 * 33 + 32) * sizeof(cplx) + 32 * sizeof(int);
+    lu_total = std::max(lu_total, small);
+  }
   return asm_bytes > lu_total ? asm_bytes : lu_total;
 }
 
@@ -606,8 +672,12 @@ static void launch_tangent(const TmxTangentArgs &a, size_t smem,
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
+    // the block limit (227 KiB) covers the kernel's static shared memory too
+    cudaFuncAttributes fa;
+    cudaFuncGetAttributes(&fa, k_tangent<TR, TC, NT, MINB>);
     cudaFuncSetAttribute(k_tangent<TR, TC, NT, MINB>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(227 * 1024 - fa.sharedSizeBytes));
     attr_dev = dev;
   }
   dim3 grid(a.nitems, a.nparams);

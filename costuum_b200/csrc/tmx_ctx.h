@@ -97,6 +97,13 @@ struct tmx_ctx {
   std::vector<TmxSlot> p2_slots;
   std::vector<TmxItem> p2_items;
   std::vector<int> p2_nb;
+  // block items of one grain of order N, in (m, class) order: m << 8 | cls
+  // and the class size; and the (size, count) bins of that list
+  struct ItemTemplate {
+    std::vector<int32_t> mc, nb;
+    std::vector<std::pair<int32_t, int32_t>> bins;
+  };
+  std::vector<ItemTemplate> item_tpl; // indexed by N
   int64_t p2_scr_total = 0, p2_t_total = 0;
   DevBuf lu, dT, tscr, dTa, dS; // tangent buffers
   int o_nsj = 0, o_nqj = 0;     // per-grain observable job counts

@@ -492,20 +492,39 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     slots[s].wig_n = full_sets[key_idx[std::make_pair(slots[s].nmax, slots[s].ngauss)]];
   }
   // items, ordered by class size (largest first; a counting sort, stable in
-  // (slot, m, class) order)
+  // (slot, m, class) order), from a per-order template of a grain's items
+  for (int s = 0; s < np2; ++s) {
+    const int N = slots[s].nmax;
+    if ((int)ctx->item_tpl.size() <= N) {
+      ctx->item_tpl.resize(N + 1);
+    }
+    tmx_ctx::ItemTemplate &tp = ctx->item_tpl[N];
+    if (tp.mc.empty() && N > 0) {
+      std::vector<int32_t> c(TMX_MAX_NB + 2, 0);
+      for (int m = 0; m <= N; ++m) {
+        const int ncls = (m == 0) ? 4 : 2;
+        for (int cl = 0; cl < ncls; ++cl) {
+          const int nb = tmx_host_class_size(N, m, cl);
+          if (nb > 0) {
+            tp.mc.push_back((m << 8) | cl);
+            tp.nb.push_back(nb);
+            c[std::min(nb, TMX_MAX_NB + 1)] += 1;
+          }
+        }
+      }
+      for (int b = 0; b < TMX_MAX_NB + 2; ++b) {
+        if (c[b]) {
+          tp.bins.push_back(std::make_pair(b, c[b]));
+        }
+      }
+    }
+  }
   std::vector<int64_t> cnt(TMX_MAX_NB + 2, 0);
   int64_t nitems = 0;
   for (int s = 0; s < np2; ++s) {
-    const int N = slots[s].nmax;
-    for (int m = 0; m <= N; ++m) {
-      const int ncls = (m == 0) ? 4 : 2;
-      for (int c = 0; c < ncls; ++c) {
-        const int nb = tmx_host_class_size(N, m, c);
-        if (nb > 0) {
-          cnt[std::min(nb, TMX_MAX_NB + 1)] += 1;
-          ++nitems;
-        }
-      }
+    for (const auto &bc : ctx->item_tpl[slots[s].nmax].bins) {
+      cnt[bc.first] += bc.second;
+      nitems += bc.second;
     }
   }
   std::vector<int64_t> pos(TMX_MAX_NB + 2, 0);
@@ -518,20 +537,16 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   items.resize(nitems);
   inb.resize(nitems);
   for (int s = 0; s < np2; ++s) {
-    const int N = slots[s].nmax;
-    for (int m = 0; m <= N; ++m) {
-      const int ncls = (m == 0) ? 4 : 2;
-      for (int c = 0; c < ncls; ++c) {
-        const int nb = tmx_host_class_size(N, m, c);
-        if (nb <= 0) {
-          continue;
-        }
-        const int64_t i = pos[std::min(nb, TMX_MAX_NB + 1)]++;
-        items[i].slot = s;
-        items[i].m = (int16_t)m;
-        items[i].cls = (int16_t)c;
-        inb[i] = nb;
-      }
+    const tmx_ctx::ItemTemplate &tp = ctx->item_tpl[slots[s].nmax];
+    const int ni = (int)tp.mc.size();
+    for (int j = 0; j < ni; ++j) {
+      const int nb = tp.nb[j];
+      const int64_t i = pos[std::min(nb, TMX_MAX_NB + 1)]++;
+      TmxItem &it = items[i];
+      it.slot = s;
+      it.m = (int16_t)(tp.mc[j] >> 8);
+      it.cls = (int16_t)(tp.mc[j] & 0xff);
+      inb[i] = nb;
     }
   }
   ctx->p2_slots = slots;
@@ -848,6 +863,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   }
   CK(cudaMemsetAsync(ctx->count.p, 0, 2 * sizeof(int32_t), st));
   const int64_t round_min = std::max<int64_t>(256, ctx->up_nact / 16);
+  const int64_t round_max = std::max<int64_t>(768, round_min);
   int64_t done_seen = 0;
   std::vector<int32_t> ready, pending;
   std::vector<char> launched(n, 0);
@@ -1001,11 +1017,14 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     done_seen = done_now;
     k += G;
     if (nact > 0 && (int64_t)ready.size() >= round_min) {
-      for (int32_t g : ready) {
+      // at most round_max grains per round: a round's host set-up runs
+      // while the GPU computes the next order, and should not outlast it
+      const size_t take = std::min<size_t>(ready.size(), (size_t)round_max);
+      pending.assign(ready.begin(), ready.begin() + take);
+      ready.erase(ready.begin(), ready.begin() + take);
+      for (int32_t g : pending) {
         launched[g] = 1;
       }
-      pending.swap(ready);
-      ready.clear();
     }
   }
   chain_range.reset();

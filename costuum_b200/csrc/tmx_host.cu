@@ -614,14 +614,15 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   if ((rc = prof_begin(ctx, 1, &pe, st))) {
     return rc;
   }
-  int ngmax = 1;
+  int ngmax = 1, nmmax = 1;
   for (const TmxSlot &sl : slots) {
     ngmax = std::max(ngmax, sl.ngauss);
+    nmmax = std::max(nmmax, sl.nmax);
   }
   tmx_launch_tables(dslots, np2, (const TmxGrain *)ctx->grains.p,
                     (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
                     (const int64_t *)ctx->gl_off.p, tab, nsc,
-                    ctx->up_sched.bessel_start, ngmax, st);
+                    ctx->up_sched.bessel_start, ngmax, nmmax, st);
   LAUNCHED();
   if ((rc = prof_end(ctx, 1, pe, 0., st))) {
     return rc;
@@ -934,7 +935,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
                         (const TmxGrain *)ctx->grains.p,
                         (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
                         (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
-                        (double *)ctx->nsc.p, S.bessel_start, glf * kl, st);
+                        (double *)ctx->nsc.p, S.bessel_start, glf * kl, kl, st);
       LAUNCHED();
       if ((rc = prof_end(ctx, 1, pe, 0.))) {
         return rc;

@@ -27,11 +27,13 @@ struct TmxChainState {
   int32_t status;
 };
 
-// node scalars and Bessel tables of every slot; ngmax >= every slot's ngauss
+// node scalars and Bessel tables of every slot; ngmax >= every slot's
+// ngauss, nmax_max >= every slot's nmax
 void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
                        const double *gl_x, const double *gl_w,
                        const int64_t *gl_off, double *tab, double *nsc,
-                       int bessel_start, int ngmax, cudaStream_t stream);
+                       int bessel_start, int ngmax, int nmax_max,
+                       cudaStream_t stream);
 
 void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,
                        const double *gl_x, const int64_t *gl_off, double *out,

@@ -222,7 +222,8 @@ extern "C" int tmx_tmatrix_fixed_noalloc(double r_ev, double wavelength,
                     reinterpret_cast<const double *>(base + NA_GLW),
                     reinterpret_cast<const int64_t *>(base + NA_GLOFF),
                     reinterpret_cast<double *>(base + NA_TAB),
-                    reinterpret_cast<double *>(base + NA_NSC), 800, ngauss, st);
+                    reinterpret_cast<double *>(base + NA_NSC), 800, ngauss, nmax,
+                    st);
   NA_CK(cudaGetLastError());
   // structural zeros of the T blocks (entries outside each parity class)
   NA_CK(cudaMemsetAsync(T_dev, 0, tmx_tmatrix_size(nmax) * sizeof(cplx), st));

@@ -57,7 +57,7 @@ int m0_step(tmx_ctx *ctx, const std::vector<int32_t> &g, const std::vector<int> 
   std::vector<TmxSlot> slots(ns);
   diag_off.assign(ns, 0);
   int64_t tab = 0, nsc = 0, dg = 0;
-  int ngmax = 1;
+  int ngmax = 1, nmmax = 1;
   for (int s = 0; s < ns; ++s) {
     TmxSlot &sl = slots[s];
     sl.grain = g[s];
@@ -73,6 +73,7 @@ int m0_step(tmx_ctx *ctx, const std::vector<int32_t> &g, const std::vector<int> 
     nsc += (int64_t)NG[s] * TMX_NS;
     dg += 2 * (int64_t)N[s];
     ngmax = std::max(ngmax, NG[s]);
+    nmmax = std::max(nmmax, N[s]);
   }
   // the four m = 0 classes of every slot, largest first
   struct It {
@@ -118,7 +119,7 @@ int m0_step(tmx_ctx *ctx, const std::vector<int32_t> &g, const std::vector<int> 
   tmx_launch_tables((const TmxSlot *)ctx->slots.p, ns, (const TmxGrain *)ctx->grains.p,
                     (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
                     (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
-                    (double *)ctx->nsc.p, ctx->up_sched.bessel_start, ngmax, st);
+                    (double *)ctx->nsc.p, ctx->up_sched.bessel_start, ngmax, nmmax, st);
   LAUNCHED();
   const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
   size_t i0 = 0;

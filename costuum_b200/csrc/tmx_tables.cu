@@ -8,6 +8,8 @@
 // (see bessel_j_complex).
 // Transcendentals (sin, cos, cosh, sinh) come from CUDA's libdevice and may
 // differ from the C library by an ulp.
+#include <algorithm>
+
 #include "tmx_common.cuh"
 #include "tmx_kernels.h"
 
@@ -16,7 +18,7 @@
 // Start index of the downward ratio recurrence. The reference starts at
 // n = 800 for every argument (SPECIALFUNCTIONS_BESSEL_NMAX). Above
 // max(nmax, |z|) the recurrence contracts errors by about (|z| / 2n)^2 per
-// step, so a start 64 orders above max(nmax, |z|) reaches the same doubles
+// step, so a start 48 orders above max(nmax, |z|) reaches the same doubles
 // as a start at 800 (tests/test_bessel_start.py checks this bit for bit).
 // bessel_start > 0 forces a fixed start.
 __device__ __forceinline__ int bessel_nstart(int bessel_start, int nmax,
@@ -320,20 +322,24 @@ __global__ void k_wigner(const TmxWigJob *__restrict__ jobs, int njobs,
 void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
                        const double *gl_x, const double *gl_w,
                        const int64_t *gl_off, double *tab, double *nsc,
-                       int bessel_start, int ngmax, cudaStream_t stream) {
+                       int bessel_start, int ngmax, int nmax_max,
+                       cudaStream_t stream) {
   if (nslots <= 0 || ngmax <= 0) {
     return;
   }
-  const int threads = 64;
-  // ratios in shared memory for orders up to 48 (48 KB per CTA)
-  const int rho_smem = 48;
+  // one thread per node: a warp per slot and argument kind when every slot
+  // has at most 32 nodes (the order loop up to order 16), else chunks of 64
+  const int threads = (ngmax <= 32) ? 32 : 64;
+  // ratios in shared memory for orders up to 48, sized by the launch's
+  // largest order (more CTAs per SM for small orders)
+  const int rho_smem = std::max(1, std::min(48, nmax_max));
   const size_t smem = (size_t)threads * rho_smem * sizeof(cplx);
   static int attr_dev = -1;
   int dev = 0;
   cudaGetDevice(&dev);
   if (attr_dev != dev) {
     cudaFuncSetAttribute(k_tables, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+                         (int)(64 * 48 * sizeof(cplx)));
     attr_dev = dev;
   }
   dim3 grid(nslots, (ngmax + threads - 1) / threads, 2);

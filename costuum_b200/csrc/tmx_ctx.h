@@ -96,6 +96,7 @@ struct tmx_ctx {
   int p2_rounds = 0;
   std::vector<TmxSlot> p2_slots;
   std::vector<TmxItem> p2_items;
+  bool lu_ready = false; // ctx->lu holds the LU factors of every p2 item
   std::vector<int> p2_nb;
   // block items of one grain of order N, in (m, class) order: m << 8 | cls
   // and the class size; and the (size, count) bins of that list

@@ -454,7 +454,8 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
 // (Wigner tables), which the round then waits for.
 static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
                             cudaStream_t st, int64_t t_base, bool keep_T,
-                            int64_t *t_end, bool temp = false) {
+                            int64_t *t_end, bool temp = false,
+                            bool keep_lu = false) {
   int rc;
   NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
@@ -573,6 +574,12 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
        (rc = ensure(ctx, ctx->p2items, std::max<int64_t>(1, nitems) * sizeof(TmxItem))))) {
     return rc;
   }
+  // a single round on persistent buffers can keep the LU factors of every
+  // item for a later gradient pass (same item order and scratch offsets)
+  if (keep_lu &&
+      (rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, scr_total) * sizeof(cplx)))) {
+    return rc;
+  }
   if (ctx->q.cap < (size_t)2 * ctx->n * sizeof(double)) {
     // Q sums of every grain of the batch; rounds on the second stream may
     // still write the old buffer
@@ -668,6 +675,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = inb[i0];
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+      B.lu = keep_lu ? (cplx *)ctx->lu.p : nullptr;
       double fl = 0.;
       if (ctx->profiling) {
         for (int64_t q = i0; q < i1; ++q) {
@@ -763,10 +771,11 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
 // Phase 2 in one round for the grains in p2 (all grains with an order).
 static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
   int64_t t_end = 0;
-  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end);
+  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end, false, true);
   if (rc) {
     return rc;
   }
+  ctx->lu_ready = true;
   return finish_blocks(ctx, t_end, 1);
 }
 
@@ -780,13 +789,14 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
     }
   }
   int64_t t_end = 0;
-  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end);
+  int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end, false, true);
   if (rc) {
     return rc;
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->p2_t_total = t_end;
   ctx->p2_rounds = 1;
+  ctx->lu_ready = true;
   return TMX_OK;
 }
 
@@ -805,6 +815,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   const int glf = S.gauss_legendre_factor;
   int rc;
   ctx->have_batch = false;
+  ctx->lu_ready = false;
   ctx->n = n;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);
@@ -1097,6 +1108,7 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
   }
   CK(cudaSetDevice(ctx->device));
   ctx->have_batch = false;
+  ctx->lu_ready = false;
   ctx->n = n;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);

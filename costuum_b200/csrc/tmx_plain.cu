@@ -185,6 +185,7 @@ extern "C" int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n,
   CK(cudaSetDevice(ctx->device));
   NvtxRange range("tmx_calculator");
   ctx->have_batch = false;
+  ctx->lu_ready = false;
   ctx->n = n;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);

@@ -940,8 +940,9 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   }
   if (nitems > 0) {
     CK(cudaMemsetAsync(ctx->dT.p, 0, 3 * tt * sizeof(cplx), st));
-    // forward blocks again, now keeping the LU factors, then the tangents;
-    // both in the class-size buckets of the forward schedule
+    // the tangents need the LU factors of every item: a single-round batch
+    // kept them; otherwise the forward blocks run again keeping them. Both
+    // in the class-size buckets of the forward schedule
     const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
     int64_t i0 = 0;
     for (int b = 0; b < 5; ++b) {
@@ -967,8 +968,10 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
         B.max_nb = max_nb;
         B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
         B.lu = (cplx *)ctx->lu.p;
-        tmx_launch_blocks(B, st);
-        LAUNCHED();
+        if (!ctx->lu_ready) {
+          tmx_launch_blocks(B, st);
+          LAUNCHED();
+        }
         TmxTangentArgs A;
         A.items = B.items;
         A.nitems = B.nitems;

@@ -688,6 +688,10 @@ void tmx_launch_tangents(const TmxTangentArgs &a, cudaStream_t stream) {
   if (a.nitems <= 0 || a.nparams <= 0) {
     return;
   }
+  if (a.max_nb <= 8) {
+    launch_tangent_warp<1, 2, 3>(a, stream);
+    return;
+  }
   if (a.max_nb <= 16) {
     launch_tangent_warp<2, 4, 2>(a, stream);
     return;

@@ -380,7 +380,7 @@ __device__ static void wigner_col(double cosx, double sinx, double sinx_inv,
 //   S = (1/k) sum_m (2 cos m phi, 2 sin m phi) X_m
 // with e^{i m phi} built by repeated multiplication as in the reference.
 template <int NMAT>
-__global__ void __launch_bounds__(256, (NMAT > 1) ? 2 : 1)
+__global__ void __launch_bounds__(256, (NMAT > 1) ? 2 : 3)
 k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const TmxSJob *__restrict__ jobs, const TmxObsGrain *__restrict__ og,
       TmxMatSet mats, const TmxAngle *__restrict__ angles,

@@ -698,7 +698,7 @@ void tmx_launch_tangents(const TmxTangentArgs &a, cudaStream_t stream) {
   }
   const size_t smem = tmx_tangent_smem_bytes(a.max_nb, a.chunk_nodes);
   if (a.max_nb <= 32) {
-    launch_tangent<2, 4, 128, 4>(a, smem, stream);
+    launch_tangent<2, 4, 128, 3>(a, smem, stream);
   } else {
     launch_tangent<4, 4, 256, 1>(a, smem, stream);
   }

@@ -701,11 +701,15 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
   const int64_t want = (npairs + 7) / 8;
   const int blocks = (int)std::min<int64_t>(want, 148 * 8);
   if (nmat == 4) {
+    // four warps per CTA: the four matrices' buffers of 8 warps would
+    // leave room for one CTA per SM
+    const size_t smem4 = (size_t)4 * wcap * nmat * sizeof(double2);
+    const int blocks4 = (int)std::min<int64_t>((npairs + 3) / 4, 148 * 16);
     cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    k_orient_pairs<4><<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs,
-                                                     mats, coeffs, ncoef, cg_off, cg,
-                                                     cg_nmax, wcap, fold);
+                         (int)smem4);
+    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pair_base, ngrains, npairs,
+                                                       mats, coeffs, ncoef, cg_off, cg,
+                                                       cg_nmax, wcap, fold);
   } else {
     cudaFuncSetAttribute(k_orient_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);

@@ -1046,7 +1046,7 @@ __host__ __device__ constexpr int cta32_elems() {
                                                       : 2 * 32 * 33 + 3 * 32;
 }
 
-__global__ void __launch_bounds__(128, 3) k_blocks_cta32(TmxBlockArgs A) {
+__global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   constexpr int NBM = 32;
   constexpr int LD = NBM + 1;
   extern __shared__ __align__(16) unsigned char tmx_c32smem[];

@@ -20,6 +20,8 @@ maximum_memory_size, the QuickSched and memory logs) are accepted; the GPU
 schedule does not need them.
 """
 import ctypes
+import math
+import os
 
 import numpy as np
 
@@ -240,14 +242,128 @@ class CustomDustProperties:
         return complex(v.reshape(()))
 
 
-class DraineDustProperties:
-    """The reference's tabulated Draine (2003) optical properties need its
-    data files, which are not part of this package."""
+def _read_index_table(path):
+    """Rows of a Draine optical-constant file: every line that does not start
+    with '#', five columns (wavelength in micron, eps_1 - 1, eps_2,
+    Re(n) - 1, Im(n)); Table::from_ascii_file (Table.hpp:126-142)."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            if line.startswith("#"):
+                continue
+            parts = line.split()
+            if len(parts) < 5:
+                continue
+            rows.append([float(v) for v in parts[:5]])
+    return rows
 
-    def __init__(self, dust_temperature=20.0):
-        raise NotImplementedError(
-            "DraineDustProperties needs the reference's tabulated optical data; "
-            "use CustomDustProperties with those tables instead")
+
+def _interpolated_row(rows, x):
+    """Linear interpolation of every column at column-0 value x: bisection
+    for the bracketing rows (increasing or decreasing column 0), then
+    (1 - f) row_low + f row_high with f = (x - x_low) / (x_high - x_low);
+    outside the table the end pair is extrapolated
+    (LinearInterpolatedTable::get_row, Table.hpp:201-260)."""
+    lo, hi = 0, len(rows) - 1
+    xlo, xhi = rows[lo][0], rows[hi][0]
+    if xlo == xhi:
+        raise ValueError("Table endpoints are the same!")
+    increasing = xlo < xhi
+    while lo + 1 != hi:
+        mid = (lo + hi) >> 1
+        xm = rows[mid][0]
+        if (xm <= x) if increasing else (xm >= x):
+            xlo, lo = xm, mid
+        else:
+            xhi, hi = xm, mid
+    f = (x - xlo) / (xhi - xlo)
+    return [(1.0 - f) * a + f * b for a, b in zip(rows[lo], rows[hi])]
+
+
+def _carbon_free_electron_eps(T, wavelength, grain_size, parallel):
+    """Free-electron term of the graphite dielectric function (Draine & Lee
+    1984, eq. 2.2 with table 1 and the 1987 erratum; size dependence of the
+    damping time by eqs. 2.5-2.6), as DraineDustProperties::get_C_epsilon_free
+    (DraineDustProperties.hpp:73-107) evaluates it."""
+    if parallel:
+        omega_p, tau_bulk, TF, vF = 1.53e14, 1.4e-14, 255.0, 3.7e4
+    else:
+        T2 = T * T
+        omega_p = 4.33e14 * math.sqrt(1.0 - 6.24e-3 * T + 3.66e-5 * T2)
+        tau_bulk = 4.2e-11 / (1.0 + 0.322 * T + 0.0013 * T2)
+        TF, vF = 255.0, 4.5e5
+    veff = vF * math.sqrt(1.0 + T / TF)
+    tau = 1.0 / (1.0 / tau_bulk + veff / grain_size)
+    omega = 2.0 * math.pi * 299792458.0 / wavelength
+    wt = omega * tau
+    wpt = omega_p * tau
+    return complex(-wpt * wpt, 0.0) / complex(wt * wt, wt)
+
+
+def _eps_to_refractive_index(eps):
+    """n = sqrt((|eps| + eps_r) / 2) + i sqrt((|eps| - eps_r) / 2)
+    (DraineDustProperties::eps_to_mr, DraineDustProperties.hpp:133-139)."""
+    er, ei = eps.real, eps.imag
+    a = math.sqrt(er * er + ei * ei)
+    return complex(math.sqrt(0.5 * (a + er)), math.sqrt(0.5 * (a - er)))
+
+
+class DraineDustProperties:
+    """Refractive indices of Draine (2003) astrosilicate and graphite (E
+    parallel and perpendicular to the c axis) from the tabulated optical
+    constants that the reference ships in its data directory
+    (DraineDustProperties.hpp:36-242): linear interpolation in wavelength,
+    and for graphite the free-electron term of the dielectric function
+    re-evaluated for the grain's size and the dust temperature (the tables
+    include it for 20 K and 0.1 micron).
+
+    The tables are not part of this package. data_directory (or the
+    environment variable COSTUUM_DRAINE_DATA) names the directory that holds
+    the reference's files callindex.out_silD03, callindex.out_CpaD03_0.10 and
+    callindex.out_CpeD03_0.10."""
+
+    FILES = {SILICON: "callindex.out_silD03",
+             CARBON_PARALLEL: "callindex.out_CpaD03_0.10",
+             CARBON_PERPENDICULAR: "callindex.out_CpeD03_0.10"}
+
+    def __init__(self, dust_temperature=20.0, data_directory=None):
+        self.dust_temperature = float(dust_temperature)
+        d = data_directory or os.environ.get("COSTUUM_DRAINE_DATA")
+        if not d:
+            raise FileNotFoundError(
+                "DraineDustProperties reads the tabulated Draine (2003) optical "
+                "constants (%s); pass data_directory= or set COSTUUM_DRAINE_DATA "
+                "to the directory that holds them" % ", ".join(sorted(self.FILES.values())))
+        self._tables = {}
+        for kind, name in self.FILES.items():
+            path = os.path.join(d, name)
+            if not os.path.isfile(path):
+                raise FileNotFoundError("Unable to open file: \"%s\"!" % path)
+            rows = _read_index_table(path)
+            for r in rows:
+                r[0] *= 1e-6   # micron -> m
+                r[1] += 1.0    # eps_1
+                r[3] += 1.0    # Re(n)
+            if kind != SILICON:
+                # remove the free-electron term of the tabulated 20 K, 0.1 um
+                parallel = kind == CARBON_PARALLEL
+                for r in rows:
+                    c = _carbon_free_electron_eps(20.0, r[0], 1e-7, parallel)
+                    r[1] -= c.real
+                    r[2] -= c.imag
+            self._tables[kind] = rows
+
+    def get_refractive_index(self, type, size, wavelength):
+        type = int(type)
+        if type not in self._tables:
+            raise ValueError("Unknown dust grain type: %d!" % type)
+        row = _interpolated_row(self._tables[type], float(wavelength))
+        if type == SILICON:
+            return complex(row[3], row[4])
+        eps = complex(row[1], row[2]) + _carbon_free_electron_eps(
+            self.dust_temperature, float(wavelength), float(size),
+            type == CARBON_PARALLEL)
+        return _eps_to_refractive_index(eps)
 
 
 # --------------------------------------------------------------- get_table --

@@ -355,6 +355,21 @@ def ref():
     return _ref
 
 
+def draine_data_directory():
+    """Directory of the reference's tabulated Draine optical constants, as
+    recorded by build_ref.sh in the generated DraineDustPropertiesDataLocation
+    header; None where the reference build or its data are absent."""
+    h = os.path.join(HERE, "_ref", "gen", "DraineDustPropertiesDataLocation.hpp")
+    if not os.path.isfile(h):
+        return None
+    with open(h) as f:
+        for line in f:
+            if line.startswith("#define DRAINEDUSTPROPERTIESDATALOCATION "):
+                d = line.split('"')[1]
+                return d if os.path.isdir(d) else None
+    return None
+
+
 def ref_module():
     """The reference's own CPython module (CosTuuM), built by build_ref.sh."""
     d = os.path.join(HERE, "_ref")

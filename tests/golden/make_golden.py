@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the unmodified reference.
 
 Run in a container where the reference has been built (oracle/build_ref.sh):
-    python tests/golden/make_golden.py [stages tmatrices tables plain]
+    python tests/golden/make_golden.py [stages tmatrices tables plain draine]
 It imports the reference's own CPython module (oracle/_ref/CosTuuM*.so) and
 its task objects (oracle/_ref/libref_driver.so) and stores their outputs.
 The fixtures pin the C restatement in oracle/ (tests/test_oracle_golden.py).
@@ -217,10 +217,30 @@ def plain():
     return out
 
 
+def draine():
+    """Refractive indices of the reference's DraineDustProperties (tabulated
+    Draine 2003 optical constants from its data directory) for the three
+    grain types at sizes 0.01-2 um and wavelengths across and beyond the
+    tables (0.03 um - 300 um), at dust temperatures 20 K and 50 K."""
+    C = O.ref_module()
+    sizes = np.array([1e-8, 1e-7, 5e-7, 2e-6])
+    lams = np.logspace(np.log10(3e-8), np.log10(3e-4), 41)
+    out = {"sizes": sizes, "wavelengths": lams, "temperatures": np.array([20.0, 50.0])}
+    for T in (20.0, 50.0):
+        D = C.DraineDustProperties(dust_temperature=T)
+        m = np.zeros((3, len(sizes), len(lams)), complex)
+        for t in range(3):
+            for i, a in enumerate(sizes):
+                for j, lam in enumerate(lams):
+                    m[t, i, j] = D.get_refractive_index(t, a, lam)
+        out["m_%d" % int(T)] = m
+    return out
+
+
 if __name__ == "__main__":
-    # python make_golden.py [stages tmatrices tables plain]: the named sets
-    # (default all)
-    which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain"]
+    # python make_golden.py [stages tmatrices tables plain draine]: the named
+    # sets (default all)
+    which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain", "draine"]
     for name in which:
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **globals()[name]())
     print("golden fixtures written to", HERE)

@@ -10,6 +10,8 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <system_error>
+#include <thread>
 #include <vector>
 
 #include "tmx_ctx.h"
@@ -119,8 +121,8 @@ extern "C" int tmx_orientation_coefficients(int kind, double param, int order,
       at, rt);
   const double nf = 1. / norm;
   out[0] = 1.;
-  for (int i = 1; i <= order; ++i) {
-    out[i] = gl_quadrature(
+  auto coefficient = [&](int i) {
+    return gl_quadrature(
         [&](double beta) {
           const double cb = cos(beta);
           const double sb = sin(beta);
@@ -128,6 +130,39 @@ extern "C" int tmx_orientation_coefficients(int kind, double param, int order,
           return sb * pb * wigner_d00(cb, i);
         },
         0., M_PI, 2 * (i + 1), 100 * (i + 1), at, rt);
+  };
+  // the coefficients are independent quadratures (their cost grows with
+  // the order): random orientation spreads them over host threads,
+  // interleaved; a custom p(beta) calls into Python and stays on this thread
+  if (kind == 0 && order >= 32) {
+    const int nt = std::max(
+        1, std::min<int>((int)std::thread::hardware_concurrency(), 32));
+    std::vector<std::thread> pool;
+    int started = 0;
+    try {
+      for (int t = 0; t < nt; ++t) {
+        pool.emplace_back([&, t]() {
+          for (int i = 1 + t; i <= order; i += nt) {
+            out[i] = coefficient(i);
+          }
+        });
+        ++started;
+      }
+    } catch (const std::system_error &) {
+      // fewer threads than asked for: the residues of the missing ones below
+    }
+    for (std::thread &th : pool) {
+      th.join();
+    }
+    for (int t = started; t < nt; ++t) {
+      for (int i = 1 + t; i <= order; i += nt) {
+        out[i] = coefficient(i);
+      }
+    }
+    return TMX_OK;
+  }
+  for (int i = 1; i <= order; ++i) {
+    out[i] = coefficient(i);
   }
   return TMX_OK;
 }

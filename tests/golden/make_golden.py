@@ -58,6 +58,10 @@ def stages():
         R.ref_orientation_coefficients(kind, par, 20, _p(c))
         out["od_%d" % i] = c
         out["od_%d_arg" % i] = np.array([kind, par])
+    # random orientation at order 200 (the coefficients of maximum_order 100)
+    c = np.zeros(201)
+    R.ref_orientation_coefficients(0, 0., 200, _p(c))
+    out["od_random_200"] = c
     A = (np.random.default_rng(0).standard_normal((7, 7))
          + 1j * np.random.default_rng(1).standard_normal((7, 7)))
     Ai = A.copy()

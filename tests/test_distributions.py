@@ -32,6 +32,9 @@ def test_orientation_coefficients(stages, CT):
                    (2, lambda: CT.DavisGreensteinOrientationDistribution(2.0, 20)),
                    (3, lambda: CT.DavisGreensteinOrientationDistribution(0.5, 20))):
         assert np.array_equal(cls().coefficients, stages["od_%d" % i]), i
+    # order 200: the quadratures run on several host threads
+    assert np.array_equal(CT.RandomOrientationDistribution(200).coefficients,
+                          stages["od_random_200"])
 
 
 def test_custom_orientation(stages, CT):

@@ -377,6 +377,21 @@ def run_ours(args):
             t2 = time.perf_counter()
             times.append((t1 - t0, t2 - t0))
         tm, tz = min(t[0] for t in times), min(t[1] for t in times)
+        # forward Q_ext and its adjoint (derivatives in Re m, Im m, r_ev, d) at
+        # 32 zenith angles for random orientation, on the same grains
+        th32 = np.arccos(np.linspace(-1, 1, 32))
+        co5 = RandomOrientationDistribution(2 * int(nm5.max())).coefficients
+        fa = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.tmatrix_batch_calculator(r5, lam5, m5, d5)
+            ctx.observables(th32, co5)
+            t1 = time.perf_counter()
+            _, dq5 = ctx.gradients(th32, co5)
+            t2 = time.perf_counter()
+            fa.append((t1 - t0, t2 - t1))
+        tf5, ta5 = min(t[0] for t in fa), min(t[1] for t in fa)
         c5 = {"what": "256 grains x~U[10,30], d log-U[0.33,3], calculator "
                       "schedule (maximum_order 200, ngauss loop to 500), "
                       "random-orientation average, Z at 181 angles; host wall "
@@ -388,7 +403,15 @@ def run_ours(args):
               "status_nonzero": int((res5.status != 0).sum()),
               "status_note": "grains the reference's calculator cannot converge "
                              "either (it aborts); flagged, not aborted",
-              "z_finite": bool(np.isfinite(Z5).all())}
+              "z_finite": bool(np.isfinite(Z5).all()),
+              "forward_q_ms": tf5 * 1e3,
+              "adjoint_ms": ta5 * 1e3,
+              "adjoint_over_forward": ta5 / tf5,
+              "adjoint_what": "forward = calculator schedule + Q_ext/Q_abs at 32 "
+                              "angles (random orientation); adjoint = their "
+                              "derivatives in (Re m, Im m, r_ev, d) with the kept "
+                              "LU factors",
+              "adjoint_finite": bool(np.isfinite(dq5[res5.status == 0]).all())}
 
     # roofline of the dominant kernel (block kernels: assembly + LU + solve),
     # algorithmic flops of the per-grain model (every chain order and every

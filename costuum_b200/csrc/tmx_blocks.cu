@@ -1211,8 +1211,25 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
           const cplx pinv = cinv_lu(Qm[i * LD + i]);
           const cplx l = cmul(Qm[lane * LD + i], pinv);
           Qm[lane * LD + i] = l;
-          for (int k = i + 1; k < nb; ++k) {
-            Qm[lane * LD + k] = csub(Qm[lane * LD + k], cmul(l, Qm[i * LD + k]));
+          // four entries at a time: all loads before the stores (the pivot
+          // row is only read in this step), so the updates overlap
+          cplx *qr = Qm + lane * LD;
+          const cplx *pr = Qm + i * LD;
+          int k = i + 1;
+          for (; k + 3 < nb; k += 4) {
+            cplx a0 = qr[k], a1 = qr[k + 1], a2 = qr[k + 2], a3 = qr[k + 3];
+            const cplx b0 = pr[k], b1 = pr[k + 1], b2 = pr[k + 2], b3 = pr[k + 3];
+            a0 = csub(a0, cmul(l, b0));
+            a1 = csub(a1, cmul(l, b1));
+            a2 = csub(a2, cmul(l, b2));
+            a3 = csub(a3, cmul(l, b3));
+            qr[k] = a0;
+            qr[k + 1] = a1;
+            qr[k + 2] = a2;
+            qr[k + 3] = a3;
+          }
+          for (; k < nb; ++k) {
+            qr[k] = csub(qr[k], cmul(l, pr[k]));
           }
         }
         __syncwarp();

@@ -1290,6 +1290,276 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   }
 }
 
+// ------------------------------------------ eight warps per item (<= 64) --
+//
+// Classes of 33..64 members: one CTA of eight warps per item. As in
+// k_blocks_cta32 the warps build each chunk of TMX_WG32 nodes together and
+// warp w accumulates column tile w over all eight row tiles with DMMA, so
+// the node factors are built once per item; the LU pivots with warp 0 and
+// updates with all threads (four barriers per step), and the solves keep
+// each row in the registers of four lanes (row tid / 4).
+
+__host__ __device__ constexpr int cta64_elems() {
+  // F[WG][4][64] + W[2][WG][4][64], or Q, RgQ [64][65], 1/U_jj, pivot and
+  // gather indices and a flag
+  return (12 * TMX_WG32 * 64 > 2 * 64 * 65 + 64 + 66) ? 12 * TMX_WG32 * 64
+                                                        : 2 * 64 * 65 + 64 + 66;
+}
+
+__global__ void __launch_bounds__(256, 1) k_blocks_cta64(TmxBlockArgs A) {
+  constexpr int NBM = 64;
+  constexpr int LD = NBM + 1;
+  constexpr int NTH = 256;
+  extern __shared__ __align__(16) unsigned char tmx_c64smem[];
+  cplx *base = reinterpret_cast<cplx *>(tmx_c64smem);
+  cplx *Fs = base;                    // [WG][4][NBM]
+  cplx *Ws = Fs + TMX_WG32 * 4 * NBM; // [2][WG][4][NBM]
+  cplx *Qm = base;                    // [NBM][LD]  (after the assembly)
+  cplx *Rm = Qm + NBM * LD;           // [NBM][LD]
+  cplx *uinv = Rm + NBM * LD;         // [NBM]
+  int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
+  int *piv = perm + NBM;                           // [NBM]
+  int *flag = piv + NBM;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int wib = tid >> 5;
+  const int q = lane & 3;
+  const int rr = lane >> 2;
+  for (int it = blockIdx.x; it < A.nitems; it += gridDim.x) {
+    const TmxItem item = A.items[it];
+    const TmxSlot sl = A.slots[item.slot];
+    const TmxGrain Gr = A.grains[sl.grain];
+    const int N = sl.nmax;
+    const int ng = sl.ngauss;
+    const int m = item.m;
+    const ClassDesc D = describe<1>(N, m, item.cls);
+    const int nb = D.nb;
+    if (nb <= 0) {
+      continue;
+    }
+    if (nb > NBM) {
+      if (tid == 0) {
+        atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
+      }
+      continue;
+    }
+    const double *T = A.tab + sl.tab;
+    const double *S = A.nsc + sl.nsc;
+    const double *Wg = A.wig + A.wig_off[sl.wig_n] + (int64_t)m * ng * N * 2;
+    const double k2 = Gr.k * Gr.k;
+    const cplx k2mr = mkc(Gr.mr * k2, Gr.mi * k2);
+    const int ngroups = (D.R1 > 0 && m > 0) ? 2 : 1;
+    const int nrt = (nb + 7) >> 3;
+    const int col = wib * 8 + rr; // B-fragment column of this lane
+    double acc[8][4][2];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        acc[r][p][0] = acc[r][p][1] = 0.;
+      }
+    }
+    for (int g0 = 0; g0 < ng; g0 += TMX_WG32) {
+      __syncthreads();
+      for (int u = tid; u < TMX_WG32 * nb; u += NTH) {
+        const int gl = u / nb;
+        const int a = u - gl * nb;
+        cplx *fp = Fs + gl * 4 * NBM + a;
+        cplx *wp = Ws + gl * 4 * NBM + a;
+        if (g0 + gl < ng) {
+          a_side<true>(D, a, N, g0 + gl, T, S, Wg, fp, NBM, m);
+          b_side<true>(D, a, N, m, g0 + gl, ngroups, T, S, Wg, k2, k2mr, wp, NBM,
+                       TMX_WG32 * 4 * NBM);
+        } else {
+          zero_side(fp, NBM, 4);
+          for (int g = 0; g < ngroups; ++g) {
+            zero_side(wp + g * TMX_WG32 * 4 * NBM, NBM, 4);
+          }
+        }
+      }
+      __syncthreads();
+      if (wib * 8 < nb) {
+        const int gmax = min(TMX_WG32, ng - g0);
+        const int nsl = (m == 0) ? (gmax + 1) >> 1 : gmax;
+        for (int sx = 0; sx < nsl; ++sx) {
+          const int gl = (m == 0) ? 2 * sx + (q >> 1) : sx;
+          const int t = (m == 0) ? 1 + 2 * (q & 1) : q;
+          cplx w[2];
+#pragma unroll
+          for (int g = 0; g < 2; ++g) {
+            w[g] = (col < nb && g < ngroups)
+                       ? Ws[((g * TMX_WG32 + gl) * 4 + t) * NBM + col]
+                       : mkc(0., 0.);
+          }
+#pragma unroll
+          for (int rti = 0; rti < 8; ++rti) {
+            if (rti < nrt) {
+              const int row = rti * 8 + rr;
+              const cplx f = (row < nb) ? Fs[(gl * 4 + t) * NBM + row] : mkc(0., 0.);
+              const int grp = (row < D.R0) ? 0 : 1;
+              const int lo = rti * 8, hi = min(rti * 8 + 8, nb);
+#pragma unroll
+              for (int g = 0; g < 2; ++g) {
+                const bool present = (g == 0) ? (lo < D.R0) : (ngroups == 2 && hi > D.R0);
+                if (present) {
+                  const double fj = (grp == g) ? f.x : 0.;
+                  const double fy = (grp == g) ? f.y : 0.;
+                  double *a4 = &acc[rti][0][0];
+                  dmma(a4[0], a4[1], fj, w[g].x);
+                  dmma(a4[2], a4[3], fj, w[g].y);
+                  dmma(a4[4], a4[5], fy, w[g].x);
+                  dmma(a4[6], a4[7], fy, w[g].y);
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    // a_n of each member once per item (in the 1/U_jj slots)
+    double *an_s = reinterpret_cast<double *>(uinv);
+    if (tid < nb) {
+      int ia, na;
+      member(D, tid, ia, na);
+      an_s[tid] = a_n(na);
+    }
+    if (tid == 0) {
+      *flag = 0;
+    }
+    __syncthreads();
+    // Q = G^j + i G^y, RgQ = G^j (times a_n1 a_n2), into the chunk buffers
+#pragma unroll
+    for (int rti = 0; rti < 8; ++rti) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int a = rti * 8 + rr;
+        const int b = wib * 8 + 2 * q + i;
+        if (a < nb && b < nb) {
+          const double sc = an_s[a] * an_s[b];
+          const double jr = acc[rti][0][i], ji = acc[rti][1][i];
+          const double yr = acc[rti][2][i], yi = acc[rti][3][i];
+          Qm[a * LD + b] = mkc((jr - yi) * sc, (ji + yr) * sc);
+          Rm[a * LD + b] = mkc(jr * sc, ji * sc);
+        }
+      }
+    }
+    __syncthreads();
+    // LU in place in Qm: pivot of column i by warp 0 (first row with the
+    // largest |Q_ri|), row exchange, column scaling, rank-1 update
+    for (int i = 0; i < nb; ++i) {
+      if (wib == 0) {
+        double best = -1.;
+        int bi = i;
+        for (int j = i + lane; j < nb; j += 32) {
+          const double v = cabs_dev(Qm[j * LD + i]);
+          if (v > best) {
+            best = v;
+            bi = j;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ov = __shfl_down_sync(0xffffffffu, best, o);
+          const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+          if (ov > best || (ov == best && oi < bi)) {
+            best = ov;
+            bi = oi;
+          }
+        }
+        if (lane == 0) {
+          piv[i] = bi;
+          if (!(best > 0.)) {
+            *flag = 1;
+          }
+        }
+      }
+      __syncthreads();
+      const int ip = piv[i];
+      if (ip != i) {
+        for (int j = tid; j < nb; j += NTH) {
+          const cplx t = Qm[i * LD + j];
+          Qm[i * LD + j] = Qm[ip * LD + j];
+          Qm[ip * LD + j] = t;
+        }
+        __syncthreads();
+      }
+      const cplx pinv = cinv_lu(Qm[i * LD + i]);
+      for (int j = i + 1 + tid; j < nb; j += NTH) {
+        Qm[j * LD + i] = cmul(Qm[j * LD + i], pinv);
+      }
+      __syncthreads();
+      const int rem = nb - i - 1;
+      for (int u = tid; u < rem * rem; u += NTH) {
+        const int j = i + 1 + u / rem;
+        const int k = i + 1 + u % rem;
+        Qm[j * LD + k] = csub(Qm[j * LD + k], cmul(Qm[j * LD + i], Qm[i * LD + k]));
+      }
+      __syncthreads();
+    }
+    for (int j = tid; j < nb; j += NTH) {
+      uinv[j] = cinv_lu(Qm[j * LD + j]);
+    }
+    if (tid == 0) {
+      // column exchanges of Matrix::plu_inverse step 4, as a gather index
+      for (int j = 0; j < nb; ++j) {
+        perm[j] = j;
+      }
+      for (int j = nb - 1; j >= 0; --j) {
+        const int p = piv[j];
+        const int t = perm[j];
+        perm[j] = perm[p];
+        perm[p] = t;
+      }
+      if (*flag) {
+        atomicOr(&A.status[sl.grain], TMX_ST_SINGULAR);
+      }
+    }
+    __syncthreads();
+    if (A.lu) {
+      cplx *Ls = A.lu + item.scratch;
+      for (int u = tid; u < nb * nb; u += NTH) {
+        Ls[u] = Qm[(u / nb) * LD + (u % nb)];
+      }
+      int *ps = reinterpret_cast<int *>(Ls + (int64_t)nb * nb);
+      for (int j = tid; j < nb; j += NTH) {
+        ps[j] = perm[j];
+      }
+    }
+    // solve T_c Q_c = -RgQ_c: four lanes per row
+    solve_rows<NBM, 4>(Rm, Qm, LD, uinv, nb, tid >> 2, tid & 3);
+    __syncthreads();
+    // write out: T_c[a][b] = Y[a][perm[b]]
+    if (sl.tout < 0) {
+      for (int a = tid; a < nb; a += NTH) {
+        int ia, na;
+        member(D, a, ia, na);
+        A.diag[sl.diag + ia * N + (na - 1)] = Rm[a * LD + perm[a]];
+      }
+    } else {
+      cplx *Tb = A.tout + sl.tout + block_offset(N, m);
+      const int w2 = 2 * D.nbb;
+      for (int u = tid; u < nb * nb; u += NTH) {
+        const int a = u / nb;
+        const int b = u - a * nb;
+        int ia, na, ib, nbn;
+        member(D, a, ia, na);
+        member(D, b, ib, nbn);
+        Tb[(int64_t)(ia * D.nbb + (na - D.nmin)) * w2 + ib * D.nbb + (nbn - D.nmin)] =
+            Rm[a * LD + perm[b]];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+static void launch_cta64(const TmxBlockArgs &a, cudaStream_t stream) {
+  const size_t smem = (size_t)cta64_elems() * sizeof(cplx);
+  cudaFuncSetAttribute(k_blocks_cta64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  const int blocks = (int)std::min<int64_t>(a.nitems, 148 * 4);
+  k_blocks_cta64<<<blocks, 256, smem, stream>>>(a);
+}
+
 static void launch_cta32(const TmxBlockArgs &a, cudaStream_t stream) {
   const size_t smem = (size_t)cta32_elems() * sizeof(cplx);
   cudaFuncSetAttribute(k_blocks_cta32, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1350,6 +1620,10 @@ void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
   }
   if (a.max_nb <= 32) {
     launch_cta32(a, stream);
+    return;
+  }
+  if (a.max_nb <= 64) {
+    launch_cta64(a, stream);
     return;
   }
   const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);

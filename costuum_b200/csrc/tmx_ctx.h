@@ -81,6 +81,12 @@ struct tmx_ctx {
     int64_t launches = 0;
     double flops = 0.;
   } prof[2]; // 0: block kernel, 1: table kernel
+  // timing events, reused once their pairs are resolved (at the next read of
+  // the profile), so that a profiled batch creates none
+  std::vector<cudaEvent_t> prof_pool;
+  size_t prof_used = 0;
+  std::vector<double> survey_cache; // survey-model flops per order, this glf
+  int survey_glf = 0, survey_min = 0;
   double flops_survey = 0.; // survey-model flops of the last batch
   // last batch
   int64_t n = 0;
@@ -103,6 +109,8 @@ struct tmx_ctx {
   struct ItemTemplate {
     std::vector<int32_t> mc, nb;
     std::vector<std::pair<int32_t, int32_t>> bins;
+    // flops of the grain's items: fl_a * ngauss + fl_b (item_flops)
+    double fl_a = 0., fl_b = 0.;
   };
   std::vector<ItemTemplate> item_tpl; // indexed by N
   int64_t p2_scr_total = 0, p2_t_total = 0;
@@ -134,12 +142,25 @@ static inline double item_flops(int nb, int m, int ng) {
   return 8. * terms * b * b * ng + (8. / 3.) * b * b * b + 8. * b * b * b;
 }
 
+static inline int prof_event(tmx_ctx *ctx, cudaEvent_t *e) {
+  if (ctx->prof_used == ctx->prof_pool.size()) {
+    cudaEvent_t n;
+    CK(cudaEventCreate(&n));
+    ctx->prof_pool.push_back(n);
+  }
+  *e = ctx->prof_pool[ctx->prof_used++];
+  return 0;
+}
+
 static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a,
                              cudaStream_t st = nullptr) {
   if (!ctx->profiling) {
     return 0;
   }
-  CK(cudaEventCreate(a));
+  int rc = prof_event(ctx, a);
+  if (rc) {
+    return rc;
+  }
   CK(cudaEventRecord(*a, st ? st : ctx->stream));
   (void)k;
   return 0;
@@ -151,7 +172,10 @@ static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
     return 0;
   }
   cudaEvent_t b;
-  CK(cudaEventCreate(&b));
+  int rc = prof_event(ctx, &b);
+  if (rc) {
+    return rc;
+  }
   CK(cudaEventRecord(b, st ? st : ctx->stream));
   ctx->prof[k].pending.push_back({a, b});
   ctx->prof[k].launches += 1;
@@ -159,18 +183,19 @@ static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
   return 0;
 }
 
-// resolve recorded event pairs (after the stream has been synchronised)
+// resolve recorded event pairs (after every stream has finished them) and
+// return their events to the pool
 static inline int prof_resolve(tmx_ctx *ctx) {
   for (auto &p : ctx->prof) {
     for (auto &e : p.pending) {
       float ms = 0.f;
+      CK(cudaEventSynchronize(e.second));
       CK(cudaEventElapsedTime(&ms, e.first, e.second));
       p.ms += ms;
-      cudaEventDestroy(e.first);
-      cudaEventDestroy(e.second);
     }
     p.pending.clear();
   }
+  ctx->prof_used = 0;
   return 0;
 }
 

@@ -296,6 +296,9 @@ void tmx_destroy(tmx_ctx *ctx) {
     cudaEventDestroy(ctx->t0);
     cudaEventDestroy(ctx->t1);
   }
+  for (cudaEvent_t e : ctx->prof_pool) {
+    cudaEventDestroy(e);
+  }
   DevBuf *bufs[] = {&ctx->lu, &ctx->dT, &ctx->tscr, &ctx->dTa, &ctx->dS,
                     &ctx->cg, &ctx->cg_off, &ctx->Ta, &ctx->o_angles,
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
@@ -510,6 +513,8 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
             tp.mc.push_back((m << 8) | cl);
             tp.nb.push_back(nb);
             c[std::min(nb, TMX_MAX_NB + 1)] += 1;
+            tp.fl_a += item_flops(nb, m, 1) - item_flops(nb, m, 0);
+            tp.fl_b += item_flops(nb, m, 0);
           }
         }
       }
@@ -676,10 +681,12 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       B.max_nb = inb[i0];
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
       B.lu = keep_lu ? (cplx *)ctx->lu.p : nullptr;
+      // the round's flops are booked on its first launch
       double fl = 0.;
-      if (ctx->profiling) {
-        for (int64_t q = i0; q < i1; ++q) {
-          fl += item_flops(inb[q], items[q].m, slots[items[q].slot].ngauss);
+      if (ctx->profiling && nbuckets == 1) {
+        for (int s = 0; s < np2; ++s) {
+          const tmx_ctx::ItemTemplate &tp = ctx->item_tpl[slots[s].nmax];
+          fl += tp.fl_a * slots[s].ngauss + tp.fl_b;
         }
       }
       if ((rc = prof_begin(ctx, 0, &pe, bs))) {
@@ -747,21 +754,39 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   }
   // survey-model flops (per grain: every order of the m = 0 chain on the
   // unreduced 2k x 2k block, then every m >= 1 block on 2nm x 2nm)
+  // (cumulative per-order sums, cached for this glf and minimum order):
+  // grain flops = chain[N] + ng * mg[N] + mc[N]
+  std::vector<double> &sc = ctx->survey_cache;
+  if (ctx->profiling && (ctx->survey_glf != glf || ctx->survey_min != S.min_order)) {
+    sc.clear();
+    ctx->survey_glf = glf;
+    ctx->survey_min = S.min_order;
+  }
   for (int64_t i = 0; ctx->profiling && i < n; ++i) {
     const int N = ctx->nmax_h[i];
     if (N <= 0) {
       continue;
     }
-    for (int k = S.min_order; k <= N; ++k) {
+    for (int k = (int)(sc.size() / 3); k <= N; ++k) {
       const double b = k, g = glf * k, t = 2. * k;
-      ctx->flops_survey += 8. * 4. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+      double chain = k ? sc[3 * (k - 1)] : 0., mg = k ? sc[3 * k - 2] : 0.,
+             mc = k ? sc[3 * k - 1] : 0.;
+      if (k >= S.min_order) {
+        chain += 8. * 4. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
+      }
+      if (k >= 1) { // the m >= 1 block of size b = k
+        mg += 8. * 10. * b * b;
+        mc += (8. / 3.) * t * t * t + 8. * t * t * t;
+      }
+      sc.push_back(chain);
+      sc.push_back(mg);
+      sc.push_back(mc);
     }
-    for (int m = 1; m <= N; ++m) {
-      const double b = N + 1 - m, g = ctx->ngauss_h[i], t = 2. * b;
-      ctx->flops_survey += 8. * 10. * b * b * g + (8. / 3.) * t * t * t + 8. * t * t * t;
-    }
+    ctx->flops_survey += sc[3 * N] + ctx->ngauss_h[i] * sc[3 * N + 1] + sc[3 * N + 2];
   }
-  if ((rc = prof_resolve(ctx))) {
+  // event pairs are resolved when the profile is read; a long profiled run
+  // resolves here now and then so that the pool stays bounded
+  if (ctx->prof_used > 8192 && (rc = prof_resolve(ctx))) {
     return rc;
   }
   ctx->have_batch = true;
@@ -1209,11 +1234,21 @@ int tmx_profile_enable(tmx_ctx *ctx, int on) {
   if (!ctx) {
     return TMX_ERR_INVALID;
   }
-  ctx->profiling = on != 0;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());
   for (auto &p : ctx->prof) {
+    p.pending.clear();
     p.ms = 0.;
     p.launches = 0;
     p.flops = 0.;
+  }
+  ctx->prof_used = 0;
+  ctx->profiling = on != 0;
+  // events for a few batches, made before any timed work
+  while (ctx->profiling && ctx->prof_pool.size() < 2048) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    ctx->prof_pool.push_back(e);
   }
   return TMX_OK;
 }
@@ -1222,6 +1257,12 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
                      double *flops) {
   if (!ctx || kernel < 0 || kernel > 1) {
     return TMX_ERR_INVALID;
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());
+  const int rc = prof_resolve(ctx);
+  if (rc) {
+    return rc;
   }
   if (ms) {
     *ms = ctx->prof[kernel].ms;

@@ -417,6 +417,11 @@ def run_ours(args):
     # algorithmic flops of the per-grain model (every chain order and every
     # m block as a full 2nb x 2nb assembly, LU and solve) over the summed
     # CUDA-event time of the block launches
+    # DRAM bytes (read + write) per block launch from one ncu capture of
+    # this command (--steps 1 --warmup 3 --skip-cpu --skip-extras, metrics
+    # dram__bytes_read.sum and dram__bytes_write.sum): the mean over the 38
+    # block launches of the timed step, with L2 flushed before each launch
+    BLOCK_TRAFFIC_PER_LAUNCH = 30.76e6
     bk_launches = max(1, bk_n.value)
     bk_s = bk_ms[0] * 1e-3
     achieved = flops_survey * args.steps / bk_s / 1e12 if bk_s > 0 else 0.0
@@ -457,7 +462,8 @@ def run_ours(args):
                          "executed_tflops": executed,
                          "launches": int(bk_n.value),
                          "share_of_step": bk_ms[0] / max(total, 1e-9),
-                         "traffic": None},
+                         "traffic": BLOCK_TRAFFIC_PER_LAUNCH,
+                         "traffic_unit": "bytes per block launch (ncu, cold L2)"},
             "phases_ms_per_step": {"blocks": bk_ms[0] / args.steps,
                                    "tables": tb_ms[0] / args.steps},
             "gpu_launches": int(launches),

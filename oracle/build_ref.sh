@@ -15,15 +15,24 @@
 # cmake_minimum_required and the missing .git breaks its version parsing), so
 # the two generated headers are written here by sed, as its CMake would.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [--optional] [REFERENCE_ROOT]
+#        (default /root/reference; --optional: exit 0 when it is absent)
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OPTIONAL=0
+if [ "${1:-}" = "--optional" ]; then
+  OPTIONAL=1
+  shift
+fi
 REF="${1:-/root/reference}"
 OUT="$HERE/_ref"
 GEN="$OUT/gen"
 
 if [ ! -f "$REF/src/CTMModule.cpp" ]; then
+  if [ "$OPTIONAL" = 1 ]; then
+    exit 0
+  fi
   echo "build_ref.sh: reference sources not found under $REF" >&2
   exit 1
 fi

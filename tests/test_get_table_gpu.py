@@ -1,7 +1,7 @@
 """get_table on the GPU against the reference module's own outputs
 (tests/golden/tables.npz, made by the unmodified reference).
 
-Tolerance: relative 1e-8 on every coefficient (the BASELINE bound on
+Tolerance: relative 1e-8 on every coefficient (the stated parity bound on
 Q_ext/Q_abs); scattering matrices: 1e-8 relative to the largest element of
 each 4x4 matrix."""
 import os

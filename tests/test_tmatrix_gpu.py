@@ -1,6 +1,6 @@
 """GPU parity of the batched T-matrix path against the CPU oracle.
 
-Tolerances: T-matrix elements 1e-9 relative in norm
+Tolerances (the stated parity bounds): T-matrix elements 1e-9 relative in norm
 (per m block, Frobenius), Q_ext 1e-8 relative.
 """
 import numpy as np

@@ -43,6 +43,20 @@ def t_error(Ta, Tb, nmax):
     return worst
 
 
+def oracle_sensitivity(r, lam, m, d, nmax, ngauss, T, q, rel=1e-15):
+    """The oracle's own change when r_ev moves by +-rel (a few ulps): the
+    worst per-m-block relative change of T and the worst relative change of
+    the four sums. For an ill-conditioned grain this is the part of any
+    difference between two correct implementations that rounding alone
+    produces."""
+    t_s, q_s = 0.0, 0.0
+    for f in (1 + rel, 1 - rel):
+        T2, q2 = oracle_at(r * f, lam, m, d, nmax, ngauss)
+        t_s = max(t_s, t_error(T2, T, nmax))
+        q_s = max(q_s, max(abs(q2[j] - q[j]) / abs(q[j]) for j in range(4)))
+    return t_s, q_s
+
+
 def check_grain(res, i, r, lam, m, d, ref):
     """Compare grain i of a GPU batch with the oracle's convergence run.
 

@@ -1,0 +1,99 @@
+"""The batched T-matrix path at the benchmark's full size: 4096 grains of the
+config-2 distributions (seed 1, the grains bench.py times), schedule
+min_order 10, max_order 100, ngauss = 2 order, tolerance 1e-4.
+
+At this size the oracle cannot redo every grain in seconds, so the checks are
+properties that do not depend on the batch size, plus oracle parity on the
+grains with the smallest, median and largest converged order:
+
+* every grain converges, at an order inside the schedule;
+* determinism across round layouts: the same blocks computed in one round at
+  the converged orders (tmatrix_batch_fixed) give the same doubles;
+* the per-grain Q sums that k_qsums reduces on the device equal the
+  reference's sums (TMatrix Qsca/Qext loops, restated in the oracle) over the
+  T-matrix downloaded from the device, for all 4096 grains (relative 1e-12:
+  only the summation order differs);
+* oracle parity at the GPU's orders on the order-extreme grains and a seeded
+  random sample: T within 1e-9 relative per m block and the sums within 1e-8,
+  or, for a grain whose T the oracle itself changes by more than that when
+  r_ev moves by 1e-15 relative, within 4x that change. Grain 1234 of this
+  set (x 9.47, d 0.52, m 1.96 + 0.80i, order 32) is such a grain: a 1e-15
+  change of r_ev changes the oracle's m = 2 block by 6.8e-8, and the GPU's
+  T (FMA contractions, other summation order) differs from it by 5.7e-8.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import _helpers as H
+
+pytestmark = pytest.mark.gpu
+
+SCHEDULE = dict(min_order=10, max_order=100, gauss_legendre_factor=2,
+                tolerance=1e-4)
+N_GRAINS = 4096
+SUM_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def full(ctx):
+    r, lam, m, d = H.config2_sample(N_GRAINS, 1)
+    res = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+    nm, ng = res.nmax.copy(), res.ngauss.copy()
+    q, status = res.q.copy(), res.status.copy()
+    T = [res.tmatrix(i) for i in range(N_GRAINS)]
+    return dict(r=r, lam=lam, m=m, d=d, res=res, nmax=nm, ngauss=ng, q=q,
+                status=status, T=T)
+
+
+def test_all_converged(full):
+    assert (full["status"] == 0).all()
+    nm = full["nmax"]
+    assert nm.min() >= SCHEDULE["min_order"]
+    assert nm.max() < SCHEDULE["max_order"]
+    assert (full["ngauss"] == 2 * nm).all()
+
+
+def test_q_sums_equal_reference_sums_of_device_t(full):
+    worst = 0.0
+    for i in range(N_GRAINS):
+        qs, qe = O.tmatrix_q(full["T"][i], int(full["nmax"][i]))
+        for got, ref in ((full["q"][i, 2], qs), (full["q"][i, 3], qe)):
+            err = abs(got - ref) / abs(ref)
+            worst = max(worst, err)
+            assert err <= SUM_TOL, (i, got, ref)
+    print("worst relative Q-sum difference %.3g" % worst)
+
+
+def test_one_round_at_converged_orders_same_doubles(ctx, full):
+    fix = ctx.tmatrix_batch_fixed(full["r"], full["lam"], full["m"], full["d"],
+                                  full["nmax"], full["ngauss"])
+    assert (fix.status == 0).all()
+    assert np.array_equal(fix.q[:, 2:4], full["q"][:, 2:4])
+    for i in range(N_GRAINS):
+        assert np.array_equal(fix.tmatrix(i), full["T"][i]), i
+
+
+def test_oracle_parity_on_order_extremes(full):
+    nm = full["nmax"]
+    order = np.argsort(nm, kind="stable")
+    pick = {int(order[0]), int(order[len(order) // 2]), int(order[-1]),
+            int(order[-2]), int(order[-3])}
+    rng = np.random.default_rng(2024)
+    pick.update(int(i) for i in rng.choice(N_GRAINS, 5, replace=False))
+    pick.add(1234)  # conditioning-limited at the rounding level
+    worst = 0.0
+    for i in sorted(pick):
+        N, ng = int(nm[i]), int(full["ngauss"][i])
+        args = (full["r"][i], full["lam"], full["m"][i], full["d"][i], N, ng)
+        T, q = H.oracle_at(*args)
+        t_s, q_s = H.oracle_sensitivity(*args, T, q)
+        t_tol = max(H.T_TOL, 4 * t_s)
+        q_tol = max(H.Q_TOL, 4 * q_s)
+        err = H.t_error(full["T"][i], T, N)
+        worst = max(worst, err / t_tol)
+        print("grain %d order %d: T err %.3g (oracle sensitivity %.3g)" % (i, N, err, t_s))
+        assert err <= t_tol, (i, N, err, t_s)
+        for j in range(4):
+            assert abs(full["q"][i, j] - q[j]) <= q_tol * abs(q[j]), (i, j, q_s)
+    print("worst T error / bound %.3g" % worst)

@@ -234,6 +234,17 @@ def run_ours(args):
                              SCHEDULE["gauss_legendre_factor"], 0,
                              SCHEDULE["tolerance"])
     P = _lib.ptr
+    # untimed: the block-kernel dispatch table tuned on these grains at their
+    # converged orders (every family in every size bucket it can run)
+    conv = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+    table, tune_ms = ctx.autotune(r, lam, m, d, conv.nmax.copy(),
+                                  conv.ngauss.copy(), reps=3)
+    autotune = {"table": [Context.FAMILIES[f] for f in table],
+                "buckets": ["nb<=8", "9..16", "17..32", "33..64", "65..128"],
+                "median_ms": [[round(float(x), 4) for x in row] for row in tune_ms],
+                "what": "per size bucket, median ms per batch of each kernel "
+                        "family (columns: %s; -1 not run), buckets serialised"
+                        % ", ".join(Context.FAMILIES)}
     _lib.check(h, lib.tmx_batch_upload(h, N_GRAINS, P(r), P(lam), P(mr), P(mi),
                                        P(d), sched), "upload")
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda:%d" % local)
@@ -467,6 +478,7 @@ def run_ours(args):
             "phases_ms_per_step": {"blocks": bk_ms[0] / args.steps,
                                    "tables": tb_ms[0] / args.steps},
             "gpu_launches": int(launches),
+            "autotune": autotune,
             "plain_gpu": plain,
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "gradient": grad,

@@ -65,6 +65,10 @@ SIGNATURES = {
     "tmx_profile_read": (ctypes.c_int, [_VP, ctypes.c_int, _D,
                                         ctypes.POINTER(ctypes.c_int64), _D]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
+    "tmx_get_dispatch": (ctypes.c_int, [_VP, _I32]),
+    "tmx_set_dispatch": (ctypes.c_int, [_VP, _I32]),
+    "tmx_autotune": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D, _D, _D,
+                                    _I32, _I32, ctypes.c_int, _D]),
     "tmx_orientation_coefficients": (ctypes.c_int, [ctypes.c_int, ctypes.c_double,
                                                      ctypes.c_int, _VP, _VP, _D]),
     "tmx_shape_distribution": (ctypes.c_int, [ctypes.c_int, ctypes.c_int,

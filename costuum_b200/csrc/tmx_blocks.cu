@@ -1606,28 +1606,56 @@ static void launch_variant(const TmxBlockArgs &a, size_t smem,
   k_blocks<TR, TC, NT, MINB><<<a.nitems, NT, smem, stream>>>(a, smem);
 }
 
+int tmx_block_family_capacity(int family) {
+  switch (family) {
+  case TMX_BLOCKS_WARP_DFMA:
+    return 8;
+  case TMX_BLOCKS_WARP_DMMA:
+    return 16;
+  case TMX_BLOCKS_CTA32:
+    return 32;
+  case TMX_BLOCKS_CTA64:
+    return 64;
+  case TMX_BLOCKS_CTA:
+    return TMX_MAX_NB;
+  default:
+    return 0;
+  }
+}
+
+// The family given in a.family (set by the host's dispatch table), else the
+// smallest one whose capacity covers a.max_nb. A family whose capacity is
+// below an item's class size flags that grain TMX_ST_TOO_LARGE.
 void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
   if (a.nitems <= 0) {
     return;
   }
-  if (a.max_nb <= 8) {
+  int f = a.family;
+  if (f < 0 || f >= TMX_BLOCK_FAMILIES) {
+    f = (a.max_nb <= 8)    ? TMX_BLOCKS_WARP_DFMA
+        : (a.max_nb <= 16) ? TMX_BLOCKS_WARP_DMMA
+        : (a.max_nb <= 32) ? TMX_BLOCKS_CTA32
+        : (a.max_nb <= 64) ? TMX_BLOCKS_CTA64
+                           : TMX_BLOCKS_CTA;
+  }
+  switch (f) {
+  case TMX_BLOCKS_WARP_DFMA:
     launch_warp_variant<1, 2, 4, false>(a, stream);
     return;
-  }
-  if (a.max_nb <= 16) {
+  case TMX_BLOCKS_WARP_DMMA:
     launch_warp_variant<1, 1, 3, true>(a, stream);
     return;
-  }
-  if (a.max_nb <= 32) {
+  case TMX_BLOCKS_CTA32:
     launch_cta32(a, stream);
     return;
-  }
-  if (a.max_nb <= 64) {
+  case TMX_BLOCKS_CTA64:
     launch_cta64(a, stream);
     return;
+  default: {
+    const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
+    launch_variant<4, 4, 256, 1>(a, smem, stream);
   }
-  const size_t smem = tmx_block_smem_bytes(a.max_nb, a.chunk_nodes);
-  launch_variant<4, 4, 256, 1>(a, smem, stream);
+  }
 }
 
 // ----------------------------------------------------------- convergence --

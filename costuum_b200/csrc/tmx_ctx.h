@@ -85,6 +85,12 @@ struct tmx_ctx {
   // the profile), so that a profiled batch creates none
   std::vector<cudaEvent_t> prof_pool;
   size_t prof_used = 0;
+  // block-kernel family per size bucket (tmx_set_dispatch, tmx_autotune)
+  int32_t dispatch[TMX_DISPATCH_BUCKETS] = {0, 1, 2, 3, 4};
+  // autotuning: bucket launches serialised on the round's stream and timed
+  // (bucket, start, end)
+  bool tuning = false;
+  std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> tune_ev;
   std::vector<double> survey_cache; // survey-model flops per order, this glf
   int survey_glf = 0, survey_min = 0;
   double flops_survey = 0.; // survey-model flops of the last batch

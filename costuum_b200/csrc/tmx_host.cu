@@ -170,6 +170,22 @@ static int ensure_wigner(tmx_ctx *ctx,
 
 // number of members of class `cls` of block m at order N (see describe() in
 // tmx_blocks.cu)
+static_assert(TMX_FAMILY_WARP_DFMA == TMX_BLOCKS_WARP_DFMA &&
+                  TMX_FAMILY_WARP_DMMA == TMX_BLOCKS_WARP_DMMA &&
+                  TMX_FAMILY_CTA32 == TMX_BLOCKS_CTA32 &&
+                  TMX_FAMILY_CTA64 == TMX_BLOCKS_CTA64 &&
+                  TMX_FAMILY_CTA == TMX_BLOCKS_CTA &&
+                  TMX_DISPATCH_FAMILIES == TMX_BLOCK_FAMILIES,
+              "public and kernel family numbers");
+
+// dispatch bucket of a launch whose largest class has nb members, and the
+// largest class size of each bucket
+static int dispatch_bucket(int nb) {
+  return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
+}
+static const int kBucketTop[TMX_DISPATCH_BUCKETS] = {8, 16, 32, 64, TMX_MAX_NB};
+static const int32_t kDefaultDispatch[TMX_DISPATCH_BUCKETS] = {0, 1, 2, 3, 4};
+
 int tmx_host_class_size(int N, int m, int cls) {
   if (m == 0) {
     const int n0 = (cls & 1) ? 1 : 2;
@@ -656,7 +672,8 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     }
     if (i1 > i0) {
       cudaStream_t bs = st;
-      if (nbuckets > 0) {
+      // while tuning, every bucket runs alone on the round's stream
+      if (nbuckets > 0 && !ctx->tuning) {
         bs = aux[(nbuckets - 1) & 1];
         if (!fork) {
           CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
@@ -681,6 +698,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       B.max_nb = inb[i0];
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
       B.lu = keep_lu ? (cplx *)ctx->lu.p : nullptr;
+      B.family = ctx->dispatch[dispatch_bucket(B.max_nb)];
       // the round's flops are booked on its first launch
       double fl = 0.;
       if (ctx->profiling && nbuckets == 1) {
@@ -692,8 +710,18 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       if ((rc = prof_begin(ctx, 0, &pe, bs))) {
         return rc;
       }
+      cudaEvent_t ta = nullptr, tb = nullptr;
+      if (ctx->tuning) {
+        CK(cudaEventCreate(&ta));
+        CK(cudaEventCreate(&tb));
+        CK(cudaEventRecord(ta, bs));
+      }
       tmx_launch_blocks(B, bs);
       LAUNCHED();
+      if (ctx->tuning) {
+        CK(cudaEventRecord(tb, bs));
+        ctx->tune_ev.emplace_back(dispatch_bucket(B.max_nb), ta, tb);
+      }
       if ((rc = prof_end(ctx, 0, pe, fl, bs))) {
         return rc;
       }
@@ -991,6 +1019,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = (kl + 1) / 2;
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+      B.family = ctx->dispatch[dispatch_bucket(B.max_nb)];
       double fl = 0.;
       for (int s = 0; s < G; ++s) {
         for (int c = 0; c < 4; ++c) {
@@ -1161,6 +1190,117 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
     return TMX_OK;
   }
   return run_blocks(ctx, p2);
+}
+
+int tmx_get_dispatch(const tmx_ctx *ctx, int32_t *family) {
+  if (!ctx || !family) {
+    return TMX_ERR_INVALID;
+  }
+  memcpy(family, ctx->dispatch, sizeof(ctx->dispatch));
+  return TMX_OK;
+}
+
+int tmx_set_dispatch(tmx_ctx *ctx, const int32_t *family) {
+  if (!ctx || !family) {
+    return TMX_ERR_INVALID;
+  }
+  for (int b = 0; b < TMX_DISPATCH_BUCKETS; ++b) {
+    if (family[b] < 0 || family[b] >= TMX_DISPATCH_FAMILIES ||
+        tmx_block_family_capacity(family[b]) < kBucketTop[b]) {
+      return fail(ctx, TMX_ERR_INVALID, "block family cannot run this size bucket");
+    }
+  }
+  memcpy(ctx->dispatch, family, sizeof(ctx->dispatch));
+  return TMX_OK;
+}
+
+static void drop_tune_events(tmx_ctx *ctx) {
+  for (auto &e : ctx->tune_ev) {
+    cudaEventDestroy(std::get<1>(e));
+    cudaEventDestroy(std::get<2>(e));
+  }
+  ctx->tune_ev.clear();
+}
+
+int tmx_autotune(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                 const double *wavelength, const double *mr, const double *mi,
+                 const double *axis_ratio, const int32_t *nmax,
+                 const int32_t *ngauss, int reps, double *ms) {
+  if (!ctx || n <= 0 || reps < 1) {
+    return TMX_ERR_INVALID;
+  }
+  int32_t saved[TMX_DISPATCH_BUCKETS];
+  memcpy(saved, ctx->dispatch, sizeof(saved));
+  // per-batch milliseconds of each bucket under each family
+  std::vector<double> t[TMX_DISPATCH_BUCKETS][TMX_DISPATCH_FAMILIES];
+  int rc = TMX_OK;
+  ctx->tuning = true;
+  for (int f = 0; f < TMX_DISPATCH_FAMILIES && rc == TMX_OK; ++f) {
+    // family f in every bucket it can run, the default elsewhere
+    bool any = false;
+    for (int b = 0; b < TMX_DISPATCH_BUCKETS; ++b) {
+      const bool can = tmx_block_family_capacity(f) >= kBucketTop[b];
+      ctx->dispatch[b] = can ? f : kDefaultDispatch[b];
+      any = any || can;
+    }
+    if (!any) {
+      continue;
+    }
+    // one untimed batch, then reps timed ones
+    for (int r = 0; r <= reps && rc == TMX_OK; ++r) {
+      drop_tune_events(ctx);
+      rc = tmx_tmatrix_batch_fixed(ctx, n, r_ev, wavelength, mr, mi, axis_ratio,
+                                   nmax, ngauss);
+      if (rc != TMX_OK) {
+        break;
+      }
+      double sum[TMX_DISPATCH_BUCKETS] = {0.};
+      bool seen[TMX_DISPATCH_BUCKETS] = {false};
+      for (auto &e : ctx->tune_ev) {
+        float x = 0.f;
+        if (cudaEventSynchronize(std::get<2>(e)) != cudaSuccess ||
+            cudaEventElapsedTime(&x, std::get<1>(e), std::get<2>(e)) != cudaSuccess) {
+          rc = fail(ctx, TMX_ERR_CUDA, "autotune: event timing failed");
+          break;
+        }
+        sum[std::get<0>(e)] += x;
+        seen[std::get<0>(e)] = true;
+      }
+      for (int b = 0; b < TMX_DISPATCH_BUCKETS && r > 0; ++b) {
+        if (seen[b] && ctx->dispatch[b] == f) {
+          t[b][f].push_back(sum[b]);
+        }
+      }
+    }
+  }
+  ctx->tuning = false;
+  drop_tune_events(ctx);
+  memcpy(ctx->dispatch, saved, sizeof(saved));
+  if (rc != TMX_OK) {
+    return rc;
+  }
+  for (int b = 0; b < TMX_DISPATCH_BUCKETS; ++b) {
+    double best = 0.;
+    bool have = false;
+    for (int f = 0; f < TMX_DISPATCH_FAMILIES; ++f) {
+      double med = -1.;
+      std::vector<double> &v = t[b][f];
+      if (!v.empty()) {
+        std::sort(v.begin(), v.end());
+        med = (v.size() & 1) ? v[v.size() / 2]
+                             : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
+        if (!have || med < best) {
+          have = true;
+          best = med;
+          ctx->dispatch[b] = f;
+        }
+      }
+      if (ms) {
+        ms[b * TMX_DISPATCH_FAMILIES + f] = med;
+      }
+    }
+  }
+  return TMX_OK;
 }
 
 int tmx_batch_results(tmx_ctx *ctx, int32_t *nmax, int32_t *ngauss,

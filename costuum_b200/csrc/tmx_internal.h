@@ -83,6 +83,16 @@ enum {
 
 #define TMX_MAX_NB 128 // largest class size handled on chip
 
+// block-kernel families (values of tmx_block_family in tmx.h)
+enum {
+  TMX_BLOCKS_WARP_DFMA = 0, // warp per item, DFMA register tiles, nb <= 8
+  TMX_BLOCKS_WARP_DMMA = 1, // warp per item, DMMA m8n8k4 tiles, nb <= 16
+  TMX_BLOCKS_CTA32 = 2,     // four warps per item, nb <= 32
+  TMX_BLOCKS_CTA64 = 3,     // eight warps per item, nb <= 64
+  TMX_BLOCKS_CTA = 4,       // 256 threads per item, 4x4 tiles, nb <= 128
+  TMX_BLOCK_FAMILIES = 5
+};
+
 // orders above max(nmax, |z|) at which the Bessel ratio recurrence starts
 // when no fixed start is requested
 #define TMX_BESSEL_MARGIN 48

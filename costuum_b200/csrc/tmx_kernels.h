@@ -57,7 +57,10 @@ struct TmxBlockArgs {
   int max_nb;                  // largest class size in this launch
   double2 *lu = nullptr;       // if set: LU factors + pivots saved per item
                                // at the item's scratch offset (2 nb^2)
+  int family = -1;             // tmx_block_family to run, -1: by max_nb
 };
+// largest class size each tmx_block_family can run
+int tmx_block_family_capacity(int family);
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes);
 void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream);
 

@@ -148,6 +148,50 @@ class Context:
             _lib.check(self._h, rc, "tmx_tmatrix_batch_fixed")
             return self._results(n)
 
+    # block-kernel families (tmx_block_family) and the largest class size of
+    # each dispatch bucket
+    FAMILIES = ("warp_dfma", "warp_dmma", "cta32", "cta64", "cta")
+    BUCKET_TOP = (8, 16, 32, 64, 128)
+
+    def get_dispatch(self):
+        """Block-kernel family of each class-size bucket (<= 8, 9..16,
+        17..32, 33..64, 65..128) as an int32 array of 5."""
+        out = np.zeros(5, np.int32)
+        rc = _lib.load().tmx_get_dispatch(self._h, _lib.iptr(out))
+        _lib.check(self._h, rc, "tmx_get_dispatch")
+        return out
+
+    def set_dispatch(self, families):
+        fam = np.ascontiguousarray(families, np.int32).ravel()
+        if fam.size != 5:
+            raise ValueError("one family per bucket (5)")
+        with self._lock:
+            rc = _lib.load().tmx_set_dispatch(self._h, _lib.iptr(fam))
+            _lib.check(self._h, rc, "tmx_set_dispatch")
+
+    def autotune(self, r_ev, wavelength, m, axis_ratio, nmax, ngauss, reps=3):
+        """Time every block-kernel family on the given grains at fixed orders
+        and keep the fastest per bucket. Returns (table, ms) with ms[bucket,
+        family] the median milliseconds per batch (-1: not run)."""
+        r_ev = np.ascontiguousarray(r_ev, np.float64).ravel()
+        n = r_ev.size
+        wl = np.ascontiguousarray(np.broadcast_to(wavelength, (n,)), np.float64)
+        mm = np.broadcast_to(np.asarray(m, np.complex128), (n,))
+        mr = np.ascontiguousarray(mm.real)
+        mi = np.ascontiguousarray(mm.imag)
+        d = np.ascontiguousarray(np.broadcast_to(axis_ratio, (n,)), np.float64)
+        nm = np.ascontiguousarray(np.broadcast_to(nmax, (n,)), np.int32)
+        ng = np.ascontiguousarray(np.broadcast_to(ngauss, (n,)), np.int32)
+        ms = np.zeros((5, 5), np.float64)
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_autotune(self._h, n, _lib.ptr(r_ev), _lib.ptr(wl),
+                                  _lib.ptr(mr), _lib.ptr(mi), _lib.ptr(d),
+                                  _lib.iptr(nm), _lib.iptr(ng), int(reps),
+                                  _lib.ptr(ms))
+            _lib.check(self._h, rc, "tmx_autotune")
+        return self.get_dispatch(), ms
+
     def tmatrix_batch_calculator(self, r_ev, wavelength, m, axis_ratio,
                                  maximum_order=200, tolerance=1e-4,
                                  gauss_legendre_factor=2, maximum_ngauss=500):

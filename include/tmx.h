@@ -161,6 +161,45 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
  * counted only for batches computed while profiling is enabled, else 0. */
 double tmx_batch_flops_survey(const tmx_ctx *ctx);
 
+/* ------------------------------------------------ block-kernel dispatch ---
+ *
+ * The class items of a block round are launched in buckets by class size nb:
+ * bucket 0 nb <= 8, 1 nb 9..16, 2 nb 17..32, 3 nb 33..64, 4 nb 65..128. Each
+ * bucket runs one kernel family; a family can run a bucket when its capacity
+ * covers the bucket's sizes. The table applies to the block rounds and the
+ * order loop's m = 0 blocks of tmx_tmatrix_batch, tmx_tmatrix_batch_fixed
+ * and the gradients; the plain path and tmx_tmatrix_fixed_noalloc keep the
+ * default. Families compute the same sums in different orders, so results
+ * differ in the last bits between tables. */
+enum tmx_block_family {
+  TMX_FAMILY_WARP_DFMA = 0, /* one warp per item, DFMA register tiles; nb <= 8 */
+  TMX_FAMILY_WARP_DMMA = 1, /* one warp per item, DMMA m8n8k4 tiles; nb <= 16 */
+  TMX_FAMILY_CTA32 = 2,     /* four warps per item; nb <= 32 */
+  TMX_FAMILY_CTA64 = 3,     /* eight warps per item; nb <= 64 */
+  TMX_FAMILY_CTA = 4        /* 256 threads per item, 4x4 tiles; nb <= 128 */
+};
+#define TMX_DISPATCH_BUCKETS 5
+#define TMX_DISPATCH_FAMILIES 5
+
+/* family[5]: the family of each bucket (default 0, 1, 2, 3, 4). */
+int tmx_get_dispatch(const tmx_ctx *ctx, int32_t *family);
+/* Sets the family of each bucket; TMX_ERR_INVALID (table unchanged) if a
+ * family cannot run its bucket. */
+int tmx_set_dispatch(tmx_ctx *ctx, const int32_t *family);
+
+/* Autotuner for the dispatch table: computes the given grains at fixed
+ * orders (as tmx_tmatrix_batch_fixed) reps times with each family in every
+ * bucket it can run, the buckets' launches serialised on the library stream
+ * and timed with CUDA events, then sets each bucket that the sample reaches
+ * to the family with the smallest median time (ties: the lower family).
+ * ms (may be NULL) receives [bucket][family] median milliseconds per batch,
+ * -1 where the family cannot run the bucket or the sample has no item of
+ * that size. Afterwards the last tuning batch is the current batch. */
+int tmx_autotune(tmx_ctx *ctx, int64_t n, const double *r_ev,
+                 const double *wavelength, const double *mr, const double *mi,
+                 const double *axis_ratio, const int32_t *nmax,
+                 const int32_t *ngauss, int reps, double *ms);
+
 /* ------------------------------------------------ averaged observables ---
  *
  * Orientation distribution expansion coefficients p_0 .. p_order

@@ -148,6 +148,15 @@ static inline double item_flops(int nb, int m, int ng) {
   return 8. * terms * b * b * ng + (8. / 3.) * b * b * b + 8. * b * b * b;
 }
 
+// dispatch bucket of a launch whose largest class has nb members, and the
+// family the context's table names for it
+static inline int dispatch_bucket(int nb) {
+  return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
+}
+static inline int dispatch_family(const tmx_ctx *ctx, int max_nb) {
+  return ctx->dispatch[dispatch_bucket(max_nb)];
+}
+
 static inline int prof_event(tmx_ctx *ctx, cudaEvent_t *e) {
   if (ctx->prof_used == ctx->prof_pool.size()) {
     cudaEvent_t n;

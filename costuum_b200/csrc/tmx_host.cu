@@ -178,11 +178,7 @@ static_assert(TMX_FAMILY_WARP_DFMA == TMX_BLOCKS_WARP_DFMA &&
                   TMX_DISPATCH_FAMILIES == TMX_BLOCK_FAMILIES,
               "public and kernel family numbers");
 
-// dispatch bucket of a launch whose largest class has nb members, and the
-// largest class size of each bucket
-static int dispatch_bucket(int nb) {
-  return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
-}
+// largest class size of each dispatch bucket
 static const int kBucketTop[TMX_DISPATCH_BUCKETS] = {8, 16, 32, 64, TMX_MAX_NB};
 static const int32_t kDefaultDispatch[TMX_DISPATCH_BUCKETS] = {0, 1, 2, 3, 4};
 
@@ -698,7 +694,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       B.max_nb = inb[i0];
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
       B.lu = keep_lu ? (cplx *)ctx->lu.p : nullptr;
-      B.family = ctx->dispatch[dispatch_bucket(B.max_nb)];
+      B.family = dispatch_family(ctx, B.max_nb);
       // the round's flops are booked on its first launch
       double fl = 0.;
       if (ctx->profiling && nbuckets == 1) {
@@ -1019,7 +1015,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = (kl + 1) / 2;
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
-      B.family = ctx->dispatch[dispatch_bucket(B.max_nb)];
+      B.family = dispatch_family(ctx, B.max_nb);
       double fl = 0.;
       for (int s = 0; s < G; ++s) {
         for (int c = 0; c < 4; ++c) {
@@ -1279,25 +1275,31 @@ int tmx_autotune(tmx_ctx *ctx, int64_t n, const double *r_ev,
   if (rc != TMX_OK) {
     return rc;
   }
+  // a bucket leaves its current family only for one at least kTuneMargin
+  // faster: differences within timing noise keep the table as it was
+  const double kTuneMargin = 0.05;
   for (int b = 0; b < TMX_DISPATCH_BUCKETS; ++b) {
-    double best = 0.;
-    bool have = false;
+    double med[TMX_DISPATCH_FAMILIES];
+    int best = -1;
     for (int f = 0; f < TMX_DISPATCH_FAMILIES; ++f) {
-      double med = -1.;
+      med[f] = -1.;
       std::vector<double> &v = t[b][f];
       if (!v.empty()) {
         std::sort(v.begin(), v.end());
-        med = (v.size() & 1) ? v[v.size() / 2]
-                             : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
-        if (!have || med < best) {
-          have = true;
-          best = med;
-          ctx->dispatch[b] = f;
+        med[f] = (v.size() & 1) ? v[v.size() / 2]
+                                : 0.5 * (v[v.size() / 2 - 1] + v[v.size() / 2]);
+        if (best < 0 || med[f] < med[best]) {
+          best = f;
         }
       }
       if (ms) {
-        ms[b * TMX_DISPATCH_FAMILIES + f] = med;
+        ms[b * TMX_DISPATCH_FAMILIES + f] = med[f];
       }
+    }
+    const int cur = saved[b];
+    if (best >= 0 && best != cur &&
+        (med[cur] < 0. || med[best] < (1. - kTuneMargin) * med[cur])) {
+      ctx->dispatch[b] = best;
     }
   }
   return TMX_OK;

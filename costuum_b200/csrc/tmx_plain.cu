@@ -144,6 +144,7 @@ int m0_step(tmx_ctx *ctx, const std::vector<int32_t> &g, const std::vector<int> 
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = its[i0].nb;
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+      B.family = dispatch_family(ctx, B.max_nb);
       tmx_launch_blocks(B, st);
       LAUNCHED();
     }

@@ -1002,6 +1002,7 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
         B.status = (int32_t *)ctx->status.p;
         B.max_nb = max_nb;
         B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
+        B.family = dispatch_family(ctx, max_nb);
         B.lu = (cplx *)ctx->lu.p;
         if (!ctx->lu_ready) {
           tmx_launch_blocks(B, st);

@@ -166,11 +166,11 @@ double tmx_batch_flops_survey(const tmx_ctx *ctx);
  * The class items of a block round are launched in buckets by class size nb:
  * bucket 0 nb <= 8, 1 nb 9..16, 2 nb 17..32, 3 nb 33..64, 4 nb 65..128. Each
  * bucket runs one kernel family; a family can run a bucket when its capacity
- * covers the bucket's sizes. The table applies to the block rounds and the
- * order loop's m = 0 blocks of tmx_tmatrix_batch, tmx_tmatrix_batch_fixed
- * and the gradients; the plain path and tmx_tmatrix_fixed_noalloc keep the
- * default. Families compute the same sums in different orders, so results
- * differ in the last bits between tables. */
+ * covers the bucket's sizes. The table applies to every block launch of the
+ * context (batched, fixed-order and calculator schedules, gradients);
+ * tmx_tmatrix_fixed_noalloc keeps the default. Families compute the same
+ * sums in different orders, so results differ in the last bits between
+ * tables. */
 enum tmx_block_family {
   TMX_FAMILY_WARP_DFMA = 0, /* one warp per item, DFMA register tiles; nb <= 8 */
   TMX_FAMILY_WARP_DMMA = 1, /* one warp per item, DMMA m8n8k4 tiles; nb <= 16 */
@@ -190,8 +190,9 @@ int tmx_set_dispatch(tmx_ctx *ctx, const int32_t *family);
 /* Autotuner for the dispatch table: computes the given grains at fixed
  * orders (as tmx_tmatrix_batch_fixed) reps times with each family in every
  * bucket it can run, the buckets' launches serialised on the library stream
- * and timed with CUDA events, then sets each bucket that the sample reaches
- * to the family with the smallest median time (ties: the lower family).
+ * and timed with CUDA events, then moves each bucket that the sample reaches
+ * to the family with the smallest median time if that is at least 5 % below
+ * the median of its current family (else the bucket keeps its family).
  * ms (may be NULL) receives [bucket][family] median milliseconds per batch,
  * -1 where the family cannot run the bucket or the sample has no item of
  * that size. Afterwards the last tuning batch is the current batch. */

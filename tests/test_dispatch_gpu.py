@@ -6,8 +6,9 @@ at fixed orders whose parity classes cover all five buckets (order 40:
 classes of 1..40 members; order 70: up to 70), and compared with the oracle
 (T within 1e-9 relative per m block, or 4x the oracle's own change under a
 1e-15 change of r_ev where that is larger; the full-T sums within 1e-8).
-The autotuner must time each family in each bucket it can serve, keep the
-fastest, and leave results that still match the oracle.
+The autotuner must time each family in each bucket it can serve, move a
+bucket only to the fastest family and only when it beats the current one by
+5 %, and leave results that still match the oracle.
 """
 import numpy as np
 import pytest
@@ -83,8 +84,13 @@ def test_autotune(ctx, refs):
                     assert ms[b, f] > 0, (b, f)
                 else:
                     assert ms[b, f] == -1, (b, f)
-            timed = [ms[b, f] for f in range(5) if ms[b, f] > 0]
-            assert ms[b, table[b]] == min(timed), b
+            # the fastest family, when at least 5 % faster than the default
+            best = min(ms[b, f] for f in range(5) if ms[b, f] > 0)
+            if table[b] != DEFAULT[b]:
+                assert ms[b, table[b]] == best, b
+                assert best < 0.95 * ms[b, DEFAULT[b]], b
+            else:
+                assert best >= 0.95 * ms[b, DEFAULT[b]], b
         _check(ctx.tmatrix_batch_fixed(R_EV, LAM, M, D, NMAX, NGAUSS), refs)
     finally:
         ctx.set_dispatch(DEFAULT)

@@ -32,10 +32,12 @@ struct tmx_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;  // every launch unless noted (high priority)
   cudaStream_t stream2 = nullptr; // blocks of grains that converged while the
-                                  // order loop continues (low priority)
-  cudaStream_t aux[4] = {};       // further class-size buckets of a block
+  cudaStream_t stream3 = nullptr; // order loop continues (low priority);
+                                  // rounds alternate between the two, so a
+                                  // round starts while the previous drains
+  cudaStream_t aux[6] = {};       // further class-size buckets of a block
                                   // round: [0, 1] beside stream, [2, 3]
-                                  // beside stream2
+                                  // beside stream2, [4, 5] beside stream3
   cudaMemPool_t pool = nullptr;   // device memory of this context; keeps
                                   // freed blocks for reuse (no release)
   std::string err;

@@ -243,6 +243,8 @@ int tmx_create(tmx_ctx **out, int device) {
                                    prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&ctx->stream2, cudaStreamNonBlocking,
                                    prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->stream3, cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&ctx->aux[0], cudaStreamNonBlocking,
                                    prio_hi) != cudaSuccess ||
       cudaStreamCreateWithPriority(&ctx->aux[1], cudaStreamNonBlocking,
@@ -251,10 +253,15 @@ int tmx_create(tmx_ctx **out, int device) {
                                    prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&ctx->aux[3], cudaStreamNonBlocking,
                                    prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[4], cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&ctx->aux[5], cudaStreamNonBlocking,
+                                   prio_lo) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->pinned, 64) != cudaSuccess) {
     cudaGetLastError();
-    for (cudaStream_t x : {ctx->stream, ctx->stream2, ctx->aux[0], ctx->aux[1],
-                           ctx->aux[2], ctx->aux[3]}) {
+    for (cudaStream_t x : {ctx->stream, ctx->stream2, ctx->stream3, ctx->aux[0],
+                           ctx->aux[1], ctx->aux[2], ctx->aux[3], ctx->aux[4],
+                           ctx->aux[5]}) {
       if (x) {
         cudaStreamDestroy(x);
       }
@@ -279,6 +286,7 @@ int tmx_create(tmx_ctx **out, int device) {
     cudaGetLastError();
     cudaStreamDestroy(ctx->stream);
     cudaStreamDestroy(ctx->stream2);
+    cudaStreamDestroy(ctx->stream3);
     for (cudaStream_t x : ctx->aux) {
       cudaStreamDestroy(x);
     }
@@ -298,6 +306,9 @@ void tmx_destroy(tmx_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->stream2) {
     cudaStreamSynchronize(ctx->stream2);
+  }
+  if (ctx->stream3) {
+    cudaStreamSynchronize(ctx->stream3);
   }
   for (cudaStream_t x : ctx->aux) {
     if (x) {
@@ -341,6 +352,9 @@ void tmx_destroy(tmx_ctx *ctx) {
   cudaStreamDestroy(ctx->stream);
   if (ctx->stream2) {
     cudaStreamDestroy(ctx->stream2);
+  }
+  if (ctx->stream3) {
+    cudaStreamDestroy(ctx->stream3);
   }
   for (cudaStream_t x : ctx->aux) {
     if (x) {
@@ -575,8 +589,9 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   }
   ctx->p2_scr_total = scr_total;
   if (keep_T && (size_t)t_total * sizeof(cplx) > ctx->T.cap) {
-    // growing T moves it: earlier rounds on the second stream must be done
+    // growing T moves it: earlier rounds on the round streams must be done
     CK(cudaStreamSynchronize(ctx->stream2));
+    CK(cudaStreamSynchronize(ctx->stream3));
   }
   if ((rc = (keep_T ? ensure_keep(ctx, ctx->T, std::max<int64_t>(1, t_total) * sizeof(cplx),
                                   t_base * sizeof(cplx))
@@ -598,9 +613,10 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     return rc;
   }
   if (ctx->q.cap < (size_t)2 * ctx->n * sizeof(double)) {
-    // Q sums of every grain of the batch; rounds on the second stream may
+    // Q sums of every grain of the batch; rounds on the round streams may
     // still write the old buffer
     CK(cudaStreamSynchronize(ctx->stream2));
+    CK(cudaStreamSynchronize(ctx->stream3));
     if ((rc = ensure(ctx, ctx->q, std::max<int64_t>(1, 2 * ctx->n) * sizeof(double)))) {
       return rc;
     }
@@ -655,7 +671,9 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   // the others on the two auxiliary streams beside it, so that the smaller
   // buckets fill the SMs that the tail of the larger one leaves idle; the
   // round ends (Q sums, buffer release) when all of them are done
-  cudaStream_t *aux = (st == ctx->stream) ? &ctx->aux[0] : &ctx->aux[2];
+  cudaStream_t *aux = (st == ctx->stream)    ? &ctx->aux[0]
+                      : (st == ctx->stream2) ? &ctx->aux[2]
+                                             : &ctx->aux[4];
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> joins;
   int nbuckets = 0;
@@ -1054,7 +1072,8 @@ int tmx_batch_compute(tmx_ctx *ctx) {
                        (int32_t *)ctx->done.p + n + done_seen, nact * sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
     if (!pending.empty()) {
-      if ((rc = run_blocks_round(ctx, pending, ctx->stream2, t_next, rounds > 0,
+      if ((rc = run_blocks_round(ctx, pending, (rounds & 1) ? ctx->stream3 : ctx->stream2,
+                                 t_next, rounds > 0,
                                  &t_next, true))) {
         return rc;
       }
@@ -1111,13 +1130,15 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   if (rounds == 0) {
     return run_blocks(ctx, p2);
   }
-  // the last round on this stream, then wait for the second stream's rounds
+  // the last round on this stream, then wait for the round streams
   if ((rc = run_blocks_round(ctx, p2, st, t_next, true, &t_next, true))) {
     return rc;
   }
   cudaEvent_t rounds_done;
   CK(cudaEventCreateWithFlags(&rounds_done, cudaEventDisableTiming));
   CK(cudaEventRecord(rounds_done, ctx->stream2));
+  CK(cudaStreamWaitEvent(st, rounds_done, 0));
+  CK(cudaEventRecord(rounds_done, ctx->stream3));
   CK(cudaStreamWaitEvent(st, rounds_done, 0));
   CK(cudaEventDestroy(rounds_done));
   return finish_blocks(ctx, t_next, rounds + 1);
@@ -1186,6 +1207,21 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
     return TMX_OK;
   }
   return run_blocks(ctx, p2);
+}
+
+void *tmx_host_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (bytes == 0 || cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+void tmx_host_free(void *p) {
+  if (p) {
+    cudaFreeHost(p);
+  }
 }
 
 int tmx_get_dispatch(const tmx_ctx *ctx, int32_t *family) {

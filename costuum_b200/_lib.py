@@ -65,6 +65,8 @@ SIGNATURES = {
     "tmx_profile_read": (ctypes.c_int, [_VP, ctypes.c_int, _D,
                                         ctypes.POINTER(ctypes.c_int64), _D]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
+    "tmx_host_alloc": (ctypes.c_void_p, [ctypes.c_size_t]),
+    "tmx_host_free": (None, [ctypes.c_void_p]),
     "tmx_get_dispatch": (ctypes.c_int, [_VP, _I32]),
     "tmx_set_dispatch": (ctypes.c_int, [_VP, _I32]),
     "tmx_autotune": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _D, _D, _D, _D,

@@ -7,6 +7,7 @@ Qsca and Qext converge, then every m block) for every grain at once.
 """
 import ctypes
 import threading
+import weakref
 
 import numpy as np
 
@@ -69,6 +70,48 @@ class BatchResult:
         return out
 
 
+class _PinnedPool:
+    """Page-locked host buffers for result arrays. A result views a pooled
+    buffer; the buffer returns to the pool when the last view of it is
+    released, so repeated calls reuse the same page-locked memory and their
+    device-to-host copies run as direct DMA."""
+
+    def __init__(self):
+        self._free = []  # (capacity, address)
+        self._closed = False
+
+    def _release(self, cap, ptr):
+        if self._closed:
+            _lib.load().tmx_host_free(ptr)
+        else:
+            self._free.append((cap, ptr))
+
+    def array(self, shape):
+        count = int(np.prod(shape))
+        nbytes = max(8, 8 * count)
+        pick = None
+        for i, (cap, ptr) in enumerate(self._free):
+            if cap >= nbytes and (pick is None or cap < self._free[pick][0]):
+                pick = i
+        if pick is not None:
+            cap, ptr = self._free.pop(pick)
+        else:
+            cap = max(nbytes, 1 << 16)
+            ptr = _lib.load().tmx_host_alloc(cap)
+            if not ptr:
+                return np.empty(shape)  # pageable fallback
+        buf = (ctypes.c_char * cap).from_address(ptr)
+        weakref.finalize(buf, self._release, cap, ptr)
+        return np.frombuffer(buf, dtype=np.float64, count=count).reshape(shape)
+
+    def close(self):
+        self._closed = True
+        lib = _lib.load()
+        for _, ptr in self._free:
+            lib.tmx_host_free(ptr)
+        self._free = []
+
+
 class Context:
     """A CUDA device context: owns device buffers and cached tables."""
 
@@ -82,8 +125,11 @@ class Context:
         self._h = h
         self.device = device
         self._lock = threading.Lock()
+        self._pinned = _PinnedPool()
 
     def close(self):
+        if getattr(self, "_pinned", None):
+            self._pinned.close()
         if getattr(self, "_h", None):
             _lib.load().tmx_destroy(self._h)
             self._h = None
@@ -300,7 +346,7 @@ class Context:
         c = None if coefficients is None else np.ascontiguousarray(coefficients, np.float64)
         lib = _lib.load()
         n = self._last_n()
-        q = np.zeros((n, len(th), 3))
+        q = self._pinned.array((n, len(th), 3))
         with self._lock:
             rc = lib.tmx_batch_observables(self._h, len(th), _lib.ptr(th),
                                            None if c is None else _lib.ptr(c),
@@ -315,8 +361,8 @@ class Context:
         c = None if coefficients is None else np.ascontiguousarray(coefficients, np.float64)
         lib = _lib.load()
         n = self._last_n()
-        q = np.zeros((n, len(th), 3))
-        dq = np.zeros((n, len(th), 3, 4))
+        q = self._pinned.array((n, len(th), 3))
+        dq = self._pinned.array((n, len(th), 3, 4))
         with self._lock:
             rc = lib.tmx_batch_gradients(self._h, len(th), _lib.ptr(th),
                                          None if c is None else _lib.ptr(c),

@@ -23,6 +23,7 @@
 #ifndef TMX_H
 #define TMX_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -180,6 +181,12 @@ enum tmx_block_family {
 };
 #define TMX_DISPATCH_BUCKETS 5
 #define TMX_DISPATCH_FAMILIES 5
+
+/* Page-locked host memory (cudaMallocHost) for result arrays: device to
+ * host copies into it run as direct DMA instead of through the driver's
+ * staging buffers. NULL on failure; release with tmx_host_free. */
+void *tmx_host_alloc(size_t bytes);
+void tmx_host_free(void *p);
 
 /* family[5]: the family of each bucket (default 0, 1, 2, 3, 4). */
 int tmx_get_dispatch(const tmx_ctx *ctx, int32_t *family);

@@ -471,6 +471,11 @@ def run_ours(args):
                                         "blocks F_asm(N+1-m,2N,10)+F_lu+F_solve",
                          "flops_per_step": flops_survey,
                          "executed_tflops": executed,
+                         # launches of several streams overlap, so their summed
+                         # event time exceeds the step; the model flops over the
+                         # step time is the rate the whole step sustains
+                         "step_tflops": flops_survey / (ms_step * 1e-3) / 1e12,
+                         "step_frac": flops_survey / (ms_step * 1e-3) / 1e12 / dmma,
                          "launches": int(bk_n.value),
                          "share_of_step": bk_ms[0] / max(total, 1e-9),
                          "traffic": BLOCK_TRAFFIC_PER_LAUNCH,

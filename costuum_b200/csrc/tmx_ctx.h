@@ -87,6 +87,21 @@ struct tmx_ctx {
   // the profile), so that a profiled batch creates none
   std::vector<cudaEvent_t> prof_pool;
   size_t prof_used = 0;
+  // Block rounds of the last tmx_batch_compute, kept for the gradients: each
+  // round's tables, slot and item lists and LU factors (pool allocations
+  // released when the next batch starts). rounds_lu: they cover every grain
+  // of the batch, so the gradients need no second pass of the blocks.
+  struct RoundRec {
+    double *tab = nullptr, *nsc = nullptr;
+    TmxSlot *slots = nullptr;
+    TmxItem *items = nullptr;
+    cplx *lu = nullptr;
+    std::vector<int> nb; // class size per item (descending)
+    int64_t scr_total = 0;
+  };
+  std::vector<RoundRec> rounds_kept;
+  bool keep_rounds = false;
+  bool rounds_lu = false;
   // block-kernel family per size bucket (tmx_set_dispatch, tmx_autotune)
   int32_t dispatch[TMX_DISPATCH_BUCKETS] = {0, 1, 2, 3, 4};
   // autotuning: bucket launches serialised on the round's stream and timed
@@ -291,3 +306,4 @@ TMX_HIDDEN int tmx_run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &grains);
 // Blocks of the last batch again in one round (tmx_host.cu), so that the p2
 // buffers hold the whole schedule for the tangent kernels.
 extern "C" __attribute__((visibility("hidden"))) int tmx_rerun_blocks(tmx_ctx *ctx);
+extern "C" __attribute__((visibility("hidden"))) int tmx_release_rounds(tmx_ctx *ctx);

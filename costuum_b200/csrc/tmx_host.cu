@@ -412,6 +412,9 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   ctx->uploaded = false;
   ctx->have_batch = false;
   int rc;
+  if ((rc = tmx_release_rounds(ctx))) {
+    return rc;
+  }
 
   // ---- grains (host constants, as the reference computes them)
   std::vector<TmxGrain> gr(n);
@@ -645,6 +648,12 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     CK(cudaMallocFromPoolAsync((void **)&dslots, np2 * sizeof(TmxSlot), ctx->pool, st));
     CK(cudaMallocFromPoolAsync((void **)&ditems, std::max<int64_t>(1, nitems) * sizeof(TmxItem), ctx->pool, st));
   }
+  // a kept round also keeps its items' LU factors for the gradients
+  cplx *lu_keep = nullptr;
+  if (temp && ctx->keep_rounds) {
+    CK(cudaMallocFromPoolAsync((void **)&lu_keep, std::max<int64_t>(1, scr_total) * sizeof(cplx),
+                               ctx->pool, st));
+  }
   CK(cudaMemcpyAsync(dslots, slots.data(), np2 * sizeof(TmxSlot),
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ditems, items.data(), nitems * sizeof(TmxItem),
@@ -711,7 +720,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       B.status = (int32_t *)ctx->status.p;
       B.max_nb = inb[i0];
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
-      B.lu = keep_lu ? (cplx *)ctx->lu.p : nullptr;
+      B.lu = keep_lu ? (cplx *)ctx->lu.p : lu_keep;
       B.family = dispatch_family(ctx, B.max_nb);
       // the round's flops are booked on its first launch
       double fl = 0.;
@@ -757,7 +766,18 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   }
   tmx_launch_qsums(dslots, np2, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
   LAUNCHED();
-  if (temp) {
+  if (temp && ctx->keep_rounds) {
+    tmx_ctx::RoundRec rec;
+    rec.tab = tab;
+    rec.nsc = nsc;
+    rec.slots = dslots;
+    rec.items = ditems;
+    rec.lu = lu_keep;
+    rec.nb = inb;
+    rec.scr_total = scr_total;
+    ctx->rounds_kept.push_back(std::move(rec));
+    CK(cudaFreeAsync(scratch, st));
+  } else if (temp) {
     CK(cudaFreeAsync(tab, st));
     CK(cudaFreeAsync(nsc, st));
     CK(cudaFreeAsync(scratch, st));
@@ -835,6 +855,22 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   return TMX_OK;
 }
 
+// Buffers of the kept rounds of the previous batch back to the pool (that
+// batch has finished: every batch ends with a host synchronisation).
+int tmx_release_rounds(tmx_ctx *ctx) {
+  for (auto &r : ctx->rounds_kept) {
+    for (void *p : {(void *)r.tab, (void *)r.nsc, (void *)r.slots, (void *)r.items,
+                    (void *)r.lu}) {
+      if (p) {
+        CK(cudaFreeAsync(p, ctx->stream));
+      }
+    }
+  }
+  ctx->rounds_kept.clear();
+  ctx->rounds_lu = false;
+  return TMX_OK;
+}
+
 // Phase 2 in one round for the grains in p2 (all grains with an order).
 static int run_blocks(tmx_ctx *ctx, const std::vector<int32_t> &p2) {
   int64_t t_end = 0;
@@ -883,6 +919,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   int rc;
   ctx->have_batch = false;
   ctx->lu_ready = false;
+  if ((rc = tmx_release_rounds(ctx))) {
+    return rc;
+  }
   ctx->n = n;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);
@@ -941,6 +980,12 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     ctx->pinned_done_cap = 2 * n;
   }
   CK(cudaMemsetAsync(ctx->count.p, 0, 2 * sizeof(int32_t), st));
+  // the rounds of this batch keep their buffers and LU factors
+  struct KeepGuard {
+    tmx_ctx *c;
+    ~KeepGuard() { c->keep_rounds = false; }
+  } keep_guard{ctx};
+  ctx->keep_rounds = true;
   const int64_t round_min = std::max<int64_t>(256, ctx->up_nact / 16);
   const int64_t round_max = std::max<int64_t>(768, round_min);
   int64_t done_seen = 0;
@@ -1141,7 +1186,11 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   CK(cudaEventRecord(rounds_done, ctx->stream3));
   CK(cudaStreamWaitEvent(st, rounds_done, 0));
   CK(cudaEventDestroy(rounds_done));
-  return finish_blocks(ctx, t_next, rounds + 1);
+  if ((rc = finish_blocks(ctx, t_next, rounds + 1))) {
+    return rc;
+  }
+  ctx->rounds_lu = true;
+  return TMX_OK;
 }
 
 int tmx_tmatrix_batch(tmx_ctx *ctx, int64_t n, const double *r_ev,
@@ -1180,6 +1229,9 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
   CK(cudaSetDevice(ctx->device));
   ctx->have_batch = false;
   ctx->lu_ready = false;
+  if ((rc = tmx_release_rounds(ctx))) {
+    return rc;
+  }
   ctx->n = n;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);

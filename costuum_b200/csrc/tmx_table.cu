@@ -958,70 +958,94 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
     return fail(ctx, TMX_ERR_STATE,
                 "gradients need the batch's own T-matrices, not orientation averages");
   }
-  if (ctx->p2_rounds > 1 && (rc = tmx_rerun_blocks(ctx))) {
+  // LU factors of every item: kept by the batch's block rounds, or by a
+  // single-round batch in the p2 set; otherwise the forward blocks run again
+  // in one round that keeps them
+  if (!ctx->rounds_lu && ctx->p2_rounds > 1 && (rc = tmx_rerun_blocks(ctx))) {
     return rc;
   }
-  const int64_t nitems = (int64_t)ctx->p2_items.size();
-  const int64_t scr = ctx->p2_scr_total;
+  struct RoundView {
+    const TmxItem *items;
+    const TmxSlot *slots;
+    const double *tab, *nsc;
+    cplx *lu;
+    const std::vector<int> *nb;
+    int64_t scr;
+  };
+  std::vector<RoundView> views;
+  if (ctx->rounds_lu) {
+    for (const auto &r : ctx->rounds_kept) {
+      views.push_back({r.items, r.slots, r.tab, r.nsc, r.lu, &r.nb, r.scr_total});
+    }
+  } else {
+    if ((rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, ctx->p2_scr_total) * sizeof(cplx)))) {
+      return rc;
+    }
+    views.push_back({(const TmxItem *)ctx->p2items.p, (const TmxSlot *)ctx->p2slots.p,
+                     (const double *)ctx->p2tab.p, (const double *)ctx->p2nsc.p,
+                     (cplx *)ctx->lu.p, &ctx->p2_nb, ctx->p2_scr_total});
+  }
+  int64_t scr_max = 1;
+  for (const RoundView &v : views) {
+    scr_max = std::max(scr_max, v.scr);
+  }
   const int64_t tt = ctx->p2_t_total;
   NvtxRange range("tmx_gradients");
-  if ((rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, scr) * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->tscr, std::max<int64_t>(1, 3 * scr) * sizeof(cplx))) ||
+  if ((rc = ensure(ctx, ctx->tscr, 3 * scr_max * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->dT, std::max<int64_t>(1, 3 * tt) * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->dS, std::max<int64_t>(1, 4 * n * ntheta) * 4 * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double))) ||
       (rc = ensure(ctx, ctx->o_gz, std::max<int64_t>(1, n * ntheta * 12) * sizeof(double)))) {
     return rc;
   }
-  if (nitems > 0) {
-    CK(cudaMemsetAsync(ctx->dT.p, 0, 3 * tt * sizeof(cplx), st));
-    // the tangents need the LU factors of every item: a single-round batch
-    // kept them; otherwise the forward blocks run again keeping them. Both
-    // in the class-size buckets of the forward schedule
+  CK(cudaMemsetAsync(ctx->dT.p, 0, std::max<int64_t>(1, 3 * tt) * sizeof(cplx), st));
+  for (const RoundView &v : views) {
+    const int64_t nitems = (int64_t)v.nb->size();
+    // the class-size buckets of the forward schedule (items sorted by size)
     const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
     int64_t i0 = 0;
     for (int b = 0; b < 5; ++b) {
       int64_t i1 = i0;
-      while (i1 < nitems && ctx->p2_nb[i1] > edges[b + 1]) {
+      while (i1 < nitems && (*v.nb)[i1] > edges[b + 1]) {
         ++i1;
       }
       if (i1 > i0) {
-        const int max_nb = ctx->p2_nb[i0];
-        TmxBlockArgs B;
-        B.items = (const TmxItem *)ctx->p2items.p + i0;
-        B.nitems = (int)(i1 - i0);
-        B.slots = (const TmxSlot *)ctx->p2slots.p;
-        B.grains = (const TmxGrain *)ctx->grains.p;
-        B.tab = (const double *)ctx->p2tab.p;
-        B.nsc = (const double *)ctx->p2nsc.p;
-        B.wig = (const double *)ctx->wig.p;
-        B.wig_off = (const int64_t *)ctx->wig_off.p;
-        B.scratch = (cplx *)ctx->p2scratch.p;
-        B.tout = (cplx *)ctx->T.p;
-        B.diag = nullptr;
-        B.status = (int32_t *)ctx->status.p;
-        B.max_nb = max_nb;
-        B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
-        B.family = dispatch_family(ctx, max_nb);
-        B.lu = (cplx *)ctx->lu.p;
-        if (!ctx->lu_ready) {
+        const int max_nb = (*v.nb)[i0];
+        if (!ctx->rounds_lu && !ctx->lu_ready) {
+          TmxBlockArgs B;
+          B.items = v.items + i0;
+          B.nitems = (int)(i1 - i0);
+          B.slots = v.slots;
+          B.grains = (const TmxGrain *)ctx->grains.p;
+          B.tab = v.tab;
+          B.nsc = v.nsc;
+          B.wig = (const double *)ctx->wig.p;
+          B.wig_off = (const int64_t *)ctx->wig_off.p;
+          B.scratch = (cplx *)ctx->p2scratch.p;
+          B.tout = (cplx *)ctx->T.p;
+          B.diag = nullptr;
+          B.status = (int32_t *)ctx->status.p;
+          B.max_nb = max_nb;
+          B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
+          B.family = dispatch_family(ctx, max_nb);
+          B.lu = v.lu;
           tmx_launch_blocks(B, st);
           LAUNCHED();
         }
         TmxTangentArgs A;
-        A.items = B.items;
-        A.nitems = B.nitems;
+        A.items = v.items + i0;
+        A.nitems = (int)(i1 - i0);
         A.nparams = 3;
-        A.slots = B.slots;
-        A.grains = B.grains;
-        A.tab = B.tab;
-        A.nsc = B.nsc;
-        A.wig = B.wig;
-        A.wig_off = B.wig_off;
-        A.lu = (const cplx *)ctx->lu.p;
+        A.slots = v.slots;
+        A.grains = (const TmxGrain *)ctx->grains.p;
+        A.tab = v.tab;
+        A.nsc = v.nsc;
+        A.wig = (const double *)ctx->wig.p;
+        A.wig_off = (const int64_t *)ctx->wig_off.p;
+        A.lu = v.lu;
         A.T = (const cplx *)ctx->T.p;
         A.scratch = (cplx *)ctx->tscr.p;
-        A.scratch_stride = scr;
+        A.scratch_stride = v.scr;
         A.dT = (cplx *)ctx->dT.p;
         A.dT_stride = tt;
         A.chunk_nodes = std::max(1, tmx_host_chunk_nodes(max_nb) / 2);

@@ -837,6 +837,8 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
   std::vector<TmxObsGrain> og(n);
   std::vector<TmxSJob> sj;
   std::vector<TmxQJob> qj;
+  sj.reserve((size_t)n * ntheta);
+  qj.reserve((size_t)n * ntheta);
   for (int64_t g = 0; g < n; ++g) {
     og[g].nmax = ctx->nmax_h[g];
     og[g].coef_set = coeffs ? 0 : -1;

@@ -32,7 +32,10 @@ sys.path.insert(0, ROOT)
 N_GRAINS = 4096
 SCHEDULE = dict(min_order=10, max_order=100, gauss_legendre_factor=2,
                 tolerance=1e-4)
-CPU_SAMPLE = 96  # grains per reference-CPU step (bounded sample)
+# grains per reference-CPU step: a bounded sample of the 4096-grain
+# workload (step s takes slice s mod 4 of the same seeded grains), so that a
+# 25-step reference run ends within a few minutes on 16 host cores
+CPU_SAMPLE = 1024
 
 
 def grains(n, seed):
@@ -153,12 +156,26 @@ def flush_l2(buf):
     buf.zero_()
 
 
-def reference_sample(nthreads, seed):
-    """One bounded sample of the same workload through the reference's own
-    task objects under QuickSched (oracle/_ref, built from the reference)."""
+def workload_config():
+    """The workload both arms name in their JSON line."""
+    return {"workload": "batched T-matrices, config-2 distribution "
+                        "(4096 spheroids, x in [0.1,10])",
+            "grains_per_gpu": N_GRAINS, **SCHEDULE,
+            "l2": "flushed between steps (256 MB write); working set > L2"}
+
+
+def reference_sample(nthreads, step):
+    """One bounded sample of the workload through the reference's own task
+    objects under QuickSched (oracle/_ref, built from the reference): slice
+    step mod (N_GRAINS / CPU_SAMPLE) of the seeded grains the GPU arm times
+    on rank 0."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    r, lam, m, d = grains(CPU_SAMPLE, seed)
+    r, lam, m, d = grains(N_GRAINS, rank_seed(0))
+    nsl = max(1, N_GRAINS // CPU_SAMPLE)
+    lo = (step % nsl) * CPU_SAMPLE
+    sl = slice(lo, min(N_GRAINS, lo + CPU_SAMPLE))
+    r, lam, m, d = r[sl], lam[sl], m[sl], d[sl]
     t = time.perf_counter()
     out = O.ref_batch(r, lam, m, d, nthreads=nthreads, want_t=False, **{
         "min_order": SCHEDULE["min_order"], "max_order": SCHEDULE["max_order"],
@@ -168,18 +185,22 @@ def reference_sample(nthreads, seed):
     return len(out), dt
 
 
-def cpu_baseline_block(nthreads, steps=1):
+def cpu_baseline_block(nthreads, steps=3, warmup=1):
+    """The reference arm's measurement on a bounded sample: warm-up slices,
+    then the median rate of `steps` slices of the same workload."""
     vals = []
-    for s in range(steps):
-        n, dt = reference_sample(nthreads, 1000 + s)
-        vals.append(n / dt)
+    for s in range(warmup + steps):
+        n, dt = reference_sample(nthreads, s)
+        if s >= warmup:
+            vals.append(n / dt)
     v = float(np.median(vals))
     return {"value": v, "unit": "T-matrices/s", "cores": nthreads,
             "kind": "reference",
-            "sample": "%d grains of the same distribution (seeded), reference "
+            "sample": "%d-grain slices of the same 4096 seeded grains, reference "
                       "task objects (InteractionTask/TMatrixM0Task chain + "
                       "TMatrixMAllTask) under QuickSched, maximum_order 100, "
-                      "%d threads, median of %d" % (CPU_SAMPLE, nthreads, steps)}
+                      "%d threads, %d warm-up slice(s), median of %d slices"
+                      % (CPU_SAMPLE, nthreads, warmup, steps)}
 
 
 def run_reference(args):
@@ -187,12 +208,13 @@ def run_reference(args):
     if rank != 0:
         return 0
     nthreads = os.cpu_count() or 1
-    times = []
+    times, done = [], 0
     for s in range(args.warmup + args.steps):
-        n, dt = reference_sample(nthreads, 2000 + s)
+        n, dt = reference_sample(nthreads, s)
         if s >= args.warmup:
             times.append(dt)
-    value = CPU_SAMPLE * len(times) / sum(times)
+            done += n
+    value = done / sum(times)
     line = {
         "impl": "reference", "metric": "T-matrices/s (converged, batched)",
         "value": value, "unit": "T-matrices/s", "n_gpus": args.gpus,
@@ -200,12 +222,13 @@ def run_reference(args):
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "batched T-matrices, config-2 distribution",
-                   "grains_per_step": CPU_SAMPLE, **SCHEDULE},
+        "config": workload_config(),
         "cpu_baseline": {"value": value, "unit": "T-matrices/s",
                          "cores": nthreads, "kind": "reference",
-                         "sample": "%d grains per step, reference QuickSched "
-                                   "path, %d threads" % (CPU_SAMPLE, nthreads)},
+                         "sample": "each step a %d-grain slice of the same 4096 "
+                                   "seeded grains (4 slices in turn), reference "
+                                   "task objects under QuickSched, %d threads"
+                                   % (CPU_SAMPLE, nthreads)},
         "e2e": {"value": value, "unit": "T-matrices/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -293,18 +316,31 @@ def run_ours(args):
     q = np.zeros((N_GRAINS, 6))
     lib.tmx_batch_results(h, _lib.iptr(nmax), None, _lib.iptr(status), P(q))
 
-    # ---- end to end through the public API with host buffers
-    e2e_ms = 0.0
+    # ---- end to end through the public API with host buffers: the inputs
+    # from host arrays, and every converged T-matrix back in page-locked host
+    # memory (each block round streams its range while the batch runs; the
+    # rest follows in tmatrices()) together with the per-grain results
+    flat, _ = ctx.tmatrices()
+    ctx.stream_tmatrices(int(flat.size * 1.25) + 4096)
+    ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+    ctx.tmatrices()
+    e2e_ms, t_bytes = 0.0, 0
     for s in range(max(1, args.steps)):
         flush_l2(flush)
         torch.cuda.synchronize()
         dist.barrier()
         t0 = time.perf_counter()
         res = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+        flat, off = ctx.tmatrices()
         e2e_ms += (time.perf_counter() - t0) * 1e3
+        t_bytes = flat.nbytes
+    ctx.stream_tmatrices(0)
     e2e_max = dist.max(e2e_ms) / max(1, args.steps)
+    # host -> device: five input arrays; device -> host: the T-matrices, the
+    # chain states (64 B), done list (8 B), Q sums (16 B) and status (4 B)
+    # per grain
     h2d = N_GRAINS * 5 * 8
-    d2h = N_GRAINS * (3 * 4 + 6 * 8)
+    d2h = t_bytes + N_GRAINS * (64 + 8 + 16 + 4)
 
     # ---- plain path: the same kernels, one grain per call (no batching)
     plain = None
@@ -440,24 +476,23 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if world == 1 and not args.skip_cpu:
-            cpu = cpu_baseline_block(os.cpu_count() or 1, steps=1)
+            cpu = cpu_baseline_block(os.cpu_count() or 1)
         out = {
             "metric": "T-matrices/s (converged, batched)",
             "value": value, "unit": "T-matrices/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "batched T-matrices, config-2 distribution "
-                                   "(4096 spheroids, x in [0.1,10])",
-                       "grains_per_gpu": N_GRAINS, **SCHEDULE,
-                       "l2": "flushed between steps (256 MB write); working "
-                             "set > L2",
-                       "nmax_mean": float(nmax[nmax > 0].mean()),
-                       "nmax_max": int(nmax.max()),
-                       "status_nonzero": int((status != 0).sum())},
+            "config": workload_config(),
+            "batch": {"nmax_mean": float(nmax[nmax > 0].mean()),
+                      "nmax_max": int(nmax.max()),
+                      "status_nonzero": int((status != 0).sum())},
             "e2e": {"value": world * N_GRAINS / (e2e_max * 1e-3),
                     "unit": "T-matrices/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h,
+                    "what": "tmatrix_batch from host arrays + every converged "
+                            "T-matrix in host memory (tmatrices(), streamed "
+                            "by the block rounds) + per-grain results"},
             "roofline": {"bound": "tensor",
                          "kernel": "block kernels (k_blocks_warp, k_blocks): "
                                    "assembly + LU + solve",

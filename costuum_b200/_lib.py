@@ -57,6 +57,9 @@ SIGNATURES = {
     "tmx_batch_gradients": (ctypes.c_int, [_VP, ctypes.c_int32, _D, _D,
                                            ctypes.c_int32, _D, _D]),
     "tmx_batch_tmatrix": (ctypes.c_int, [_VP, ctypes.c_int64, _D]),
+    "tmx_batch_tmatrix_total": (ctypes.c_int, [_VP, _I64]),
+    "tmx_batch_tmatrices": (ctypes.c_int, [_VP, _D, _I64]),
+    "tmx_set_tmatrix_sink": (ctypes.c_int, [_VP, _D, ctypes.c_int64]),
     "tmx_probe_fp64": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "tmx_kernel_launches": (ctypes.c_int64, [_VP]),
     "tmx_timer_start": (ctypes.c_int, [_VP]),
@@ -84,7 +87,7 @@ SIGNATURES = {
                                      ctypes.c_int32, ctypes.c_int32,
                                      ctypes.POINTER(TmxSchedule), _D, _D, _I32]),
     "tmx_tmatrix_fixed_noalloc": (ctypes.c_int, [ctypes.c_double] * 5
-                                  + [ctypes.c_int32, ctypes.c_int32, _VP, _VP]),
+                                  + [ctypes.c_int32, ctypes.c_int32, _VP, _VP, _VP]),
 }
 
 _lib = None

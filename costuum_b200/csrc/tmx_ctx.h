@@ -139,6 +139,16 @@ struct tmx_ctx {
   int64_t p2_scr_total = 0, p2_t_total = 0;
   DevBuf lu, dT, tscr, dTa, dS; // tangent buffers
   int o_nsj = 0, o_nqj = 0;     // per-grain observable job counts
+  // events that order a free on `stream` after the work queued so far on the
+  // round streams and their bucket streams (stream2, stream3, aux[0..5])
+  cudaEvent_t drain_ev[8] = {};
+  // page-locked host destination of the T-matrices (tmx_set_tmatrix_sink):
+  // every block round copies its T range there as soon as its blocks are
+  // done; sink_done = complex elements [0, sink_done) already copied for the
+  // current batch
+  double *sink = nullptr;
+  int64_t sink_cap = 0;
+  int64_t sink_done = 0;
 };
 
 #define CK(call)                                                               \
@@ -155,6 +165,28 @@ struct tmx_ctx {
     ++ctx->launches;                                                           \
     CK(cudaGetLastError());                                                    \
   } while (0)
+
+// Makes ctx->stream wait for everything queued so far on the other streams
+// of the context. Every free of a shared buffer (Wigner and quadrature
+// tables, T, the Q sums) is issued on ctx->stream while block rounds may
+// still run on the round streams and read it; the pool may hand a freed
+// block to the next allocation as soon as the free is complete in stream
+// order, so the free must come after those readers.
+static inline int order_after_rounds(tmx_ctx *ctx) {
+  cudaStream_t others[8] = {ctx->stream2, ctx->stream3, ctx->aux[0], ctx->aux[1],
+                            ctx->aux[2],  ctx->aux[3],  ctx->aux[4], ctx->aux[5]};
+  for (int i = 0; i < 8; ++i) {
+    if (!others[i]) {
+      continue;
+    }
+    if (!ctx->drain_ev[i]) {
+      CK(cudaEventCreateWithFlags(&ctx->drain_ev[i], cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(ctx->drain_ev[i], others[i]));
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->drain_ev[i], 0));
+  }
+  return TMX_OK;
+}
 
 // executed flops of one class item: assembly (4 real FMAs per entry, node
 // and term; 2 terms for m = 0), LU (8/3 nb^3) and the two triangular solves
@@ -247,6 +279,10 @@ static inline int ensure(tmx_ctx *ctx, DevBuf &b, size_t bytes) {
     return TMX_OK;
   }
   if (b.p) {
+    int rc = order_after_rounds(ctx);
+    if (rc) {
+      return rc;
+    }
     CK(cudaFreeAsync(b.p, ctx->stream));
     b.p = nullptr;
     b.cap = 0;
@@ -280,6 +316,10 @@ static inline int ensure_keep(tmx_ctx *ctx, DevBuf &b, size_t bytes, size_t keep
   }
   nb.cap = want;
   if (b.p) {
+    int rc = order_after_rounds(ctx);
+    if (rc) {
+      return rc;
+    }
     if (keep) {
       CK(cudaMemcpyAsync(nb.p, b.p, keep, cudaMemcpyDeviceToDevice,
                          ctx->stream));

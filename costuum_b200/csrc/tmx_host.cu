@@ -322,6 +322,11 @@ void tmx_destroy(tmx_ctx *ctx) {
   for (cudaEvent_t e : ctx->prof_pool) {
     cudaEventDestroy(e);
   }
+  for (cudaEvent_t e : ctx->drain_ev) {
+    if (e) {
+      cudaEventDestroy(e);
+    }
+  }
   DevBuf *bufs[] = {&ctx->lu, &ctx->dT, &ctx->tscr, &ctx->dTa, &ctx->dS,
                     &ctx->cg, &ctx->cg_off, &ctx->Ta, &ctx->o_angles,
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
@@ -491,6 +496,9 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   int rc;
   NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
+  if (!keep_T) {
+    ctx->sink_done = 0; // a new set of T-matrices starts at offset 0
+  }
   std::vector<TmxSlot> slots(np2);
   std::vector<std::pair<int, int>> keys;
   std::map<std::pair<int, int>, int> key_idx;
@@ -766,6 +774,15 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   }
   tmx_launch_qsums(dslots, np2, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
   LAUNCHED();
+  // the round's T-matrices to the caller's page-locked sink, on the round's
+  // stream: the copy overlaps the order loop and the rounds that follow
+  if (ctx->sink && t_base == ctx->sink_done && t_total <= ctx->sink_cap &&
+      t_total > t_base) {
+    CK(cudaMemcpyAsync(ctx->sink + 2 * t_base, (const cplx *)ctx->T.p + t_base,
+                       (t_total - t_base) * sizeof(cplx), cudaMemcpyDeviceToHost,
+                       st));
+    ctx->sink_done = t_total;
+  }
   if (temp && ctx->keep_rounds) {
     tmx_ctx::RoundRec rec;
     rec.tab = tab;
@@ -892,7 +909,13 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
     }
   }
   int64_t t_end = 0;
+  // the same T-matrices again: what the sink holds stays valid
+  double *sink = ctx->sink;
+  const int64_t sink_done = ctx->sink_done;
+  ctx->sink = nullptr;
   int rc = run_blocks_round(ctx, p2, ctx->stream, 0, false, &t_end, false, true);
+  ctx->sink = sink;
+  ctx->sink_done = sink_done;
   if (rc) {
     return rc;
   }
@@ -930,6 +953,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   ctx->t_off_h.assign(n, 0);
   ctx->flops_survey = 0.;
   if (n == 0) {
+    ctx->p2_t_total = 0;
     ctx->have_batch = true;
     return TMX_OK;
   }
@@ -1255,6 +1279,7 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
   }
   CK(cudaMemsetAsync(ctx->status.p, 0, n * sizeof(int32_t), ctx->stream));
   if (n == 0) {
+    ctx->p2_t_total = 0;
     ctx->have_batch = true;
     return TMX_OK;
   }
@@ -1432,6 +1457,70 @@ int tmx_batch_tmatrix(tmx_ctx *ctx, int64_t grain, double *out) {
   CK(cudaMemcpyAsync(out, (const cplx *)ctx->T.p + ctx->t_off_h[grain],
                      sz * sizeof(cplx), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
+  return TMX_OK;
+}
+
+int tmx_batch_tmatrix_total(tmx_ctx *ctx, int64_t *total) {
+  if (!ctx || !total) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  *total = ctx->p2_t_total;
+  return TMX_OK;
+}
+
+int tmx_batch_tmatrices(tmx_ctx *ctx, double *out, int64_t *offsets) {
+  if (!ctx || (!out && !offsets)) {
+    return TMX_ERR_INVALID;
+  }
+  if (!ctx->have_batch) {
+    return fail(ctx, TMX_ERR_STATE, "no batch has been computed");
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (offsets) {
+    for (int64_t i = 0; i < ctx->n; ++i) {
+      offsets[i] = (ctx->nmax_h[i] > 0) ? ctx->t_off_h[i] : -1;
+    }
+  }
+  const int64_t total = ctx->p2_t_total;
+  if (out && total > 0) {
+    // into the sink only what the block rounds have not streamed already
+    const int64_t from = (out == ctx->sink) ? std::min(ctx->sink_done, total) : 0;
+    if (from < total) {
+      CK(cudaMemcpyAsync(out + 2 * from, (const cplx *)ctx->T.p + from,
+                         (total - from) * sizeof(cplx), cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    }
+    // the streamed copies ran on the round streams, which ctx->stream
+    // joined at the end of the batch
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  return TMX_OK;
+}
+
+int tmx_set_tmatrix_sink(tmx_ctx *ctx, double *host, int64_t capacity) {
+  if (!ctx || capacity < 0 || (capacity > 0 && !host)) {
+    return TMX_ERR_INVALID;
+  }
+  if (host) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, host) != cudaSuccess ||
+        at.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      return fail(ctx, TMX_ERR_INVALID,
+                  "the T-matrix sink must be page-locked host memory "
+                  "(tmx_host_alloc or cudaHostRegister)");
+    }
+  }
+  // copies into the previous sink must be complete before it is released
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream2));
+  CK(cudaStreamSynchronize(ctx->stream3));
+  ctx->sink = host;
+  ctx->sink_cap = host ? capacity : 0;
+  ctx->sink_done = 0;
   return TMX_OK;
 }
 

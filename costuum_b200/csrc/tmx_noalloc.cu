@@ -145,7 +145,7 @@ extern "C" int tmx_tmatrix_fixed_noalloc(double r_ev, double wavelength,
                                          double mr, double mi,
                                          double axis_ratio, int32_t nmax,
                                          int32_t ngauss, double *T_dev,
-                                         void *stream) {
+                                         int32_t *status_dev, void *stream) {
   if (nmax < 2 || nmax > NA_MAX_NMAX || ngauss < 1 || ngauss > NA_MAX_NG) {
     fprintf(stderr,
             "tmx_tmatrix_fixed_noalloc: nmax %d / ngauss %d outside the static "
@@ -244,5 +244,11 @@ extern "C" int tmx_tmatrix_fixed_noalloc(double r_ev, double wavelength,
   B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
   tmx_launch_blocks(B, st);
   NA_CK(cudaGetLastError());
+  // the grain's status bits (singular pivot, non-finite entries) into the
+  // caller's device word: a stream-ordered copy, no allocation
+  if (status_dev) {
+    NA_CK(cudaMemcpyAsync(status_dev, base + NA_STATUS, sizeof(int32_t),
+                          cudaMemcpyDeviceToDevice, st));
+  }
   return TMX_OK;
 }

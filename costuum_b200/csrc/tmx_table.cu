@@ -1491,6 +1491,7 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
   }
   CK(cudaStreamSynchronize(st));
   ctx->t_averaged = true;
+  ctx->sink_done = 0; // the T-matrices a sink holds are the unaveraged ones
   return TMX_OK;
 }
 

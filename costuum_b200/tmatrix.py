@@ -133,6 +133,9 @@ class Context:
         if getattr(self, "_h", None):
             _lib.load().tmx_destroy(self._h)
             self._h = None
+        if getattr(self, "_sink", None):
+            _lib.load().tmx_host_free(self._sink[0])
+            self._sink = None
 
     def __del__(self):
         try:
@@ -326,6 +329,57 @@ class Context:
                                                                 _lib.ptr(out))
             _lib.check(self._h, rc, "tmx_batch_average_absorption_cross_section")
         return float(out[0])
+
+    def stream_tmatrices(self, capacity):
+        """Stream the T-matrices of every following batch into a page-locked
+        host buffer of `capacity` complex elements while the batch runs (each
+        block round copies its range as soon as it is done); 0 stops."""
+        lib = _lib.load()
+        with self._lock:
+            rc = lib.tmx_set_tmatrix_sink(self._h, None, 0)
+            _lib.check(self._h, rc, "tmx_set_tmatrix_sink")
+            if getattr(self, "_sink", None):
+                lib.tmx_host_free(self._sink[0])
+                self._sink = None
+            if capacity <= 0:
+                return
+            ptr = lib.tmx_host_alloc(16 * int(capacity))
+            if not ptr:
+                raise _lib.TmxError("page-locked allocation of %d bytes failed"
+                                    % (16 * int(capacity)))
+            rc = lib.tmx_set_tmatrix_sink(
+                self._h, ctypes.cast(ptr, ctypes.POINTER(ctypes.c_double)),
+                int(capacity))
+            if rc != 0:
+                lib.tmx_host_free(ptr)
+            _lib.check(self._h, rc, "tmx_set_tmatrix_sink")
+            self._sink = (ptr, int(capacity))
+
+    def tmatrices(self):
+        """Every T-matrix of the last batch in one transfer: (flat complex
+        array, offsets) with grain i's T-matrix at flat[offsets[i]:] in the
+        reference block layout (offsets[i] = -1: none). With a stream buffer
+        (stream_tmatrices) the array is a view of it that the next batch
+        overwrites, and only what was not streamed yet is copied."""
+        lib = _lib.load()
+        n = self._last_n()
+        total = ctypes.c_int64()
+        offsets = np.zeros(n, np.int64)
+        with self._lock:
+            rc = lib.tmx_batch_tmatrix_total(self._h, ctypes.byref(total))
+            _lib.check(self._h, rc, "tmx_batch_tmatrix_total")
+            total = total.value
+            sink = getattr(self, "_sink", None)
+            if sink and sink[1] >= total:
+                buf = (ctypes.c_char * (16 * max(1, total))).from_address(sink[0])
+                flat = np.frombuffer(buf, dtype=np.complex128, count=total)
+                dst = ctypes.cast(sink[0], ctypes.POINTER(ctypes.c_double))
+            else:
+                flat = self._pinned.array((2 * max(1, total),)).view(np.complex128)[:total]
+                dst = flat.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            rc = lib.tmx_batch_tmatrices(self._h, dst, _lib.lptr(offsets))
+            _lib.check(self._h, rc, "tmx_batch_tmatrices")
+        return flat, offsets
 
     def _results(self, n):
         self._n = n

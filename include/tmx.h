@@ -139,6 +139,27 @@ int tmx_batch_results(tmx_ctx *ctx, int32_t *nmax, int32_t *ngauss,
  * (2 * tmx_tmatrix_size(nmax) doubles). */
 int tmx_batch_tmatrix(tmx_ctx *ctx, int64_t grain, double *out);
 
+/* Every T-matrix of the last batch in one transfer: the reference keeps one
+ * TMatrixResource per grain (src/TMatrixResource.hpp:60-276) that its
+ * callers read in place; here they sit in one ragged device buffer.
+ * *total = complex elements of that buffer. tmx_batch_tmatrices copies it
+ * into out (2 * total doubles, may be NULL) and writes offsets[i] (may be
+ * NULL) = complex offset of grain i's T-matrix in out (tmx_tmatrix_size(
+ * nmax[i]) elements in the block layout above), -1 for a grain without
+ * one. When out is the sink set below, only the part that the block rounds
+ * have not already streamed is copied. */
+int tmx_batch_tmatrix_total(tmx_ctx *ctx, int64_t *total);
+int tmx_batch_tmatrices(tmx_ctx *ctx, double *out, int64_t *offsets);
+
+/* Stream the T-matrices of every following batch into page-locked host
+ * memory (tmx_host_alloc or cudaHostRegister; capacity in complex
+ * elements): each block round copies its range as soon as its blocks are
+ * done, overlapping the rest of the batch, at the offsets that
+ * tmx_batch_tmatrices reports; ranges beyond the capacity are left to
+ * tmx_batch_tmatrices. The buffer is rewritten by every batch. host = NULL
+ * stops streaming. TMX_ERR_INVALID if host is not page-locked. */
+int tmx_set_tmatrix_sink(tmx_ctx *ctx, double *host, int64_t capacity);
+
 /* Measured FP64 throughput of this device in TFLOP/s: kind 0 = DFMA pipe,
  * kind 1 = DMMA tensor pipe (mma.sync m8n8k4 f64). */
 int tmx_probe_fp64(tmx_ctx *ctx, int kind, double *tflops);
@@ -343,12 +364,18 @@ int tmx_batch_average_absorption_cross_section(tmx_ctx *ctx, int64_t grain,
  * stderr). The caller passes the grain (SI units) and a device buffer T_dev
  * of 2 * tmx_tmatrix_size(nmax) doubles; the work is enqueued on `stream`
  * (a cudaStream_t, NULL = legacy default stream) and is complete when that
- * stream is. The first call on a device looks up the array's device address
- * with that device current; make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU race. */
+ * stream is. status_dev (a device int32_t, may be NULL) receives the grain's
+ * status bits in stream order (tmx_grain_status: 0, or TMX_GRAIN_SINGULAR /
+ * TMX_GRAIN_NAN when a class block had a zero pivot or non-finite entries);
+ * the return value reports argument and CUDA errors only, so a caller that
+ * passes NULL cannot tell a failed solve from a valid T-matrix. The first
+ * call on a device looks up the array's device address with that device
+ * current; make that first call before any stream capture. All calls share
+ * the array: calls that overlap on the GPU race. */
 int tmx_tmatrix_fixed_noalloc(double r_ev, double wavelength, double mr,
                               double mi, double axis_ratio, int32_t nmax,
-                              int32_t ngauss, double *T_dev, void *stream);
+                              int32_t ngauss, double *T_dev,
+                              int32_t *status_dev, void *stream);
 
 /* Number of this library's kernels launched since the context was created. */
 int64_t tmx_kernel_launches(const tmx_ctx *ctx);

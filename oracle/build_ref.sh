@@ -16,7 +16,8 @@
 # the two generated headers are written here by sed, as its CMake would.
 #
 # Usage: oracle/build_ref.sh [--optional] [REFERENCE_ROOT]
-#        (default /root/reference; --optional: exit 0 when it is absent)
+#        (REFERENCE_ROOT defaults to $COSTUUM_REFERENCE; --optional: exit 0
+#        when neither names a reference source tree)
 set -euo pipefail
 
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -25,11 +26,11 @@ if [ "${1:-}" = "--optional" ]; then
   OPTIONAL=1
   shift
 fi
-REF="${1:-/root/reference}"
+REF="${1:-${COSTUUM_REFERENCE:-}}"
 OUT="$HERE/_ref"
 GEN="$OUT/gen"
 
-if [ ! -f "$REF/src/CTMModule.cpp" ]; then
+if [ -z "$REF" ] || [ ! -f "$REF/src/CTMModule.cpp" ]; then
   if [ "$OPTIONAL" = 1 ]; then
     exit 0
   fi

@@ -1,7 +1,9 @@
 """Generate the golden fixtures in tests/golden/ from the unmodified reference.
 
-Run in a container where the reference has been built (oracle/build_ref.sh):
-    python tests/golden/make_golden.py [stages tmatrices tables plain draine]
+Run in a container where the reference has been built (oracle/build_ref.sh),
+with COSTUUM_REFERENCE naming the reference source tree (for its test data):
+    COSTUUM_REFERENCE=<reference root> python tests/golden/make_golden.py \
+        [stages tmatrices tables plain draine]
 It imports the reference's own CPython module (oracle/_ref/CosTuuM*.so) and
 its task objects (oracle/_ref/libref_driver.so) and stores their outputs.
 The fixtures pin the C restatement in oracle/ (tests/test_oracle_golden.py).
@@ -12,7 +14,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = os.environ.get("COSTUUM_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("COSTUUM_REFERENCE", "")
 sys.path.insert(0, os.path.join(HERE, "..", "..", "oracle"))
 import oracle as O  # noqa: E402
 from oracle import _p  # noqa: E402

@@ -7,7 +7,8 @@ intermediates in a static device array shared by every call. This test calls
 it through the C ABI and compares it with the batched entry point on calls
 in a row (different grains back to back, so leftovers of one call in the
 shared array must not leak into the next). The output buffer is filled with
-NaN first, so every element must be written.
+NaN first, so every element must be written, and the device status word
+starts at -1, so the call must report the grain's status bits (0 here).
 """
 import ctypes
 
@@ -22,11 +23,12 @@ pytestmark = pytest.mark.gpu
 T_TOL = 1e-9
 
 
-def _call(lib, g, nmax, ngauss, buf, stream):
+def _call(lib, g, nmax, ngauss, buf, stream, status=None):
     r, lam, m, d = g
+    st = ctypes.c_void_p(status.data_ptr() if status is not None else None)
     return lib.tmx_tmatrix_fixed_noalloc(r, lam, m.real, m.imag, d, int(nmax),
                                          int(ngauss), ctypes.c_void_p(buf.data_ptr()),
-                                         ctypes.c_void_p(stream))
+                                         st, ctypes.c_void_p(stream))
 
 
 def test_noalloc_matches_batch(ctx):
@@ -42,9 +44,11 @@ def test_noalloc_matches_batch(ctx):
         assert N <= 32 and ng <= 64
         buf = torch.full((2 * TM.tmatrix_size(N),), float("nan"),
                          dtype=torch.float64, device="cuda")
-        rc = _call(lib, grains[i], N, ng, buf, stream)
+        status = torch.full((1,), -1, dtype=torch.int32, device="cuda")
+        rc = _call(lib, grains[i], N, ng, buf, stream, status)
         assert rc == 0
         torch.cuda.current_stream().synchronize()
+        assert int(status.item()) == 0
         got = buf.cpu().numpy().view(np.complex128)
         want = res.tmatrix(i)
         for m in range(N + 1):

@@ -445,6 +445,7 @@ def get_table(types, sizes, wavelengths, thetas, shape_distribution,
                                _lib.ptr(out_q) if nq else None,
                                _lib.ptr(out_z) if do_scattering else None,
                                _lib.iptr(status))
+        ctx._batch_id = ctx.batch_id + 1  # the grid's batches replaced the last one
         _lib.check(ctx._h, rc, "tmx_get_table")
     res = []
     if nq:

@@ -40,15 +40,21 @@ class Extinction(torch.autograd.Function):
         res = tm.tmatrix_batch(p[:, 2], wavelength, p[:, 0] + 1j * p[:, 1], p[:, 3],
                                **schedule)
         q = tm.observables(th, c)
-        ctx.state = (p, wavelength, th, c, res.nmax.copy(), res.ngauss.copy())
+        ctx.state = (p, wavelength, th, c, res.nmax.copy(), res.ngauss.copy(),
+                     tm.batch_id)
         return torch.as_tensor(q, dtype=params.dtype, device=params.device)
 
     @staticmethod
     def backward(ctx, grad):
-        p, wavelength, th, c, nmax, ngauss = ctx.state
+        p, wavelength, th, c, nmax, ngauss, batch = ctx.state
         tm = _context()
-        tm.tmatrix_batch_fixed(p[:, 2], wavelength, p[:, 0] + 1j * p[:, 1], p[:, 3],
-                               nmax, ngauss)
+        if tm.batch_id != batch:
+            # another batch ran since the forward: its T-matrices and LU
+            # factors are gone, so recompute the blocks at the forward's orders
+            tm.tmatrix_batch_fixed(p[:, 2], wavelength, p[:, 0] + 1j * p[:, 1],
+                                   p[:, 3], nmax, ngauss)
+        # else the context still holds the forward's batch, whose block
+        # rounds kept their LU factors: only the tangent kernels run
         _, dq = tm.gradients(th, c)
         g = grad.detach().cpu().numpy().astype(np.float64)
         gp = np.einsum("ntk,ntkp->np", g, dq)

@@ -301,21 +301,30 @@ __global__ void __launch_bounds__(NT, MINB)
   __syncthreads();
 
   // ------------------------------------------------------------------ LU
-  const int lda = nb | 1; // odd stride: conflict-free column access
-  cplx *Am = reinterpret_cast<cplx *>(tmx_smem);
-  cplx *uinv = Am + (int64_t)nb * lda;
+  // The factors live in shared memory (odd stride: conflict-free column
+  // access) when they fit beside a chunk of at least 8 right-hand-side rows;
+  // larger classes factor Q_c in place in its global scratch and solve on
+  // -RgQ_c in place (L2-resident), with only the pivots in shared memory.
+  const int lda_s = nb | 1;
+  size_t lu_need = ((size_t)nb * lda_s + nb) * sizeof(cplx) + (3 * nb + 1) * sizeof(int);
+  lu_need = (lu_need + 15) & ~(size_t)15;
+  const bool lu_global =
+      lu_need + (size_t)(nb < 8 ? nb : 8) * lda_s * sizeof(cplx) > smem_bytes;
+  const int lda = lu_global ? nb : lda_s;
+  cplx *Am = lu_global ? Qs : reinterpret_cast<cplx *>(tmx_smem);
+  cplx *uinv = lu_global ? reinterpret_cast<cplx *>(tmx_smem) : Am + (int64_t)nb * lda;
   int *piv = reinterpret_cast<int *>(uinv + nb);
   int *perm = piv + nb;
   int *flag = perm + nb;
-  size_t used = ((size_t)nb * lda + nb) * sizeof(cplx) + (3 * nb + 1) * sizeof(int);
-  used = (used + 15) & ~(size_t)15;
-  cplx *X = reinterpret_cast<cplx *>(tmx_smem + used);
-  int Rchunk = (int)((smem_bytes - used) / (sizeof(cplx) * lda));
+  cplx *X = lu_global ? Rs : reinterpret_cast<cplx *>(tmx_smem + lu_need);
+  int Rchunk = lu_global ? nb : (int)((smem_bytes - lu_need) / (sizeof(cplx) * lda));
   if (Rchunk > nb) {
     Rchunk = nb;
   }
-  for (int u = threadIdx.x; u < nb * nb; u += blockDim.x) {
-    Am[(u / nb) * lda + (u % nb)] = Qs[u];
+  if (!lu_global) {
+    for (int u = threadIdx.x; u < nb * nb; u += blockDim.x) {
+      Am[(u / nb) * lda + (u % nb)] = Qs[u];
+    }
   }
   if (threadIdx.x == 0) {
     *flag = 0;
@@ -409,6 +418,8 @@ __global__ void __launch_bounds__(NT, MINB)
   const bool chain = sl.tout < 0;
   for (int r0 = 0; r0 < nb; r0 += Rchunk) {
     const int R = min(Rchunk, nb - r0);
+    // (in place when X is Rs itself: each element is read and written by
+    // the same thread)
     for (int u = threadIdx.x; u < R * nb; u += blockDim.x) {
       const cplx v = Rs[(int64_t)(r0 + u / nb) * nb + (u % nb)];
       X[(u / nb) * lda + (u % nb)] = mkc(-v.x, -v.y);
@@ -1568,8 +1579,12 @@ static void launch_cta32(const TmxBlockArgs &a, cudaStream_t stream) {
   k_blocks_cta32<<<blocks, 128, smem, stream>>>(a);
 }
 
+// dynamic shared memory the CTA kernel may use (of the 227 KB per block)
+#define TMX_BLOCK_SMEM_MAX (227u * 1024u)
+
 // shared memory of one block: the larger of the assembly chunk buffers and
-// the LU phase (factors, pivots and a right-hand-side chunk)
+// the LU phase (factors, pivots and a right-hand-side chunk, or the pivot
+// data alone for classes whose factors do not fit)
 size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
   const int nrp = (max_nb + 3) / 4 * 4 + 4;
   const int ncol = (max_nb + 3) / 4 * 4;
@@ -1587,6 +1602,12 @@ size_t tmx_block_smem_bytes(int max_nb, int chunk_nodes) {
   const size_t full = lu + (size_t)max_nb * lda * sizeof(cplx);
   if (full <= 200 * 1024) {
     lu_total = full;
+  }
+  if (lu_total > TMX_BLOCK_SMEM_MAX) {
+    // the kernel factors such classes in global memory: shared memory holds
+    // the pivot data only
+    lu_total = ((size_t)max_nb * sizeof(cplx) + (3 * max_nb + 1) * sizeof(int) + 15) &
+               ~(size_t)15;
   }
   return asm_bytes > lu_total ? asm_bytes : lu_total;
 }

@@ -248,7 +248,8 @@ extern "C" int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n,
       }
       const int Ni = c.nmax;
       const int NGi = (c.phase == 0) ? ndgs * c.nmax : c.ngauss;
-      if (Ni < 1 || Ni > TMX_MAX_NB) {
+      // the m = 0 classes of order N have at most (N + 1) / 2 members
+      if (Ni < 1 || Ni > 2 * TMX_MAX_NB - 1) {
         ctx->status_h[i] |= TMX_GRAIN_TOO_LARGE;
         c.phase = 2;
         c.nmax = 0;
@@ -298,10 +299,17 @@ extern "C" int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n,
       }
     }
   }
-  // every m block at the final orders
+  // every m block at the final orders; a grain whose final order has
+  // classes above the block kernels' limit (in practice one that ran to
+  // maximum_order without converging, where the reference aborts) gets no
+  // T-matrix
   std::vector<int32_t> p2;
   std::vector<int> ngs;
   for (int64_t i = 0; i < n; ++i) {
+    if (cs[i].phase == 2 && cs[i].nmax > TMX_MAX_NB) {
+      ctx->status_h[i] |= TMX_GRAIN_TOO_LARGE;
+      continue;
+    }
     if (cs[i].phase == 2 && cs[i].nmax > 0 && cs[i].ngauss > 0 && !ctx->up_status[i]) {
       ctx->nmax_h[i] = cs[i].nmax;
       ctx->ngauss_h[i] = cs[i].ngauss;

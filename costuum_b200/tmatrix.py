@@ -238,6 +238,7 @@ class Context:
                                   _lib.ptr(mr), _lib.ptr(mi), _lib.ptr(d),
                                   _lib.iptr(nm), _lib.iptr(ng), int(reps),
                                   _lib.ptr(ms))
+            self._batch_id = self.batch_id + 1  # the last tuning batch is current
             _lib.check(self._h, rc, "tmx_autotune")
         return self.get_dispatch(), ms
 
@@ -271,6 +272,7 @@ class Context:
         with self._lock:
             rc = lib.tmx_batch_orientation_average(self._h, _lib.ptr(c), c.shape[0],
                                                    c.shape[1], _lib.iptr(idx))
+            self._batch_id = self.batch_id + 1
             _lib.check(self._h, rc, "tmx_batch_orientation_average")
 
     @staticmethod
@@ -381,8 +383,15 @@ class Context:
             _lib.check(self._h, rc, "tmx_batch_tmatrices")
         return flat, offsets
 
+    @property
+    def batch_id(self):
+        """Counter of the batches (and T-matrix replacements) of this
+        context: results of an earlier id are gone."""
+        return getattr(self, "_batch_id", 0)
+
     def _results(self, n):
         self._n = n
+        self._batch_id = self.batch_id + 1
         lib = _lib.load()
         nmax = np.zeros(n, np.int32)
         ngauss = np.zeros(n, np.int32)

@@ -117,8 +117,11 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
  * ndgs nmax + 1 until they change by <= tolerance; then every m block at the
  * final (nmax, ngauss). r_ev is the equal-volume radius. A grain that reaches
  * maximum_order or maximum_ngauss (the reference aborts) gets
- * TMX_GRAIN_NOT_CONVERGED and keeps its last order; one that needs an order
- * above 128 gets TMX_GRAIN_TOO_LARGE. Results as for tmx_tmatrix_batch;
+ * TMX_GRAIN_NOT_CONVERGED and keeps its last order. The m = 0 steps run to
+ * order 255; a grain whose final order is above 128 (the block kernels'
+ * class limit; in practice a grain that ran to maximum_order 200 without
+ * converging) also gets TMX_GRAIN_TOO_LARGE and no T-matrix (nmax 0).
+ * Results as for tmx_tmatrix_batch;
  * q[6 i + 0], q[6 i + 1] hold the m = 0 sums of the last step and
  * q[6 i + 4], q[6 i + 5] their relative changes. */
 int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n, const double *r_ev,

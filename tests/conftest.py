@@ -14,6 +14,17 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session")
+def oracle_pool():
+    """Worker processes for oracle computations. Started with spawn, so that
+    no worker is forked from a process that holds a CUDA context."""
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1))
+    yield pool
+    pool.close()
+    pool.join()
+
+
+@pytest.fixture(scope="session")
 def ctx():
     from costuum_b200.tmatrix import Context
     c = Context(0)

@@ -3,7 +3,7 @@
 Run in a container where the reference has been built (oracle/build_ref.sh),
 with COSTUUM_REFERENCE naming the reference source tree (for its test data):
     COSTUUM_REFERENCE=<reference root> python tests/golden/make_golden.py \
-        [stages tmatrices tables plain draine]
+        [stages tmatrices tables plain draine config5]
 It imports the reference's own CPython module (oracle/_ref/CosTuuM*.so) and
 its task objects (oracle/_ref/libref_driver.so) and stores their outputs.
 The fixtures pin the C restatement in oracle/ (tests/test_oracle_golden.py).
@@ -223,6 +223,113 @@ def plain():
     return out
 
 
+def _config5_grains():
+    """Seeded large, elongated grains: x uniform in [20, 30], axis ratio
+    log-uniform in [0.33, 3], Re m in [1.3, 2], Im m log-uniform in
+    [1e-3, 1], lambda = 1 um (equal-volume radii)."""
+    rng = np.random.default_rng(505)
+    n = 12
+    x = rng.uniform(20.0, 30.0, n)
+    d = np.exp(rng.uniform(np.log(0.33), np.log(3.0), n))
+    m = rng.uniform(1.3, 2.0, n) + 1j * np.exp(rng.uniform(np.log(1e-3), 0.0, n))
+    lam = 1e-6
+    return x * lam / (2 * np.pi), lam, m, d
+
+
+def _config5_one(i):
+    """One grain through the reference module's TMatrix (calculator
+    schedule, maximum_order 200, random orientation): its nmax and Z at
+    181 scattering angles for incidence along the axis. Runs in a child
+    process: the reference aborts the process when a grain does not
+    converge."""
+    r, lam, m, d = _config5_grains()
+    C = O.ref_module()
+    T = C.TMatrix(r[i], d[i], lam, m[i], cos2beta=1.0 / 3.0)
+    tout = np.radians(np.arange(181.0))
+    return T.get_nmax(), T.get_scattering_matrix(0.0, 0.0, tout, 0.0)
+
+
+def _bench5_grains():
+    """The 256 grains of bench.py's large-grain workload (seed 55): x
+    uniform in [10, 30], axis ratio log-uniform in [0.33, 3]."""
+    rng = np.random.default_rng(55)
+    n = 256
+    x = rng.uniform(10.0, 30.0, n)
+    d = np.exp(rng.uniform(np.log(0.33), np.log(3.0), n))
+    m = rng.uniform(1.3, 2.0, n) + 1j * np.exp(rng.uniform(np.log(1e-3), 0.0, n))
+    lam = 1e-6
+    return x * lam / (2 * np.pi), lam, m, d
+
+
+def _bench5_one(i):
+    """nmax of one bench grain from the reference module's TMatrix
+    (calculator schedule, maximum_order 200, no orientation average)."""
+    r, lam, m, d = _bench5_grains()
+    T = O.ref_module().TMatrix(r[i], d[i], lam, m[i], cos2beta=-1.0)
+    return T.get_nmax()
+
+
+def _child(fn_name, i, q):
+    q.put(globals()[fn_name](i))
+
+
+def _isolated(fn_name, n, nproc=8):
+    """fn(i) for i < n, each in a process of its own (at most nproc at a
+    time), because the reference aborts the process when a grain does not
+    converge. Returns the results, None where the process aborted."""
+    import multiprocessing as mp
+    import queue
+    import time
+    ctx = mp.get_context("spawn")
+    out = [None] * n
+    running = {}
+    nxt = 0
+    while nxt < n or running:
+        while nxt < n and len(running) < nproc:
+            q = ctx.Queue()
+            p = ctx.Process(target=_child, args=(fn_name, nxt, q))
+            p.start()
+            running[nxt] = (p, q)
+            nxt += 1
+        for i in list(running):
+            p, q = running[i]
+            try:
+                out[i] = q.get_nowait()
+            except queue.Empty:
+                if p.is_alive():
+                    continue
+                try:
+                    out[i] = q.get(timeout=1)
+                except queue.Empty:
+                    pass  # aborted: not converged
+            p.join()
+            del running[i]
+        time.sleep(0.2)
+    return out
+
+
+def config5():
+    """Calculator-schedule outcomes of the reference module: for the seeded
+    large grains, converged or aborted ("Unable to converge!"), nmax, and
+    the random-orientation Z at 181 angles of the converged ones; for the
+    256 grains of bench.py's large-grain workload, converged or aborted and
+    nmax."""
+    r, lam, m, d = _config5_grains()
+    n = len(r)
+    res = _isolated("_config5_one", n)
+    conv = np.array([v is not None for v in res], np.int32)
+    nmax = np.array([v[0] if v is not None else 0 for v in res], np.int32)
+    Z = np.stack([v[1] if v is not None else np.zeros((181, 4, 4)) for v in res])
+    rb, lamb, mb, db = _bench5_grains()
+    resb = _isolated("_bench5_one", len(rb))
+    return {"r_ev": r, "wavelength": np.array([lam]), "m": m, "d": d,
+            "converged": conv, "nmax": nmax, "z181": Z,
+            "bench_r_ev": rb, "bench_m": mb, "bench_d": db,
+            "bench_converged": np.array([v is not None for v in resb], np.int32),
+            "bench_nmax": np.array([v if v is not None else 0 for v in resb],
+                                   np.int32)}
+
+
 def draine():
     """Refractive indices of the reference's DraineDustProperties (tabulated
     Draine 2003 optical constants from its data directory) for the three
@@ -244,9 +351,10 @@ def draine():
 
 
 if __name__ == "__main__":
-    # python make_golden.py [stages tmatrices tables plain draine]: the named
+    # python make_golden.py [stages tmatrices tables plain draine config5]: the named
     # sets (default all)
-    which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain", "draine"]
+    which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain", "draine",
+                             "config5"]
     for name in which:
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **globals()[name]())
     print("golden fixtures written to", HERE)

@@ -153,6 +153,51 @@ def test_tangents_vs_oracle_finite_differences(ctx):
     _compare(dq, fds, q)
 
 
+def _oracle_fd_grain(job):
+    """Central differences of the oracle's averaged extinction for one grain
+    at its fixed order: (params, lam, nmax, ngauss, coeffs) -> fd[rel][theta,
+    k, p] for the relative steps 1e-6 and 1e-5 (runs in a pool worker)."""
+    params, lam, nmax, ngauss, coeffs = job
+    out = []
+    for rel in (1e-6, 1e-5):
+        fd = np.zeros((len(THETAS), 3, 4))
+        for p in range(4):
+            h = _step(params, p) * (rel / FD_STEP)
+            vals = []
+            for sgn in (1, -1):
+                x = params.copy()
+                x[p] += sgn * h
+                vals.append(_oracle_q(x[2], lam, x[0] + 1j * x[1], x[3], nmax,
+                                      ngauss, coeffs))
+            fd[:, :, p] = (vals[0] - vals[1]) / (2 * h)
+        out.append(fd)
+    return out
+
+
+def test_tangents_vs_oracle_fd_64_grains(ctx, oracle_pool):
+    """The seeded 64-grain subset of the 4096-grain batch (config-2
+    distributions, seed 1; x in [0.1, 10], orders 10-32): tangents at the
+    converged orders against central differences of the CPU oracle (the
+    reference's algorithm, pinned bit for bit to it) at the same orders,
+    within 1e-6."""
+    r, lam, m, d = H.config2_sample(4096, 1)
+    pick = np.sort(np.random.default_rng(64).choice(4096, 64, replace=False))
+    r, m, d = r[pick], m[pick], d[pick]
+    res = ctx.tmatrix_batch(r, lam, m, d, min_order=10, max_order=100)
+    assert (res.status == 0).all()
+    nmax, ngauss = res.nmax.copy(), res.ngauss.copy()
+    coeffs = _coeffs(2, 0.5, order=2 * int(nmax.max()))
+    q, dq = ctx.gradients(THETAS, coeffs)
+    params = np.stack([m.real, m.imag, r, d], axis=1)
+    jobs = [(params[i], lam, int(nmax[i]), int(ngauss[i]), coeffs)
+            for i in range(len(r))]
+    per = oracle_pool.map(_oracle_fd_grain, jobs)
+    fds = [np.stack([p[k] for p in per]) for k in range(2)]
+    worst = _compare(dq, fds, q)
+    print("64 grains (orders %d-%d): worst relative error vs oracle FD %.3g"
+          % (nmax.min(), nmax.max(), worst))
+
+
 def test_autograd_function(ctx):
     import torch
     from costuum_b200.autograd import extinction
@@ -169,3 +214,25 @@ def test_autograd_function(ctx):
     assert np.allclose(q.detach().numpy(), qq, rtol=1e-12)
     want = np.einsum("ntk,ntkp->np", w.numpy(), dq)
     assert np.allclose(params.grad.numpy(), want, rtol=1e-12, atol=0)
+
+
+def test_autograd_backward_after_another_batch(ctx):
+    """Backward right after its forward reuses the forward's LU factors;
+    backward after another batch ran on the same context recomputes the
+    blocks at the forward's orders. Both give the same gradient."""
+    import torch
+    from costuum_b200 import autograd as AG
+    r, lam, m, d = H.config2_sample(6, 31, xmax=8.0)
+    coeffs = _coeffs(0, 0.0)
+    w = torch.tensor(np.random.default_rng(1).standard_normal((6, len(THETAS), 3)))
+    grads = []
+    for other in (False, True):
+        params = torch.tensor(np.stack([m.real, m.imag, r, d], axis=1),
+                              dtype=torch.float64, requires_grad=True)
+        q = AG.extinction(params, lam, THETAS, coeffs, max_order=60)
+        if other:
+            r2, lam2, m2, d2 = H.config2_sample(5, 32)
+            AG._context().tmatrix_batch(r2, lam2, m2, d2, max_order=60)
+        (q * w).sum().backward()
+        grads.append(params.grad.numpy().copy())
+    assert np.allclose(grads[0], grads[1], rtol=1e-12, atol=0)

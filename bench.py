@@ -459,6 +459,10 @@ def run_ours(args):
                               "LU factors",
               "adjoint_finite": bool(np.isfinite(dq5[res5.status == 0]).all())}
 
+    avg = None
+    if rank == 0 and world == 1 and not args.skip_extras:
+        avg = averaging_leg(ctx, lib, dmma)
+
     # roofline of the dominant kernel (block kernels: assembly + LU + solve),
     # algorithmic flops of the per-grain model (every chain order and every
     # m block as a full 2nb x 2nb assembly, LU and solve) over the summed
@@ -522,6 +526,7 @@ def run_ours(args):
             "batched_vs_plain": (value / plain["value"]) if plain else None,
             "gradient": grad,
             "plain_path_config5": c5,
+            "averaging": avg,
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
@@ -529,6 +534,86 @@ def run_ours(args):
     ctx.close()
     dist.close()
     return 0
+
+
+def hbm_peak():
+    """Measured HBM copy bandwidth of this pool's B200s (GB/s) and its
+    source: MEASURED_PEAKS.json beside this file, else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError):
+        pass
+    return 6650.0, "fallback (no MEASURED_PEAKS.json)"
+
+
+def averaging_leg(ctx, lib, fp64_peak):
+    """The averaging kernels on a sub-grid of the averaged-coefficients
+    workload: 16 of the 64 radii (0.01-2 um) x every 8th wavelength of
+    logspace(0.1, 100 um, 200) with x <= 50 x the 20-node Draine-Hensley
+    shape distribution, Davis-Greenstein alignment above 0.1 um, Qabs and
+    Qext at 32 zenith angles, through get_table. Per kernel: device time
+    (CUDA events), algorithmic bytes and flops over that time, against the
+    measured HBM and FP64 peaks."""
+    from costuum_b200 import CosTuuM as C
+    P = ctypes.c_double
+    sizes = np.logspace(np.log10(0.01e-6), np.log10(2e-6), 64)[::4]
+    lams = np.logspace(-7, -4, 200)
+    lams = lams[2 * np.pi * sizes[-1] / lams <= 50.0][::8]
+    th = np.arccos(np.linspace(-1, 1, 32))
+
+    def run():
+        return C.get_table(
+            types=np.array([0]), sizes=sizes, wavelengths=lams, thetas=th,
+            shape_distribution=C.DraineHensleyShapeDistribution(20),
+            alignment_distribution=C.SizeBasedAlignmentDistribution(
+                1e-7, C.DAVIS_GREENSTEIN_ALIGNMENT, maximum_order=100),
+            dust_properties=C.CustomDustProperties(lambda w, s, t: dielectric_m(w)),
+            maximum_order=100, do_absorption=True, do_extinction=True,
+            context=ctx)
+
+    run()  # tables, plans and buffers of this grid
+    h = ctx._h
+    lib.tmx_profile_enable(h, 1)
+    t0 = time.perf_counter()
+    out = run()
+    wall = time.perf_counter() - t0
+    peak_gbs, peak_src = hbm_peak()
+    kernels = {}
+    for k, name in ((2, "k_orient_pairs"), (3, "k_amp"), (4, "k_shape_avg")):
+        ms = np.zeros(1)
+        n = ctypes.c_int64()
+        fl = np.zeros(1)
+        by = P()
+        lib.tmx_profile_read(h, k, _ptr(ms), ctypes.byref(n), _ptr(fl))
+        lib.tmx_profile_bytes(h, k, ctypes.byref(by))
+        s = max(ms[0] * 1e-3, 1e-12)
+        kernels[name] = {"ms": ms[0], "launches": n.value,
+                         "bytes": by.value, "gbs": by.value / s / 1e9,
+                         "hbm_frac": by.value / s / 1e9 / peak_gbs,
+                         "flops": fl[0], "tflops": fl[0] / s / 1e12,
+                         "fp64_frac": fl[0] / s / 1e12 / fp64_peak}
+    lib.tmx_profile_enable(h, 0)
+    return {"what": "averaging kernels on a 16-radius x %d-wavelength x 20-shape "
+                    "sub-grid of the averaged-coefficients workload (%d grains; "
+                    "Draine-Hensley shapes, Davis-Greenstein alignment above "
+                    "0.1 um, Qabs and Qext at 32 angles)"
+                    % (len(lams), len(sizes) * len(lams) * 20),
+            "grains": len(sizes) * len(lams) * 20, "get_table_s": wall,
+            "hbm_peak_gbs": peak_gbs, "hbm_peak": peak_src,
+            "fp64_peak_tflops": fp64_peak,
+            "bytes_model": "orientation average: T in + averaged T out; "
+                           "amplitudes: averaged T in + 4 complex per job and "
+                           "azimuth out; shape average: 8 (n_shape + 1) n_theta "
+                           "n_coef per (size, wavelength) + weights",
+            "kernels": kernels, "finite": bool(np.isfinite(out).all())}
+
+
+def _ptr(a):
+    from costuum_b200 import _lib
+    return _lib.ptr(a)
 
 
 def dielectric_m(lam):

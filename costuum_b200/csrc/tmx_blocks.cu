@@ -488,7 +488,17 @@ __global__ void __launch_bounds__(NT, MINB)
 // memory. Solve: lane r owns row r of -RgQ_c and runs both triangular solves
 // on it against the factors, so no lane waits on another.
 
-#define TMX_WG 4 // quadrature nodes per warp chunk
+#ifndef TMX_WG
+#define TMX_WG 4 // quadrature nodes per warp chunk (a multiple of 4)
+#endif
+// resident CTAs of four warps per SM the warp kernels are compiled for
+// (register budget 65536 / (128 x MINB) per thread)
+#ifndef TMX_WARP_DFMA_MINB
+#define TMX_WARP_DFMA_MINB 4
+#endif
+#ifndef TMX_WARP_DMMA_MINB
+#define TMX_WARP_DMMA_MINB 3
+#endif
 
 template <int NBM>
 __host__ __device__ constexpr int warp_elems() {
@@ -530,11 +540,15 @@ __device__ __forceinline__ void cp_wait_all() {
 template <int NBM>
 struct StagePlan {
   static constexpr int SL_MAX = (NBM * 5 + 31) / 32;
+  // TMX_WG nodes x TMX_NS / 2 pieces of node scalars, SS per lane
+  static constexpr int SS = TMX_WG * (TMX_NS / 2) / 32;
+  static_assert(SS * 32 == TMX_WG * (TMX_NS / 2), "node-scalar pieces per lane");
   const double *src[SL_MAX]; // piece at node 0
   int stride[SL_MAX];        // doubles per node
   int dst[SL_MAX];           // double offset in the stage (node 0); -1: none
-  const double *ssrc;        // node-scalar piece at node 0
-  int sdst;                  // -1: none
+  const double *ssrc[SS];    // node-scalar pieces (at chunk start 0)
+  int sdst[SS];
+  int sgl[SS];               // node of each piece within the chunk
 
   __device__ __forceinline__ void init(const ClassDesc &D, int N,
                                        const double *__restrict__ T,
@@ -558,12 +572,15 @@ struct StagePlan {
         dst[j] = a * TMX_ROW + 2 * p;
       }
     }
-    // TMX_WG nodes x TMX_NS / 2 pieces of node scalars = 32
-    static_assert(TMX_WG * (TMX_NS / 2) == 32, "one node-scalar piece per lane");
-    const int gl = lane / (TMX_NS / 2);
-    const int p = lane - gl * (TMX_NS / 2);
-    ssrc = S + (int64_t)gl * TMX_NS + 2 * p;
-    sdst = TMX_WG * NBM * TMX_ROW + gl * TMX_NS + 2 * p;
+#pragma unroll
+    for (int j = 0; j < SS; ++j) {
+      const int q = lane + 32 * j;
+      const int gl = q / (TMX_NS / 2);
+      const int p = q - gl * (TMX_NS / 2);
+      ssrc[j] = S + (int64_t)gl * TMX_NS + 2 * p;
+      sdst[j] = TMX_WG * NBM * TMX_ROW + gl * TMX_NS + 2 * p;
+      sgl[j] = gl;
+    }
   }
 
   // copies of nodes [g0, g0 + TMX_WG) (one commit group per lane)
@@ -581,8 +598,11 @@ struct StagePlan {
         }
       }
     }
-    if (g0 + (sdst - TMX_WG * NBM * TMX_ROW) / TMX_NS < ng) {
-      cp16(st + sdst, ssrc + (int64_t)g0 * TMX_NS);
+#pragma unroll
+    for (int j = 0; j < SS; ++j) {
+      if (g0 + sgl[j] < ng) {
+        cp16(st + sdst[j], ssrc[j] + (int64_t)g0 * TMX_NS);
+      }
     }
     cp_commit();
   }
@@ -1052,9 +1072,10 @@ static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
 #define TMX_WG32 4
 
 __host__ __device__ constexpr int cta32_elems() {
-  // F[WG][4][32] + W[2][WG][4][32], or Q, RgQ [32][33], 1/U_jj, indices
-  return (12 * TMX_WG32 * 32 > 2 * 32 * 33 + 3 * 32) ? 12 * TMX_WG32 * 32
-                                                      : 2 * 32 * 33 + 3 * 32;
+  // F[WG][4][32] + W[2][WG][4][32], or Q, RgQ [32][33], 1/U_jj, indices and
+  // two copies of a pivot column
+  return (12 * TMX_WG32 * 32 > 2 * 32 * 33 + 5 * 32) ? 12 * TMX_WG32 * 32
+                                                      : 2 * 32 * 33 + 5 * 32;
 }
 
 __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
@@ -1069,6 +1090,7 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   cplx *uinv = Rm + NBM * LD;        // [NBM]
   int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
   int *piv = perm + NBM;                           // [NBM]
+  cplx *colbuf = uinv + 3 * NBM;     // [2][NBM]: column i of LU step i
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int wib = tid >> 5;
@@ -1190,12 +1212,23 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
         }
       }
     }
+    if (wib == 0 && lane < nb) {
+      colbuf[lane] = Qm[lane * LD];
+    }
     __syncthreads();
-    if (wib == 0) {
-      // LU in place in Qm, lane r updates row r
+    {
+      // LU in place in Qm on all four warps: thread (lane r, warp w) holds
+      // row position r and the columns k = w, w + 4, ... Every warp finds
+      // the pivot of step i itself from a copy of column i (colbuf[i & 1],
+      // written by the column's owner at the end of step i - 1; the same
+      // first-maximum rule as Matrix::plu_inverse), so one barrier per step
+      // suffices: the rows i and bi are swapped column by column by the
+      // owners of the columns, and the multiplier of row r comes from the
+      // copy of column i.
       bool singular = false;
       for (int i = 0; i < nb; ++i) {
-        double best = (lane >= i && lane < nb) ? cabs_dev(Qm[lane * LD + i]) : -1.;
+        const cplx cr = (lane < nb) ? colbuf[(i & 1) * NBM + lane] : mkc(0., 0.);
+        double best = (lane >= i && lane < nb) ? cabs_dev(cr) : -1.;
         int bi = lane;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -1207,11 +1240,17 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
           }
         }
         singular = singular || !(best > 0.);
-        if (lane == 0) {
+        // column i after the swap: the pivot at i, the old Q_ii at bi
+        const cplx piv_v = mkc(__shfl_sync(0xffffffffu, cr.x, bi),
+                               __shfl_sync(0xffffffffu, cr.y, bi));
+        const cplx cii = mkc(__shfl_sync(0xffffffffu, cr.x, i),
+                             __shfl_sync(0xffffffffu, cr.y, i));
+        if (wib == 0 && lane == 0) {
           piv[i] = bi;
         }
         if (bi != i) {
-          for (int k = lane; k < nb; k += 32) {
+          // rows i and bi exchange their entries in this warp's columns
+          for (int k = wib + 4 * lane; k < nb && lane < 8; k += 128) {
             const cplx t = Qm[i * LD + k];
             Qm[i * LD + k] = Qm[bi * LD + k];
             Qm[bi * LD + k] = t;
@@ -1219,36 +1258,39 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
         }
         __syncwarp();
         if (lane > i && lane < nb) {
-          const cplx pinv = cinv_lu(Qm[i * LD + i]);
-          const cplx l = cmul(Qm[lane * LD + i], pinv);
-          Qm[lane * LD + i] = l;
-          // four entries at a time: all loads before the stores (the pivot
-          // row is only read in this step), so the updates overlap
+          const cplx pinv = cinv_lu(piv_v);
+          const cplx l = cmul((lane == bi) ? cii : cr, pinv);
+          if ((i & 3) == wib) {
+            Qm[lane * LD + i] = l;
+          }
           cplx *qr = Qm + lane * LD;
           const cplx *pr = Qm + i * LD;
-          int k = i + 1;
-          for (; k + 3 < nb; k += 4) {
-            cplx a0 = qr[k], a1 = qr[k + 1], a2 = qr[k + 2], a3 = qr[k + 3];
-            const cplx b0 = pr[k], b1 = pr[k + 1], b2 = pr[k + 2], b3 = pr[k + 3];
-            a0 = csub(a0, cmul(l, b0));
-            a1 = csub(a1, cmul(l, b1));
-            a2 = csub(a2, cmul(l, b2));
-            a3 = csub(a3, cmul(l, b3));
-            qr[k] = a0;
-            qr[k + 1] = a1;
-            qr[k + 2] = a2;
-            qr[k + 3] = a3;
+          // this warp's columns k > i: the first is the smallest k > i with
+          // k = wib (mod 4); it is column i + 1 for the owner of that column,
+          // which also copies it for the next step's pivot search
+          int k = i + 1 + ((wib - (i + 1)) & 3);
+          if (k == i + 1 && k < nb) {
+            const cplx v = csub(qr[k], cmul(l, pr[k]));
+            qr[k] = v;
+            colbuf[(k & 1) * NBM + lane] = v;
+            k += 4;
           }
-          for (; k < nb; ++k) {
+          for (; k + 4 < nb; k += 8) {
+            cplx a0 = qr[k], a1 = qr[k + 4];
+            const cplx b0 = pr[k], b1 = pr[k + 4];
+            qr[k] = csub(a0, cmul(l, b0));
+            qr[k + 4] = csub(a1, cmul(l, b1));
+          }
+          for (; k < nb; k += 4) {
             qr[k] = csub(qr[k], cmul(l, pr[k]));
           }
         }
-        __syncwarp();
+        __syncthreads();
       }
-      if (lane < nb) {
+      if (wib == 0 && lane < nb) {
         uinv[lane] = cinv_lu(Qm[lane * LD + lane]);
       }
-      if (lane == 0) {
+      if (wib == 0 && lane == 0) {
         // column exchanges of Matrix::plu_inverse step 4, as a gather index
         for (int j = 0; j < nb; ++j) {
           perm[j] = j;
@@ -1661,10 +1703,10 @@ void tmx_launch_blocks(const TmxBlockArgs &a, cudaStream_t stream) {
   }
   switch (f) {
   case TMX_BLOCKS_WARP_DFMA:
-    launch_warp_variant<1, 2, 4, false>(a, stream);
+    launch_warp_variant<1, 2, TMX_WARP_DFMA_MINB, false>(a, stream);
     return;
   case TMX_BLOCKS_WARP_DMMA:
-    launch_warp_variant<1, 1, 3, true>(a, stream);
+    launch_warp_variant<1, 1, TMX_WARP_DMMA_MINB, true>(a, stream);
     return;
   case TMX_BLOCKS_CTA32:
     launch_cta32(a, stream);
@@ -1690,7 +1732,7 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
                            double tolerance, int order, int last_order,
                            int32_t *next_active, int32_t *next_count,
                            int32_t *done_list, int32_t *done_ord,
-                           int32_t *done_count) {
+                           int32_t *done_pos, int32_t *done_count) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive) {
     return;
@@ -1755,6 +1797,7 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
     const int q = atomicAdd(done_count, 1);
     done_list[q] = g;
     done_ord[q] = order;
+    done_pos[q] = p;
   }
 }
 
@@ -1763,14 +1806,83 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
-                         int32_t *done_ord, int32_t *done_count,
-                         cudaStream_t stream) {
+                         int32_t *done_ord, int32_t *done_pos,
+                         int32_t *done_count, cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
       active, nactive, slots, diag, state, tolerance, order, last_order,
-      next_active, next_count, done_list, done_ord, done_count);
+      next_active, next_count, done_list, done_ord, done_pos, done_count);
+}
+
+// ------------------------------------------------------------- kept tables --
+
+// The node scalars and Bessel tables of a grain's final order are the ones
+// its block round needs. Right after the convergence test of a group of
+// orders (before the next group overwrites the order loop's table buffers),
+// every grain that became final in the group -- done-list entries
+// [*next, counters[1]) -- has its tables copied into the batch's arena at a
+// reserved offset (in doubles, a multiple of 16), recorded per grain and per
+// done-list entry; -1 where the arena is full (the round then recomputes
+// them). One CTA per entry, grid-stride; the last CTA to finish moves *next
+// to the end of the range.
+__global__ void k_keep_tables(TmxKeepArgs K) {
+  __shared__ long long s_off;
+  __shared__ unsigned s_last;
+  const int begin = *K.next;
+  const int end = K.counters[1];
+  for (int q = begin + blockIdx.x; q < end; q += gridDim.x) {
+    const int g = K.done_list[q];
+    const int s = K.done_ord[q] - K.order0;
+    const int p = K.done_pos[q];
+    const TmxChainBase b = K.base[s];
+    const int64_t tsz = b.tab_stride, nsz = b.nsc_stride;
+    const int64_t want = ((tsz + 15) & ~(int64_t)15) + ((nsz + 15) & ~(int64_t)15);
+    if (threadIdx.x == 0) {
+      const long long off =
+          (long long)atomicAdd(K.used, (unsigned long long)want);
+      s_off = (off + want <= K.cap) ? off : -1;
+    }
+    __syncthreads();
+    const long long off = s_off;
+    if (off >= 0) {
+      const double2 *ts = reinterpret_cast<const double2 *>(K.tab + b.tab + p * tsz);
+      double2 *td = reinterpret_cast<double2 *>(K.arena + off);
+      for (int64_t u = threadIdx.x; u < tsz / 2; u += blockDim.x) {
+        td[u] = ts[u];
+      }
+      const int64_t noff = off + ((tsz + 15) & ~(int64_t)15);
+      const double2 *ns = reinterpret_cast<const double2 *>(K.nsc + b.nsc + p * nsz);
+      double2 *nd = reinterpret_cast<double2 *>(K.arena + noff);
+      for (int64_t u = threadIdx.x; u < nsz / 2; u += blockDim.x) {
+        nd[u] = ns[u];
+      }
+    }
+    if (threadIdx.x == 0) {
+      K.keep_tab[g] = off;
+      K.keep_q[q] = off;
+    }
+    __syncthreads();
+  }
+  // the last CTA moves the start of the next range
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s_last = (atomicAdd(K.ticket, 1u) == gridDim.x - 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    *K.next = end;
+    *K.ticket = 0u;
+    __threadfence();
+  }
+}
+
+void tmx_launch_keep_tables(const TmxKeepArgs &K, int max_entries,
+                            cudaStream_t stream) {
+  const int blocks = std::max(1, std::min(max_entries, 148 * 4));
+  k_keep_tables<<<blocks, 128, 0, stream>>>(K);
 }
 
 // ------------------------------------------------------------- Q sums ------

@@ -70,6 +70,9 @@ struct tmx_ctx {
   // plan of the observable kernels (first pair of each grain, job groups)
   int64_t o_ngrains = 0, o_npairs = 0;
   int o_nbmax = 1, o_ngrp = 0;
+  // flops of one matrix set in the orientation average and the amplitudes
+  // of the current plan (counted while profiling)
+  double o_fl_orient = 0., o_fl_amp = 0.;
   int32_t *pinned = nullptr;     // [0] active count, [1] done count
   DevBuf done;                    // grains whose order became final, in order
   int32_t *pinned_done = nullptr; // host copy of new done-list entries
@@ -82,7 +85,8 @@ struct tmx_ctx {
     double ms = 0.;
     int64_t launches = 0;
     double flops = 0.;
-  } prof[2]; // 0: block kernel, 1: table kernel
+    double bytes = 0.; // algorithmic bytes (each operand read or written once)
+  } prof[TMX_PROF_KERNELS]; // tmx_profile_kernel
   // timing events, reused once their pairs are resolved (at the next read of
   // the profile), so that a profiled batch creates none
   std::vector<cudaEvent_t> prof_pool;
@@ -93,6 +97,7 @@ struct tmx_ctx {
   // of the batch, so the gradients need no second pass of the blocks.
   struct RoundRec {
     double *tab = nullptr, *nsc = nullptr;
+    bool own_tables = true; // false: tab and nsc are the batch's table arena
     TmxSlot *slots = nullptr;
     TmxItem *items = nullptr;
     cplx *lu = nullptr;
@@ -149,6 +154,17 @@ struct tmx_ctx {
   double *sink = nullptr;
   int64_t sink_cap = 0;
   int64_t sink_done = 0;
+  // final-order tables of the grains of a batched computation, copied out of
+  // the order loop's buffers as the grains become final (k_keep_tables):
+  // arena, per-grain offsets (device and host, -1: none), per done-list
+  // entry offsets, done-list positions, and the copy kernel's counters
+  // ({next entry, ticket, doubles used})
+  DevBuf keep_arena, keep_tab, keep_q, done_pos, keep_ctl;
+  std::vector<int64_t> keep_off_h;
+  int64_t *pinned_keep = nullptr;
+  int64_t pinned_keep_cap = 0;
+  bool keep_valid = false;
+  int64_t keep_used_last = 0; // doubles the last batch used
 };
 
 #define CK(call)                                                               \
@@ -231,7 +247,7 @@ static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a,
 }
 
 static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
-                           cudaStream_t st = nullptr) {
+                           cudaStream_t st = nullptr, double bytes = 0.) {
   if (!ctx->profiling) {
     return 0;
   }
@@ -244,6 +260,7 @@ static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
   ctx->prof[k].pending.push_back({a, b});
   ctx->prof[k].launches += 1;
   ctx->prof[k].flops += flops;
+  ctx->prof[k].bytes += bytes;
   return 0;
 }
 

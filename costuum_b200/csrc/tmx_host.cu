@@ -334,7 +334,8 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
                     &ctx->o_pairs, &ctx->o_grp, &ctx->o_x,
                     &ctx->p2tab, &ctx->p2nsc, &ctx->p2scratch, &ctx->p2slots,
-                    &ctx->p2items, &ctx->done,
+                    &ctx->p2items, &ctx->done, &ctx->keep_arena, &ctx->keep_tab,
+                    &ctx->keep_q, &ctx->done_pos, &ctx->keep_ctl,
                     &ctx->state0, &ctx->actinit,
                     &ctx->gl_x,  &ctx->gl_w,   &ctx->gl_off,  &ctx->wig,
                     &ctx->wig_off, &ctx->grains, &ctx->state,  &ctx->act0,
@@ -350,6 +351,9 @@ void tmx_destroy(tmx_ctx *ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->pinned_done) {
     cudaFreeHost(ctx->pinned_done);
+  }
+  if (ctx->pinned_keep) {
+    cudaFreeHost(ctx->pinned_keep);
   }
   if (ctx->pinned) {
     cudaFreeHost(ctx->pinned);
@@ -415,6 +419,7 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   ctx->uploaded = false;
+  ctx->keep_valid = false;
   ctx->have_batch = false;
   int rc;
   if ((rc = tmx_release_rounds(ctx))) {
@@ -525,6 +530,20 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     t_total += tmx_tmatrix_size(N);
   }
   *t_end = t_total;
+  // A round of the order loop takes its grains' final-order tables from
+  // the batch's arena, where the loop copied them (k_keep_tables), instead
+  // of computing them again -- if every grain of the round has a copy.
+  bool kept = temp && ctx->keep_valid && np2 > 0;
+  for (int s = 0; kept && s < np2; ++s) {
+    kept = ctx->keep_off_h[p2[s]] >= 0;
+  }
+  if (kept) {
+    for (int s = 0; s < np2; ++s) {
+      TmxSlot &sl = slots[s];
+      sl.tab = ctx->keep_off_h[sl.grain];
+      sl.nsc = sl.tab + (int64_t)sl.ngauss * sl.nmax * TMX_NQ;
+    }
+  }
   std::vector<int> full_sets;
   if ((rc = ensure_wigner(ctx, keys, true, full_sets))) {
     return rc;
@@ -649,9 +668,13 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   cplx *scratch = (cplx *)ctx->p2scratch.p;
   TmxSlot *dslots = (TmxSlot *)ctx->p2slots.p;
   TmxItem *ditems = (TmxItem *)ctx->p2items.p;
-  if (temp) {
+  if (kept) {
+    tab = nsc = (double *)ctx->keep_arena.p;
+  } else if (temp) {
     CK(cudaMallocFromPoolAsync((void **)&tab, std::max<int64_t>(1, tab_total) * sizeof(double), ctx->pool, st));
     CK(cudaMallocFromPoolAsync((void **)&nsc, std::max<int64_t>(1, nsc_total) * sizeof(double), ctx->pool, st));
+  }
+  if (temp) {
     CK(cudaMallocFromPoolAsync((void **)&scratch, std::max<int64_t>(1, scr_total) * sizeof(cplx), ctx->pool, st));
     CK(cudaMallocFromPoolAsync((void **)&dslots, np2 * sizeof(TmxSlot), ctx->pool, st));
     CK(cudaMallocFromPoolAsync((void **)&ditems, std::max<int64_t>(1, nitems) * sizeof(TmxItem), ctx->pool, st));
@@ -668,21 +691,23 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync((cplx *)ctx->T.p + t_base, 0, (t_total - t_base) * sizeof(cplx), st));
   cudaEvent_t pe = nullptr;
-  if ((rc = prof_begin(ctx, 1, &pe, st))) {
-    return rc;
-  }
-  int ngmax = 1, nmmax = 1;
-  for (const TmxSlot &sl : slots) {
-    ngmax = std::max(ngmax, sl.ngauss);
-    nmmax = std::max(nmmax, sl.nmax);
-  }
-  tmx_launch_tables(dslots, np2, (const TmxGrain *)ctx->grains.p,
-                    (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
-                    (const int64_t *)ctx->gl_off.p, tab, nsc,
-                    ctx->up_sched.bessel_start, ngmax, nmmax, st);
-  LAUNCHED();
-  if ((rc = prof_end(ctx, 1, pe, 0., st))) {
-    return rc;
+  if (!kept) {
+    if ((rc = prof_begin(ctx, 1, &pe, st))) {
+      return rc;
+    }
+    int ngmax = 1, nmmax = 1;
+    for (const TmxSlot &sl : slots) {
+      ngmax = std::max(ngmax, sl.ngauss);
+      nmmax = std::max(nmmax, sl.nmax);
+    }
+    tmx_launch_tables(dslots, np2, (const TmxGrain *)ctx->grains.p,
+                      (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
+                      (const int64_t *)ctx->gl_off.p, tab, nsc,
+                      ctx->up_sched.bessel_start, ngmax, nmmax, st);
+    LAUNCHED();
+    if ((rc = prof_end(ctx, 1, pe, 0., st))) {
+      return rc;
+    }
   }
   // class-size buckets, one launch each (largest first): the first on `st`,
   // the others on the two auxiliary streams beside it, so that the smaller
@@ -787,6 +812,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     tmx_ctx::RoundRec rec;
     rec.tab = tab;
     rec.nsc = nsc;
+    rec.own_tables = !kept;
     rec.slots = dslots;
     rec.items = ditems;
     rec.lu = lu_keep;
@@ -795,8 +821,10 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     ctx->rounds_kept.push_back(std::move(rec));
     CK(cudaFreeAsync(scratch, st));
   } else if (temp) {
-    CK(cudaFreeAsync(tab, st));
-    CK(cudaFreeAsync(nsc, st));
+    if (!kept) {
+      CK(cudaFreeAsync(tab, st));
+      CK(cudaFreeAsync(nsc, st));
+    }
     CK(cudaFreeAsync(scratch, st));
     CK(cudaFreeAsync(dslots, st));
     CK(cudaFreeAsync(ditems, st));
@@ -876,6 +904,9 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
 // batch has finished: every batch ends with a host synchronisation).
 int tmx_release_rounds(tmx_ctx *ctx) {
   for (auto &r : ctx->rounds_kept) {
+    if (!r.own_tables) {
+      r.tab = r.nsc = nullptr; // the batch's table arena
+    }
     for (void *p : {(void *)r.tab, (void *)r.nsc, (void *)r.slots, (void *)r.items,
                     (void *)r.lu}) {
       if (p) {
@@ -1004,6 +1035,37 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     ctx->pinned_done_cap = 2 * n;
   }
   CK(cudaMemsetAsync(ctx->count.p, 0, 2 * sizeof(int32_t), st));
+  // arena for the final-order tables of every grain (k_keep_tables): sized
+  // from the last batch's use, else for orders up to 40; at most 8 GiB. A
+  // grain that does not fit keeps no copy and its round computes its tables.
+  ctx->keep_valid = false;
+  int64_t keep_cap = 0;
+  {
+    const int64_t topk = std::min(S.max_order - 1, 40);
+    const int64_t per = glf * topk * topk * TMX_NQ + glf * topk * TMX_NS + 32;
+    keep_cap = std::max<int64_t>(ctx->keep_used_last + ctx->keep_used_last / 4,
+                                 std::min<int64_t>(n * per, (int64_t)1 << 27));
+    keep_cap = std::min<int64_t>(keep_cap, (int64_t)1 << 30);
+    if ((rc = ensure(ctx, ctx->keep_arena, keep_cap * sizeof(double))) ||
+        (rc = ensure(ctx, ctx->keep_tab, n * sizeof(int64_t))) ||
+        (rc = ensure(ctx, ctx->keep_q, n * sizeof(int64_t))) ||
+        (rc = ensure(ctx, ctx->done_pos, n * sizeof(int32_t))) ||
+        (rc = ensure(ctx, ctx->keep_ctl, 32))) {
+      return rc;
+    }
+    CK(cudaMemsetAsync(ctx->keep_ctl.p, 0, 32, st));
+    if (ctx->pinned_keep_cap < n) {
+      if (ctx->pinned_keep) {
+        CK(cudaFreeHost(ctx->pinned_keep));
+        ctx->pinned_keep = nullptr;
+        ctx->pinned_keep_cap = 0;
+      }
+      CK(cudaMallocHost((void **)&ctx->pinned_keep, n * sizeof(int64_t)));
+      ctx->pinned_keep_cap = n;
+    }
+    ctx->keep_off_h.assign(n, -1);
+    ctx->keep_valid = true;
+  }
   // the rounds of this batch keep their buffers and LU factors
   struct KeepGuard {
     tmx_ctx *c;
@@ -1127,7 +1189,32 @@ int tmx_batch_compute(tmx_ctx *ctx) {
                             (TmxChainState *)ctx->state.p, S.tolerance, k + s, last,
                             (int32_t *)nxt->p, (int32_t *)ctx->count.p,
                             (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
-                            (int32_t *)ctx->count.p + 1, st);
+                            (int32_t *)ctx->done_pos.p, (int32_t *)ctx->count.p + 1,
+                            st);
+        LAUNCHED();
+      }
+      if (ctx->keep_valid) {
+        // the tables of the grains this chunk made final, before the next
+        // chunk or group overwrites them
+        TmxKeepArgs K;
+        K.done_list = (const int32_t *)ctx->done.p;
+        K.done_ord = (const int32_t *)ctx->done.p + n;
+        K.done_pos = (const int32_t *)ctx->done_pos.p;
+        K.counters = (const int32_t *)ctx->count.p;
+        K.next = (int32_t *)ctx->keep_ctl.p;
+        K.ticket = (unsigned *)ctx->keep_ctl.p + 1;
+        K.used = (unsigned long long *)ctx->keep_ctl.p + 1;
+        K.order0 = k;
+        for (int s = 0; s < G; ++s) {
+          K.base[s] = base[s];
+        }
+        K.tab = (const double *)ctx->tab.p;
+        K.nsc = (const double *)ctx->nsc.p;
+        K.arena = (double *)ctx->keep_arena.p;
+        K.cap = keep_cap;
+        K.keep_tab = (int64_t *)ctx->keep_tab.p;
+        K.keep_q = (int64_t *)ctx->keep_q.p;
+        tmx_launch_keep_tables(K, cn, st);
         LAUNCHED();
       }
     }
@@ -1140,6 +1227,11 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     CK(cudaMemcpyAsync(ctx->pinned_done + n + done_seen,
                        (int32_t *)ctx->done.p + n + done_seen, nact * sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
+    if (ctx->keep_valid) {
+      CK(cudaMemcpyAsync(ctx->pinned_keep + done_seen,
+                         (int64_t *)ctx->keep_q.p + done_seen, nact * sizeof(int64_t),
+                         cudaMemcpyDeviceToHost, st));
+    }
     if (!pending.empty()) {
       if ((rc = run_blocks_round(ctx, pending, (rounds & 1) ? ctx->stream3 : ctx->stream2,
                                  t_next, rounds > 0,
@@ -1162,6 +1254,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       const int32_t ko = ctx->pinned_done[n + j];
       ctx->nmax_h[g] = ko;
       ctx->ngauss_h[g] = glf * ko;
+      if (ctx->keep_valid) {
+        ctx->keep_off_h[g] = ctx->pinned_keep[j];
+      }
       ready.push_back(g);
     }
     done_seen = done_now;
@@ -1182,7 +1277,16 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   // ---- per-grain outcome of the order loop
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToHost, st));
+  if (ctx->keep_valid) {
+    CK(cudaMemcpyAsync(ctx->pinned + 4, ctx->keep_ctl.p, 4 * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost, st));
+  }
   CK(cudaStreamSynchronize(st));
+  if (ctx->keep_valid) {
+    uint64_t used = 0;
+    memcpy(&used, ctx->pinned + 6, sizeof(used));
+    ctx->keep_used_last = (int64_t)used;
+  }
   std::vector<int32_t> p2; // grains whose blocks have not been launched
   for (int64_t i = 0; i < n; ++i) {
     ctx->nmax_h[i] = st0[i].nmax;
@@ -1560,6 +1664,7 @@ int tmx_profile_enable(tmx_ctx *ctx, int on) {
     p.ms = 0.;
     p.launches = 0;
     p.flops = 0.;
+    p.bytes = 0.;
   }
   ctx->prof_used = 0;
   ctx->profiling = on != 0;
@@ -1572,9 +1677,17 @@ int tmx_profile_enable(tmx_ctx *ctx, int on) {
   return TMX_OK;
 }
 
+int tmx_profile_bytes(tmx_ctx *ctx, int kernel, double *bytes) {
+  if (!ctx || !bytes || kernel < 0 || kernel >= TMX_PROF_KERNELS) {
+    return TMX_ERR_INVALID;
+  }
+  *bytes = ctx->prof[kernel].bytes;
+  return TMX_OK;
+}
+
 int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
                      double *flops) {
-  if (!ctx || kernel < 0 || kernel > 1) {
+  if (!ctx || kernel < 0 || kernel >= TMX_PROF_KERNELS) {
     return TMX_ERR_INVALID;
   }
   CK(cudaSetDevice(ctx->device));

@@ -82,13 +82,34 @@ void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
 // m = 0 sums and the convergence test of one order; grains that continue go
 // to next_active, grains whose order is final are appended to done_list
 // (with that order in done_ord); grains already final are skipped
+// (done_pos: the grain's position in `active`)
 void tmx_launch_converge(const int32_t *active, int nactive,
                          const TmxSlot *slots, const double2 *diag,
                          TmxChainState *state, double tolerance, int order,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
-                         int32_t *done_ord, int32_t *done_count,
-                         cudaStream_t stream);
+                         int32_t *done_ord, int32_t *done_pos,
+                         int32_t *done_count, cudaStream_t stream);
+
+// copies of the final-order tables of the grains that became final in one
+// group of orders, into the batch's table arena (k_keep_tables)
+#define TMX_MAX_GROUP 8
+struct TmxKeepArgs {
+  const int32_t *done_list, *done_ord, *done_pos;
+  const int32_t *counters;          // [1]: entries in the done list
+  int32_t *next;                    // first entry not yet kept
+  unsigned *ticket;                 // CTAs finished (last one resets it)
+  int order0;                       // first order of the group
+  TmxChainBase base[TMX_MAX_GROUP]; // table layout of each order of the group
+  const double *tab, *nsc;          // the order loop's table buffers
+  double *arena;
+  long long cap;                    // arena capacity (doubles)
+  unsigned long long *used;         // doubles reserved so far
+  int64_t *keep_tab;                // per grain: arena offset (-1: none)
+  int64_t *keep_q;                  // per done-list entry: the same
+};
+void tmx_launch_keep_tables(const TmxKeepArgs &K, int max_entries,
+                            cudaStream_t stream);
 
 // full Q sums over all m blocks (TMatrixQTask) of the grains of a block round: q_out[2 g], q_out[2 g + 1]
 // for g = slots[s].grain

@@ -412,6 +412,40 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
   ctx->o_npairs = npairs;
   ctx->o_nbmax = nbmax;
   ctx->o_ngrp = (int)grp.size();
+  if (ctx->profiling) {
+    // flops of one matrix set over the kernels' index spaces: the
+    // orientation average 16 (2M + 1)(M + 1) per (n1, n2), M = min(n1, n2),
+    // of every averaged grain; the amplitudes 16 (2 nb)^2 per m block and job
+    double fo = 0., fa = 0.;
+    std::vector<double> per_job(nbmax + 1, -1.);
+    for (int64_t g = 0; g < n; ++g) {
+      const int N = og[g].nmax;
+      if (N > 0 && og[g].coef_set >= 0) {
+        for (int a = 1; a <= N; ++a) {
+          for (int b = 1; b <= N; ++b) {
+            const double M = std::min(a, b);
+            fo += 16. * (2. * M + 1.) * (M + 1.);
+          }
+        }
+      }
+    }
+    for (const TmxSJob &j : sj) {
+      const int N = og[j.grain].nmax;
+      if (N <= 0) {
+        continue;
+      }
+      if (per_job[N] < 0.) {
+        double s = 16. * 4. * N * N;
+        for (int k = 1; k <= N; ++k) {
+          s += 16. * 4. * k * k;
+        }
+        per_job[N] = s;
+      }
+      fa += per_job[N];
+    }
+    ctx->o_fl_orient = fo;
+    ctx->o_fl_amp = fa;
+  }
   return TMX_OK;
 }
 
@@ -441,6 +475,15 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
     amp.src[k] = avg.dst[k];
     amp.dst[k] = S_out[k];
   }
+  const int grid = tmx_amp_grid(ctx->o_nbmax, nmat);
+  if ((rc = ensure(ctx, ctx->o_x,
+                   (size_t)grid * nmat * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
+    return rc;
+  }
+  cudaEvent_t pe = nullptr;
+  if ((rc = prof_begin(ctx, TMX_PROF_ORIENT, &pe))) {
+    return rc;
+  }
   tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
                           (const int64_t *)ctx->o_pairs.p, (int)ctx->o_ngrains,
                           ctx->o_npairs, avg, nmat, (const double *)ctx->o_coef.p,
@@ -448,9 +491,12 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
                           (const double *)ctx->cg.p, ctx->cg_nmax, ctx->o_nbmax, 1,
                           st);
   LAUNCHED();
-  const int grid = tmx_amp_grid(ctx->o_nbmax, nmat);
-  if ((rc = ensure(ctx, ctx->o_x,
-                   (size_t)grid * nmat * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
+  // T-matrices in and averaged T-matrices out, once each
+  if ((rc = prof_end(ctx, TMX_PROF_ORIENT, pe, nmat * ctx->o_fl_orient, st,
+                     2. * nmat * t_total * sizeof(cplx)))) {
+    return rc;
+  }
+  if ((rc = prof_begin(ctx, TMX_PROF_AMP, &pe))) {
     return rc;
   }
   tmx_launch_amp((const TmxAmpGroup *)ctx->o_grp.p, ctx->o_ngrp,
@@ -458,6 +504,11 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
                  nmat, (const TmxAngle *)ctx->o_angles.p, (const cplx *)ctx->o_phis.p,
                  (cplx *)ctx->o_x.p, ctx->o_nbmax, grid, st);
   LAUNCHED();
+  // averaged T-matrices in, four complex amplitudes per job and azimuth out
+  if ((rc = prof_end(ctx, TMX_PROF_AMP, pe, nmat * ctx->o_fl_amp, st,
+                     nmat * (t_total + 4. * s_total) * sizeof(cplx)))) {
+    return rc;
+  }
   return TMX_OK;
 }
 
@@ -752,9 +803,18 @@ extern "C" int tmx_get_table(
                             (const double *)ctx->o_wts.p, account ? ngauss : 0,
                             (double *)ctx->o_gq.p, nq, do_abs, do_ext, st);
       LAUNCHED();
+      cudaEvent_t pe = nullptr;
+      if ((rc = prof_begin(ctx, TMX_PROF_SHAPE_AVG, &pe))) {
+        return rc;
+      }
       tmx_launch_shape_avg((int)nc, nshape, ntheta * nq, (const double *)ctx->o_gq.p,
                            (const double *)ctx->o_shw.p, (double *)ctx->o_cq.p, st);
       LAUNCHED();
+      // per cell: nshape inputs and one output per coefficient, the weights
+      if ((rc = prof_end(ctx, TMX_PROF_SHAPE_AVG, pe, 0., st,
+                         8. * (nc * (nshape + 1.) * ntheta * nq + nshape)))) {
+        return rc;
+      }
       CK(cudaMemcpyAsync(out_q + c0 * ntheta * nq, ctx->o_cq.p,
                          nc * ntheta * nq * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
@@ -762,10 +822,18 @@ extern "C" int tmx_get_table(
       tmx_launch_z_epilogue((int)nsca, (const cplx *)ctx->o_S.p + sca_base * 4,
                             (double *)ctx->o_gz.p, st);
       LAUNCHED();
+      cudaEvent_t pz = nullptr;
+      if ((rc = prof_begin(ctx, TMX_PROF_SHAPE_AVG, &pz))) {
+        return rc;
+      }
       tmx_launch_shape_avg((int)nc, nshape, ntheta * nphi_sca * 16,
                            (const double *)ctx->o_gz.p, (const double *)ctx->o_shw.p,
                            (double *)ctx->o_cz.p, st);
       LAUNCHED();
+      if ((rc = prof_end(ctx, TMX_PROF_SHAPE_AVG, pz, 0., st,
+                         8. * (nc * (nshape + 1.) * ntheta * nphi_sca * 16 + nshape)))) {
+        return rc;
+      }
       CK(cudaMemcpyAsync(out_z + c0 * ntheta * nphi_sca * 16, ctx->o_cz.p,
                          nc * ntheta * nphi_sca * 16 * sizeof(double),
                          cudaMemcpyDeviceToHost, st));

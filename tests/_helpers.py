@@ -57,6 +57,45 @@ def oracle_sensitivity(r, lam, m, d, nmax, ngauss, T, q, rel=1e-15):
     return t_s, q_s
 
 
+def oracle_z181(r, lam, m, d, nmax, ngauss, coeffs):
+    """The oracle's random-orientation (coeffs) scattering matrices for
+    incidence along the axis at the 181 scattering angles 0..180 deg."""
+    T, _ = oracle_at(r, lam, m, d, nmax, ngauss)
+    Ta = O.orientation_average(T, nmax, coeffs[:2 * nmax + 1])
+    tout = np.radians(np.arange(181.0))
+    return np.stack([O.z_from_s(O.amplitude_lab(Ta, nmax, lam, 0., 0., 0., 0., t, 0.))
+                     for t in tout])
+
+
+def z_sensitivity(r, lam, m, d, nmax, ngauss, coeffs, rel=1e-15):
+    """The oracle's own change of those 181 matrices (relative to each
+    matrix's largest element) when r_ev moves by +-rel."""
+    z0 = oracle_z181(r, lam, m, d, nmax, ngauss, coeffs)
+    scale = np.max(np.abs(z0), axis=(-1, -2))
+    s = 0.0
+    for f in (1 + rel, 1 - rel):
+        z = oracle_z181(r * f, lam, m, d, nmax, ngauss, coeffs)
+        s = max(s, float(np.max(np.max(np.abs(z - z0), axis=(-1, -2)) / scale)))
+    return s
+
+
+def calculator_decision_band(r, lam, m, d, nmax, ndgs=2, tol=1e-4, rel=1e-15):
+    """For the calculator's order test between orders nmax - 1 and nmax
+    (ngauss = ndgs order): the oracle's change d = max(dQsca, dQext) and the
+    rounding noise of the m = 0 sums (their relative change when r_ev moves
+    by +-rel). Returns (|d - tol|, noise): a decision with |d - tol| within
+    a few times the noise is set by rounding."""
+    def sums(rr, k):
+        return np.array(O.tmatrix_m0(rr, lam, m, d, k, ndgs * k)[1:])
+    qa, qb = sums(r, nmax - 1), sums(r, nmax)
+    dq = np.max(np.abs((qa - qb) / qb))
+    noise = 0.0
+    for f in (1 + rel, 1 - rel):
+        for k, q0 in ((nmax - 1, qa), (nmax, qb)):
+            noise = max(noise, float(np.max(np.abs((sums(r * f, k) - q0) / q0))))
+    return abs(dq - tol), noise
+
+
 def check_grain(res, i, r, lam, m, d, ref):
     """Compare grain i of a GPU batch with the oracle's convergence run.
 

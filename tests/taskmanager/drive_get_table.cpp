@@ -165,7 +165,8 @@ int main(int argc, char **argv) {
     // one grain, Q_ext / Q_abs at 32 zenith angles uniform in cos(theta)
     std::vector<double> th1(32);
     for (int i = 0; i < 32; ++i) {
-      th1[i] = std::acos(-1. + 2. * i / 31.);
+      // numpy.linspace(-1, 1, 32): i * (2 / 31) - 1, the last point exactly 1
+      th1[i] = std::acos(i == 31 ? 1. : i * (2. / 31.) + -1.);
     }
     {
       SingleShapeShapeDistribution shape(2.);

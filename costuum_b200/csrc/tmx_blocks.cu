@@ -1732,9 +1732,10 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
                            double tolerance, int order, int last_order,
                            int32_t *next_active, int32_t *next_count,
                            int32_t *done_list, int32_t *done_ord,
-                           int32_t *done_pos, int32_t *done_count) {
+                           int32_t *done_pos, int32_t *done_count,
+                           const int32_t *nact_dev, int base) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nactive) {
+  if (p >= nactive || (nact_dev && base + p >= *nact_dev)) {
     return;
   }
   const int g = active[p];
@@ -1807,13 +1808,15 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
                          int32_t *done_ord, int32_t *done_pos,
-                         int32_t *done_count, cudaStream_t stream) {
+                         int32_t *done_count, const int32_t *nact_dev,
+                         int base, cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
       active, nactive, slots, diag, state, tolerance, order, last_order,
-      next_active, next_count, done_list, done_ord, done_pos, done_count);
+      next_active, next_count, done_list, done_ord, done_pos, done_count,
+      nact_dev, base);
 }
 
 // ------------------------------------------------------------- kept tables --
@@ -1972,16 +1975,21 @@ void tmx_launch_qsums(const TmxSlot *slots, int ns, const cplx *T,
 // Slots and items of one order step: active position p gets the tables at
 // p * strides and the four m = 0 classes as items 4p .. 4p + 3.
 __global__ void k_chain_prep(const int32_t *__restrict__ active, int nactive,
+                             const int32_t *__restrict__ nact_dev, int base,
                              int order, int ngauss, int wig_n, TmxChainBase b,
                              TmxSlot *slots, TmxItem *items) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive) {
     return;
   }
+  // positions past the list's length on the device (the host launched for
+  // an upper bound) get an empty slot: order 0 has no classes and no nodes,
+  // so every kernel of the step skips it
+  const bool valid = !nact_dev || base + p < *nact_dev;
   TmxSlot s;
-  s.grain = active[p];
-  s.nmax = order;
-  s.ngauss = ngauss;
+  s.grain = valid ? active[p] : 0;
+  s.nmax = valid ? order : 0;
+  s.ngauss = valid ? ngauss : 0;
   s.wig_n = wig_n;
   s.tab = b.tab + p * b.tab_stride;
   s.nsc = b.nsc + p * b.nsc_stride;
@@ -1998,12 +2006,13 @@ __global__ void k_chain_prep(const int32_t *__restrict__ active, int nactive,
   }
 }
 
-void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
+void tmx_launch_chain_prep(const int32_t *active, int nactive,
+                           const int32_t *nact_dev, int base, int order,
                            int ngauss, int wig_n, const TmxChainBase &b,
                            TmxSlot *slots, TmxItem *items, cudaStream_t stream) {
   if (nactive <= 0) {
     return;
   }
   k_chain_prep<<<(nactive + 127) / 128, 128, 0, stream>>>(
-      active, nactive, order, ngauss, wig_n, b, slots, items);
+      active, nactive, nact_dev, base, order, ngauss, wig_n, b, slots, items);
 }

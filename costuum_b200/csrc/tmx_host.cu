@@ -501,6 +501,8 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   int rc;
   NvtxRange blocks_range("tmx_blocks");
   const int np2 = (int)p2.size();
+  const int64_t wig_used0 = ctx->wig_used;
+  const void *T_before = ctx->T.p, *q_before = ctx->q.p;
   if (!keep_T) {
     ctx->sink_done = 0; // a new set of T-matrices starts at offset 0
   }
@@ -654,8 +656,11 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   if (np2 == 0) {
     return TMX_OK;
   }
-  if (st != ctx->stream) {
-    // the allocations and Wigner tables above are ordered on ctx->stream
+  if (st != ctx->stream && (!temp || ctx->wig_used != wig_used0 ||
+                            ctx->T.p != T_before || ctx->q.p != q_before)) {
+    // new Wigner tables or a moved T / Q-sum buffer above are ordered on
+    // ctx->stream (a round of the order loop that needs none of them does
+    // not wait for the orders queued there)
     cudaEvent_t ready;
     CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
     CK(cudaEventRecord(ready, ctx->stream));
@@ -1012,6 +1017,19 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   if ((rc = ensure_wigner(ctx, chain_keys, false, chain_sets))) {
     return rc;
   }
+  {
+    // every m of the orders the blocks of most grains run at, made before
+    // the loop (cached in the context), so that block rounds need not wait
+    // for table jobs queued behind the order loop
+    std::vector<std::pair<int, int>> full_keys;
+    for (int k = S.min_order; k < std::min(S.max_order, 65); ++k) {
+      full_keys.push_back({k, glf * k});
+    }
+    std::vector<int> full_sets;
+    if ((rc = ensure_wigner(ctx, full_keys, true, full_sets))) {
+      return rc;
+    }
+  }
 
   // ---- 1. order loop
   // Grains whose order became final are collected from the done list after
@@ -1020,7 +1038,6 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   // blocks fill the GPU during the latency-bound tail of the loop. A round's
   // host set-up is issued after the next order's launches, so it overlaps
   // that order on the GPU.
-  int nact = ctx->up_nact;
   // done list: grains [0, n) and their final orders [n, 2n)
   if ((rc = ensure(ctx, ctx->done, std::max<int64_t>(1, 2 * n) * sizeof(int32_t)))) {
     return rc;
@@ -1079,16 +1096,45 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   std::vector<char> launched(n, 0);
   int rounds = 0;
   int64_t t_next = 0;
-  DevBuf *cur = &ctx->act0, *nxt = &ctx->act1;
   const size_t budget = (size_t)8 << 30; // table bytes per chunk
   std::unique_ptr<NvtxRange> chain_range(new NvtxRange("tmx_chain"));
   const int last = S.max_order - 1;
-  for (int k = S.min_order; k < S.max_order && nact > 0;) {
-    // Few grains left: evaluate the next G orders of every active grain at
-    // once (the convergence rule is then applied order by order), which
-    // cuts the latency-bound tail of the loop at the cost of orders past
-    // convergence.
-    const int G = std::min(S.max_order - k, nact <= 32 ? 8 : (nact <= 128 ? 4 : 1));
+  // The loop runs one group of orders ahead of the host: group j + 1 is
+  // queued before the host waits for group j's outcome, with the length of
+  // its active list read on the device (the host launches for an upper
+  // bound, the input length of group j; surplus positions are empty
+  // slots). So the GPU never waits for the host between orders; the host
+  // reads each group's counts and done-list entries while the next group
+  // runs. Active lists alternate between act0 and act1; their lengths are
+  // count[0] and count[2], the done-list length count[1].
+  DevBuf *lists[2] = {&ctx->act0, &ctx->act1};
+  int32_t *cnt = (int32_t *)ctx->count.p;
+  ctx->pinned[12] = ctx->up_nact;
+  CK(cudaMemcpyAsync(cnt, ctx->pinned + 12, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(cnt + 2, 0, sizeof(int32_t), st));
+  struct Group {
+    int k = 0, G = 0;
+    int nact_up = 0; // upper bound of the group's input list length
+    int issued = 0;  // the bound it was launched for
+    int list = 0, par = 0;
+  };
+  cudaEvent_t gev[2];
+  CK(cudaEventCreateWithFlags(&gev[0], cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&gev[1], cudaEventDisableTiming));
+  struct EvGuard {
+    cudaEvent_t *e;
+    ~EvGuard() {
+      cudaEventDestroy(e[0]);
+      cudaEventDestroy(e[1]);
+    }
+  } ev_guard{gev};
+  int64_t unprocessed_bound = 0; // done entries groups in flight may add
+  auto issue = [&](Group &grp) -> int {
+    const int k = grp.k, G = grp.G, nact = grp.nact_up;
+    grp.issued = nact;
+    const int32_t *cur_cnt = cnt + (grp.list ? 2 : 0);
+    int32_t *nxt_cnt = cnt + (grp.list ? 0 : 2);
+    DevBuf *cur = lists[grp.list], *nxt = lists[grp.list ^ 1];
     std::vector<TmxChainBase> base(G);
     int64_t tab_t = 0, nsc_t = 0, diag_t = 0, scr_t = 0;
     int chunk = nact;
@@ -1115,30 +1161,31 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       diag_t += chunk * b.diag_stride;
       scr_t += 4 * chunk * b.scr_stride;
     }
-    if ((rc = ensure(ctx, ctx->tab, tab_t * sizeof(double))) ||
-        (rc = ensure(ctx, ctx->nsc, nsc_t * sizeof(double))) ||
-        (rc = ensure(ctx, ctx->scratch, scr_t * sizeof(cplx))) ||
-        (rc = ensure(ctx, ctx->diag, diag_t * sizeof(cplx))) ||
-        (rc = ensure(ctx, ctx->slots, (size_t)G * chunk * sizeof(TmxSlot))) ||
-        (rc = ensure(ctx, ctx->items, 4 * (size_t)G * chunk * sizeof(TmxItem)))) {
-      return rc;
+    int rc2;
+    if ((rc2 = ensure(ctx, ctx->tab, tab_t * sizeof(double))) ||
+        (rc2 = ensure(ctx, ctx->nsc, nsc_t * sizeof(double))) ||
+        (rc2 = ensure(ctx, ctx->scratch, scr_t * sizeof(cplx))) ||
+        (rc2 = ensure(ctx, ctx->diag, diag_t * sizeof(cplx))) ||
+        (rc2 = ensure(ctx, ctx->slots, (size_t)G * chunk * sizeof(TmxSlot))) ||
+        (rc2 = ensure(ctx, ctx->items, 4 * (size_t)G * chunk * sizeof(TmxItem)))) {
+      return rc2;
     }
-    CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(int32_t), st));
+    CK(cudaMemsetAsync(nxt_cnt, 0, sizeof(int32_t), st));
     const int kl = k + G - 1;
     for (int c0 = 0; c0 < nact; c0 += chunk) {
       const int cn = std::min(chunk, nact - c0);
       const int32_t *a = (const int32_t *)cur->p + c0;
       for (int s = 0; s < G; ++s) {
-        tmx_launch_chain_prep(a, cn, k + s, glf * (k + s), chain_sets[k + s - S.min_order],
-                              base[s], (TmxSlot *)ctx->slots.p,
-                              (TmxItem *)ctx->items.p, st);
+        tmx_launch_chain_prep(a, cn, cur_cnt, c0, k + s, glf * (k + s),
+                              chain_sets[k + s - S.min_order], base[s],
+                              (TmxSlot *)ctx->slots.p, (TmxItem *)ctx->items.p, st);
         LAUNCHED();
       }
       // slots and items of the group are contiguous: [s][p]
       const int nsl = (G == 1) ? cn : G * chunk;
       cudaEvent_t pe = nullptr;
-      if ((rc = prof_begin(ctx, 1, &pe))) {
-        return rc;
+      if ((rc2 = prof_begin(ctx, 1, &pe))) {
+        return rc2;
       }
       tmx_launch_tables((const TmxSlot *)ctx->slots.p, nsl,
                         (const TmxGrain *)ctx->grains.p,
@@ -1146,8 +1193,8 @@ int tmx_batch_compute(tmx_ctx *ctx) {
                         (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
                         (double *)ctx->nsc.p, S.bessel_start, glf * kl, kl, st);
       LAUNCHED();
-      if ((rc = prof_end(ctx, 1, pe, 0.))) {
-        return rc;
+      if ((rc2 = prof_end(ctx, 1, pe, 0.))) {
+        return rc2;
       }
       TmxBlockArgs B;
       B.items = (const TmxItem *)ctx->items.p;
@@ -1165,32 +1212,33 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       B.max_nb = (kl + 1) / 2;
       B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
       B.family = dispatch_family(ctx, B.max_nb);
+      // (flops of the upper bound of slots: the profiled figure is an
+      // estimate until the group's length is known)
       double fl = 0.;
       for (int s = 0; s < G; ++s) {
         for (int c = 0; c < 4; ++c) {
           fl += item_flops(tmx_host_class_size(k + s, 0, c), 0, glf * (k + s)) * cn;
         }
       }
-      if ((rc = prof_begin(ctx, 0, &pe))) {
-        return rc;
+      if ((rc2 = prof_begin(ctx, 0, &pe))) {
+        return rc2;
       }
       tmx_launch_blocks(B, st);
       LAUNCHED();
-      if ((rc = prof_end(ctx, 0, pe, fl))) {
-        return rc;
+      if ((rc2 = prof_end(ctx, 0, pe, fl))) {
+        return rc2;
       }
       for (int s = 0; s < G; ++s) {
         if (G > 1) {
           // the active list after the group is the one of its last order
-          CK(cudaMemsetAsync(ctx->count.p, 0, sizeof(int32_t), st));
+          CK(cudaMemsetAsync(nxt_cnt, 0, sizeof(int32_t), st));
         }
         tmx_launch_converge(a, cn, (const TmxSlot *)ctx->slots.p + base[s].slot,
                             (const cplx *)ctx->diag.p,
                             (TmxChainState *)ctx->state.p, S.tolerance, k + s, last,
-                            (int32_t *)nxt->p, (int32_t *)ctx->count.p,
-                            (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
-                            (int32_t *)ctx->done_pos.p, (int32_t *)ctx->count.p + 1,
-                            st);
+                            (int32_t *)nxt->p, nxt_cnt, (int32_t *)ctx->done.p,
+                            (int32_t *)ctx->done.p + n, (int32_t *)ctx->done_pos.p,
+                            cnt + 1, cur_cnt, c0, st);
         LAUNCHED();
       }
       if (ctx->keep_valid) {
@@ -1200,7 +1248,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
         K.done_list = (const int32_t *)ctx->done.p;
         K.done_ord = (const int32_t *)ctx->done.p + n;
         K.done_pos = (const int32_t *)ctx->done_pos.p;
-        K.counters = (const int32_t *)ctx->count.p;
+        K.counters = cnt;
         K.next = (int32_t *)ctx->keep_ctl.p;
         K.ticket = (unsigned *)ctx->keep_ctl.p + 1;
         K.used = (unsigned long long *)ctx->keep_ctl.p + 1;
@@ -1218,35 +1266,81 @@ int tmx_batch_compute(tmx_ctx *ctx) {
         LAUNCHED();
       }
     }
-    // active count, done count, and the done-list entries (grain, order)
-    // this group can add
-    CK(cudaMemcpyAsync(ctx->pinned, ctx->count.p, 2 * sizeof(int32_t),
+    // the group's outcome for the host: the new list length and the
+    // done-list length (pinned slots of this group's parity), and every
+    // done-list entry that the groups in flight can have added
+    unprocessed_bound += nact;
+    const int64_t w = std::min<int64_t>(n - done_seen, unprocessed_bound);
+    CK(cudaMemcpyAsync(ctx->pinned + 8 + 2 * grp.par, nxt_cnt, sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ctx->pinned_done + done_seen, (int32_t *)ctx->done.p + done_seen,
-                       nact * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(ctx->pinned_done + n + done_seen,
-                       (int32_t *)ctx->done.p + n + done_seen, nact * sizeof(int32_t),
+    CK(cudaMemcpyAsync(ctx->pinned + 9 + 2 * grp.par, cnt + 1, sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
-    if (ctx->keep_valid) {
-      CK(cudaMemcpyAsync(ctx->pinned_keep + done_seen,
-                         (int64_t *)ctx->keep_q.p + done_seen, nact * sizeof(int64_t),
+    if (w > 0) {
+      CK(cudaMemcpyAsync(ctx->pinned_done + done_seen, (int32_t *)ctx->done.p + done_seen,
+                         w * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(ctx->pinned_done + n + done_seen,
+                         (int32_t *)ctx->done.p + n + done_seen, w * sizeof(int32_t),
                          cudaMemcpyDeviceToHost, st));
+      if (ctx->keep_valid) {
+        CK(cudaMemcpyAsync(ctx->pinned_keep + done_seen,
+                           (int64_t *)ctx->keep_q.p + done_seen, w * sizeof(int64_t),
+                           cudaMemcpyDeviceToHost, st));
+      }
     }
+    CK(cudaEventRecord(gev[grp.par], st));
+    return TMX_OK;
+  };
+  // speculative group length for a list of at most nact grains: few grains
+  // left -- evaluate the next G orders of every active grain at once (the
+  // convergence rule is then applied order by order), which cuts the
+  // latency-bound tail at the cost of orders past convergence
+  auto group_len = [&](int k, int nact) {
+    return std::min(S.max_order - k, nact <= 32 ? 8 : (nact <= 128 ? 4 : 1));
+  };
+  Group inflight;
+  bool have_inflight = false;
+  if (ctx->up_nact > 0) {
+    inflight.k = S.min_order;
+    inflight.nact_up = ctx->up_nact;
+    inflight.G = group_len(inflight.k, inflight.nact_up);
+    inflight.list = 0;
+    inflight.par = 0;
+    if ((rc = issue(inflight))) {
+      return rc;
+    }
+    have_inflight = true;
+  }
+  int nact_known = ctx->up_nact;
+  while (have_inflight) {
+    // queue the next group before waiting for this one
+    Group next;
+    bool have_next = false;
+    const int k_next = inflight.k + inflight.G;
+    if (k_next < S.max_order && nact_known > 0) {
+      next.k = k_next;
+      next.nact_up = inflight.nact_up; // the list can only shrink
+      next.G = group_len(next.k, next.nact_up);
+      next.list = inflight.list ^ 1;
+      next.par = inflight.par ^ 1;
+      if ((rc = issue(next))) {
+        return rc;
+      }
+      have_next = true;
+    }
+    // a round's host set-up overlaps the groups on the GPU
     if (!pending.empty()) {
       if ((rc = run_blocks_round(ctx, pending, (rounds & 1) ? ctx->stream3 : ctx->stream2,
-                                 t_next, rounds > 0,
-                                 &t_next, true))) {
+                                 t_next, rounds > 0, &t_next, true))) {
         return rc;
       }
       ++rounds;
       pending.clear();
     }
-    CK(cudaStreamSynchronize(st));
-    const int prev = nact;
-    nact = ctx->pinned[0];
-    const int64_t done_now = ctx->pinned[1];
-    std::swap(cur, nxt);
-    if (done_now > done_seen + prev) {
+    CK(cudaEventSynchronize(gev[inflight.par]));
+    const int nact_out = ctx->pinned[8 + 2 * inflight.par];
+    const int64_t done_now = ctx->pinned[9 + 2 * inflight.par];
+    unprocessed_bound -= inflight.issued;
+    if (nact_out > inflight.nact_up || done_now > n || done_now < done_seen) {
       return fail(ctx, TMX_ERR_CUDA, "order loop: inconsistent done list");
     }
     for (int64_t j = done_seen; j < done_now; ++j) {
@@ -1260,10 +1354,16 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       ready.push_back(g);
     }
     done_seen = done_now;
-    k += G;
-    if (nact > 0 && (int64_t)ready.size() >= round_min) {
+    nact_known = nact_out;
+    if (have_next) {
+      // the queued group's bound can be tightened for the one after it
+      next.nact_up = std::min(next.nact_up, nact_out);
+      inflight = next;
+    }
+    have_inflight = have_next;
+    if (nact_out > 0 && (int64_t)ready.size() >= round_min) {
       // at most round_max grains per round: a round's host set-up runs
-      // while the GPU computes the next order, and should not outlast it
+      // while the GPU computes the next orders, and should not outlast them
       const size_t take = std::min<size_t>(ready.size(), (size_t)round_max);
       pending.assign(ready.begin(), ready.begin() + take);
       ready.erase(ready.begin(), ready.begin() + take);

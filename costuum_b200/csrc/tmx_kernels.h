@@ -74,7 +74,11 @@ struct TmxChainBase {
   int64_t diag, diag_stride;
   int64_t scr, scr_stride;
 };
-void tmx_launch_chain_prep(const int32_t *active, int nactive, int order,
+// nact_dev (may be NULL): the list's length on the device; positions
+// p >= *nact_dev - base of this launch (for nactive, an upper bound) get empty
+// slots
+void tmx_launch_chain_prep(const int32_t *active, int nactive,
+                           const int32_t *nact_dev, int base, int order,
                            int ngauss, int wig_n, const TmxChainBase &b,
                            TmxSlot *slots, TmxItem *items, cudaStream_t stream);
 
@@ -89,7 +93,8 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          int last_order, int32_t *next_active,
                          int32_t *next_count, int32_t *done_list,
                          int32_t *done_ord, int32_t *done_pos,
-                         int32_t *done_count, cudaStream_t stream);
+                         int32_t *done_count, const int32_t *nact_dev,
+                         int base, cudaStream_t stream);
 
 // copies of the final-order tables of the grains that became final in one
 // group of orders, into the batch's table arena (k_keep_tables)

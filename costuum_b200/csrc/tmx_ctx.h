@@ -70,10 +70,17 @@ struct tmx_ctx {
   // plan of the observable kernels (first pair of each grain, job groups)
   int64_t o_ngrains = 0, o_npairs = 0;
   int o_nbmax = 1, o_ngrp = 0;
+  // orientation-average work order: pair-major item starts (o_pairs, pmax^2
+  // + 1) and the grains by descending order (o_ord)
+  DevBuf o_ord;
+  int o_pmax = 1;
   // flops of one matrix set in the orientation average and the amplitudes
   // of the current plan (counted while profiling)
   double o_fl_orient = 0., o_fl_amp = 0.;
-  int32_t *pinned = nullptr;     // [0] active count, [1] done count
+  int32_t *pinned = nullptr;     // 16 words: [4..7] the table arena's
+                                 // counters, [8 + 2 p] / [9 + 2 p] list and
+                                 // done-list lengths after an order group of
+                                 // parity p, [12] the first list's length
   DevBuf done;                    // grains whose order became final, in order
   int32_t *pinned_done = nullptr; // host copy of new done-list entries
   int64_t pinned_done_cap = 0;

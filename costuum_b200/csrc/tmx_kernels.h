@@ -185,10 +185,14 @@ struct TmxMatSet {
 };
 // orientation average (coef_set >= 0) or copy of every grain's T-matrix,
 // with the amplitude factors c_{n' n} folded in when fold != 0;
-// pair_base[g] = first (n1, n2) pair of grain g (nmax^2 pairs per grain),
+// work items (pair (n1, n2), grain) pair-major: pair q = (n1 - 1) pmax +
+// n2 - 1 owns items [pstart[q], pstart[q + 1]), for the grains
+// order[0 .. pstart[q + 1] - pstart[q]) (grains by descending nmax, so the
+// grains of order >= max(n1, n2) come first); npairs = sum of nmax^2;
 // mmax >= every nmax; nmat (1 or 4) sets src[k] -> dst[k]
-void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
-                             int ngrains, int64_t npairs, const TmxMatSet &mats,
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
+                             const int32_t *order, int pmax, int64_t npairs,
+                             const TmxMatSet &mats,
                              int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,

@@ -172,7 +172,8 @@ __device__ __forceinline__ cplx c_fold(int nin, int nout, double a, cplx z) {
 template <int NMAT>
 __global__ void __launch_bounds__(256)
 k_orient_pairs(const TmxObsGrain *__restrict__ og,
-               const int64_t *__restrict__ pair_base, int ngrains,
+               const int64_t *__restrict__ pstart,
+               const int32_t *__restrict__ order, int pmax,
                int64_t npairs, TmxMatSet mats, const double *__restrict__ coeffs,
                int ncoef, const int64_t *__restrict__ cg_off,
                const double *__restrict__ cg, int cg_nmax, int wcap, int fold) {
@@ -183,21 +184,25 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
   cplx *tv = osh + (int64_t)warp * wcap * NMAT;
   for (int64_t w = (int64_t)blockIdx.x * nwarps + warp; w < npairs;
        w += (int64_t)gridDim.x * nwarps) {
-    // grain of pair w: the last g with pair_base[g] <= w
-    int lo = 0, hi = ngrains - 1;
+    // work item w = (pair (n1, n2), grain): pair-major, so that the warps
+    // of a CTA (and CTAs running together) contract the same Clebsch-Gordan
+    // rows for different grains and read them from cache. Pair
+    // q = (n1 - 1) pmax + (n2 - 1) owns items [pstart[q], pstart[q + 1]),
+    // one per grain of order >= max(n1, n2), in the order `order` (grains by
+    // descending order).
+    int lo = 0, hi = pmax * pmax - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (pair_base[mid] <= w) {
+      if (pstart[mid] <= w) {
         lo = mid;
       } else {
         hi = mid - 1;
       }
     }
-    const TmxObsGrain G = og[lo];
+    const int n1 = lo / pmax + 1;
+    const int n2 = lo % pmax + 1;
+    const TmxObsGrain G = og[order[w - pstart[lo]]];
     const int N = G.nmax;
-    const int pair = (int)(w - pair_base[lo]);
-    const int n1 = pair / N + 1;
-    const int n2 = pair % N + 1;
     const int M = min(n1, n2);
     // fold = 0: the plain averaged T-matrix (c = 1: i^0 times 1)
     const double afold = fold ? a_fac(n1) * a_fac(n2) : 1.;
@@ -687,8 +692,9 @@ void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
   k_cg<<<blocks, 128, 0, stream>>>(nmax, cg_off, cg, work);
 }
 
-void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
-                             int ngrains, int64_t npairs, const TmxMatSet &mats,
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
+                             const int32_t *order, int pmax, int64_t npairs,
+                             const TmxMatSet &mats,
                              int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,
@@ -707,13 +713,13 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pair_base,
     const int blocks4 = (int)std::min<int64_t>((npairs + 3) / 4, 148 * 16);
     cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem4);
-    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pair_base, ngrains, npairs,
+    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pstart, order, pmax, npairs,
                                                        mats, coeffs, ncoef, cg_off, cg,
                                                        cg_nmax, wcap, fold);
   } else {
     cudaFuncSetAttribute(k_orient_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    k_orient_pairs<1><<<blocks, 256, smem, stream>>>(og, pair_base, ngrains, npairs,
+    k_orient_pairs<1><<<blocks, 256, smem, stream>>>(og, pstart, order, pmax, npairs,
                                                      mats, coeffs, ncoef, cg_off, cg,
                                                      cg_nmax, wcap, fold);
   }

@@ -374,16 +374,47 @@ int64_t est_nmax(double x, int min_order, int max_order) {
 // kernel.
 int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
                     const std::vector<TmxSJob> &sj) {
+  int rc0;
   cudaStream_t st = ctx->stream;
   const int64_t n = (int64_t)og.size();
-  std::vector<int64_t> base(std::max<int64_t>(1, n), 0);
-  int64_t npairs = 0;
+  // orientation-average work items, pair-major (tmx_launch_orient_pairs):
+  // grains by descending order; pair (n1, n2) has one item per grain of
+  // order >= max(n1, n2)
   int nbmax = 1;
   for (int64_t g = 0; g < n; ++g) {
-    base[g] = npairs;
-    const int64_t N = std::max(0, og[g].nmax);
-    npairs += N * N;
     nbmax = std::max(nbmax, og[g].nmax);
+  }
+  std::vector<int32_t> order;
+  for (int64_t g = 0; g < n; ++g) {
+    if (og[g].nmax > 0) {
+      order.push_back((int32_t)g);
+    }
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    return og[a].nmax > og[b].nmax;
+  });
+  std::vector<int64_t> at_least(nbmax + 2, 0); // grains of order >= k
+  for (int32_t g : order) {
+    at_least[og[g].nmax] += 1;
+  }
+  for (int k = nbmax; k >= 1; --k) {
+    at_least[k] += at_least[k + 1];
+  }
+  std::vector<int64_t> base((size_t)nbmax * nbmax + 1, 0);
+  int64_t npairs = 0;
+  for (int n1 = 1; n1 <= nbmax; ++n1) {
+    for (int n2 = 1; n2 <= nbmax; ++n2) {
+      base[(size_t)(n1 - 1) * nbmax + (n2 - 1)] = npairs;
+      npairs += at_least[std::max(n1, n2)];
+    }
+  }
+  base.back() = npairs;
+  if ((rc0 = ensure(ctx, ctx->o_ord, std::max<size_t>(1, order.size()) * sizeof(int32_t)))) {
+    return rc0;
+  }
+  if (!order.empty()) {
+    CK(cudaMemcpyAsync(ctx->o_ord.p, order.data(), order.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
   }
   std::vector<TmxAmpGroup> grp;
   for (size_t j = 0; j < sj.size(); ++j) {
@@ -411,6 +442,7 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
   ctx->o_ngrains = n;
   ctx->o_npairs = npairs;
   ctx->o_nbmax = nbmax;
+  ctx->o_pmax = nbmax;
   ctx->o_ngrp = (int)grp.size();
   if (ctx->profiling) {
     // flops of one matrix set over the kernels' index spaces: the
@@ -485,8 +517,9 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
     return rc;
   }
   tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
-                          (const int64_t *)ctx->o_pairs.p, (int)ctx->o_ngrains,
-                          ctx->o_npairs, avg, nmat, (const double *)ctx->o_coef.p,
+                          (const int64_t *)ctx->o_pairs.p, (const int32_t *)ctx->o_ord.p,
+                          ctx->o_pmax, ctx->o_npairs, avg, nmat,
+                          (const double *)ctx->o_coef.p,
                           ncoef, (const int64_t *)ctx->cg_off.p,
                           (const double *)ctx->cg.p, ctx->cg_nmax, ctx->o_nbmax, 1,
                           st);
@@ -1550,7 +1583,8 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
     avg.src[0] = (const cplx *)ctx->T.p;
     avg.dst[0] = (cplx *)ctx->Ta.p;
     tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
-                            (const int64_t *)ctx->o_pairs.p, (int)n, ctx->o_npairs,
+                            (const int64_t *)ctx->o_pairs.p,
+                            (const int32_t *)ctx->o_ord.p, ctx->o_pmax, ctx->o_npairs,
                             avg, 1, (const double *)ctx->o_coef.p, ncoef,
                             (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
                             ctx->cg_nmax, ctx->o_nbmax, 0, st);

@@ -1072,10 +1072,9 @@ static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
 #define TMX_WG32 4
 
 __host__ __device__ constexpr int cta32_elems() {
-  // F[WG][4][32] + W[2][WG][4][32], or Q, RgQ [32][33], 1/U_jj, indices and
-  // two copies of a pivot column
-  return (12 * TMX_WG32 * 32 > 2 * 32 * 33 + 5 * 32) ? 12 * TMX_WG32 * 32
-                                                      : 2 * 32 * 33 + 5 * 32;
+  // F[WG][4][32] + W[2][WG][4][32], or Q, RgQ [32][33], 1/U_jj, indices
+  return (12 * TMX_WG32 * 32 > 2 * 32 * 33 + 3 * 32) ? 12 * TMX_WG32 * 32
+                                                      : 2 * 32 * 33 + 3 * 32;
 }
 
 __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
@@ -1090,7 +1089,6 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   cplx *uinv = Rm + NBM * LD;        // [NBM]
   int *perm = reinterpret_cast<int *>(uinv + NBM); // [NBM]
   int *piv = perm + NBM;                           // [NBM]
-  cplx *colbuf = uinv + 3 * NBM;     // [2][NBM]: column i of LU step i
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int wib = tid >> 5;
@@ -1212,23 +1210,11 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
         }
       }
     }
-    if (wib == 0 && lane < nb) {
-      colbuf[lane] = Qm[lane * LD];
-    }
-    __syncthreads();
-    {
-      // LU in place in Qm on all four warps: thread (lane r, warp w) holds
-      // row position r and the columns k = w, w + 4, ... Every warp finds
-      // the pivot of step i itself from a copy of column i (colbuf[i & 1],
-      // written by the column's owner at the end of step i - 1; the same
-      // first-maximum rule as Matrix::plu_inverse), so one barrier per step
-      // suffices: the rows i and bi are swapped column by column by the
-      // owners of the columns, and the multiplier of row r comes from the
-      // copy of column i.
+    if (wib == 0) {
+      // LU in place in Qm, lane r updates row r
       bool singular = false;
       for (int i = 0; i < nb; ++i) {
-        const cplx cr = (lane < nb) ? colbuf[(i & 1) * NBM + lane] : mkc(0., 0.);
-        double best = (lane >= i && lane < nb) ? cabs_dev(cr) : -1.;
+        double best = (lane >= i && lane < nb) ? cabs_dev(Qm[lane * LD + i]) : -1.;
         int bi = lane;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -1240,17 +1226,11 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
           }
         }
         singular = singular || !(best > 0.);
-        // column i after the swap: the pivot at i, the old Q_ii at bi
-        const cplx piv_v = mkc(__shfl_sync(0xffffffffu, cr.x, bi),
-                               __shfl_sync(0xffffffffu, cr.y, bi));
-        const cplx cii = mkc(__shfl_sync(0xffffffffu, cr.x, i),
-                             __shfl_sync(0xffffffffu, cr.y, i));
-        if (wib == 0 && lane == 0) {
+        if (lane == 0) {
           piv[i] = bi;
         }
         if (bi != i) {
-          // rows i and bi exchange their entries in this warp's columns
-          for (int k = wib + 4 * lane; k < nb && lane < 8; k += 128) {
+          for (int k = lane; k < nb; k += 32) {
             const cplx t = Qm[i * LD + k];
             Qm[i * LD + k] = Qm[bi * LD + k];
             Qm[bi * LD + k] = t;
@@ -1258,39 +1238,36 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
         }
         __syncwarp();
         if (lane > i && lane < nb) {
-          const cplx pinv = cinv_lu(piv_v);
-          const cplx l = cmul((lane == bi) ? cii : cr, pinv);
-          if ((i & 3) == wib) {
-            Qm[lane * LD + i] = l;
-          }
+          const cplx pinv = cinv_lu(Qm[i * LD + i]);
+          const cplx l = cmul(Qm[lane * LD + i], pinv);
+          Qm[lane * LD + i] = l;
+          // four entries at a time: all loads before the stores (the pivot
+          // row is only read in this step), so the updates overlap
           cplx *qr = Qm + lane * LD;
           const cplx *pr = Qm + i * LD;
-          // this warp's columns k > i: the first is the smallest k > i with
-          // k = wib (mod 4); it is column i + 1 for the owner of that column,
-          // which also copies it for the next step's pivot search
-          int k = i + 1 + ((wib - (i + 1)) & 3);
-          if (k == i + 1 && k < nb) {
-            const cplx v = csub(qr[k], cmul(l, pr[k]));
-            qr[k] = v;
-            colbuf[(k & 1) * NBM + lane] = v;
-            k += 4;
+          int k = i + 1;
+          for (; k + 3 < nb; k += 4) {
+            cplx a0 = qr[k], a1 = qr[k + 1], a2 = qr[k + 2], a3 = qr[k + 3];
+            const cplx b0 = pr[k], b1 = pr[k + 1], b2 = pr[k + 2], b3 = pr[k + 3];
+            a0 = csub(a0, cmul(l, b0));
+            a1 = csub(a1, cmul(l, b1));
+            a2 = csub(a2, cmul(l, b2));
+            a3 = csub(a3, cmul(l, b3));
+            qr[k] = a0;
+            qr[k + 1] = a1;
+            qr[k + 2] = a2;
+            qr[k + 3] = a3;
           }
-          for (; k + 4 < nb; k += 8) {
-            cplx a0 = qr[k], a1 = qr[k + 4];
-            const cplx b0 = pr[k], b1 = pr[k + 4];
-            qr[k] = csub(a0, cmul(l, b0));
-            qr[k + 4] = csub(a1, cmul(l, b1));
-          }
-          for (; k < nb; k += 4) {
+          for (; k < nb; ++k) {
             qr[k] = csub(qr[k], cmul(l, pr[k]));
           }
         }
-        __syncthreads();
+        __syncwarp();
       }
-      if (wib == 0 && lane < nb) {
+      if (lane < nb) {
         uinv[lane] = cinv_lu(Qm[lane * LD + lane]);
       }
-      if (wib == 0 && lane == 0) {
+      if (lane == 0) {
         // column exchanges of Matrix::plu_inverse step 4, as a gather index
         for (int j = 0; j < nb; ++j) {
           perm[j] = j;

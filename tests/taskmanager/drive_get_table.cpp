@@ -174,7 +174,9 @@ int main(int argc, char **argv) {
       CustomDustProperties dust(m_const_15);
       Table t = get_table({0}, {0.2e-6}, {1e-6}, th1, shape, align, dust, 10, 40,
                           2, 1e-4, 20, true, true, false, false);
-      if (!write(dir, "gt1", t.q)) {
+      // (the angles too: the C library's acos and numpy's arccos may round
+      // differently in the last bit)
+      if (!write(dir, "gt1", t.q) || !write(dir, "gt1_theta", th1)) {
         return 1;
       }
     }

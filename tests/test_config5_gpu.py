@@ -111,17 +111,16 @@ def test_bench_workload_orders_against_reference(ctx, c5):
     print("reference: %d of %d converged; %d rounding-set decisions (%s)"
           % (ref_conv.sum(), len(r), rounding.sum(), np.flatnonzero(rounding)))
     assert rounding.sum() <= 0.03 * len(r)
-    odd = np.flatnonzero(rounding & (gpu_nm != ref_nm) & (gpu_nm != orc_nm))
-    assert len(odd) == 0, [(i, gpu_nm[i], ref_nm[i], orc_nm[i]) for i in odd]
-    # where the GPU alone differs, the decision must lie inside the rounding
-    # band of the sums it compares: |max(dQsca, dQext) - tolerance| within
-    # 10 x the sums' own change under a few-ulp change of r_ev (in the
-    # oracle, at the order the GPU or the reference stopped at)
-    other = np.flatnonzero(~rounding & (gpu_nm != ref_nm))
-    for i in other:
+    # where the GPU differs from the reference, the decision must lie inside
+    # the rounding band of the sums it compares: |max(dQsca, dQext) -
+    # tolerance| within 10 x the sums' own change under a few-ulp change of
+    # r_ev (in the oracle, at the order the GPU stopped at, or the
+    # reference's where the GPU did not converge)
+    differ = np.flatnonzero(gpu_nm != ref_nm)
+    for i in differ:
         n_dec = gpu_nm[i] if gpu_nm[i] > 0 else ref_nm[i]
         gap, noise = H.calculator_decision_band(r[i], 1e-6, m[i], d[i], int(n_dec))
-        print("grain %d: GPU %d, reference %d; |dQ - tol| %.3g, rounding noise %.3g"
-              % (i, gpu_nm[i], ref_nm[i], gap, noise))
+        print("grain %d: GPU %d, reference %d, oracle %d; |dQ - tol| %.3g, "
+              "rounding noise %.3g" % (i, gpu_nm[i], ref_nm[i], orc_nm[i], gap, noise))
         assert gap <= 10 * noise, (i, gpu_nm[i], ref_nm[i], gap, noise)
-    assert len(other) + rounding.sum() <= 0.04 * len(r)
+    assert len(differ) <= 0.04 * len(r)

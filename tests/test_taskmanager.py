@@ -73,7 +73,7 @@ def test_golden_tables(driven, tab):
 @pytest.mark.gpu
 def test_same_doubles_as_module_mirror(driven, tab):
     from costuum_b200 import CosTuuM as C
-    th1 = np.arccos(np.linspace(-1, 1, 32))
+    th1 = driven["gt1_theta"]  # the driver's angles, bit for bit
     r1 = C.get_table(types=np.array([0]), sizes=np.array([0.2e-6]),
                      wavelengths=np.array([1e-6]), thetas=th1,
                      shape_distribution=C.SingleShapeShapeDistribution(2.0),

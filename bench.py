@@ -260,14 +260,16 @@ def run_ours(args):
     # untimed: the block-kernel dispatch table tuned on these grains at their
     # converged orders (every family in every size bucket it can run)
     conv = ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
-    table, tune_ms = ctx.autotune(r, lam, m, d, conv.nmax.copy(),
-                                  conv.ngauss.copy(), reps=3)
-    autotune = {"table": [Context.FAMILIES[f] for f in table],
-                "buckets": ["nb<=8", "9..16", "17..32", "33..64", "65..128"],
-                "median_ms": [[round(float(x), 4) for x in row] for row in tune_ms],
-                "what": "per size bucket, median ms per batch of each kernel "
-                        "family (columns: %s; -1 not run), buckets serialised"
-                        % ", ".join(Context.FAMILIES)}
+    autotune = None
+    if not args.skip_tune:
+        table, tune_ms = ctx.autotune(r, lam, m, d, conv.nmax.copy(),
+                                      conv.ngauss.copy(), reps=3)
+        autotune = {"table": [Context.FAMILIES[f] for f in table],
+                    "buckets": ["nb<=8", "9..16", "17..32", "33..64", "65..128"],
+                    "median_ms": [[round(float(x), 4) for x in row] for row in tune_ms],
+                    "what": "per size bucket, median ms per batch of each kernel "
+                            "family (columns: %s; -1 not run), buckets serialised"
+                            % ", ".join(Context.FAMILIES)}
     _lib.check(h, lib.tmx_batch_upload(h, N_GRAINS, P(r), P(lam), P(mr), P(mi),
                                        P(d), sched), "upload")
     flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda:%d" % local)
@@ -616,6 +618,11 @@ def _ptr(a):
     return _lib.ptr(a)
 
 
+def _lib_load():
+    from costuum_b200 import _lib
+    return _lib.load()
+
+
 def dielectric_m(lam):
     """Seeded-style refractive index model of the averaged-grid workload:
     eps = eps_inf + sum_j f_j w_j^2 / (w_j^2 - w^2 - i g_j w) - wp^2 / (w^2 +
@@ -702,12 +709,22 @@ def main():
                     help="grains per GPU (smaller cases for profiling)")
     ap.add_argument("--config3", action="store_true",
                     help="measure the averaged get_table grid instead")
+    ap.add_argument("--averaging", action="store_true",
+                    help="only the averaging kernels' sub-grid leg (for profiling)")
+    ap.add_argument("--skip-tune", action="store_true",
+                    help="keep the default dispatch table (for profiling)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     N_GRAINS = args.grains
     if args.config3:
         return run_config3(args)
+    if args.averaging:
+        from costuum_b200.tmatrix import Context
+        ctx = Context(0)
+        print(json.dumps(averaging_leg(ctx, _lib_load(), ctx.probe_fp64(1))))
+        ctx.close()
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -396,6 +396,31 @@ def run_ours(args):
                         "forward) = tangents for (Re m, Im m, r_ev, d) on the "
                         "LU factors the forward's block rounds kept + their "
                         "observables"}
+        # the same through torch.autograd (costuum_b200.autograd.extinction):
+        # forward, then backward of a weighted sum of the coefficients
+        from costuum_b200 import autograd as AG
+        params = np.stack([m.real, m.imag, r, d], axis=1)
+        wts = torch.tensor(np.random.default_rng(7).standard_normal((N_GRAINS, len(th), 3)))
+        tf, tb = [], []
+        for it in range(4):  # the first pass is untimed
+            pt = torch.tensor(params, dtype=torch.float64, requires_grad=True)
+            flush_l2(flush)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            qt = AG.extinction(pt, 1e-6, th, co, **SCHEDULE)
+            t1 = time.perf_counter()
+            (qt * wts).sum().backward()
+            t2 = time.perf_counter()
+            if it:
+                tf.append(t1 - t0)
+                tb.append(t2 - t1)
+        grad["torch_autograd"] = {
+            "forward_ms": 1e3 * min(tf), "backward_ms": 1e3 * min(tb),
+            "ratio": min(tb) / min(tf),
+            "what": "Extinction.apply (convergence loop + blocks + averaged "
+                    "Qext at 32 angles) and .backward() of a weighted sum, "
+                    "host wall time; backward runs the tangent kernels on the "
+                    "forward's kept LU factors"}
 
     # ---- plain-path workload: 256 grains, x in [10, 30], d log-uniform in
     # [0.33, 3], calculator schedule, random-orientation average, Z at 181

@@ -74,6 +74,9 @@ struct tmx_ctx {
   // + 1) and the grains by descending order (o_ord)
   DevBuf o_ord;
   int o_pmax = 1;
+  // angles of the current plan (o_angles) and their pi / tau columns
+  int o_nangles = 0;
+  DevBuf o_wcol;
   // flops of one matrix set in the orientation average and the amplitudes
   // of the current plan (counted while profiling)
   double o_fl_orient = 0., o_fl_amp = 0.;

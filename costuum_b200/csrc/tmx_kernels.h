@@ -201,10 +201,17 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
 // work slots: grid x nmat x 32 x (nbmax + 1) x 4 complex)
 int tmx_amp_grid(int nbmax, int nmat);
 // amplitudes of nmat (1 or 4) averaged sets: src[k] -> S at dst[k]
+// wpi / wtau (may be NULL: the kernel runs the recurrences itself): the
+// plan's pi and tau columns from tmx_launch_wigner_cols for nmax wnmax
 void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
                     const TmxObsGrain *og, const TmxMatSet &mats, int nmat,
                     const TmxAngle *angles, const double2 *phis, double2 *xslot,
-                    int nbmax, int grid, cudaStream_t stream);
+                    int nbmax, int grid, const double *wpi, const double *wtau,
+                    int wnmax, cudaStream_t stream);
+// pi and tau columns of every (angle, m <= nmax): column (a, m) holds orders
+// max(m, 1) .. nmax at ((a (nmax + 1) + m) nmax)
+void tmx_launch_wigner_cols(const TmxAngle *angles, int nangles, int nmax,
+                            double *pi, double *tau, cudaStream_t stream);
 void tmx_launch_q_epilogue(const TmxQJob *jobs, int njobs, const TmxObsGrain *og,
                            const double2 *S, const double *wts, int nacc,
                            double *qout, int qstride, int do_abs, int do_ext,

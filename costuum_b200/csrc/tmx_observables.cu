@@ -372,6 +372,23 @@ __device__ static void wigner_col(double cosx, double sinx, double sinx_inv,
   }
 }
 
+// pi and tau columns of every (angle, m <= nmax) of an amplitude plan, the
+// recurrence of k_amp done once for all grains and jobs that share an angle:
+// column (a, m) holds orders n = max(m, 1) .. nmax at ((a (nmax + 1) + m)
+// nmax). (The values of orders <= N do not depend on how far the
+// recurrence runs, so a grain of order N reads the first entries.)
+__global__ void k_wigner_cols(const TmxAngle *__restrict__ angles, int nangles,
+                              int nmax, double *pi, double *tau) {
+  const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= (int64_t)nangles * (nmax + 1)) {
+    return;
+  }
+  const int a = (int)(u / (nmax + 1));
+  const int m = (int)(u - (int64_t)a * (nmax + 1));
+  const TmxAngle A = angles[a];
+  wigner_col(A.c, A.s, A.si, nmax, m, pi + u * nmax, tau + u * nmax, 1);
+}
+
 // One CTA per group of up to 32 amplitude jobs of one grain (lane = job).
 // For every m, with u = (pi_n, tau_n) at the outgoing angle and v at the
 // incoming one (n the row order, n' the column order of block m),
@@ -389,7 +406,9 @@ __global__ void __launch_bounds__(256, (NMAT > 1) ? 2 : 3)
 k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const TmxSJob *__restrict__ jobs, const TmxObsGrain *__restrict__ og,
       TmxMatSet mats, const TmxAngle *__restrict__ angles,
-      const cplx *__restrict__ phis, cplx *__restrict__ xslot, int nbmax) {
+      const cplx *__restrict__ phis, cplx *__restrict__ xslot, int nbmax,
+      const double *__restrict__ wpi, const double *__restrict__ wtau,
+      int wnmax) {
   extern __shared__ double ash[];
   double *po = ash;
   double *to = po + nbmax * 32;
@@ -420,7 +439,23 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
     for (int m = 0; m <= N; ++m) {
       const int nmin = (m > 1) ? m : 1;
       const int nb = N + 1 - nmin;
-      if (tid < 64) {
+      if (wpi) {
+        // the columns of this m from the plan's table (k_wigner_cols)
+        for (int u = tid; u < 64 * nb; u += blockDim.x) {
+          const int side = u / (32 * nb); // 0: outgoing angle, 1: incoming
+          const int k = (u - side * 32 * nb) >> 5;
+          const int p = u & 31;
+          double pv = 0., tv = 0.;
+          if (p < nj) {
+            const int a = side ? sj[p].angle_in : sj[p].angle_out;
+            const int64_t off = ((int64_t)a * (wnmax + 1) + m) * wnmax + k;
+            pv = wpi[off];
+            tv = wtau[off];
+          }
+          (side ? pi : po)[k * 32 + p] = pv;
+          (side ? ti : to)[k * 32 + p] = tv;
+        }
+      } else if (tid < 64) {
         const int p = tid & 31;
         const int side = tid >> 5; // 0: outgoing angle, 1: incoming angle
         double *P = side ? pi : po;
@@ -748,10 +783,21 @@ int tmx_amp_grid(int nbmax, int nmat) {
   return std::max(1, sms * std::max(1, per_sm));
 }
 
+void tmx_launch_wigner_cols(const TmxAngle *angles, int nangles, int nmax,
+                            double *pi, double *tau, cudaStream_t stream) {
+  const int64_t n = (int64_t)nangles * (nmax + 1);
+  if (n <= 0) {
+    return;
+  }
+  k_wigner_cols<<<(int)((n + 127) / 128), 128, 0, stream>>>(angles, nangles, nmax,
+                                                           pi, tau);
+}
+
 void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
                     const TmxObsGrain *og, const TmxMatSet &mats, int nmat,
                     const TmxAngle *angles, const double2 *phis, double2 *xslot,
-                    int nbmax, int grid, cudaStream_t stream) {
+                    int nbmax, int grid, const double *wpi, const double *wtau,
+                    int wnmax, cudaStream_t stream) {
   if (ngroups <= 0) {
     return;
   }
@@ -759,11 +805,11 @@ void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
   if (nmat == 4) {
     k_amp<4><<<blocks, 256, amp_smem(nbmax, 4), stream>>>(groups, ngroups, jobs, og,
                                                           mats, angles, phis, xslot,
-                                                          nbmax);
+                                                          nbmax, wpi, wtau, wnmax);
   } else {
     k_amp<1><<<blocks, 256, amp_smem(nbmax, 1), stream>>>(groups, ngroups, jobs, og,
                                                           mats, angles, phis, xslot,
-                                                          nbmax);
+                                                          nbmax, wpi, wtau, wnmax);
   }
 }
 

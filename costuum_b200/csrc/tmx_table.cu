@@ -532,10 +532,25 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
   if ((rc = prof_begin(ctx, TMX_PROF_AMP, &pe))) {
     return rc;
   }
+  // the pi / tau columns of every angle of the plan, once for all grains
+  // (unless the table would be large: then each CTA runs the recurrences)
+  const double *wpi = nullptr, *wtau = nullptr;
+  const int wn = ctx->o_nbmax;
+  const size_t wcol = (size_t)ctx->o_nangles * (wn + 1) * wn;
+  if (ctx->o_nangles > 0 && 2 * wcol * sizeof(double) <= ((size_t)512 << 20)) {
+    if ((rc = ensure(ctx, ctx->o_wcol, 2 * wcol * sizeof(double)))) {
+      return rc;
+    }
+    wpi = (const double *)ctx->o_wcol.p;
+    wtau = wpi + wcol;
+    tmx_launch_wigner_cols((const TmxAngle *)ctx->o_angles.p, ctx->o_nangles, wn,
+                           (double *)ctx->o_wcol.p, (double *)ctx->o_wcol.p + wcol, st);
+    LAUNCHED();
+  }
   tmx_launch_amp((const TmxAmpGroup *)ctx->o_grp.p, ctx->o_ngrp,
                  (const TmxSJob *)ctx->o_sj.p, (const TmxObsGrain *)ctx->o_og.p, amp,
                  nmat, (const TmxAngle *)ctx->o_angles.p, (const cplx *)ctx->o_phis.p,
-                 (cplx *)ctx->o_x.p, ctx->o_nbmax, grid, st);
+                 (cplx *)ctx->o_x.p, ctx->o_nbmax, grid, wpi, wtau, wn, st);
   LAUNCHED();
   // averaged T-matrices in, four complex amplitudes per job and azimuth out
   if ((rc = prof_end(ctx, TMX_PROF_AMP, pe, nmat * ctx->o_fl_amp, st,
@@ -644,6 +659,7 @@ extern "C" int tmx_get_table(
   }
   CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
                      cudaMemcpyHostToDevice, st));
+  ctx->o_nangles = (int)ang.size();
   CK(cudaMemcpyAsync(ctx->o_phis.p, phis.data(), phis.size() * sizeof(cplx),
                      cudaMemcpyHostToDevice, st));
   if (!acc_w.empty()) {
@@ -981,6 +997,7 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
   }
   CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ntheta * sizeof(TmxAngle),
                      cudaMemcpyHostToDevice, st));
+  ctx->o_nangles = ntheta;
   CK(cudaMemcpyAsync(ctx->o_phis.p, phis.data(), sizeof(cplx),
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
@@ -1375,6 +1392,7 @@ int plain_amplitudes(tmx_ctx *ctx, const std::vector<int32_t> &grain,
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
                      cudaMemcpyHostToDevice, st));
+  ctx->o_nangles = (int)ang.size();
   CK(cudaMemcpyAsync(ctx->o_phis.p, e1.data(), e1.size() * sizeof(cplx),
                      cudaMemcpyHostToDevice, st));
   if (!sj.empty()) {

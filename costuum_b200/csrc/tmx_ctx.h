@@ -101,6 +101,16 @@ struct tmx_ctx {
   // the profile), so that a profiled batch creates none
   std::vector<cudaEvent_t> prof_pool;
   size_t prof_used = 0;
+  // timeline of the profiled launches (tmx_profile_timeline): kind, stream
+  // and launch size with the events around the launch, resolved to ms after
+  // tl_origin (recorded by tmx_profile_enable on the library stream)
+  struct TlRec {
+    int32_t kind, stream, info;
+    cudaEvent_t a, b;
+  };
+  std::vector<TlRec> tl_pending;
+  std::vector<double> tl_done; // 5 per record: kind, stream, info, start, end
+  cudaEvent_t tl_origin = nullptr;
   // Block rounds of the last tmx_batch_compute, kept for the gradients: each
   // round's tables, slot and item lists and LU factors (pool allocations
   // released when the next batch starts). rounds_lu: they cover every grain
@@ -256,8 +266,45 @@ static inline int prof_begin(tmx_ctx *ctx, int k, cudaEvent_t *a,
   return 0;
 }
 
+// index of a context stream in the timeline: 0 library stream, 1 and 2 the
+// round streams, 3..8 the bucket streams, -1 any other
+static inline int stream_index(const tmx_ctx *ctx, cudaStream_t st) {
+  if (!st || st == ctx->stream) {
+    return 0;
+  }
+  if (st == ctx->stream2) {
+    return 1;
+  }
+  if (st == ctx->stream3) {
+    return 2;
+  }
+  for (int i = 0; i < 6; ++i) {
+    if (st == ctx->aux[i]) {
+      return 3 + i;
+    }
+  }
+  return -1;
+}
+
+// a point on the timeline (kind < 0: TMX_TL_* marks)
+static inline int tl_mark(tmx_ctx *ctx, int kind, cudaStream_t st) {
+  if (!ctx->profiling) {
+    return 0;
+  }
+  cudaEvent_t a;
+  int rc = prof_event(ctx, &a);
+  if (rc) {
+    return rc;
+  }
+  CK(cudaEventRecord(a, st ? st : ctx->stream));
+  ctx->tl_pending.push_back({kind, stream_index(ctx, st), 0, a, a});
+  return 0;
+}
+
+// info: the launch's work items (timeline only)
 static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
-                           cudaStream_t st = nullptr, double bytes = 0.) {
+                           cudaStream_t st = nullptr, double bytes = 0.,
+                           int info = 0) {
   if (!ctx->profiling) {
     return 0;
   }
@@ -267,6 +314,7 @@ static inline int prof_end(tmx_ctx *ctx, int k, cudaEvent_t a, double flops,
     return rc;
   }
   CK(cudaEventRecord(b, st ? st : ctx->stream));
+  ctx->tl_pending.push_back({k, stream_index(ctx, st), info, a, b});
   ctx->prof[k].pending.push_back({a, b});
   ctx->prof[k].launches += 1;
   ctx->prof[k].flops += flops;
@@ -286,6 +334,16 @@ static inline int prof_resolve(tmx_ctx *ctx) {
     }
     p.pending.clear();
   }
+  for (const auto &r : ctx->tl_pending) {
+    float t0 = 0.f, t1 = 0.f;
+    CK(cudaEventSynchronize(r.b));
+    CK(cudaEventElapsedTime(&t0, ctx->tl_origin, r.a));
+    CK(cudaEventElapsedTime(&t1, ctx->tl_origin, r.b));
+    const double v[5] = {(double)r.kind, (double)r.stream, (double)r.info,
+                         (double)t0, (double)t1};
+    ctx->tl_done.insert(ctx->tl_done.end(), v, v + 5);
+  }
+  ctx->tl_pending.clear();
   ctx->prof_used = 0;
   return 0;
 }

@@ -322,6 +322,9 @@ void tmx_destroy(tmx_ctx *ctx) {
   for (cudaEvent_t e : ctx->prof_pool) {
     cudaEventDestroy(e);
   }
+  if (ctx->tl_origin) {
+    cudaEventDestroy(ctx->tl_origin);
+  }
   for (cudaEvent_t e : ctx->drain_ev) {
     if (e) {
       cudaEventDestroy(e);
@@ -710,7 +713,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
                       (const int64_t *)ctx->gl_off.p, tab, nsc,
                       ctx->up_sched.bessel_start, ngmax, nmmax, st);
     LAUNCHED();
-    if ((rc = prof_end(ctx, 1, pe, 0., st))) {
+    if ((rc = prof_end(ctx, 1, pe, 0., st, 0., np2))) {
       return rc;
     }
   }
@@ -783,7 +786,7 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
         CK(cudaEventRecord(tb, bs));
         ctx->tune_ev.emplace_back(dispatch_bucket(B.max_nb), ta, tb);
       }
-      if ((rc = prof_end(ctx, 0, pe, fl, bs))) {
+      if ((rc = prof_end(ctx, 0, pe, fl, bs, 0., B.nitems))) {
         return rc;
       }
       if (bs != st) {
@@ -994,6 +997,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     return TMX_OK;
   }
   std::vector<TmxChainState> st0(n);
+  if ((rc = tl_mark(ctx, TMX_TL_BATCH_START, st))) {
+    return rc;
+  }
   CK(cudaMemcpyAsync(ctx->state.p, ctx->state0.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToDevice, st));
   if (ctx->up_nact > 0) {
@@ -1193,7 +1199,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
                         (const int64_t *)ctx->gl_off.p, (double *)ctx->tab.p,
                         (double *)ctx->nsc.p, S.bessel_start, glf * kl, kl, st);
       LAUNCHED();
-      if ((rc2 = prof_end(ctx, 1, pe, 0.))) {
+      if ((rc2 = prof_end(ctx, 1, pe, 0., nullptr, 0., nsl))) {
         return rc2;
       }
       TmxBlockArgs B;
@@ -1225,7 +1231,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       }
       tmx_launch_blocks(B, st);
       LAUNCHED();
-      if ((rc2 = prof_end(ctx, 0, pe, fl))) {
+      if ((rc2 = prof_end(ctx, 0, pe, fl, nullptr, 0., B.nitems))) {
         return rc2;
       }
       for (int s = 0; s < G; ++s) {
@@ -1373,6 +1379,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
   }
   chain_range.reset();
+  if ((rc = tl_mark(ctx, TMX_TL_LOOP_END, st))) {
+    return rc;
+  }
 
   // ---- per-grain outcome of the order loop
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
@@ -1401,7 +1410,10 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
   }
   if (rounds == 0) {
-    return run_blocks(ctx, p2);
+    if ((rc = run_blocks(ctx, p2))) {
+      return rc;
+    }
+    return tl_mark(ctx, TMX_TL_BATCH_END, st);
   }
   // the last round on this stream, then wait for the round streams
   if ((rc = run_blocks_round(ctx, p2, st, t_next, true, &t_next, true))) {
@@ -1415,6 +1427,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   CK(cudaStreamWaitEvent(st, rounds_done, 0));
   CK(cudaEventDestroy(rounds_done));
   if ((rc = finish_blocks(ctx, t_next, rounds + 1))) {
+    return rc;
+  }
+  if ((rc = tl_mark(ctx, TMX_TL_BATCH_END, st))) {
     return rc;
   }
   ctx->rounds_lu = true;
@@ -1767,7 +1782,15 @@ int tmx_profile_enable(tmx_ctx *ctx, int on) {
     p.bytes = 0.;
   }
   ctx->prof_used = 0;
+  ctx->tl_pending.clear();
+  ctx->tl_done.clear();
   ctx->profiling = on != 0;
+  if (ctx->profiling) {
+    if (!ctx->tl_origin) {
+      CK(cudaEventCreate(&ctx->tl_origin));
+    }
+    CK(cudaEventRecord(ctx->tl_origin, ctx->stream));
+  }
   // events for a few batches, made before any timed work
   while (ctx->profiling && ctx->prof_pool.size() < 2048) {
     cudaEvent_t e;
@@ -1782,6 +1805,28 @@ int tmx_profile_bytes(tmx_ctx *ctx, int kernel, double *bytes) {
     return TMX_ERR_INVALID;
   }
   *bytes = ctx->prof[kernel].bytes;
+  return TMX_OK;
+}
+
+int tmx_profile_timeline(tmx_ctx *ctx, int64_t cap, double *records,
+                         int64_t *count) {
+  if (!ctx || cap < 0 || (cap > 0 && !records) || !count) {
+    return TMX_ERR_INVALID;
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaDeviceSynchronize());
+  if (ctx->profiling || !ctx->tl_pending.empty()) {
+    const int rc = prof_resolve(ctx);
+    if (rc) {
+      return rc;
+    }
+  }
+  const int64_t nrec = (int64_t)ctx->tl_done.size() / 5;
+  *count = nrec;
+  if (cap > 0) {
+    memcpy(records, ctx->tl_done.data(),
+           (size_t)std::min(cap, nrec) * 5 * sizeof(double));
+  }
   return TMX_OK;
 }
 

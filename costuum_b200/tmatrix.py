@@ -154,6 +154,32 @@ class Context:
         _lib.check(self._h, rc, "tmx_probe_fp64")
         return float(v[0])
 
+    def profile(self, on=True):
+        """Switch the per-kernel CUDA-event profile on or off
+        (tmx_profile_enable); resets its counters and the timeline."""
+        rc = _lib.load().tmx_profile_enable(self._h, int(bool(on)))
+        _lib.check(self._h, rc, "tmx_profile_enable")
+
+    TIMELINE_DTYPE = np.dtype([("kind", np.int32), ("stream", np.int32),
+                               ("items", np.int32), ("start_ms", np.float64),
+                               ("end_ms", np.float64)])
+
+    def timeline(self):
+        """Launch timeline since profile(True) (tmx_profile_timeline): one
+        record per profiled launch or mark, times in ms."""
+        lib = _lib.load()
+        cnt = np.zeros(1, np.int64)
+        rc = lib.tmx_profile_timeline(self._h, 0, None, _lib.lptr(cnt))
+        _lib.check(self._h, rc, "tmx_profile_timeline")
+        rec = np.zeros((int(cnt[0]), 5))
+        rc = lib.tmx_profile_timeline(self._h, rec.shape[0], _lib.ptr(rec),
+                                      _lib.lptr(cnt))
+        _lib.check(self._h, rc, "tmx_profile_timeline")
+        out = np.zeros(rec.shape[0], self.TIMELINE_DTYPE)
+        for i, name in enumerate(self.TIMELINE_DTYPE.names):
+            out[name] = rec[:, i]
+        return out
+
     def tmatrix_batch(self, r_ev, wavelength, m, axis_ratio, min_order=10,
                       max_order=100, gauss_legendre_factor=2, tolerance=1e-4,
                       bessel_start=0):

@@ -195,6 +195,22 @@ int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,
                      double *flops);
 int tmx_profile_bytes(tmx_ctx *ctx, int kernel, double *bytes);
 
+/* Timeline of the profiled launches since tmx_profile_enable (the device-side
+ * counterpart of the reference's per-task log, QuickSched's task output):
+ * 5 doubles per record, {kind, stream, items, start_ms, end_ms}, times from
+ * the enable call on the library stream. kind: a tmx_profile_kernel, or a
+ * mark (start == end) below; stream: 0 the library stream (convergence
+ * loop), 1 and 2 the block-round streams, 3..8 their bucket streams; items:
+ * work items of a block launch. At most cap records are written; *count
+ * receives the number available. */
+enum tmx_timeline_mark {
+  TMX_TL_BATCH_START = -1, /* tmx_batch_compute's first launch */
+  TMX_TL_LOOP_END = -2,    /* the order loop's last launch has finished */
+  TMX_TL_BATCH_END = -3    /* every launch of the batch has finished */
+};
+int tmx_profile_timeline(tmx_ctx *ctx, int64_t cap, double *records,
+                         int64_t *count);
+
 /* FP64 flops of the last batch counted with the unreduced per-grain model
  * (every chain order and every m block as a full 2nb x 2nb LU + solve);
  * counted only for batches computed while profiling is enabled, else 0. */

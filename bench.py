@@ -97,18 +97,68 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    """SM clock and throttle-reason samples during the timed region: NVML
+    polled every few milliseconds from a thread (a timed region of a few
+    steps lasts tens of ms), else nvidia-smi at its 200 ms minimum."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+             "sw_power_cap"]
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.002):
         self.device = device
+        self.period = period_s
         self.proc = None
+        self.nvml = None
         self.lines = []
+        self.samples = []  # (sm MHz, reason bits)
+        self.smax = None
+        self.bits = {}
+        self.done = threading.Event()
+
+    def _nvml_start(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        idx = self.device
+        if hasattr(torch.cuda, "_get_nvml_device_index"):
+            idx = torch.cuda._get_nvml_device_index(self.device)
+        h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons",
+                              None) or pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+
+        def bit(name, default):
+            for pre in ("nvmlClocksEventReason", "nvmlClocksThrottleReason"):
+                if hasattr(pynvml, pre + name):
+                    return getattr(pynvml, pre + name)
+            return default
+        self.bits = {"hw_slowdown": bit("HwSlowdown", 0x8),
+                     "hw_thermal_slowdown": bit("HwThermalSlowdown", 0x40),
+                     "sw_thermal_slowdown": bit("SwThermalSlowdown", 0x20),
+                     "sw_power_cap": bit("SwPowerCap", 0x4)}
+        self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+
+        def poll():
+            while not self.done.is_set():
+                try:
+                    self.samples.append(
+                        (float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                         int(get_reasons(h))))
+                except pynvml.NVMLError:
+                    pass
+                time.sleep(self.period)
+        self.nvml = pynvml
+        self.th = threading.Thread(target=poll, daemon=True)
+        self.th.start()
 
     def start(self):
+        try:
+            self._nvml_start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
@@ -124,6 +174,20 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.done.set()
+            self.th.join(timeout=5)
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({nm for _, b in self.samples
+                              for nm, v in self.bits.items() if b & v})
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return {"sm_mhz": float(np.median(sm)) if sm else None,
+                    "sm_max_mhz": self.smax, "samples": len(sm),
+                    "source": "NVML every %g ms" % (1e3 * self.period),
+                    "reasons": reasons}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         self.proc.terminate()
@@ -132,8 +196,6 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
-                 "sw_power_cap"]
         for ln in self.lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 8:
@@ -143,12 +205,12 @@ class ClockSampler:
                 smax = float(p[1])
             except ValueError:
                 continue
-            for nm, v in zip(names, p[4:8]):
+            for nm, v in zip(self.NAMES, p[4:8]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": smax, "samples": len(sm),
-                "reasons": sorted(reasons)}
+                "source": "nvidia-smi every 200 ms", "reasons": sorted(reasons)}
 
 
 def flush_l2(buf):

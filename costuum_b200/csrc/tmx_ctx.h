@@ -70,11 +70,10 @@ struct tmx_ctx {
   // plan of the observable kernels (first pair of each grain, job groups)
   int64_t o_ngrains = 0, o_npairs = 0;
   int o_nbmax = 1, o_ngrp = 0;
-  // orientation-average work order: grain tiles (o_pairs, TmxOrientTile),
-  // their per-order grain counts (o_tcnt) and the grains by descending order
-  // (o_ord); o_npairs counts the (tile, pair) units
-  DevBuf o_ord, o_tcnt;
-  int o_ntiles = 0;
+  // orientation-average work order: pair-major item starts (o_pairs, pmax^2
+  // + 1) and the grains by descending order (o_ord)
+  DevBuf o_ord;
+  int o_pmax = 1;
   // angles of the current plan (o_angles) and their pi / tau columns
   int o_nangles = 0;
   DevBuf o_wcol;

@@ -335,7 +335,7 @@ void tmx_destroy(tmx_ctx *ctx) {
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
                     &ctx->o_og, &ctx->o_work, &ctx->o_sj, &ctx->o_qj, &ctx->o_S,
                     &ctx->o_gq, &ctx->o_gz, &ctx->o_cq, &ctx->o_cz,
-                    &ctx->o_pairs, &ctx->o_grp, &ctx->o_x, &ctx->o_ord, &ctx->o_tcnt, &ctx->o_wcol,
+                    &ctx->o_pairs, &ctx->o_grp, &ctx->o_x, &ctx->o_ord, &ctx->o_wcol,
                     &ctx->p2tab, &ctx->p2nsc, &ctx->p2scratch, &ctx->p2slots,
                     &ctx->p2items, &ctx->done, &ctx->keep_arena, &ctx->keep_tab,
                     &ctx->keep_q, &ctx->done_pos, &ctx->keep_ctl,

@@ -183,22 +183,15 @@ struct TmxMatSet {
   const double2 *src[4];
   double2 *dst[4];
 };
-// tile of consecutive grains order[g0 .. g0 + ng) (by descending nmax) of
-// the orientation average: units [unit0, unit0 + pmax^2) are its pairs
-// (n1, n2), pmax = the first grain's nmax, and tcnt[cnt0 + k - 1] is the
-// number of its grains of order >= k
-struct TmxOrientTile {
-  int64_t unit0;
-  int32_t g0, ng;
-  int32_t pmax, cnt0;
-};
 // orientation average (coef_set >= 0) or copy of every grain's T-matrix,
-// with the amplitude factors c_{n' n} folded in when fold != 0; one warp
-// per unit (tile, pair), nunits = sum over tiles of pmax^2; mmax >= every
-// nmax; nmat (1 or 4) sets src[k] -> dst[k]
-void tmx_launch_orient_pairs(const TmxObsGrain *og, const TmxOrientTile *tiles,
-                             int ntiles, const int32_t *tcnt,
-                             const int32_t *order, int64_t nunits,
+// with the amplitude factors c_{n' n} folded in when fold != 0;
+// work items (pair (n1, n2), grain) pair-major: pair q = (n1 - 1) pmax +
+// n2 - 1 owns items [pstart[q], pstart[q + 1]), for the grains
+// order[0 .. pstart[q + 1] - pstart[q]) (grains by descending nmax, so the
+// grains of order >= max(n1, n2) come first); npairs = sum of nmax^2;
+// mmax >= every nmax; nmat (1 or 4) sets src[k] -> dst[k]
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
+                             const int32_t *order, int pmax, int64_t npairs,
                              const TmxMatSet &mats,
                              int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,

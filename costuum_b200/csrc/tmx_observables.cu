@@ -155,8 +155,7 @@ __device__ __forceinline__ cplx c_fold(int nin, int nout, double a, cplx z) {
   }
 }
 
-// One warp per (grain tile, n1, n2), looping over the tile's grains of
-// order >= max(n1, n2). AlignmentAverageTask::execute (Alignment
+// One warp per (grain, n1, n2). AlignmentAverageTask::execute (Alignment
 // AverageTask.hpp:115-215) forms, for every m,
 //   Ta_m = sum_N' p_N' (-1)^m CG(n1 m n2 -m|N'0) sum_m1 f(m1) (-1)^m1
 //          CG(n1 m1 n2 -m1|N'0) T_m1,
@@ -170,18 +169,12 @@ __device__ __forceinline__ cplx c_fold(int nin, int nout, double a, cplx z) {
 // Shared memory per warp and matrix: t[4][M + 1] and S[2][2M + 1] complex.
 // NMAT matrices (a T-matrix and its tangents) share the Clebsch-Gordan
 // reads and the loops; each is summed in the same order as alone.
-// Work order: tiles of consecutive grains (by descending order) whose
-// T-matrices together fit well inside L2; within a tile, (n1, n2) row-major,
-// so the warps of a CTA read neighbouring columns n2 of the same rows of the
-// same grains (shared sectors), each tile's T-matrices come from DRAM once,
-// and a warp reuses its pair's Clebsch-Gordan rows for every grain.
 template <int NMAT>
 __global__ void __launch_bounds__(256)
 k_orient_pairs(const TmxObsGrain *__restrict__ og,
-               const TmxOrientTile *__restrict__ tiles, int ntiles,
-               const int32_t *__restrict__ tcnt,
-               const int32_t *__restrict__ order, int64_t nunits,
-               TmxMatSet mats, const double *__restrict__ coeffs,
+               const int64_t *__restrict__ pstart,
+               const int32_t *__restrict__ order, int pmax,
+               int64_t npairs, TmxMatSet mats, const double *__restrict__ coeffs,
                int ncoef, const int64_t *__restrict__ cg_off,
                const double *__restrict__ cg, int cg_nmax, int wcap, int fold) {
   extern __shared__ cplx osh[];
@@ -189,32 +182,31 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   cplx *tv = osh + (int64_t)warp * wcap * NMAT;
-  for (int64_t u = (int64_t)blockIdx.x * nwarps + warp; u < nunits;
-       u += (int64_t)gridDim.x * nwarps) {
-    // unit u = (tile, pair (n1, n2)): tile t owns units [unit0, unit0 +
-    // pmax^2), pair q = (n1 - 1) pmax + (n2 - 1)
-    int lo = 0, hi = ntiles - 1;
+  for (int64_t w = (int64_t)blockIdx.x * nwarps + warp; w < npairs;
+       w += (int64_t)gridDim.x * nwarps) {
+    // work item w = (pair (n1, n2), grain): pair-major, so that the warps
+    // of a CTA (and CTAs running together) contract the same Clebsch-Gordan
+    // rows for different grains and read them from cache. Pair
+    // q = (n1 - 1) pmax + (n2 - 1) owns items [pstart[q], pstart[q + 1]),
+    // one per grain of order >= max(n1, n2), in the order `order` (grains by
+    // descending order).
+    int lo = 0, hi = pmax * pmax - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (tiles[mid].unit0 <= u) {
+      if (pstart[mid] <= w) {
         lo = mid;
       } else {
         hi = mid - 1;
       }
     }
-    const TmxOrientTile tt = tiles[lo];
-    const int q = (int)(u - tt.unit0);
-    const int n1 = q / tt.pmax + 1;
-    const int n2 = q - (n1 - 1) * tt.pmax + 1;
-    // the tile's grains of order >= max(n1, n2) are its first `cnt`
-    const int cnt = tcnt[tt.cnt0 + max(n1, n2) - 1];
+    const int n1 = lo / pmax + 1;
+    const int n2 = lo % pmax + 1;
+    const TmxObsGrain G = og[order[w - pstart[lo]]];
+    const int N = G.nmax;
     const int M = min(n1, n2);
     // fold = 0: the plain averaged T-matrix (c = 1: i^0 times 1)
     const double afold = fold ? a_fac(n1) * a_fac(n2) : 1.;
     const int nfold = fold ? n1 : n2 - 1;
-    for (int gi = 0; gi < cnt; ++gi) {
-    const TmxObsGrain G = og[order[tt.g0 + gi]];
-    const int N = G.nmax;
     if (G.coef_set < 0) {
       for (int m = lane; m <= M; m += 32) {
         for (int q = 0; q < 4; ++q) {
@@ -307,7 +299,6 @@ k_orient_pairs(const TmxObsGrain *__restrict__ og,
       }
     }
     __syncwarp();
-    }
   }
 }
 
@@ -769,35 +760,34 @@ void tmx_launch_cg(int nmax, const int64_t *cg_off, double *cg, double *work,
   k_cg<<<blocks, 128, 0, stream>>>(nmax, cg_off, cg, work);
 }
 
-void tmx_launch_orient_pairs(const TmxObsGrain *og, const TmxOrientTile *tiles,
-                             int ntiles, const int32_t *tcnt,
-                             const int32_t *order, int64_t nunits,
+void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
+                             const int32_t *order, int pmax, int64_t npairs,
                              const TmxMatSet &mats,
                              int nmat, const double *coeffs, int ncoef,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,
                              cudaStream_t stream) {
-  if (nunits <= 0) {
+  if (npairs <= 0) {
     return;
   }
   const int wcap = 4 * (mmax + 1) + 2 * (2 * mmax + 1);
   const size_t smem = (size_t)8 * wcap * nmat * sizeof(double2);
-  const int64_t want = (nunits + 7) / 8;
+  const int64_t want = (npairs + 7) / 8;
   const int blocks = (int)std::min<int64_t>(want, 148 * 8);
   if (nmat == 4) {
     // four warps per CTA: the four matrices' buffers of 8 warps would
     // leave room for one CTA per SM
     const size_t smem4 = (size_t)4 * wcap * nmat * sizeof(double2);
-    const int blocks4 = (int)std::min<int64_t>((nunits + 3) / 4, 148 * 16);
+    const int blocks4 = (int)std::min<int64_t>((npairs + 3) / 4, 148 * 16);
     cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem4);
-    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, tiles, ntiles, tcnt, order, nunits,
+    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pstart, order, pmax, npairs,
                                                        mats, coeffs, ncoef, cg_off, cg,
                                                        cg_nmax, wcap, fold);
   } else {
     cudaFuncSetAttribute(k_orient_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    k_orient_pairs<1><<<blocks, 256, smem, stream>>>(og, tiles, ntiles, tcnt, order, nunits,
+    k_orient_pairs<1><<<blocks, 256, smem, stream>>>(og, pstart, order, pmax, npairs,
                                                      mats, coeffs, ncoef, cg_off, cg,
                                                      cg_nmax, wcap, fold);
   }

@@ -377,12 +377,9 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
   int rc0;
   cudaStream_t st = ctx->stream;
   const int64_t n = (int64_t)og.size();
-  // orientation-average work units (tmx_launch_orient_pairs): tiles of
-  // consecutive grains by descending order, each closed at about
-  // TILE_BYTES of T-matrices (the warps resident at once span a few tiles,
-  // which stay in L2 while their pairs are averaged) or TILE_GRAINS grains
-  constexpr double TILE_BYTES = 4. * (1 << 20);
-  constexpr int TILE_GRAINS = 64;
+  // orientation-average work items, pair-major (tmx_launch_orient_pairs):
+  // grains by descending order; pair (n1, n2) has one item per grain of
+  // order >= max(n1, n2)
   int nbmax = 1;
   for (int64_t g = 0; g < n; ++g) {
     nbmax = std::max(nbmax, og[g].nmax);
@@ -396,44 +393,27 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
   std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
     return og[a].nmax > og[b].nmax;
   });
-  std::vector<TmxOrientTile> tiles;
-  std::vector<int32_t> tcnt;
-  int64_t nunits = 0;
-  for (size_t i = 0; i < order.size();) {
-    TmxOrientTile t;
-    t.unit0 = nunits;
-    t.g0 = (int32_t)i;
-    t.pmax = og[order[i]].nmax;
-    t.cnt0 = (int32_t)tcnt.size();
-    double bytes = 0.;
-    size_t j = i;
-    while (j < order.size() && j - i < (size_t)TILE_GRAINS &&
-           (j == i || bytes < TILE_BYTES)) {
-      bytes += 16. * (double)tmx_tmatrix_size(og[order[j]].nmax);
-      ++j;
-    }
-    t.ng = (int32_t)(j - i);
-    int32_t c = t.ng;
-    std::vector<int32_t> cnt(t.pmax);
-    for (int k = t.pmax; k >= 1; --k) {
-      while (c > 0 && og[order[i + c - 1]].nmax < k) {
-        --c;
-      }
-      cnt[k - 1] = c;
-    }
-    tcnt.insert(tcnt.end(), cnt.begin(), cnt.end());
-    nunits += (int64_t)t.pmax * t.pmax;
-    tiles.push_back(t);
-    i = j;
+  std::vector<int64_t> at_least(nbmax + 2, 0); // grains of order >= k
+  for (int32_t g : order) {
+    at_least[og[g].nmax] += 1;
   }
-  if ((rc0 = ensure(ctx, ctx->o_ord, std::max<size_t>(1, order.size()) * sizeof(int32_t))) ||
-      (rc0 = ensure(ctx, ctx->o_tcnt, std::max<size_t>(1, tcnt.size()) * sizeof(int32_t)))) {
+  for (int k = nbmax; k >= 1; --k) {
+    at_least[k] += at_least[k + 1];
+  }
+  std::vector<int64_t> base((size_t)nbmax * nbmax + 1, 0);
+  int64_t npairs = 0;
+  for (int n1 = 1; n1 <= nbmax; ++n1) {
+    for (int n2 = 1; n2 <= nbmax; ++n2) {
+      base[(size_t)(n1 - 1) * nbmax + (n2 - 1)] = npairs;
+      npairs += at_least[std::max(n1, n2)];
+    }
+  }
+  base.back() = npairs;
+  if ((rc0 = ensure(ctx, ctx->o_ord, std::max<size_t>(1, order.size()) * sizeof(int32_t)))) {
     return rc0;
   }
   if (!order.empty()) {
     CK(cudaMemcpyAsync(ctx->o_ord.p, order.data(), order.size() * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->o_tcnt.p, tcnt.data(), tcnt.size() * sizeof(int32_t),
                        cudaMemcpyHostToDevice, st));
   }
   std::vector<TmxAmpGroup> grp;
@@ -448,24 +428,21 @@ int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
     grp.back().njobs += 1;
   }
   int rc;
-  if ((rc = ensure(ctx, ctx->o_pairs, std::max<size_t>(1, tiles.size()) *
-                                          sizeof(TmxOrientTile))) ||
+  if ((rc = ensure(ctx, ctx->o_pairs, base.size() * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->o_grp, std::max<size_t>(1, grp.size()) * sizeof(TmxAmpGroup)))) {
     return rc;
   }
-  if (!tiles.empty()) {
-    CK(cudaMemcpyAsync(ctx->o_pairs.p, tiles.data(), tiles.size() * sizeof(TmxOrientTile),
-                       cudaMemcpyHostToDevice, st));
-  }
+  CK(cudaMemcpyAsync(ctx->o_pairs.p, base.data(), base.size() * sizeof(int64_t),
+                     cudaMemcpyHostToDevice, st));
   if (!grp.empty()) {
     CK(cudaMemcpyAsync(ctx->o_grp.p, grp.data(), grp.size() * sizeof(TmxAmpGroup),
                        cudaMemcpyHostToDevice, st));
   }
   CK(cudaStreamSynchronize(st));
   ctx->o_ngrains = n;
-  ctx->o_npairs = nunits;
+  ctx->o_npairs = npairs;
   ctx->o_nbmax = nbmax;
-  ctx->o_ntiles = (int)tiles.size();
+  ctx->o_pmax = nbmax;
   ctx->o_ngrp = (int)grp.size();
   if (ctx->profiling) {
     // flops of one matrix set over the kernels' index spaces: the
@@ -547,9 +524,8 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
     return rc;
   }
   tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
-                          (const TmxOrientTile *)ctx->o_pairs.p, ctx->o_ntiles,
-                          (const int32_t *)ctx->o_tcnt.p, (const int32_t *)ctx->o_ord.p,
-                          ctx->o_npairs, avg, nmat,
+                          (const int64_t *)ctx->o_pairs.p, (const int32_t *)ctx->o_ord.p,
+                          ctx->o_pmax, ctx->o_npairs, avg, nmat,
                           (const double *)ctx->o_coef.p,
                           ncoef, (const int64_t *)ctx->cg_off.p,
                           (const double *)ctx->cg.p, ctx->cg_nmax, ctx->o_nbmax, 1,
@@ -1628,9 +1604,8 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
     avg.src[0] = (const cplx *)ctx->T.p;
     avg.dst[0] = (cplx *)ctx->Ta.p;
     tmx_launch_orient_pairs((const TmxObsGrain *)ctx->o_og.p,
-                            (const TmxOrientTile *)ctx->o_pairs.p, ctx->o_ntiles,
-                            (const int32_t *)ctx->o_tcnt.p,
-                            (const int32_t *)ctx->o_ord.p, ctx->o_npairs,
+                            (const int64_t *)ctx->o_pairs.p,
+                            (const int32_t *)ctx->o_ord.p, ctx->o_pmax, ctx->o_npairs,
                             avg, 1, (const double *)ctx->o_coef.p, ncoef,
                             (const int64_t *)ctx->cg_off.p, (const double *)ctx->cg.p,
                             ctx->cg_nmax, ctx->o_nbmax, 0, st);

@@ -197,10 +197,9 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
                              const int64_t *cg_off, const double *cg,
                              int cg_nmax, int mmax, int fold,
                              cudaStream_t stream);
-// CTAs of the amplitude kernel at full occupancy for nbmax and nmat, with
-// or without the plan's pi / tau table (its work slots: grid x nmat x 32 x
-// (nbmax + 1) x 4 complex)
-int tmx_amp_grid(int nbmax, int nmat, bool table);
+// CTAs of the amplitude kernel at full occupancy for nbmax and nmat (its
+// work slots: grid x nmat x 32 x (nbmax + 1) x 4 complex)
+int tmx_amp_grid(int nbmax, int nmat);
 // amplitudes of nmat (1 or 4) averaged sets: src[k] -> S at dst[k]
 // wpi / wtau (may be NULL: the kernel runs the recurrences itself): the
 // plan's pi and tau columns from tmx_launch_wigner_cols for nmax wnmax

@@ -401,12 +401,7 @@ __global__ void k_wigner_cols(const TmxAngle *__restrict__ angles, int nangles,
 // kept in this CTA's global slot; the azimuth pass then forms
 //   S = (1/k) sum_m (2 cos m phi, 2 sin m phi) X_m
 // with e^{i m phi} built by repeated multiplication as in the reference.
-// TAB: the angle vectors come from the plan's table (k_wigner_cols); only
-// the incoming side is staged in shared memory (the outgoing one is read
-// twice per row), which halves the CTA's shared memory. A warp contracts
-// RP rows r, r + 8, ... per pass over the columns, sharing the angle-vector
-// reads; the rows still enter X in ascending order.
-template <int NMAT, bool TAB>
+template <int NMAT>
 __global__ void __launch_bounds__(256, (NMAT > 1) ? 2 : 3)
 k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const TmxSJob *__restrict__ jobs, const TmxObsGrain *__restrict__ og,
@@ -414,13 +409,12 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
       const cplx *__restrict__ phis, cplx *__restrict__ xslot, int nbmax,
       const double *__restrict__ wpi, const double *__restrict__ wtau,
       int wnmax) {
-  constexpr int RP = (NMAT == 1) ? 2 : 1;
   extern __shared__ double ash[];
-  double *pi = ash;
-  double *ti = pi + nbmax * 32;
-  double *po = ti + nbmax * 32; // (not with TAB)
+  double *po = ash;
   double *to = po + nbmax * 32;
-  cplx *red = (cplx *)(TAB ? po : to + nbmax * 32); // [NMAT][8 warps][4][32 lanes]
+  double *pi = to + nbmax * 32;
+  double *ti = pi + nbmax * 32;
+  cplx *red = (cplx *)(ti + nbmax * 32); // [NMAT][8 warps][4][32 lanes]
   __shared__ TmxSJob sj[32];
   __shared__ int pref[33];
   const int tid = threadIdx.x;
@@ -445,24 +439,21 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
     for (int m = 0; m <= N; ++m) {
       const int nmin = (m > 1) ? m : 1;
       const int nb = N + 1 - nmin;
-      // this lane's outgoing column in the table (TAB)
-      int64_t ocol = -1;
-      if constexpr (TAB) {
-        if (lane < nj) {
-          ocol = ((int64_t)sj[lane].angle_out * (wnmax + 1) + m) * wnmax;
-        }
-        // the incoming columns of this m from the plan's table
-        for (int u = tid; u < 32 * nb; u += blockDim.x) {
-          const int k = u >> 5;
+      if (wpi) {
+        // the columns of this m from the plan's table (k_wigner_cols)
+        for (int u = tid; u < 64 * nb; u += blockDim.x) {
+          const int side = u / (32 * nb); // 0: outgoing angle, 1: incoming
+          const int k = (u - side * 32 * nb) >> 5;
           const int p = u & 31;
           double pv = 0., tv = 0.;
           if (p < nj) {
-            const int64_t off = ((int64_t)sj[p].angle_in * (wnmax + 1) + m) * wnmax + k;
+            const int a = side ? sj[p].angle_in : sj[p].angle_out;
+            const int64_t off = ((int64_t)a * (wnmax + 1) + m) * wnmax + k;
             pv = wpi[off];
             tv = wtau[off];
           }
-          pi[k * 32 + p] = pv;
-          ti[k * 32 + p] = tv;
+          (side ? pi : po)[k * 32 + p] = pv;
+          (side ? ti : to)[k * 32 + p] = tv;
         }
       } else if (tid < 64) {
         const int p = tid & 31;
@@ -486,60 +477,36 @@ k_amp(const TmxAmpGroup *__restrict__ groups, int ngroups,
         x0[q] = x1[q] = x2[q] = x3[q] = mkc(0., 0.);
       }
       const int64_t tb = G.t_off + tblock(N, m);
-      for (int r0 = warp; r0 < 2 * nb; r0 += 8 * RP) {
-        // rows r0 + 8 i (i < nr) of this pass
-        const int nr = min(RP, (2 * nb - 1 - r0) / 8 + 1);
-        cplx y0[RP][NMAT], y1[RP][NMAT];
+      for (int r = warp; r < 2 * nb; r += 8) {
+        cplx y0[NMAT], y1[NMAT];
 #pragma unroll
-        for (int i = 0; i < RP; ++i) {
-#pragma unroll
-          for (int q = 0; q < NMAT; ++q) {
-            y0[i][q] = y1[i][q] = mkc(0., 0.);
-          }
+        for (int q = 0; q < NMAT; ++q) {
+          y0[q] = y1[q] = mkc(0., 0.);
         }
-#pragma unroll 2
+#pragma unroll 4
         for (int k = 0; k < nb; ++k) {
           const double a = pi[k * 32 + lane];
           const double b = ti[k * 32 + lane];
 #pragma unroll
-          for (int i = 0; i < RP; ++i) {
-            if (i < nr) {
-#pragma unroll
-              for (int q = 0; q < NMAT; ++q) {
-                const cplx *Tr = mats.src[q] + tb + (int64_t)(r0 + 8 * i) * 2 * nb;
-                const cplx t0 = Tr[k];
-                const cplx t1 = Tr[nb + k];
-                cfma(y0[i][q], t0, a);
-                cfma(y0[i][q], t1, b);
-                cfma(y1[i][q], t0, b);
-                cfma(y1[i][q], t1, a);
-              }
-            }
+          for (int q = 0; q < NMAT; ++q) {
+            const cplx *Tr = mats.src[q] + tb + (int64_t)r * 2 * nb;
+            const cplx t0 = Tr[k];
+            const cplx t1 = Tr[nb + k];
+            cfma(y0[q], t0, a);
+            cfma(y0[q], t1, b);
+            cfma(y1[q], t0, b);
+            cfma(y1[q], t1, a);
           }
         }
+        const int kr = (r < nb) ? r : r - nb;
+        const double u = (r < nb) ? po[kr * 32 + lane] : to[kr * 32 + lane];
+        const double up = (r < nb) ? to[kr * 32 + lane] : po[kr * 32 + lane];
 #pragma unroll
-        for (int i = 0; i < RP; ++i) {
-          if (i < nr) {
-            const int r = r0 + 8 * i;
-            const int kr = (r < nb) ? r : r - nb;
-            double u, up;
-            if constexpr (TAB) {
-              const double pv = (ocol >= 0) ? wpi[ocol + kr] : 0.;
-              const double tv = (ocol >= 0) ? wtau[ocol + kr] : 0.;
-              u = (r < nb) ? pv : tv;
-              up = (r < nb) ? tv : pv;
-            } else {
-              u = (r < nb) ? po[kr * 32 + lane] : to[kr * 32 + lane];
-              up = (r < nb) ? to[kr * 32 + lane] : po[kr * 32 + lane];
-            }
-#pragma unroll
-            for (int q = 0; q < NMAT; ++q) {
-              cfma(x0[q], y0[i][q], u);
-              cfma(x1[q], y1[i][q], u);
-              cfma(x2[q], y0[i][q], up);
-              cfma(x3[q], y1[i][q], up);
-            }
-          }
+        for (int q = 0; q < NMAT; ++q) {
+          cfma(x0[q], y0[q], u);
+          cfma(x1[q], y1[q], u);
+          cfma(x2[q], y0[q], up);
+          cfma(x3[q], y1[q], up);
         }
       }
 #pragma unroll
@@ -793,29 +760,25 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
   }
 }
 
-static size_t amp_smem(int nbmax, int nmat, bool tab) {
-  return (size_t)(tab ? 2 : 4) * nbmax * 32 * sizeof(double) +
+static size_t amp_smem(int nbmax, int nmat) {
+  return (size_t)4 * nbmax * 32 * sizeof(double) +
          (size_t)nmat * 8 * 4 * 32 * sizeof(double2);
 }
 
-template <int NMAT, bool TAB>
-static int amp_per_sm(int nbmax) {
-  int per_sm = 1;
-  cudaFuncSetAttribute(k_amp<NMAT, TAB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)amp_smem(TMX_MAX_NB, NMAT, TAB));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<NMAT, TAB>, 256,
-                                                amp_smem(nbmax, NMAT, TAB));
-  return per_sm;
-}
-
-int tmx_amp_grid(int nbmax, int nmat, bool table) {
+int tmx_amp_grid(int nbmax, int nmat) {
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (nmat == 4) {
-    per_sm = table ? amp_per_sm<4, true>(nbmax) : amp_per_sm<4, false>(nbmax);
+    cudaFuncSetAttribute(k_amp<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)amp_smem(TMX_MAX_NB, 4));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<4>, 256,
+                                                  amp_smem(nbmax, 4));
   } else {
-    per_sm = table ? amp_per_sm<1, true>(nbmax) : amp_per_sm<1, false>(nbmax);
+    cudaFuncSetAttribute(k_amp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)amp_smem(TMX_MAX_NB, 1));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<1>, 256,
+                                                  amp_smem(nbmax, 1));
   }
   return std::max(1, sms * std::max(1, per_sm));
 }
@@ -839,22 +802,14 @@ void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
     return;
   }
   const int blocks = std::min(grid, ngroups);
-  const bool tab = wpi != nullptr;
-  const size_t sm = amp_smem(nbmax, nmat, tab);
   if (nmat == 4) {
-    if (tab) {
-      k_amp<4, true><<<blocks, 256, sm, stream>>>(groups, ngroups, jobs, og, mats, angles,
-                                                  phis, xslot, nbmax, wpi, wtau, wnmax);
-    } else {
-      k_amp<4, false><<<blocks, 256, sm, stream>>>(groups, ngroups, jobs, og, mats, angles,
-                                                   phis, xslot, nbmax, wpi, wtau, wnmax);
-    }
-  } else if (tab) {
-    k_amp<1, true><<<blocks, 256, sm, stream>>>(groups, ngroups, jobs, og, mats, angles,
-                                                phis, xslot, nbmax, wpi, wtau, wnmax);
+    k_amp<4><<<blocks, 256, amp_smem(nbmax, 4), stream>>>(groups, ngroups, jobs, og,
+                                                          mats, angles, phis, xslot,
+                                                          nbmax, wpi, wtau, wnmax);
   } else {
-    k_amp<1, false><<<blocks, 256, sm, stream>>>(groups, ngroups, jobs, og, mats, angles,
-                                                 phis, xslot, nbmax, wpi, wtau, wnmax);
+    k_amp<1><<<blocks, 256, amp_smem(nbmax, 1), stream>>>(groups, ngroups, jobs, og,
+                                                          mats, angles, phis, xslot,
+                                                          nbmax, wpi, wtau, wnmax);
   }
 }
 

@@ -507,14 +507,7 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
     amp.src[k] = avg.dst[k];
     amp.dst[k] = S_out[k];
   }
-  // the pi / tau columns of every angle of the plan, made once for all
-  // grains below (unless the table would be large: then each CTA of the
-  // amplitude kernel runs the recurrences)
-  const int wn = ctx->o_nbmax;
-  const size_t wcol = (size_t)ctx->o_nangles * (wn + 1) * wn;
-  const bool wtab =
-      ctx->o_nangles > 0 && 2 * wcol * sizeof(double) <= ((size_t)512 << 20);
-  const int grid = tmx_amp_grid(ctx->o_nbmax, nmat, wtab);
+  const int grid = tmx_amp_grid(ctx->o_nbmax, nmat);
   if ((rc = ensure(ctx, ctx->o_x,
                    (size_t)grid * nmat * 32 * (ctx->o_nbmax + 1) * 4 * sizeof(cplx)))) {
     return rc;
@@ -539,8 +532,12 @@ int run_amplitudes(tmx_ctx *ctx, const cplx *const *Tsrc, int nmat,
   if ((rc = prof_begin(ctx, TMX_PROF_AMP, &pe))) {
     return rc;
   }
+  // the pi / tau columns of every angle of the plan, once for all grains
+  // (unless the table would be large: then each CTA runs the recurrences)
   const double *wpi = nullptr, *wtau = nullptr;
-  if (wtab) {
+  const int wn = ctx->o_nbmax;
+  const size_t wcol = (size_t)ctx->o_nangles * (wn + 1) * wn;
+  if (ctx->o_nangles > 0 && 2 * wcol * sizeof(double) <= ((size_t)512 << 20)) {
     if ((rc = ensure(ctx, ctx->o_wcol, 2 * wcol * sizeof(double)))) {
       return rc;
     }

@@ -1057,7 +1057,10 @@ static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
       (size_t)4 * (warp_elems<NBM>() + warp_stage_elems<NBM>()) * sizeof(cplx);
   cudaFuncSetAttribute(k_blocks_warp<TR, TC, MINB, MMA>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int blocks = (int)std::min<int64_t>((a.nitems + 3) / 4, 148 * 16);
+  // one item per warp: CTAs retire after one item, so that launches of the
+  // high-priority order loop get SMs between them (a grid of long-lived
+  // CTAs looping over items held the SMs for a whole round)
+  const int blocks = (int)std::max<int64_t>(1, ((int64_t)a.nitems + 3) / 4);
   k_blocks_warp<TR, TC, MINB, MMA><<<blocks, 128, smem, stream>>>(a);
 }
 
@@ -1210,6 +1213,8 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
         }
       }
     }
+    // every warp's column tiles of Q are in place before warp 0 factors
+    __syncthreads();
     if (wib == 0) {
       // LU in place in Qm, lane r updates row r
       bool singular = false;
@@ -1586,7 +1591,8 @@ static void launch_cta64(const TmxBlockArgs &a, cudaStream_t stream) {
   const size_t smem = (size_t)cta64_elems() * sizeof(cplx);
   cudaFuncSetAttribute(k_blocks_cta64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
-  const int blocks = (int)std::min<int64_t>(a.nitems, 148 * 4);
+  // one item per CTA (see launch_warp_variant)
+  const int blocks = std::max(1, a.nitems);
   k_blocks_cta64<<<blocks, 256, smem, stream>>>(a);
 }
 
@@ -1594,7 +1600,8 @@ static void launch_cta32(const TmxBlockArgs &a, cudaStream_t stream) {
   const size_t smem = (size_t)cta32_elems() * sizeof(cplx);
   cudaFuncSetAttribute(k_blocks_cta32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
-  const int blocks = (int)std::min<int64_t>(a.nitems, 148 * 12);
+  // one item per CTA (see launch_warp_variant)
+  const int blocks = std::max(1, a.nitems);
   k_blocks_cta32<<<blocks, 128, smem, stream>>>(a);
 }
 

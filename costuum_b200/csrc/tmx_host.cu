@@ -724,7 +724,15 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   cudaStream_t *aux = (st == ctx->stream)    ? &ctx->aux[0]
                       : (st == ctx->stream2) ? &ctx->aux[2]
                                              : &ctx->aux[4];
+  // the point on `st` (tables and lists ready) after which every bucket may
+  // start: recorded before the first bucket's launch, so that the others
+  // run beside it rather than after it
   cudaEvent_t fork = nullptr;
+  if (!ctx->tuning && nitems > 0 &&
+      dispatch_bucket(inb[0]) != dispatch_bucket(inb[nitems - 1])) {
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    CK(cudaEventRecord(fork, st));
+  }
   std::vector<cudaEvent_t> joins;
   int nbuckets = 0;
   const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
@@ -739,10 +747,6 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
       // while tuning, every bucket runs alone on the round's stream
       if (nbuckets > 0 && !ctx->tuning) {
         bs = aux[(nbuckets - 1) & 1];
-        if (!fork) {
-          CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-          CK(cudaEventRecord(fork, st));
-        }
         CK(cudaStreamWaitEvent(bs, fork, 0));
       }
       ++nbuckets;

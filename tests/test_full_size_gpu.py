@@ -9,6 +9,11 @@ grains with the smallest, median and largest converged order:
 * every grain converges, at an order inside the schedule;
 * determinism across round layouts: the same blocks computed in one round at
   the converged orders (tmatrix_batch_fixed) give the same doubles;
+* determinism across repeated batches: the size buckets of a block round run
+  concurrently on their own streams, next to the order loop and other
+  rounds, so a missing barrier shows as a class block that differs between
+  runs of the same batch; six more batches must repeat every T-matrix bit
+  for bit;
 * the per-grain Q sums that k_qsums reduces on the device equal the
   reference's sums (TMatrix Qsca/Qext loops, restated in the oracle) over the
   T-matrix downloaded from the device, for all 4096 grains (relative 1e-12:
@@ -72,6 +77,19 @@ def test_one_round_at_converged_orders_same_doubles(ctx, full):
     assert np.array_equal(fix.q[:, 2:4], full["q"][:, 2:4])
     for i in range(N_GRAINS):
         assert np.array_equal(fix.tmatrix(i), full["T"][i]), i
+
+
+def test_repeated_batches_same_doubles(ctx, full):
+    for rep in range(6):
+        res = ctx.tmatrix_batch(full["r"], full["lam"], full["m"], full["d"],
+                                **SCHEDULE)
+        assert np.array_equal(res.nmax, full["nmax"]), rep
+        assert np.array_equal(res.q, full["q"]), rep
+        flat, off = ctx.tmatrices()
+        for i in range(N_GRAINS):
+            want = full["T"][i].ravel()
+            got = flat[off[i]:off[i] + want.size]
+            assert np.array_equal(got, want), (rep, i)
 
 
 def test_oracle_parity_on_order_extremes(full):

@@ -140,6 +140,18 @@ struct tmx_ctx {
   int64_t n = 0;
   bool have_batch = false;
   bool t_averaged = false; // T holds orientation averages (no gradients)
+  // generation counters: batch_seq changes whenever the batch's grains,
+  // orders, T-matrix offsets or T-matrices change, plan_seq at every upload
+  // of an observable plan; obs_key identifies the plan of the last
+  // batch_observable_setup (reused while both counters and its angles and
+  // coefficients are unchanged)
+  uint64_t batch_seq = 0, plan_seq = 0;
+  struct ObsKey {
+    bool valid = false;
+    uint64_t batch_seq = 0, plan_seq = 0;
+    std::vector<double> thetas, coeffs;
+    bool has_coeffs = false;
+  } obs_key;
   std::vector<int32_t> nmax_h, ngauss_h, status_h;
   std::vector<double> q_h;
   std::vector<int64_t> t_off_h;
@@ -363,6 +375,9 @@ static inline int ensure(tmx_ctx *ctx, DevBuf &b, size_t bytes) {
   if (b.cap >= bytes) {
     return TMX_OK;
   }
+  // a reallocated buffer has lost its contents: no cached observable plan
+  // may be reused after this
+  ++ctx->plan_seq;
   if (b.p) {
     int rc = order_after_rounds(ctx);
     if (rc) {

@@ -479,6 +479,7 @@ int tmx_batch_upload(tmx_ctx *ctx, int64_t n, const double *r_ev,
   }
   // the host arrays above are about to go out of scope
   CK(cudaStreamSynchronize(st));
+  ++ctx->batch_seq;
   ctx->up_n = n;
   ctx->up_grains = gr;
   ctx->up_nact = (int)act.size();
@@ -855,6 +856,7 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   ctx->p2_t_total = t_total;
   ctx->p2_rounds = rounds;
   ctx->t_averaged = false;
+  ++ctx->batch_seq;
   if (t_total > 0) {
     std::vector<double> q2(2 * n);
     std::vector<int32_t> stb(n);
@@ -989,6 +991,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     return rc;
   }
   ctx->n = n;
+  ++ctx->batch_seq;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);
   ctx->status_h.assign(n, 0);
@@ -1480,6 +1483,7 @@ int tmx_tmatrix_batch_fixed(tmx_ctx *ctx, int64_t n, const double *r_ev,
     return rc;
   }
   ctx->n = n;
+  ++ctx->batch_seq;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);
   ctx->status_h.assign(n, 0);

@@ -188,6 +188,7 @@ extern "C" int tmx_tmatrix_batch_calculator(tmx_ctx *ctx, int64_t n,
   ctx->have_batch = false;
   ctx->lu_ready = false;
   ctx->n = n;
+  ++ctx->batch_seq;
   ctx->nmax_h.assign(n, 0);
   ctx->ngauss_h.assign(n, 0);
   ctx->status_h.assign(n, 0);

@@ -375,6 +375,7 @@ int64_t est_nmax(double x, int min_order, int max_order) {
 int upload_obs_plan(tmx_ctx *ctx, const std::vector<TmxObsGrain> &og,
                     const std::vector<TmxSJob> &sj) {
   int rc0;
+  ++ctx->plan_seq;
   cudaStream_t st = ctx->stream;
   const int64_t n = (int64_t)og.size();
   // orientation-average work items, pair-major (tmx_launch_orient_pairs):
@@ -657,6 +658,7 @@ extern "C" int tmx_get_table(
       (rc = ensure(ctx, ctx->o_shw, nshape * sizeof(double)))) {
     return rc;
   }
+  ++ctx->plan_seq; // the observable buffers change below
   CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
                      cudaMemcpyHostToDevice, st));
   ctx->o_nangles = (int)ang.size();
@@ -761,6 +763,7 @@ extern "C" int tmx_get_table(
     if ((rc = ensure(ctx, ctx->o_og, ng * sizeof(TmxObsGrain)))) {
       return rc;
     }
+    ++ctx->plan_seq; // the observable buffers change below
     CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), ng * sizeof(TmxObsGrain),
                        cudaMemcpyHostToDevice, st));
     // ---- amplitude jobs
@@ -946,6 +949,17 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
   cudaStream_t st = ctx->stream;
   const int64_t n = ctx->n;
   int rc;
+  // the plan of the previous call, if nothing it depends on has changed
+  // since (the observables of a batch followed by its gradients)
+  tmx_ctx::ObsKey &key = ctx->obs_key;
+  if (key.valid && key.batch_seq == ctx->batch_seq && key.plan_seq == ctx->plan_seq &&
+      key.has_coeffs == (coeffs != nullptr) && (int)key.thetas.size() == ntheta &&
+      std::equal(key.thetas.begin(), key.thetas.end(), thetas) &&
+      (!coeffs || ((int)key.coeffs.size() == ncoef &&
+                   std::equal(key.coeffs.begin(), key.coeffs.end(), coeffs)))) {
+    return TMX_OK;
+  }
+  key.valid = false;
   std::vector<TmxAngle> ang(ntheta);
   for (int i = 0; i < ntheta; ++i) {
     ang[i] = make_angle(cos(thetas[i]));
@@ -1023,7 +1037,20 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
       return rc;
     }
   }
-  return upload_obs_plan(ctx, og, sj);
+  if ((rc = upload_obs_plan(ctx, og, sj))) {
+    return rc;
+  }
+  key.valid = true;
+  key.batch_seq = ctx->batch_seq;
+  key.plan_seq = ctx->plan_seq;
+  key.thetas.assign(thetas, thetas + ntheta);
+  key.has_coeffs = coeffs != nullptr;
+  if (coeffs) {
+    key.coeffs.assign(coeffs, coeffs + ncoef);
+  } else {
+    key.coeffs.clear();
+  }
+  return TMX_OK;
 }
 
 } // namespace
@@ -1105,13 +1132,15 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
                      (const double *)ctx->p2tab.p, (const double *)ctx->p2nsc.p,
                      (cplx *)ctx->lu.p, &ctx->p2_nb, ctx->p2_scr_total});
   }
-  int64_t scr_max = 1;
+  // each round's tangent scratch in its own region: the rounds' size
+  // buckets run concurrently
+  int64_t scr_sum = 1;
   for (const RoundView &v : views) {
-    scr_max = std::max(scr_max, v.scr);
+    scr_sum += v.scr;
   }
   const int64_t tt = ctx->p2_t_total;
   NvtxRange range("tmx_gradients");
-  if ((rc = ensure(ctx, ctx->tscr, 3 * scr_max * sizeof(cplx))) ||
+  if ((rc = ensure(ctx, ctx->tscr, 3 * scr_sum * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->dT, std::max<int64_t>(1, 3 * tt) * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->dS, std::max<int64_t>(1, 4 * n * ntheta) * 4 * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double))) ||
@@ -1119,6 +1148,19 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
     return rc;
   }
   CK(cudaMemsetAsync(ctx->dT.p, 0, std::max<int64_t>(1, 3 * tt) * sizeof(cplx), st));
+  // every (round, size bucket) launch may start once dT is cleared: they
+  // write disjoint blocks of dT and disjoint scratch, so they run on the
+  // library stream and the eight others side by side and join before the
+  // observables
+  cudaStream_t gstreams[9] = {st,          ctx->aux[0], ctx->aux[1],
+                              ctx->aux[2], ctx->aux[3], ctx->aux[4],
+                              ctx->aux[5], ctx->stream2, ctx->stream3};
+  cudaEvent_t gfork;
+  CK(cudaEventCreateWithFlags(&gfork, cudaEventDisableTiming));
+  CK(cudaEventRecord(gfork, st));
+  bool gused[9] = {true, false, false, false, false, false, false, false, false};
+  int glaunch = 0;
+  int64_t scr_off = 0;
   for (const RoundView &v : views) {
     const int64_t nitems = (int64_t)v.nb->size();
     // the class-size buckets of the forward schedule (items sorted by size)
@@ -1131,6 +1173,12 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
       }
       if (i1 > i0) {
         const int max_nb = (*v.nb)[i0];
+        const int gi = glaunch++ % 9;
+        cudaStream_t gs = gstreams[gi];
+        if (!gused[gi]) {
+          CK(cudaStreamWaitEvent(gs, gfork, 0));
+          gused[gi] = true;
+        }
         if (!ctx->rounds_lu && !ctx->lu_ready) {
           TmxBlockArgs B;
           B.items = v.items + i0;
@@ -1149,7 +1197,7 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
           B.chunk_nodes = tmx_host_chunk_nodes(max_nb);
           B.family = dispatch_family(ctx, max_nb);
           B.lu = v.lu;
-          tmx_launch_blocks(B, st);
+          tmx_launch_blocks(B, gs);
           LAUNCHED();
         }
         TmxTangentArgs A;
@@ -1164,18 +1212,33 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
         A.wig_off = (const int64_t *)ctx->wig_off.p;
         A.lu = v.lu;
         A.T = (const cplx *)ctx->T.p;
-        A.scratch = (cplx *)ctx->tscr.p;
+        A.scratch = (cplx *)ctx->tscr.p + 3 * scr_off;
         A.scratch_stride = v.scr;
         A.dT = (cplx *)ctx->dT.p;
         A.dT_stride = tt;
         A.chunk_nodes = std::max(1, tmx_host_chunk_nodes(max_nb) / 2);
         A.max_nb = max_nb;
-        tmx_launch_tangents(A, st);
+        cudaEvent_t pe = nullptr;
+        if ((rc = prof_begin(ctx, TMX_PROF_TANGENTS, &pe, gs))) {
+          return rc;
+        }
+        tmx_launch_tangents(A, gs);
         LAUNCHED();
+        if ((rc = prof_end(ctx, TMX_PROF_TANGENTS, pe, 0., gs, 0., A.nitems))) {
+          return rc;
+        }
       }
       i0 = i1;
     }
+    scr_off += v.scr;
   }
+  for (int gi = 1; gi < 9; ++gi) {
+    if (gused[gi]) {
+      CK(cudaEventRecord(gfork, gstreams[gi]));
+      CK(cudaStreamWaitEvent(st, gfork, 0));
+    }
+  }
+  CK(cudaEventDestroy(gfork));
   if ((rc = batch_observable_setup(ctx, ntheta, thetas, coeffs, ncoef))) {
     return rc;
   }
@@ -1388,6 +1451,7 @@ int plain_amplitudes(tmx_ctx *ctx, const std::vector<int32_t> &grain,
       (rc = ensure(ctx, ctx->o_S, std::max<int64_t>(1, nj) * 4 * sizeof(cplx)))) {
     return rc;
   }
+  ++ctx->plan_seq; // the observable buffers change below
   CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
                      cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->o_angles.p, ang.data(), ang.size() * sizeof(TmxAngle),
@@ -1587,6 +1651,7 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
       (rc = tmx_ensure_cg(ctx, nmax_b))) {
     return rc;
   }
+  ++ctx->plan_seq; // the observable buffers change below
   CK(cudaMemcpyAsync(ctx->o_og.p, og.data(), n * sizeof(TmxObsGrain),
                      cudaMemcpyHostToDevice, st));
   if (nsets > 0) {
@@ -1611,6 +1676,7 @@ extern "C" int tmx_batch_orientation_average(tmx_ctx *ctx, const double *coeffs,
   }
   CK(cudaStreamSynchronize(st));
   ctx->t_averaged = true;
+  ++ctx->batch_seq;
   ctx->sink_done = 0; // the T-matrices a sink holds are the unaveraged ones
   return TMX_OK;
 }

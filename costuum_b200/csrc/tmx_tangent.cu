@@ -636,8 +636,10 @@ static void launch_tangent_warp(const TmxTangentArgs &a, cudaStream_t stream) {
   const size_t smem = (size_t)4 * tangent_warp_elems<NBM>() * sizeof(cplx);
   cudaFuncSetAttribute(k_tangent_warp<TR, TC, MINB>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // one (item, parameter) per warp: CTAs retire quickly, so that the
+  // launches of the other size buckets running beside this one get SMs
   const int64_t work = (int64_t)a.nitems * a.nparams;
-  const int blocks = (int)std::min<int64_t>((work + 3) / 4, 148 * 16);
+  const int blocks = (int)std::max<int64_t>(1, (work + 3) / 4);
   k_tangent_warp<TR, TC, MINB><<<blocks, 128, smem, stream>>>(a);
 }
 

@@ -188,7 +188,8 @@ enum tmx_profile_kernel {
   TMX_PROF_AMP = 3,       /* scattering amplitudes (Extinction/Absorption/
                              ScatteringMatrixTask) */
   TMX_PROF_SHAPE_AVG = 4, /* shape average (ShapeAveragingTask) */
-  TMX_PROF_KERNELS = 5
+  TMX_PROF_TANGENTS = 5,  /* tangent kernels of tmx_batch_gradients */
+  TMX_PROF_KERNELS = 6
 };
 int tmx_profile_enable(tmx_ctx *ctx, int on);
 int tmx_profile_read(tmx_ctx *ctx, int kernel, double *ms, int64_t *launches,

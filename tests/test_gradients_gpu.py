@@ -236,3 +236,52 @@ def test_autograd_backward_after_another_batch(ctx):
         (q * w).sum().backward()
         grads.append(params.grad.numpy().copy())
     assert np.allclose(grads[0], grads[1], rtol=1e-12, atol=0)
+
+
+def test_observable_plan_reuse():
+    """The observable plan (jobs, angles, coefficients on the device) that
+    observables() builds is reused by the gradients of the same batch when
+    the angles and coefficients are the same, and rebuilt when they or the
+    batch differ: every call must give the doubles of a fresh context."""
+    from costuum_b200.tmatrix import Context
+    r, lam, m, d = H.config2_sample(300, 21)
+    co_a = _coeffs(0, 0.0)
+    co_b = _coeffs(2, 0.5)
+    th_b = np.array([0.2, 0.9, 2.2])
+
+    def fresh(thetas, coeffs):
+        c = Context(0)
+        try:
+            c.tmatrix_batch(r, lam, m, d)
+            return c.gradients(thetas, coeffs)
+        finally:
+            c.close()
+
+    want_a = fresh(THETAS, co_a)
+    want_b = fresh(th_b, co_b)
+    ctx = Context(0)
+    try:
+        ctx.tmatrix_batch(r, lam, m, d)
+        for thetas, coeffs, want in ((THETAS, co_a, want_a), (th_b, co_b, want_b),
+                                     (THETAS, co_a, want_a)):
+            q = ctx.observables(thetas, coeffs)
+            assert np.array_equal(q, want[0])
+            got = ctx.gradients(thetas, coeffs)  # the plan of observables()
+            assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+        # angles changed between observables() and gradients()
+        ctx.observables(THETAS, co_a)
+        got = ctx.gradients(th_b, co_b)
+        assert np.array_equal(got[1], want_b[1])
+        # a new batch of other grains with the same angles and coefficients
+        r2, lam2, m2, d2 = H.config2_sample(200, 22)
+        ctx.tmatrix_batch(r2, lam2, m2, d2)
+        c2 = Context(0)
+        try:
+            c2.tmatrix_batch(r2, lam2, m2, d2)
+            want2 = c2.gradients(THETAS, co_a)
+        finally:
+            c2.close()
+        got = ctx.gradients(THETAS, co_a)
+        assert np.array_equal(got[1], want2[1])
+    finally:
+        ctx.close()

@@ -355,8 +355,12 @@ def run_ours(args):
     dist.barrier()
     torch.cuda.synchronize()
     total = 0.0
+    host_t = []
     for _ in range(args.steps):
         total += step_device()
+        ht = np.zeros(4)
+        lib.tmx_batch_host_times(h, P(ht))
+        host_t.append(ht)
     torch.cuda.synchronize()
     dist.barrier()
     launches = ctx.kernel_launches - launches0
@@ -368,6 +372,19 @@ def run_ours(args):
     tb_ms = np.zeros(1)
     tb_n = ctypes.c_int64()
     lib.tmx_profile_read(h, 1, P(tb_ms), ctypes.byref(tb_n), P(np.zeros(1)))
+    # per timed batch, from the launch timeline: when the order loop's last
+    # launch and the batch's last launch finished after its first launch
+    tl = ctx.timeline()
+    marks = tl[tl["kind"] < 0]
+    loop_ms, gpu_ms = [], []
+    t_start = None
+    for rec in marks:
+        if rec["kind"] == -1:
+            t_start = rec["start_ms"]
+        elif t_start is not None and rec["kind"] == -2:
+            loop_ms.append(rec["start_ms"] - t_start)
+        elif t_start is not None and rec["kind"] == -3:
+            gpu_ms.append(rec["start_ms"] - t_start)
     lib.tmx_profile_enable(h, 0)
     flops_survey = lib.tmx_batch_flops_survey(h)
     total_max = dist.max(total)
@@ -609,6 +626,17 @@ def run_ours(args):
                          "traffic_unit": "bytes per block launch (ncu, cold L2)"},
             "phases_ms_per_step": {"blocks": bk_ms[0] / args.steps,
                                    "tables": tb_ms[0] / args.steps},
+            # host side of the timed steps (medians): the batch call's wall
+            # time, the time it blocked on the order loop's events and the
+            # final synchronisation, and its host set-up of block rounds
+            "timeline_ms_per_step": {
+                "order_loop": float(np.median(loop_ms)) if loop_ms else None,
+                "first_to_last_launch": float(np.median(gpu_ms)) if gpu_ms else None},
+            "host_ms_per_step": {
+                "wall": float(np.median([x[0] for x in host_t])),
+                "blocked": float(np.median([x[1] for x in host_t])),
+                "round_setup": float(np.median([x[2] for x in host_t])),
+                "order_groups": float(np.median([x[3] for x in host_t]))},
             "gpu_launches": int(launches),
             "autotune": autotune,
             "plain_gpu": plain,

@@ -69,6 +69,7 @@ SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_int64), _D]),
     "tmx_profile_bytes": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "tmx_profile_timeline": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _I64]),
+    "tmx_batch_host_times": (ctypes.c_int, [_VP, _D]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
     "tmx_host_alloc": (ctypes.c_void_p, [ctypes.c_size_t]),
     "tmx_host_free": (None, [ctypes.c_void_p]),

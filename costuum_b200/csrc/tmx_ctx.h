@@ -146,6 +146,10 @@ struct tmx_ctx {
   // batch_observable_setup (reused while both counters and its angles and
   // coefficients are unchanged)
   uint64_t batch_seq = 0, plan_seq = 0;
+  // host-side times of the last tmx_batch_compute (ms): wall time, time
+  // blocked on the order loop's events and the final synchronisation, host
+  // set-up of block rounds, and the number of order groups
+  double host_times[4] = {0., 0., 0., 0.};
   struct ObsKey {
     bool valid = false;
     uint64_t batch_seq = 0, plan_seq = 0;

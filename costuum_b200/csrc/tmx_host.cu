@@ -14,6 +14,7 @@
 //      bucketed by class size, largest first.
 //   3. full Q sums per grain (TMatrixQTask).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -972,6 +973,11 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
 }
 
 
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+      .count();
+}
+
 int tmx_batch_compute(tmx_ctx *ctx) {
   if (!ctx) {
     return TMX_ERR_INVALID;
@@ -979,6 +985,12 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   if (!ctx->uploaded) {
     return fail(ctx, TMX_ERR_STATE, "no batch uploaded");
   }
+  struct WallClock {
+    tmx_ctx *c;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    ~WallClock() { c->host_times[0] = ms_since(t0); }
+  } wall{ctx};
+  ctx->host_times[1] = ctx->host_times[2] = ctx->host_times[3] = 0.;
   CK(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   const int64_t n = ctx->up_n;
@@ -1342,14 +1354,19 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     }
     // a round's host set-up overlaps the groups on the GPU
     if (!pending.empty()) {
+      const auto tr = std::chrono::steady_clock::now();
       if ((rc = run_blocks_round(ctx, pending, (rounds & 1) ? ctx->stream3 : ctx->stream2,
                                  t_next, rounds > 0, &t_next, true))) {
         return rc;
       }
+      ctx->host_times[2] += ms_since(tr);
       ++rounds;
       pending.clear();
     }
+    const auto tw = std::chrono::steady_clock::now();
     CK(cudaEventSynchronize(gev[inflight.par]));
+    ctx->host_times[1] += ms_since(tw);
+    ctx->host_times[3] += 1.;
     const int nact_out = ctx->pinned[8 + 2 * inflight.par];
     const int64_t done_now = ctx->pinned[9 + 2 * inflight.par];
     unprocessed_bound -= inflight.issued;
@@ -1397,7 +1414,11 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     CK(cudaMemcpyAsync(ctx->pinned + 4, ctx->keep_ctl.p, 4 * sizeof(int32_t),
                        cudaMemcpyDeviceToHost, st));
   }
-  CK(cudaStreamSynchronize(st));
+  {
+    const auto tw = std::chrono::steady_clock::now();
+    CK(cudaStreamSynchronize(st));
+    ctx->host_times[1] += ms_since(tw);
+  }
   if (ctx->keep_valid) {
     uint64_t used = 0;
     memcpy(&used, ctx->pinned + 6, sizeof(used));
@@ -1813,6 +1834,16 @@ int tmx_profile_bytes(tmx_ctx *ctx, int kernel, double *bytes) {
     return TMX_ERR_INVALID;
   }
   *bytes = ctx->prof[kernel].bytes;
+  return TMX_OK;
+}
+
+int tmx_batch_host_times(tmx_ctx *ctx, double *out) {
+  if (!ctx || !out) {
+    return TMX_ERR_INVALID;
+  }
+  for (int i = 0; i < 4; ++i) {
+    out[i] = ctx->host_times[i];
+  }
   return TMX_OK;
 }
 

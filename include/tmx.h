@@ -212,6 +212,12 @@ enum tmx_timeline_mark {
 int tmx_profile_timeline(tmx_ctx *ctx, int64_t cap, double *records,
                          int64_t *count);
 
+/* Host-side times of the last tmx_batch_compute, out[4] in ms: wall time of
+ * the call, time blocked on the order loop's events and the final
+ * synchronisation, host set-up of the block rounds, and (out[3]) the number
+ * of order groups the loop waited for. Always recorded. */
+int tmx_batch_host_times(tmx_ctx *ctx, double *out);
+
 /* FP64 flops of the last batch counted with the unreduced per-grain model
  * (every chain order and every m block as a full 2nb x 2nb LU + solve);
  * counted only for batches computed while profiling is enabled, else 0. */

@@ -66,3 +66,13 @@ def test_timeline_of_a_batch(ctx):
     ctx.profile(True)
     assert ctx.timeline().size == 0
     ctx.profile(False)
+
+
+def test_host_times_of_a_batch(ctx):
+    r, lam, m, d = H.config2_sample(600, 12)
+    ctx.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+    ht = np.zeros(4)
+    assert _lib.load().tmx_batch_host_times(ctx._h, _lib.ptr(ht)) == 0
+    wall, blocked, setup, groups = ht
+    assert wall > 0 and 0 <= blocked <= wall and 0 <= setup <= wall
+    assert groups >= 1 and groups == int(groups)

@@ -70,6 +70,9 @@ SIGNATURES = {
     "tmx_profile_bytes": (ctypes.c_int, [_VP, ctypes.c_int, _D]),
     "tmx_profile_timeline": (ctypes.c_int, [_VP, ctypes.c_int64, _D, _I64]),
     "tmx_batch_host_times": (ctypes.c_int, [_VP, _D]),
+    "tmx_set_batch_mode": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "tmx_get_batch_mode": (ctypes.c_int, [_VP, _I32]),
+    "tmx_last_batch_mode": (ctypes.c_int, [_VP, _I32]),
     "tmx_batch_flops_survey": (ctypes.c_double, [_VP]),
     "tmx_host_alloc": (ctypes.c_void_p, [ctypes.c_size_t]),
     "tmx_host_free": (None, [ctypes.c_void_p]),

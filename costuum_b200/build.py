@@ -23,6 +23,7 @@ SOURCES = [
     ("tmx_table.cu", []),
     ("tmx_noalloc.cu", []),
     ("tmx_plain.cu", []),
+    ("tmx_graph.cu", []),
 ]
 
 NVCC = os.environ.get("NVCC", "nvcc")

@@ -187,13 +187,11 @@ __device__ void build_chunk(const ClassDesc &D, const AsmLayout &L, int N,
 
 extern __shared__ __align__(16) unsigned char tmx_smem[];
 
-template <int TR, int TC, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-    k_blocks(TmxBlockArgs A, size_t smem_bytes) {
-  const int it = blockIdx.x;
-  if (it >= A.nitems) {
-    return;
-  }
+// one item `it` by the whole CTA (every thread calls it; the early returns
+// are uniform over the CTA)
+template <int TR, int TC, int NT>
+__device__ __forceinline__ void block_item(const TmxBlockArgs &A, int it,
+                                           size_t smem_bytes) {
   const TmxItem item = A.items[it];
   const TmxSlot sl = A.slots[item.slot];
   const TmxGrain G = A.grains[sl.grain];
@@ -475,6 +473,21 @@ __global__ void __launch_bounds__(NT, MINB)
   }
 }
 
+template <int TR, int TC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_blocks(TmxBlockArgs A, size_t smem_bytes) {
+  if (A.gate && *A.gate != A.gate_value) {
+    return;
+  }
+  const int ilo = A.range ? A.range[0] : 0;
+  const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
+  for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {
+    block_item<TR, TC, NT>(A, it, smem_bytes);
+    // shared memory is reused by the next item
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------- warp-per-item variant --
 //
 // Classes of at most 16 members (nearly every item of grains up to order 32)
@@ -750,7 +763,12 @@ __global__ void __launch_bounds__(128, MINB)
   const double *stgS = stg + TMX_WG * NBM * TMX_ROW;
   const int rt = lane >> 2;
   const int ct = lane & 3;
-  for (int it = blockIdx.x * 4 + wib; it < A.nitems; it += gridDim.x * 4) {
+  if (A.gate && *A.gate != A.gate_value) {
+    return;
+  }
+  const int ilo = A.range ? A.range[0] : 0;
+  const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
+  for (int it = ilo + blockIdx.x * 4 + wib; it < ihi; it += gridDim.x * 4) {
     const TmxItem item = A.items[it];
     const TmxSlot sl = A.slots[item.slot];
     const TmxGrain Gr = A.grains[sl.grain];
@@ -1060,7 +1078,10 @@ static void launch_warp_variant(const TmxBlockArgs &a, cudaStream_t stream) {
   // one item per warp: CTAs retire after one item, so that launches of the
   // high-priority order loop get SMs between them (a grid of long-lived
   // CTAs looping over items held the SMs for a whole round)
-  const int blocks = (int)std::max<int64_t>(1, ((int64_t)a.nitems + 3) / 4);
+  int blocks = (int)std::max<int64_t>(1, ((int64_t)a.nitems + 3) / 4);
+  if (a.max_ctas > 0) {
+    blocks = std::min(blocks, a.max_ctas);
+  }
   k_blocks_warp<TR, TC, MINB, MMA><<<blocks, 128, smem, stream>>>(a);
 }
 
@@ -1097,7 +1118,12 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   const int wib = tid >> 5;
   const int q = lane & 3;
   const int rr = lane >> 2;
-  for (int it = blockIdx.x; it < A.nitems; it += gridDim.x) {
+  if (A.gate && *A.gate != A.gate_value) {
+    return;
+  }
+  const int ilo = A.range ? A.range[0] : 0;
+  const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
+  for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {
     const TmxItem item = A.items[it];
     const TmxSlot sl = A.slots[item.slot];
     const TmxGrain Gr = A.grains[sl.grain];
@@ -1360,7 +1386,12 @@ __global__ void __launch_bounds__(256, 1) k_blocks_cta64(TmxBlockArgs A) {
   const int wib = tid >> 5;
   const int q = lane & 3;
   const int rr = lane >> 2;
-  for (int it = blockIdx.x; it < A.nitems; it += gridDim.x) {
+  if (A.gate && *A.gate != A.gate_value) {
+    return;
+  }
+  const int ilo = A.range ? A.range[0] : 0;
+  const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
+  for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {
     const TmxItem item = A.items[it];
     const TmxSlot sl = A.slots[item.slot];
     const TmxGrain Gr = A.grains[sl.grain];
@@ -1592,7 +1623,8 @@ static void launch_cta64(const TmxBlockArgs &a, cudaStream_t stream) {
   cudaFuncSetAttribute(k_blocks_cta64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
   // one item per CTA (see launch_warp_variant)
-  const int blocks = std::max(1, a.nitems);
+  const int blocks = (a.max_ctas > 0) ? std::min(std::max(1, a.nitems), a.max_ctas)
+                                       : std::max(1, a.nitems);
   k_blocks_cta64<<<blocks, 256, smem, stream>>>(a);
 }
 
@@ -1601,7 +1633,8 @@ static void launch_cta32(const TmxBlockArgs &a, cudaStream_t stream) {
   cudaFuncSetAttribute(k_blocks_cta32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)smem);
   // one item per CTA (see launch_warp_variant)
-  const int blocks = std::max(1, a.nitems);
+  const int blocks = (a.max_ctas > 0) ? std::min(std::max(1, a.nitems), a.max_ctas)
+                                       : std::max(1, a.nitems);
   k_blocks_cta32<<<blocks, 128, smem, stream>>>(a);
 }
 
@@ -1650,7 +1683,9 @@ static void launch_variant(const TmxBlockArgs &a, size_t smem,
                          227 * 1024);
     attr_dev = dev;
   }
-  k_blocks<TR, TC, NT, MINB><<<a.nitems, NT, smem, stream>>>(a, smem);
+  const int blocks = (a.max_ctas > 0) ? std::min(std::max(1, a.nitems), a.max_ctas)
+                                       : std::max(1, a.nitems);
+  k_blocks<TR, TC, NT, MINB><<<blocks, NT, smem, stream>>>(a, smem);
 }
 
 int tmx_block_family_capacity(int family) {
@@ -1717,7 +1752,11 @@ __global__ void k_converge(const int32_t *__restrict__ active, int nactive,
                            int32_t *next_active, int32_t *next_count,
                            int32_t *done_list, int32_t *done_ord,
                            int32_t *done_pos, int32_t *done_count,
-                           const int32_t *nact_dev, int base) {
+                           const int32_t *nact_dev, int base,
+                           const int32_t *order_dev) {
+  if (order_dev) {
+    order = *order_dev;
+  }
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= nactive || (nact_dev && base + p >= *nact_dev)) {
     return;
@@ -1793,14 +1832,14 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          int32_t *next_count, int32_t *done_list,
                          int32_t *done_ord, int32_t *done_pos,
                          int32_t *done_count, const int32_t *nact_dev,
-                         int base, cudaStream_t stream) {
+                         int base, cudaStream_t stream, const int32_t *order_dev) {
   if (nactive <= 0) {
     return;
   }
   k_converge<<<(nactive + 127) / 128, 128, 0, stream>>>(
       active, nactive, slots, diag, state, tolerance, order, last_order,
       next_active, next_count, done_list, done_ord, done_pos, done_count,
-      nact_dev, base);
+      nact_dev, base, order_dev);
 }
 
 // ------------------------------------------------------------- kept tables --
@@ -1817,6 +1856,10 @@ void tmx_launch_converge(const int32_t *active, int nactive,
 __global__ void k_keep_tables(TmxKeepArgs K) {
   __shared__ long long s_off;
   __shared__ unsigned s_last;
+  if (K.order0_dev) {
+    K.order0 = *K.order0_dev;
+    K.base[0] = *K.base_dev;
+  }
   const int begin = *K.next;
   const int end = K.counters[1];
   for (int q = begin + blockIdx.x; q < end; q += gridDim.x) {
@@ -1888,11 +1931,11 @@ void tmx_launch_keep_tables(const TmxKeepArgs &K, int max_entries,
 // Row and column of an entry advance incrementally (no division per entry).
 __global__ void __launch_bounds__(QS_THREADS)
     k_qsums(const TmxSlot *__restrict__ slots, int ns,
-            const cplx *__restrict__ T, double *q_out) {
-  const int s = blockIdx.x;
-  if (s >= ns) {
-    return;
-  }
+            const cplx *__restrict__ T, double *q_out,
+            const int32_t *__restrict__ range) {
+  const int slo = range ? range[0] : 0;
+  const int shi = range ? min(range[1], ns) : ns;
+  for (int s = slo + blockIdx.x; s < shi; s += gridDim.x) {
   const TmxSlot sl = slots[s];
   const int N = sl.nmax;
   const cplx *Tg = T + sl.tout;
@@ -1944,14 +1987,19 @@ __global__ void __launch_bounds__(QS_THREADS)
     q_out[2 * sl.grain] = a;
     q_out[2 * sl.grain + 1] = b;
   }
+  // red is reused by the next slot
+  __syncthreads();
+  }
 }
 
 void tmx_launch_qsums(const TmxSlot *slots, int ns, const cplx *T,
-                      double *q_out, cudaStream_t stream) {
+                      double *q_out, cudaStream_t stream, const int32_t *range,
+                      int max_ctas) {
   if (ns <= 0) {
     return;
   }
-  k_qsums<<<ns, QS_THREADS, 0, stream>>>(slots, ns, T, q_out);
+  const int blocks = (max_ctas > 0) ? std::min(ns, max_ctas) : ns;
+  k_qsums<<<blocks, QS_THREADS, 0, stream>>>(slots, ns, T, q_out, range);
 }
 
 // ------------------------------------------------------------ chain prep --

@@ -118,6 +118,7 @@ struct tmx_ctx {
   struct RoundRec {
     double *tab = nullptr, *nsc = nullptr;
     bool own_tables = true; // false: tab and nsc are the batch's table arena
+    bool borrowed = false;  // slots, items and lu are context buffers
     TmxSlot *slots = nullptr;
     TmxItem *items = nullptr;
     cplx *lu = nullptr;
@@ -146,6 +147,19 @@ struct tmx_ctx {
   // batch_observable_setup (reused while both counters and its angles and
   // coefficients are unchanged)
   uint64_t batch_seq = 0, plan_seq = 0;
+  // device-driven batch (tmx_graph.cu): mode, buffers, the executable graph
+  // and the key (sizes and addresses) it was built for, and the T-matrix /
+  // LU storage hints grown by a batch that outgrew them
+  int batch_mode = TMX_BATCH_HOST, last_mode = TMX_BATCH_HOST;
+  DevBuf gm_state, gm_iter, gm_tab, gm_nsc, gm_scr, gm_diag, gm_slots, gm_items,
+      gm_rslots, gm_bitems, gm_bptr, gm_bcap, gm_tpl, gm_tpl_off, gm_full, gm_m0,
+      gm_tsize, gm_toff, gm_lu, gm_luscr, gm_allitems;
+  cudaGraph_t gm_graph = nullptr;
+  cudaGraphExec_t gm_exec = nullptr;
+  std::vector<uint64_t> gm_key;
+  cudaStream_t gm_cs = nullptr, gm_rs = nullptr, gm_bs[TMX_GM_BUCKETS] = {};
+  int64_t gm_t_hint = 0, gm_lu_hint = 0;
+  int64_t gm_last_t = 0;
   // host-side times of the last tmx_batch_compute (ms): wall time, time
   // blocked on the order loop's events and the final synchronisation, host
   // set-up of block rounds, and the number of order groups

@@ -331,6 +331,33 @@ void tmx_destroy(tmx_ctx *ctx) {
       cudaEventDestroy(e);
     }
   }
+  if (ctx->gm_exec) {
+    cudaGraphExecDestroy(ctx->gm_exec);
+  }
+  if (ctx->gm_graph) {
+    cudaGraphDestroy(ctx->gm_graph);
+  }
+  DevBuf *gm_bufs[] = {&ctx->gm_state, &ctx->gm_iter, &ctx->gm_tab, &ctx->gm_nsc,
+                       &ctx->gm_scr, &ctx->gm_diag, &ctx->gm_slots, &ctx->gm_items,
+                       &ctx->gm_rslots, &ctx->gm_bitems, &ctx->gm_bptr, &ctx->gm_bcap,
+                       &ctx->gm_tpl, &ctx->gm_tpl_off, &ctx->gm_full, &ctx->gm_m0,
+                       &ctx->gm_tsize, &ctx->gm_toff, &ctx->gm_lu, &ctx->gm_luscr,
+                       &ctx->gm_allitems};
+  for (DevBuf *b : gm_bufs) {
+    if (b->p) {
+      cudaFreeAsync(b->p, ctx->stream);
+    }
+  }
+  for (cudaStream_t x : {ctx->gm_cs, ctx->gm_rs}) {
+    if (x) {
+      cudaStreamDestroy(x);
+    }
+  }
+  for (cudaStream_t x : ctx->gm_bs) {
+    if (x) {
+      cudaStreamDestroy(x);
+    }
+  }
   DevBuf *bufs[] = {&ctx->lu, &ctx->dT, &ctx->tscr, &ctx->dTa, &ctx->dS,
                     &ctx->cg, &ctx->cg_off, &ctx->Ta, &ctx->o_angles,
                     &ctx->o_phis, &ctx->o_wts, &ctx->o_coef, &ctx->o_shw,
@@ -548,7 +575,8 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
     for (int s = 0; s < np2; ++s) {
       TmxSlot &sl = slots[s];
       sl.tab = ctx->keep_off_h[sl.grain];
-      sl.nsc = sl.tab + (int64_t)sl.ngauss * sl.nmax * TMX_NQ;
+      // (k_keep_tables puts the node scalars at the next multiple of 16)
+      sl.nsc = sl.tab + (((int64_t)sl.ngauss * sl.nmax * TMX_NQ + 15) & ~(int64_t)15);
     }
   }
   std::vector<int> full_sets;
@@ -922,6 +950,11 @@ int tmx_release_rounds(tmx_ctx *ctx) {
     if (!r.own_tables) {
       r.tab = r.nsc = nullptr; // the batch's table arena
     }
+    if (r.borrowed) {
+      r.slots = nullptr;
+      r.items = nullptr;
+      r.lu = nullptr;
+    }
     for (void *p : {(void *)r.tab, (void *)r.nsc, (void *)r.slots, (void *)r.items,
                     (void *)r.lu}) {
       if (p) {
@@ -973,6 +1006,479 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
 }
 
 
+// ------------------------------------------------- device-driven batch --
+//
+// tmx_batch_compute in TMX_BATCH_GRAPH mode: the kernels of tmx_graph.cu and
+// the existing step kernels captured once per batch shape into a CUDA graph
+// whose WHILE node runs the order loop and its rounds on the device.
+// Returns TMX_OK, an error, or 1 when this batch must run in the host mode
+// (not covered, or the T-matrix / LU storage ran out: the hints grow).
+
+static int gm_bucket(int nb) {
+  return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
+}
+
+static int gm_compute(tmx_ctx *ctx) {
+  cudaStream_t st = ctx->stream;
+  const int64_t n = ctx->up_n;
+  const tmx_schedule S = ctx->up_sched;
+  const int glf = S.gauss_legendre_factor;
+  const int K = S.max_order - 1;
+  const int kmin = S.min_order;
+  int rc;
+  if (ctx->up_nact <= 0 || n > (1 << 22) || K < kmin || K > 100 || ctx->profiling ||
+      ctx->tuning) {
+    return 1;
+  }
+  const double tab_per = (double)glf * K * K * TMX_NQ + (double)glf * K * TMX_NS + 32.;
+  if (2. * tab_per * sizeof(double) * n > 24e9) {
+    return 1;
+  }
+  // ---- tables shared by all grains: the quadrature and the m = 0 Wigner
+  // set of every order of the loop, every m of every order a grain can end
+  // at (cached in the context)
+  std::vector<int> ngs;
+  std::vector<std::pair<int, int>> keys;
+  for (int k = kmin; k <= K; ++k) {
+    ngs.push_back(glf * k);
+    keys.push_back({k, glf * k});
+  }
+  std::vector<int> m0_sets, full_sets;
+  if ((rc = ensure_gl(ctx, ngs)) || (rc = ensure_wigner(ctx, keys, false, m0_sets)) ||
+      (rc = ensure_wigner(ctx, keys, true, full_sets))) {
+    return rc;
+  }
+  // ---- item templates of every order: (m << 8 | class, class size), the
+  // T-matrix size and the LU storage of a grain at that order, and the most
+  // items of one grain in each size bucket
+  std::vector<int32_t> tpl, tpl_off(K + 2, 0);
+  std::vector<int64_t> tsz(K + 1, 0), lun(K + 1, 0);
+  int64_t bmax[TMX_GM_BUCKETS] = {0, 0, 0, 0, 0};
+  int nbmax_b[TMX_GM_BUCKETS] = {0, 0, 0, 0, 0};
+  for (int N = 0; N <= K; ++N) {
+    tpl_off[N] = (int32_t)(tpl.size() / 2);
+    if (N < kmin) {
+      continue;
+    }
+    int64_t bc[TMX_GM_BUCKETS] = {0, 0, 0, 0, 0};
+    for (int m = 0; m <= N; ++m) {
+      for (int cl = 0; cl < ((m == 0) ? 4 : 2); ++cl) {
+        const int nb = tmx_host_class_size(N, m, cl);
+        if (nb > 0) {
+          tpl.push_back((m << 8) | cl);
+          tpl.push_back(nb);
+          const int b = gm_bucket(nb);
+          bc[b] += 1;
+          nbmax_b[b] = std::max(nbmax_b[b], nb);
+          lun[N] += 2 * (int64_t)nb * nb;
+        }
+      }
+    }
+    for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+      bmax[b] = std::max(bmax[b], bc[b]);
+    }
+    tsz[N] = tmx_tmatrix_size(N);
+  }
+  tpl_off[K + 1] = (int32_t)(tpl.size() / 2);
+  // T-matrix and LU storage: the last graph batch's use with a margin, else
+  // every grain at order 40 (at most every grain at the largest order)
+  const int kest = std::min(K, std::max(kmin, 40));
+  int64_t t_cap = std::max(ctx->gm_t_hint, ctx->gm_last_t + ctx->gm_last_t / 4);
+  if (t_cap <= 0) {
+    t_cap = n * tsz[kest];
+  }
+  t_cap = std::min(t_cap, n * tsz[K]);
+  int64_t lu_cap = std::max(ctx->gm_lu_hint, (int64_t)((double)t_cap * lun[K] / tsz[K]) + 2 * n * K * K);
+  lu_cap = std::min(lu_cap, n * lun[K]);
+  int32_t bcap[TMX_GM_BUCKETS];
+  int64_t btot = 0;
+  for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+    bcap[b] = (int32_t)std::min<int64_t>(n * bmax[b], (int64_t)1 << 30);
+    btot += bcap[b];
+  }
+  const int cmK = (K + 1) / 2;
+  const int64_t arena_cap = (int64_t)(tab_per * n);
+  if ((rc = ensure(ctx, ctx->gm_state, sizeof(TmxGState))) ||
+      (rc = ensure(ctx, ctx->gm_iter, sizeof(TmxGIter))) ||
+      (rc = ensure(ctx, ctx->act0, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->act1, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->done, 2 * n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->done_pos, n * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->keep_tab, n * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->keep_q, n * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->keep_ctl, 32)) ||
+      (rc = ensure(ctx, ctx->keep_arena, arena_cap * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_tab, n * (int64_t)glf * K * K * TMX_NQ * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_nsc, n * (int64_t)glf * K * TMX_NS * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_scr, 4 * n * 2 * (int64_t)cmK * cmK * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_diag, n * 2 * (int64_t)K * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_slots, n * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->gm_items, 4 * n * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->gm_rslots, n * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->gm_bitems, btot * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->gm_allitems, btot * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->gm_bptr, TMX_GM_BUCKETS * sizeof(TmxItem *))) ||
+      (rc = ensure(ctx, ctx->gm_bcap, TMX_GM_BUCKETS * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->gm_tpl, std::max<size_t>(1, tpl.size()) * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->gm_tpl_off, tpl_off.size() * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->gm_full, full_sets.size() * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->gm_m0, m0_sets.size() * sizeof(int32_t))) ||
+      (rc = ensure(ctx, ctx->gm_tsize, tsz.size() * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->gm_toff, n * sizeof(int64_t))) ||
+      (rc = ensure(ctx, ctx->T, t_cap * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_lu, lu_cap * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_luscr, lu_cap * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->q, 2 * n * sizeof(double)))) {
+    return rc;
+  }
+  TmxItem *bitems[TMX_GM_BUCKETS];
+  {
+    int64_t off = 0;
+    for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+      bitems[b] = (TmxItem *)ctx->gm_bitems.p + off;
+      off += bcap[b];
+    }
+  }
+  TmxGState *G = (TmxGState *)ctx->gm_state.p;
+  TmxGIter *I = (TmxGIter *)ctx->gm_iter.p;
+  // ---- the graph, built again when the batch's shape or a buffer changed
+  std::vector<uint64_t> key = {
+      (uint64_t)n, (uint64_t)glf, (uint64_t)kmin, (uint64_t)K,
+      (uint64_t)S.bessel_start, (uint64_t)t_cap, (uint64_t)lu_cap, (uint64_t)arena_cap};
+  uint64_t tol_bits;
+  memcpy(&tol_bits, &S.tolerance, sizeof(tol_bits));
+  key.push_back(tol_bits);
+  for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+    key.push_back((uint64_t)ctx->dispatch[b]);
+    key.push_back((uint64_t)bcap[b]);
+  }
+  for (const DevBuf *b : {&ctx->gm_state, &ctx->gm_iter, &ctx->act0, &ctx->act1, &ctx->done,
+                          &ctx->done_pos, &ctx->keep_tab, &ctx->keep_q, &ctx->keep_ctl,
+                          &ctx->keep_arena, &ctx->gm_tab, &ctx->gm_nsc, &ctx->gm_scr,
+                          &ctx->gm_diag, &ctx->gm_slots, &ctx->gm_items, &ctx->gm_rslots,
+                          &ctx->gm_bitems, &ctx->gm_bptr, &ctx->gm_bcap, &ctx->gm_tpl,
+                          &ctx->gm_tpl_off, &ctx->gm_full, &ctx->gm_m0, &ctx->gm_tsize,
+                          &ctx->gm_toff, &ctx->T, &ctx->gm_lu, &ctx->gm_luscr, &ctx->q,
+                          &ctx->state, &ctx->status, &ctx->grains, &ctx->gl_x, &ctx->gl_w,
+                          &ctx->gl_off, &ctx->wig, &ctx->wig_off}) {
+    key.push_back((uint64_t)(uintptr_t)b->p);
+  }
+  if (key != ctx->gm_key || !ctx->gm_exec) {
+    if (ctx->gm_exec) {
+      CK(cudaGraphExecDestroy(ctx->gm_exec));
+      ctx->gm_exec = nullptr;
+    }
+    if (ctx->gm_graph) {
+      CK(cudaGraphDestroy(ctx->gm_graph));
+      ctx->gm_graph = nullptr;
+    }
+    // the per-order tables the graph reads
+    CK(cudaMemcpyAsync(ctx->gm_tpl.p, tpl.data(), tpl.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_tpl_off.p, tpl_off.data(), tpl_off.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_full.p, full_sets.data(), full_sets.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_m0.p, m0_sets.data(), m0_sets.size() * sizeof(int32_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_tsize.p, tsz.data(), tsz.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_bptr.p, bitems, sizeof(bitems), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->gm_bcap.p, bcap, sizeof(bcap), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (!ctx->gm_cs) {
+      CK(cudaStreamCreateWithFlags(&ctx->gm_cs, cudaStreamNonBlocking));
+      CK(cudaStreamCreateWithFlags(&ctx->gm_rs, cudaStreamNonBlocking));
+      for (cudaStream_t &x : ctx->gm_bs) {
+        CK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      }
+    }
+    cudaGraph_t graph;
+    CK(cudaGraphCreate(&graph, 0));
+    ctx->gm_graph = graph;
+    cudaGraphConditionalHandle loop;
+    CK(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t cs = ctx->gm_cs, rs = ctx->gm_rs;
+    std::vector<cudaEvent_t> evs;
+    auto link = [&](cudaStream_t from, cudaStream_t to) -> int {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      evs.push_back(e);
+      CK(cudaEventRecord(e, from));
+      CK(cudaStreamWaitEvent(to, e, 0));
+      return 0;
+    };
+    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeRelaxed));
+    // the body's launches; any error ends the capture before it returns
+    auto capture_body = [&]() -> int {
+      tmx_launch_gm_begin(G, I, (const int32_t *)ctx->gm_m0.p, kmin, glf, cs);
+      if ((rc = link(cs, rs))) {
+        return rc;
+      }
+      // loop branch: one order step of every active grain
+      tmx_launch_gm_prep(G, I, (const int32_t *)ctx->act0.p, (int)n, (TmxSlot *)ctx->gm_slots.p,
+                         (TmxItem *)ctx->gm_items.p, cs);
+      tmx_launch_tables((const TmxSlot *)ctx->gm_slots.p, (int)n, (const TmxGrain *)ctx->grains.p,
+                        (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
+                        (const int64_t *)ctx->gl_off.p, (double *)ctx->gm_tab.p,
+                        (double *)ctx->gm_nsc.p, S.bessel_start, glf * K, K, cs);
+      const int tops[TMX_GM_BUCKETS] = {8, 16, 32, 64, TMX_MAX_NB};
+      for (int b = 0; b < 4; ++b) {
+        // (buckets of the m = 0 classes, size (k + 1) / 2, that some order reaches)
+        const int lo = (b == 0) ? 1 : tops[b - 1] + 1;
+        if (lo > (K + 1) / 2 || tops[b] < (kmin + 1) / 2) {
+          continue;
+        }
+        TmxBlockArgs B;
+        B.items = (const TmxItem *)ctx->gm_items.p;
+        B.nitems = (int)(4 * n);
+        B.slots = (const TmxSlot *)ctx->gm_slots.p;
+        B.grains = (const TmxGrain *)ctx->grains.p;
+        B.tab = (const double *)ctx->gm_tab.p;
+        B.nsc = (const double *)ctx->gm_nsc.p;
+        B.wig = (const double *)ctx->wig.p;
+        B.wig_off = (const int64_t *)ctx->wig_off.p;
+        B.scratch = (cplx *)ctx->gm_scr.p;
+        B.tout = nullptr;
+        B.diag = (cplx *)ctx->gm_diag.p;
+        B.status = (int32_t *)ctx->status.p;
+        B.max_nb = std::min(tops[b], (K + 1) / 2);
+        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+        B.family = ctx->dispatch[b];
+        B.gate = &I->bucket;
+        B.gate_value = b;
+        B.max_ctas = 148 * 8;
+        tmx_launch_blocks(B, cs);
+      }
+      tmx_launch_converge((const int32_t *)ctx->act0.p, (int)n, (const TmxSlot *)ctx->gm_slots.p,
+                          (const cplx *)ctx->gm_diag.p, (TmxChainState *)ctx->state.p,
+                          S.tolerance, 0, K, (int32_t *)ctx->act1.p, &G->cnt[2],
+                          (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
+                          (int32_t *)ctx->done_pos.p, &G->cnt[1], &G->cnt[0], 0, cs,
+                          &I->order);
+      {
+        TmxKeepArgs KA;
+        KA.done_list = (const int32_t *)ctx->done.p;
+        KA.done_ord = (const int32_t *)ctx->done.p + n;
+        KA.done_pos = (const int32_t *)ctx->done_pos.p;
+        KA.counters = G->cnt;
+        KA.next = (int32_t *)ctx->keep_ctl.p;
+        KA.ticket = (unsigned *)ctx->keep_ctl.p + 1;
+        KA.used = (unsigned long long *)ctx->keep_ctl.p + 1;
+        KA.order0 = 0;
+        KA.base[0] = TmxChainBase{};
+        KA.tab = (const double *)ctx->gm_tab.p;
+        KA.nsc = (const double *)ctx->gm_nsc.p;
+        KA.arena = (double *)ctx->keep_arena.p;
+        KA.cap = arena_cap;
+        KA.keep_tab = (int64_t *)ctx->keep_tab.p;
+        KA.keep_q = (int64_t *)ctx->keep_q.p;
+        KA.order0_dev = &I->order;
+        KA.base_dev = &I->base;
+        tmx_launch_keep_tables(KA, (int)n, cs);
+      }
+      // round branch: every block of the grains that became final in the
+      // previous iteration, one launch per size bucket side by side
+      {
+        TmxGmRoundArgs RA;
+        RA.G = G;
+        RA.done_list = (const int32_t *)ctx->done.p;
+        RA.done_ord = (const int32_t *)ctx->done.p + n;
+        RA.keep_tab = (const int64_t *)ctx->keep_tab.p;
+        RA.tpl_off = (const int32_t *)ctx->gm_tpl_off.p;
+        RA.tpl = (const int32_t *)ctx->gm_tpl.p;
+        RA.full_sets = (const int32_t *)ctx->gm_full.p;
+        RA.tsize = (const int64_t *)ctx->gm_tsize.p;
+        RA.glf = glf;
+        RA.min_order = kmin;
+        RA.rslots = (TmxSlot *)ctx->gm_rslots.p;
+        RA.n = (int)n;
+        RA.bitems = (TmxItem *const *)ctx->gm_bptr.p;
+        RA.bcap = (const int32_t *)ctx->gm_bcap.p;
+        RA.t_off = (int64_t *)ctx->gm_toff.p;
+        RA.t_cap = (unsigned long long)t_cap;
+        RA.lu_cap = (unsigned long long)lu_cap;
+        tmx_launch_gm_round(RA, rs);
+        tmx_launch_gm_round_mid(G, rs);
+      }
+      for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+        if (bcap[b] == 0) {
+          continue;
+        }
+        cudaStream_t bs = ctx->gm_bs[b];
+        if ((rc = link(rs, bs))) {
+          return rc;
+        }
+        TmxBlockArgs R;
+        R.items = bitems[b];
+        R.nitems = bcap[b];
+        R.range = &G->rng[b][0];
+        R.slots = (const TmxSlot *)ctx->gm_rslots.p;
+        R.grains = (const TmxGrain *)ctx->grains.p;
+        R.tab = (const double *)ctx->keep_arena.p;
+        R.nsc = (const double *)ctx->keep_arena.p;
+        R.wig = (const double *)ctx->wig.p;
+        R.wig_off = (const int64_t *)ctx->wig_off.p;
+        R.scratch = (cplx *)ctx->gm_luscr.p;
+        R.tout = (cplx *)ctx->T.p;
+        R.diag = nullptr;
+        R.status = (int32_t *)ctx->status.p;
+        R.max_nb = nbmax_b[b];
+        R.chunk_nodes = tmx_host_chunk_nodes(R.max_nb);
+        R.lu = (cplx *)ctx->gm_lu.p;
+        R.family = ctx->dispatch[b];
+        R.max_ctas = 148 * 16;
+        tmx_launch_blocks(R, bs);
+        if ((rc = link(bs, rs))) {
+          return rc;
+        }
+      }
+      tmx_launch_qsums((const TmxSlot *)ctx->gm_rslots.p, (int)n, (const cplx *)ctx->T.p,
+                       (double *)ctx->q.p, rs, &G->srng[0], 148 * 4);
+      if ((rc = link(rs, cs))) {
+        return rc;
+      }
+      tmx_launch_gm_swap(G, (const int32_t *)ctx->act1.p, (int32_t *)ctx->act0.p, (int)n, cs);
+      tmx_launch_gm_end(G, loop, cs);
+      return 0;
+    };
+    const int crc = capture_body();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
+    for (cudaEvent_t e : evs) {
+      cudaEventDestroy(e);
+    }
+    if (crc) {
+      return crc;
+    }
+    CK(ce);
+    CK(cudaGraphInstantiate(&ctx->gm_exec, graph, 0));
+    ctx->gm_key = key;
+  }
+  // ---- this batch: initial state, the graph, the results
+  TmxGState g0 = {};
+  g0.k = kmin;
+  g0.last_order = K;
+  g0.max_iter = K - kmin + 3;
+  g0.cnt[0] = ctx->up_nact;
+  CK(cudaMemcpyAsync(G, &g0, sizeof(g0), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->state.p, ctx->state0.p, n * sizeof(TmxChainState),
+                     cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(ctx->act0.p, ctx->actinit.p, ctx->up_nact * sizeof(int32_t),
+                     cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemsetAsync(ctx->status.p, 0, n * sizeof(int32_t), st));
+  CK(cudaMemsetAsync(ctx->keep_ctl.p, 0, 32, st));
+  CK(cudaMemsetAsync(ctx->gm_toff.p, 0xff, n * sizeof(int64_t), st));
+  CK(cudaGraphLaunch(ctx->gm_exec, st));
+  LAUNCHED();
+  TmxGState g1;
+  std::vector<TmxChainState> st0(n);
+  std::vector<int64_t> toff(n);
+  CK(cudaMemcpyAsync(&g1, G, sizeof(g1), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(toff.data(), ctx->gm_toff.p, n * sizeof(int64_t),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (g1.overflow || g1.cnt[0] > 0 || g1.round_hi > g1.round_lo) {
+    // storage ran out (or the loop stopped early): grow the estimates and
+    // compute this batch in the host mode
+    ctx->gm_t_hint = std::max<int64_t>(2 * t_cap, (int64_t)g1.t_used + (int64_t)g1.t_used / 4);
+    ctx->gm_lu_hint = std::max<int64_t>(2 * lu_cap, (int64_t)g1.lu_used + (int64_t)g1.lu_used / 4);
+    return 1;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    ctx->nmax_h[i] = st0[i].nmax;
+    ctx->ngauss_h[i] = st0[i].ngauss;
+    ctx->status_h[i] = st0[i].status | ctx->up_status[i];
+    ctx->q_h[6 * i + 0] = st0[i].qsca;
+    ctx->q_h[6 * i + 1] = st0[i].qext;
+    ctx->q_h[6 * i + 4] = st0[i].dqs;
+    ctx->q_h[6 * i + 5] = st0[i].dqe;
+    ctx->t_off_h[i] = (st0[i].nmax > 0) ? toff[i] : 0;
+  }
+  // the rounds' items in one array, largest size bucket first, with their
+  // class sizes, for the gradients (their LU factors stay in gm_lu)
+  tmx_ctx::RoundRec rec;
+  rec.own_tables = false;
+  rec.borrowed = true;
+  rec.tab = rec.nsc = (double *)ctx->keep_arena.p;
+  rec.slots = (TmxSlot *)ctx->gm_rslots.p;
+  rec.items = (TmxItem *)ctx->gm_allitems.p;
+  rec.lu = (cplx *)ctx->gm_lu.p;
+  rec.scr_total = (int64_t)g1.lu_used;
+  {
+    int64_t total = 0;
+    for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+      total += std::min(g1.fill[b], bcap[b]);
+    }
+    std::vector<TmxItem> items(total);
+    std::vector<TmxSlot> rsl(std::min<int64_t>(g1.nslots, n));
+    int64_t off = 0;
+    for (int b = TMX_GM_BUCKETS - 1; b >= 0; --b) {
+      const int64_t c = std::min(g1.fill[b], bcap[b]);
+      if (c > 0) {
+        CK(cudaMemcpyAsync(rec.items + off, bitems[b], c * sizeof(TmxItem),
+                           cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(items.data() + off, bitems[b], c * sizeof(TmxItem),
+                           cudaMemcpyDeviceToHost, st));
+      }
+      off += c;
+    }
+    if (!rsl.empty()) {
+      CK(cudaMemcpyAsync(rsl.data(), rec.slots, rsl.size() * sizeof(TmxSlot),
+                         cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    rec.nb.resize(total);
+    for (int64_t i = 0; i < total; ++i) {
+      rec.nb[i] = tmx_host_class_size(rsl[items[i].slot].nmax, items[i].m, items[i].cls);
+    }
+  }
+  ctx->rounds_kept.push_back(std::move(rec));
+  ctx->gm_last_t = (int64_t)g1.t_used;
+  ctx->sink_done = 0;
+  if ((rc = finish_blocks(ctx, (int64_t)g1.t_used, 1))) {
+    return rc;
+  }
+  ctx->rounds_lu = true;
+  ctx->last_mode = TMX_BATCH_GRAPH;
+  return TMX_OK;
+}
+
+extern "C" int tmx_set_batch_mode(tmx_ctx *ctx, int mode) {
+  if (!ctx || (mode != TMX_BATCH_HOST && mode != TMX_BATCH_GRAPH)) {
+    return TMX_ERR_INVALID;
+  }
+  ctx->batch_mode = mode;
+  return TMX_OK;
+}
+
+extern "C" int tmx_get_batch_mode(tmx_ctx *ctx, int *mode) {
+  if (!ctx || !mode) {
+    return TMX_ERR_INVALID;
+  }
+  *mode = ctx->batch_mode;
+  return TMX_OK;
+}
+
+extern "C" int tmx_last_batch_mode(tmx_ctx *ctx, int *mode) {
+  if (!ctx || !mode) {
+    return TMX_ERR_INVALID;
+  }
+  *mode = ctx->last_mode;
+  return TMX_OK;
+}
+
 static double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
       .count();
@@ -1014,6 +1520,13 @@ int tmx_batch_compute(tmx_ctx *ctx) {
     ctx->p2_t_total = 0;
     ctx->have_batch = true;
     return TMX_OK;
+  }
+  ctx->last_mode = TMX_BATCH_HOST;
+  if (ctx->batch_mode == TMX_BATCH_GRAPH) {
+    rc = gm_compute(ctx);
+    if (rc != 1) {
+      return rc;
+    }
   }
   std::vector<TmxChainState> st0(n);
   if ((rc = tl_mark(ctx, TMX_TL_BATCH_START, st))) {

@@ -58,6 +58,14 @@ struct TmxBlockArgs {
   double2 *lu = nullptr;       // if set: LU factors + pivots saved per item
                                // at the item's scratch offset (2 nb^2)
   int family = -1;             // tmx_block_family to run, -1: by max_nb
+  // device-driven launches (CUDA graph): items [range[0], range[1]) of
+  // `items` (clamped to nitems) instead of [0, nitems); the launch does
+  // nothing unless *gate == gate_value; at most max_ctas CTAs (0: one item
+  // per warp or CTA)
+  const int32_t *range = nullptr;
+  const int32_t *gate = nullptr;
+  int gate_value = 0;
+  int max_ctas = 0;
 };
 // largest class size each tmx_block_family can run
 int tmx_block_family_capacity(int family);
@@ -94,7 +102,53 @@ void tmx_launch_converge(const int32_t *active, int nactive,
                          int32_t *next_count, int32_t *done_list,
                          int32_t *done_ord, int32_t *done_pos,
                          int32_t *done_count, const int32_t *nact_dev,
-                         int base, cudaStream_t stream);
+                         int base, cudaStream_t stream,
+                         const int32_t *order_dev = nullptr);
+
+// state of the device-driven order loop (tmx_graph.cu), in device memory
+#define TMX_GM_BUCKETS 5
+struct TmxGState {
+  unsigned long long t_used, lu_used; // T-matrix and LU storage handed out
+  int32_t k;                          // order of the current iteration
+  int32_t last_order;                 // maximum_order - 1
+  int32_t iter, max_iter;
+  int32_t cnt[3];   // [0] active list length, [1] done-list length, [2] next list
+  int32_t round_lo, round_hi;         // done entries of this iteration's round
+  int32_t fill[TMX_GM_BUCKETS];       // items appended per size bucket
+  int32_t rng[TMX_GM_BUCKETS][2];     // this round's items per bucket
+  int32_t nslots, srng[2];            // round slots appended; this round's
+  int32_t overflow;                   // storage or arena ran out (bit mask)
+};
+// parameters of one iteration, written by k_gm_begin
+struct TmxGIter {
+  int32_t order, ngauss, wig_n, bucket;
+  TmxChainBase base;
+};
+
+// the device-driven loop's kernels (tmx_graph.cu)
+struct TmxGmRoundArgs {
+  TmxGState *G;
+  const int32_t *done_list, *done_ord;
+  const int64_t *keep_tab;
+  const int32_t *tpl_off, *tpl, *full_sets;
+  const int64_t *tsize;
+  int glf, min_order;
+  TmxSlot *rslots;
+  int n;                     // grains of the batch (slot capacity)
+  TmxItem *const *bitems;    // item array of each size bucket (device array)
+  const int32_t *bcap;       // their capacities (device)
+  int64_t *t_off;            // per grain: T-matrix offset
+  unsigned long long t_cap, lu_cap;
+};
+void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, const int32_t *m0_sets, int min_order,
+                         int glf, cudaStream_t stream);
+void tmx_launch_gm_prep(const TmxGState *G, const TmxGIter *I, const int32_t *active, int n,
+                        TmxSlot *slots, TmxItem *items, cudaStream_t stream);
+void tmx_launch_gm_round(const TmxGmRoundArgs &a, cudaStream_t stream);
+void tmx_launch_gm_round_mid(TmxGState *G, cudaStream_t stream);
+void tmx_launch_gm_swap(const TmxGState *G, const int32_t *next, int32_t *cur, int n,
+                        cudaStream_t stream);
+void tmx_launch_gm_end(TmxGState *G, cudaGraphConditionalHandle loop, cudaStream_t stream);
 
 // copies of the final-order tables of the grains that became final in one
 // group of orders, into the batch's table arena (k_keep_tables)
@@ -112,14 +166,21 @@ struct TmxKeepArgs {
   unsigned long long *used;         // doubles reserved so far
   int64_t *keep_tab;                // per grain: arena offset (-1: none)
   int64_t *keep_q;                  // per done-list entry: the same
+  // device-driven loop: the order and table layout of the (one-order) group
+  // read on the device instead of order0 / base[0]
+  const int32_t *order0_dev = nullptr;
+  const TmxChainBase *base_dev = nullptr;
 };
 void tmx_launch_keep_tables(const TmxKeepArgs &K, int max_entries,
                             cudaStream_t stream);
 
 // full Q sums over all m blocks (TMatrixQTask) of the grains of a block round: q_out[2 g], q_out[2 g + 1]
 // for g = slots[s].grain
+// (range: slots [range[0], range[1]) of the ns, read on the device; at most
+// max_ctas CTAs, 0: one per slot)
 void tmx_launch_qsums(const TmxSlot *slots, int ns, const double2 *T,
-                      double *q_out, cudaStream_t stream);
+                      double *q_out, cudaStream_t stream,
+                      const int32_t *range = nullptr, int max_ctas = 0);
 
 // FP64 throughput probes (DFMA pipe and DMMA tensor pipe)
 void tmx_launch_probe_dfma(double *out, int iters, int blocks,

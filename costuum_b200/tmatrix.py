@@ -154,6 +154,24 @@ class Context:
         _lib.check(self._h, rc, "tmx_probe_fp64")
         return float(v[0])
 
+    BATCH_HOST, BATCH_GRAPH = 0, 1
+
+    def set_batch_mode(self, mode):
+        """How batches drive the order loop (tmx_set_batch_mode): BATCH_HOST
+        (the host issues order groups and forms block rounds) or BATCH_GRAPH
+        (one CUDA graph runs the loop and its rounds on the device)."""
+        rc = _lib.load().tmx_set_batch_mode(self._h, int(mode))
+        _lib.check(self._h, rc, "tmx_set_batch_mode")
+
+    @property
+    def last_batch_mode(self):
+        """The mode that computed the last batch (a graph-mode batch the
+        graph does not cover runs in the host mode)."""
+        v = np.zeros(1, np.int32)
+        rc = _lib.load().tmx_last_batch_mode(self._h, _lib.iptr(v))
+        _lib.check(self._h, rc, "tmx_last_batch_mode")
+        return int(v[0])
+
     def profile(self, on=True):
         """Switch the per-kernel CUDA-event profile on or off
         (tmx_profile_enable); resets its counters and the timeline."""

@@ -212,6 +212,24 @@ enum tmx_timeline_mark {
 int tmx_profile_timeline(tmx_ctx *ctx, int64_t cap, double *records,
                          int64_t *count);
 
+/* How tmx_batch_compute drives the order loop.
+ * TMX_BATCH_HOST: the host issues the order groups one ahead of the GPU,
+ * reads each group's outcome and forms the block rounds (the default).
+ * TMX_BATCH_GRAPH: one CUDA graph per batch shape whose conditional WHILE
+ * node runs the whole loop on the device -- order steps, convergence,
+ * rounds of the grains that became final, Q sums -- until no grain is left;
+ * the host only uploads the batch and reads the results (QuickSched's role,
+ * TaskManager.hpp:1146-1197 and :1313-1327, played by the device). Results
+ * are bit-identical to the host mode. Batches the graph mode does not cover
+ * (maximum_order above 101, tables beyond 24 GB, profiling or autotuning on)
+ * and a batch whose T-matrix or LU storage outgrows the estimate run in the
+ * host mode. */
+enum tmx_batch_mode { TMX_BATCH_HOST = 0, TMX_BATCH_GRAPH = 1 };
+int tmx_set_batch_mode(tmx_ctx *ctx, int mode);
+int tmx_get_batch_mode(tmx_ctx *ctx, int *mode);
+/* Which mode computed the last batch (TMX_BATCH_HOST or TMX_BATCH_GRAPH). */
+int tmx_last_batch_mode(tmx_ctx *ctx, int *mode);
+
 /* Host-side times of the last tmx_batch_compute, out[4] in ms: wall time of
  * the call, time blocked on the order loop's events and the final
  * synchronisation, host set-up of the block rounds, and (out[3]) the number

@@ -203,7 +203,8 @@ __device__ __forceinline__ void block_item(const TmxBlockArgs &A, int it,
   if (nb <= 0) {
     return;
   }
-  if (nb > TMX_MAX_NB) {
+  // (shared memory is sized for classes of at most max_nb members)
+  if (nb > TMX_MAX_NB || nb > A.max_nb) {
     if (threadIdx.x == 0) {
       atomicOr(&A.status[sl.grain], TMX_ST_TOO_LARGE);
     }

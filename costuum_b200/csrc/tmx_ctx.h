@@ -4,6 +4,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <array>
 #include <map>
 #include <string>
 #include <tuple>
@@ -123,6 +124,9 @@ struct tmx_ctx {
     TmxItem *items = nullptr;
     cplx *lu = nullptr;
     std::vector<int> nb; // class size per item (descending)
+    // or, for a device-driven batch: per size bucket, largest first, the
+    // item range [i0, i1) and an upper bound of its class sizes
+    std::vector<std::array<int64_t, 3>> seg;
     int64_t scr_total = 0;
   };
   std::vector<RoundRec> rounds_kept;
@@ -153,13 +157,15 @@ struct tmx_ctx {
   int batch_mode = TMX_BATCH_HOST, last_mode = TMX_BATCH_HOST;
   DevBuf gm_state, gm_iter, gm_tab, gm_nsc, gm_scr, gm_diag, gm_slots, gm_items,
       gm_rslots, gm_bitems, gm_bptr, gm_bcap, gm_tpl, gm_tpl_off, gm_full, gm_m0,
-      gm_tsize, gm_toff, gm_lu, gm_luscr, gm_allitems;
+      gm_tsize, gm_toff, gm_lu, gm_luscr, gm_allitems, gm_steps;
   cudaGraph_t gm_graph = nullptr;
   cudaGraphExec_t gm_exec = nullptr;
   std::vector<uint64_t> gm_key;
   cudaStream_t gm_cs = nullptr, gm_rs = nullptr, gm_bs[TMX_GM_BUCKETS] = {};
   int64_t gm_t_hint = 0, gm_lu_hint = 0;
   int64_t gm_last_t = 0;
+  int gm_body_kernels[2] = {0, 0}; // kernels of one order step and of one round
+  int gm_counts[2] = {0, 0};       // the last graph batch's order steps and rounds
   // host-side times of the last tmx_batch_compute (ms): wall time, time
   // blocked on the order loop's events and the final synchronisation, host
   // set-up of block rounds, and the number of order groups

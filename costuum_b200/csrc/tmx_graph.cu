@@ -1,31 +1,32 @@
 // Device-driven batch (TMX_BATCH_GRAPH): the order loop and the block rounds
-// of tmx_batch_compute as one CUDA graph whose conditional WHILE node runs
-// on the GPU until no grain is left, so the host uploads the batch's
-// descriptors, launches the graph once and reads the results.
+// of tmx_batch_compute as one CUDA graph, launched once; the host uploads the
+// batch's descriptors, launches the graph and reads the results.
 //
 // Reference semantics are those of the host-driven loop (TaskManager.hpp:
 // 1146-1197 chain of TMatrixM0Task per order, :1313-1327 TMatrixMAllTask
 // once the order is final): every order step of every active grain, the
 // convergence test in the reference's order, and the blocks of every m at
-// the final order. One iteration of the WHILE body is one order k:
-//   k_gm_begin      iteration parameters (order, m = 0 Wigner set, table
-//                   strides, size bucket of the m = 0 classes) and the item
-//                   ranges of the round formed below
-//   k_gm_prep       slots and m = 0 items of the active list
-//   k_tables        node scalars and Bessel tables of the active grains
-//   block kernels   the m = 0 classes (one launch per size bucket, gated)
-//   k_converge      sums, test, next active list, done list
-//   k_keep_tables   final-order tables of the grains that became final
-// and, beside them (a second branch of the body), the round of the grains
-// that became final in the previous iteration:
-//   k_gm_round      slots and items of those grains (every m and class, into
-//                   per-size-bucket item arrays), T-matrix and LU offsets
-//   k_gm_round_mid  the round's item and slot ranges
-//   block kernels   one launch per size bucket, on the round's ranges
-//   k_qsums         Q sums of the round's grains
-// then k_gm_swap / k_gm_end: the next active list becomes the current one,
-// the order advances, and the WHILE condition is set to whether a grain is
-// still active or a round is pending.
+// the final order.
+//
+// The graph has two chains of conditional (IF) nodes, one node of each per
+// order k = min_order .. maximum_order - 1:
+//   loop chain (high priority)
+//     k_gm_cond       whether step k runs (a grain is still active)
+//     IF step k:      k_gm_begin (step parameters, next list emptied),
+//                     k_gm_prep (slots and m = 0 items of the active list),
+//                     k_tables_dev, the m = 0 block launch, k_converge,
+//                     k_keep_tables, k_gm_step_end (snapshot of the done list)
+//   round chain (low priority), node k after step k and round k - 1
+//     k_gm_decide     whether to run a round now: at least a threshold of
+//                     grains final and not yet in a round, or the loop over
+//     IF round k:     k_gm_round (slots and items of those grains, every m
+//                     and class, into per-size-bucket item arrays; T-matrix
+//                     and LU offsets), k_gm_round_mid, k_gm_tzero (their
+//                     T-matrices cleared), one block launch per size bucket
+//                     side by side, k_qsums, k_gm_round_end
+// Nothing in the loop chain waits for a round, so rounds run beside the
+// later orders, as the host-driven loop's rounds do on their streams; the
+// lists alternate between two buffers by the parity of k - min_order.
 //
 // Buffers are sized before the graph is built (no allocation inside):
 // tables for every grain at the largest order, the arena for every grain's
@@ -39,18 +40,33 @@
 
 // ------------------------------------------------------------- kernels --
 
-__global__ void k_gm_begin(TmxGState *G, TmxGIter *I, const int32_t *__restrict__ m0_sets,
-                           int min_order, int glf) {
+// whether order step k runs: a grain is left in its input list (count
+// cnt[in]) and no earlier step found the list empty
+__global__ void k_gm_cond(TmxGState *G, int in, cudaGraphConditionalHandle h) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
-  const int k = G->k;
+  const bool run = !G->loop_done && G->cnt[in] > 0;
+  if (!run) {
+    G->loop_done = 1;
+  }
+  cudaGraphSetConditional(h, run ? 1u : 0u);
+}
+
+// parameters of step k; the step's output list starts empty
+__global__ void k_gm_begin(TmxGState *G, TmxGIter *I, int k, int glf, int wig_n, int in,
+                           int out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) {
+    return;
+  }
   TmxGIter it;
   it.order = k;
   it.ngauss = glf * k;
-  it.wig_n = m0_sets[min(k, G->last_order) - min_order];
+  it.wig_n = wig_n;
   const int cm = (k + 1) / 2;
   it.bucket = (cm <= 8) ? 0 : (cm <= 16) ? 1 : (cm <= 32) ? 2 : (cm <= 64) ? 3 : 4;
+  it.m0_range[0] = 0;
+  it.m0_range[1] = 4 * G->cnt[in];
   TmxChainBase &b = it.base;
   b.slot = 0;
   b.tab = b.nsc = b.diag = b.scr = 0;
@@ -59,20 +75,12 @@ __global__ void k_gm_begin(TmxGState *G, TmxGIter *I, const int32_t *__restrict_
   b.diag_stride = 2 * (int64_t)k;
   b.scr_stride = 2 * (int64_t)cm * cm;
   *I = it;
-  // the next active list starts empty; the round of this iteration covers
-  // the done entries [round_lo, round_hi) fixed by the previous iteration
-  G->cnt[2] = 0;
-  for (int q = 0; q < TMX_GM_BUCKETS; ++q) {
-    G->rng[q][0] = G->fill[q];
-    G->rng[q][1] = G->fill[q];
-  }
-  G->srng[0] = G->nslots;
-  G->srng[1] = G->nslots;
+  G->cnt[out] = 0;
 }
 
 // slots and m = 0 items of every active position p < n (positions at or past
-// the list's length get an empty slot: order 0, no classes, no nodes)
-__global__ void k_gm_prep(const TmxGState *__restrict__ G, const TmxGIter *__restrict__ I,
+// the list's length *nact get an empty slot: order 0, no classes, no nodes)
+__global__ void k_gm_prep(const int32_t *__restrict__ nact, const TmxGIter *__restrict__ I,
                           const int32_t *__restrict__ active, int n, TmxSlot *slots,
                           TmxItem *items) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -80,7 +88,7 @@ __global__ void k_gm_prep(const TmxGState *__restrict__ G, const TmxGIter *__res
     return;
   }
   const TmxGIter it = *I;
-  const bool valid = p < G->cnt[0];
+  const bool valid = p < *nact;
   TmxSlot s;
   s.grain = valid ? active[p] : 0;
   s.nmax = valid ? it.order : 0;
@@ -99,6 +107,47 @@ __global__ void k_gm_prep(const TmxGState *__restrict__ G, const TmxGIter *__res
     t.scratch = (4 * (int64_t)p + c) * it.base.scr_stride;
     items[4 * p + c] = t;
   }
+}
+
+// end of step j = k - min_order: the done list's length now (every entry
+// and its kept tables complete), and whether the output list is empty
+__global__ void k_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) {
+    return;
+  }
+  snap[j] = G->cnt[1];
+  outz[j] = (G->cnt[out] == 0) ? 1 : 0;
+  G->snap_last = G->cnt[1];
+  G->steps += 1;
+}
+
+// whether round j runs: the done entries that step j completed (or, if step
+// j did not run, every entry) not yet in a round, at least `thr` of them
+// while the loop continues (at most rmax per round), all of them once the
+// loop is over (step j found its output list empty, did not run, or was the
+// last order)
+__global__ void k_gm_decide(TmxGState *G, const int32_t *__restrict__ snap,
+                            const int32_t *__restrict__ outz, int j, int last, int thr,
+                            int rmax, cudaGraphConditionalHandle h) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) {
+    return;
+  }
+  const bool ran = snap[j] >= 0;
+  const int avail = ran ? snap[j] : G->snap_last;
+  const bool ended = !ran || outz[j] != 0 || last != 0;
+  const int pending = avail - G->round_lo;
+  const bool fire = pending > 0 && (ended || pending >= thr);
+  if (fire) {
+    G->round_hi = ended ? avail : min(avail, G->round_lo + rmax);
+    for (int q = 0; q < TMX_GM_BUCKETS; ++q) {
+      G->rng[q][0] = G->fill[q];
+      G->rng[q][1] = G->fill[q];
+    }
+    G->srng[0] = G->nslots;
+    G->srng[1] = G->nslots;
+    G->rounds += 1;
+  }
+  cudaGraphSetConditional(h, fire ? 1u : 0u);
 }
 
 // The round: one thread per done entry of [round_lo, round_hi). A grain's
@@ -193,43 +242,50 @@ __global__ void k_gm_round_mid(TmxGState *G) {
   G->srng[1] = G->nslots;
 }
 
-// the next active list (act1) becomes the current one (act0)
-__global__ void k_gm_swap(const TmxGState *__restrict__ G, const int32_t *__restrict__ next,
-                          int32_t *cur, int n) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n && p < G->cnt[2]) {
-    cur[p] = next[p];
+// The T-matrix ranges of the round's slots [srng[0], srng[1]) start at
+// zero: the parity classes write only their own entries of a block, the
+// others are zero by symmetry (the host-driven rounds clear their range the
+// same way). One CTA per slot at a time, 16-byte stores.
+__global__ void k_gm_tzero(const TmxGState *__restrict__ G, const TmxSlot *__restrict__ slots,
+                           const int64_t *__restrict__ tsize, double2 *T) {
+  const int lo = G->srng[0], hi = G->srng[1];
+  for (int s = lo + blockIdx.x; s < hi; s += gridDim.x) {
+    const TmxSlot sl = slots[s];
+    if (sl.nmax <= 0) {
+      continue;
+    }
+    double2 *t = T + sl.tout;
+    const int64_t ts = tsize[sl.nmax];
+    for (int64_t u = threadIdx.x; u < ts; u += blockDim.x) {
+      t[u] = make_double2(0., 0.);
+    }
   }
 }
 
-__global__ void k_gm_end(TmxGState *G, cudaGraphConditionalHandle loop) {
+// the round's done entries are consumed
+__global__ void k_gm_round_end(TmxGState *G) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
-  G->cnt[0] = G->cnt[2];
-  G->cnt[2] = 0;
   G->round_lo = G->round_hi;
-  G->round_hi = G->cnt[1];
-  G->k += 1;
-  G->iter += 1;
-  const bool active = G->cnt[0] > 0 && G->k <= G->last_order;
-  const bool pending = G->round_hi > G->round_lo;
-  // (a bound on the iterations: one per order, one more for the last round)
-  const bool more = (active || pending) && G->iter <= G->max_iter;
-  cudaGraphSetConditional(loop, more ? 1u : 0u);
 }
 
 
 // ------------------------------------------------------ launch wrappers --
 
-void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, const int32_t *m0_sets, int min_order,
-                         int glf, cudaStream_t stream) {
-  k_gm_begin<<<1, 32, 0, stream>>>(G, I, m0_sets, min_order, glf);
+void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, int k, int glf, int wig_n, int in, int out,
+                         cudaStream_t stream) {
+  k_gm_begin<<<1, 32, 0, stream>>>(G, I, k, glf, wig_n, in, out);
 }
 
-void tmx_launch_gm_prep(const TmxGState *G, const TmxGIter *I, const int32_t *active, int n,
+void tmx_launch_gm_prep(const int32_t *nact, const TmxGIter *I, const int32_t *active, int n,
                         TmxSlot *slots, TmxItem *items, cudaStream_t stream) {
-  k_gm_prep<<<(n + 127) / 128, 128, 0, stream>>>(G, I, active, n, slots, items);
+  k_gm_prep<<<(n + 127) / 128, 128, 0, stream>>>(nact, I, active, n, slots, items);
+}
+
+void tmx_launch_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out,
+                            cudaStream_t stream) {
+  k_gm_step_end<<<1, 32, 0, stream>>>(G, snap, outz, j, out);
 }
 
 void tmx_launch_gm_round(const TmxGmRoundArgs &a, cudaStream_t stream) {
@@ -242,11 +298,49 @@ void tmx_launch_gm_round_mid(TmxGState *G, cudaStream_t stream) {
   k_gm_round_mid<<<1, 32, 0, stream>>>(G);
 }
 
-void tmx_launch_gm_swap(const TmxGState *G, const int32_t *next, int32_t *cur, int n,
-                        cudaStream_t stream) {
-  k_gm_swap<<<(n + 127) / 128, 128, 0, stream>>>(G, next, cur, n);
+void tmx_launch_gm_tzero(const TmxGState *G, const TmxSlot *slots, const int64_t *tsize,
+                         double2 *T, cudaStream_t stream) {
+  k_gm_tzero<<<148 * 4, 256, 0, stream>>>(G, slots, tsize, T);
 }
 
-void tmx_launch_gm_end(TmxGState *G, cudaGraphConditionalHandle loop, cudaStream_t stream) {
-  k_gm_end<<<1, 32, 0, stream>>>(G, loop);
+void tmx_launch_gm_round_end(TmxGState *G, cudaStream_t stream) {
+  k_gm_round_end<<<1, 32, 0, stream>>>(G);
+}
+
+// The two control kernels of the top-level chains as graph kernel nodes
+// (they set the condition of the IF node that follows them), with the
+// given dependencies and execution priority.
+static int add_kernel_node(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd,
+                           cudaGraphNode_t *node, void *func, void **args, int priority) {
+  cudaKernelNodeParams p = {};
+  p.func = func;
+  p.gridDim = dim3(1);
+  p.blockDim = dim3(32);
+  p.sharedMemBytes = 0;
+  p.kernelParams = args;
+  p.extra = nullptr;
+  if (cudaGraphAddKernelNode(node, g, deps, nd, &p) != cudaSuccess) {
+    return -1;
+  }
+  cudaKernelNodeAttrValue v = {};
+  v.priority = priority;
+  if (cudaGraphKernelNodeSetAttribute(*node, cudaKernelNodeAttributePriority, &v) !=
+      cudaSuccess) {
+    return -1;
+  }
+  return 0;
+}
+
+int tmx_gm_add_cond(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd, cudaGraphNode_t *node,
+                    TmxGState *G, int in, cudaGraphConditionalHandle h, int priority) {
+  void *args[] = {&G, &in, &h};
+  return add_kernel_node(g, deps, nd, node, (void *)k_gm_cond, args, priority);
+}
+
+int tmx_gm_add_decide(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd,
+                      cudaGraphNode_t *node, TmxGState *G, const int32_t *snap,
+                      const int32_t *outz, int j, int last, int thr, int rmax,
+                      cudaGraphConditionalHandle h, int priority) {
+  void *args[] = {&G, &snap, &outz, &j, &last, &thr, &rmax, &h};
+  return add_kernel_node(g, deps, nd, node, (void *)k_gm_decide, args, priority);
 }

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -342,7 +343,7 @@ void tmx_destroy(tmx_ctx *ctx) {
                        &ctx->gm_rslots, &ctx->gm_bitems, &ctx->gm_bptr, &ctx->gm_bcap,
                        &ctx->gm_tpl, &ctx->gm_tpl_off, &ctx->gm_full, &ctx->gm_m0,
                        &ctx->gm_tsize, &ctx->gm_toff, &ctx->gm_lu, &ctx->gm_luscr,
-                       &ctx->gm_allitems};
+                       &ctx->gm_allitems, &ctx->gm_steps};
   for (DevBuf *b : gm_bufs) {
     if (b->p) {
       cudaFreeAsync(b->p, ctx->stream);
@@ -876,7 +877,10 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
 
 // End of a batch: full Q sums of every grain (TMatrixQTask) on ctx->stream
 // after all block rounds, per-grain results to the host.
-static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
+// (q2_in, stb_in: the Q sums and status words already read back, if given)
+static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds,
+                         const std::vector<double> *q2_in = nullptr,
+                         const std::vector<int32_t> *stb_in = nullptr) {
   cudaStream_t st = ctx->stream;
   const int64_t n = ctx->n;
   const tmx_schedule S = ctx->up_sched;
@@ -887,13 +891,20 @@ static int finish_blocks(tmx_ctx *ctx, int64_t t_total, int rounds) {
   ctx->t_averaged = false;
   ++ctx->batch_seq;
   if (t_total > 0) {
-    std::vector<double> q2(2 * n);
-    std::vector<int32_t> stb(n);
-    CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t),
-                       cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
+    std::vector<double> q2;
+    std::vector<int32_t> stb;
+    if (q2_in && stb_in) {
+      q2 = *q2_in;
+      stb = *stb_in;
+    } else {
+      q2.resize(2 * n);
+      stb.resize(n);
+      CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double),
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t),
+                         cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
     for (int64_t i = 0; i < n; ++i) {
       if (ctx->nmax_h[i] > 0) {
         ctx->q_h[6 * i + 2] = q2[2 * i];
@@ -1014,6 +1025,12 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
 // Returns TMX_OK, an error, or 1 when this batch must run in the host mode
 // (not covered, or the T-matrix / LU storage ran out: the hints grow).
 
+// most CTAs of a round's block launch (the items of a round are known only
+// on the device; each CTA loops over its share)
+#ifndef TMX_GM_ROUND_CTAS
+#define TMX_GM_ROUND_CTAS (148 * 16)
+#endif
+
 static int gm_bucket(int nb) {
   return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
 }
@@ -1098,8 +1115,14 @@ static int gm_compute(tmx_ctx *ctx) {
   }
   const int cmK = (K + 1) / 2;
   const int64_t arena_cap = (int64_t)(tab_per * n);
+  const int nsteps = K - kmin + 1;
+  // rounds: at least round_min grains final while the loop runs (at most
+  // round_max of them), as in the host-driven loop
+  const int round_min = (int)std::max<int64_t>(256, ctx->up_nact / 16);
+  const int round_max = std::max(768, round_min);
   if ((rc = ensure(ctx, ctx->gm_state, sizeof(TmxGState))) ||
       (rc = ensure(ctx, ctx->gm_iter, sizeof(TmxGIter))) ||
+      (rc = ensure(ctx, ctx->gm_steps, 2 * (size_t)nsteps * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->act0, n * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->act1, n * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->done, 2 * n * sizeof(int32_t))) ||
@@ -1122,7 +1145,6 @@ static int gm_compute(tmx_ctx *ctx) {
       (rc = ensure(ctx, ctx->gm_tpl, std::max<size_t>(1, tpl.size()) * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->gm_tpl_off, tpl_off.size() * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->gm_full, full_sets.size() * sizeof(int32_t))) ||
-      (rc = ensure(ctx, ctx->gm_m0, m0_sets.size() * sizeof(int32_t))) ||
       (rc = ensure(ctx, ctx->gm_tsize, tsz.size() * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->gm_toff, n * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->T, t_cap * sizeof(cplx))) ||
@@ -1141,10 +1163,13 @@ static int gm_compute(tmx_ctx *ctx) {
   }
   TmxGState *G = (TmxGState *)ctx->gm_state.p;
   TmxGIter *I = (TmxGIter *)ctx->gm_iter.p;
+  int32_t *snap = (int32_t *)ctx->gm_steps.p;
+  int32_t *outz = snap + nsteps;
   // ---- the graph, built again when the batch's shape or a buffer changed
   std::vector<uint64_t> key = {
       (uint64_t)n, (uint64_t)glf, (uint64_t)kmin, (uint64_t)K,
-      (uint64_t)S.bessel_start, (uint64_t)t_cap, (uint64_t)lu_cap, (uint64_t)arena_cap};
+      (uint64_t)S.bessel_start, (uint64_t)t_cap, (uint64_t)lu_cap, (uint64_t)arena_cap,
+      (uint64_t)round_min, (uint64_t)round_max};
   uint64_t tol_bits;
   memcpy(&tol_bits, &S.tolerance, sizeof(tol_bits));
   key.push_back(tol_bits);
@@ -1152,16 +1177,20 @@ static int gm_compute(tmx_ctx *ctx) {
     key.push_back((uint64_t)ctx->dispatch[b]);
     key.push_back((uint64_t)bcap[b]);
   }
-  for (const DevBuf *b : {&ctx->gm_state, &ctx->gm_iter, &ctx->act0, &ctx->act1, &ctx->done,
-                          &ctx->done_pos, &ctx->keep_tab, &ctx->keep_q, &ctx->keep_ctl,
-                          &ctx->keep_arena, &ctx->gm_tab, &ctx->gm_nsc, &ctx->gm_scr,
-                          &ctx->gm_diag, &ctx->gm_slots, &ctx->gm_items, &ctx->gm_rslots,
-                          &ctx->gm_bitems, &ctx->gm_bptr, &ctx->gm_bcap, &ctx->gm_tpl,
-                          &ctx->gm_tpl_off, &ctx->gm_full, &ctx->gm_m0, &ctx->gm_tsize,
-                          &ctx->gm_toff, &ctx->T, &ctx->gm_lu, &ctx->gm_luscr, &ctx->q,
-                          &ctx->state, &ctx->status, &ctx->grains, &ctx->gl_x, &ctx->gl_w,
-                          &ctx->gl_off, &ctx->wig, &ctx->wig_off}) {
+  for (const DevBuf *b : {&ctx->gm_state, &ctx->gm_iter, &ctx->gm_steps, &ctx->act0,
+                          &ctx->act1, &ctx->done, &ctx->done_pos, &ctx->keep_tab,
+                          &ctx->keep_q, &ctx->keep_ctl, &ctx->keep_arena, &ctx->gm_tab,
+                          &ctx->gm_nsc, &ctx->gm_scr, &ctx->gm_diag, &ctx->gm_slots,
+                          &ctx->gm_items, &ctx->gm_rslots, &ctx->gm_bitems, &ctx->gm_bptr,
+                          &ctx->gm_bcap, &ctx->gm_tpl, &ctx->gm_tpl_off, &ctx->gm_full,
+                          &ctx->gm_tsize, &ctx->gm_toff, &ctx->T, &ctx->gm_lu,
+                          &ctx->gm_luscr, &ctx->q, &ctx->state, &ctx->status, &ctx->grains,
+                          &ctx->gl_x, &ctx->gl_w, &ctx->gl_off, &ctx->wig, &ctx->wig_off}) {
     key.push_back((uint64_t)(uintptr_t)b->p);
+  }
+  int nbk = 0; // size buckets a round launches
+  for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+    nbk += (bcap[b] > 0) ? 1 : 0;
   }
   if (key != ctx->gm_key || !ctx->gm_exec) {
     if (ctx->gm_exec) {
@@ -1179,35 +1208,36 @@ static int gm_compute(tmx_ctx *ctx) {
                        cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->gm_full.p, full_sets.data(), full_sets.size() * sizeof(int32_t),
                        cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->gm_m0.p, m0_sets.data(), m0_sets.size() * sizeof(int32_t),
-                       cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->gm_tsize.p, tsz.data(), tsz.size() * sizeof(int64_t),
                        cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->gm_bptr.p, bitems, sizeof(bitems), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->gm_bcap.p, bcap, sizeof(bcap), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
+    int prio_lo = 0, prio_hi = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
     if (!ctx->gm_cs) {
-      CK(cudaStreamCreateWithFlags(&ctx->gm_cs, cudaStreamNonBlocking));
-      CK(cudaStreamCreateWithFlags(&ctx->gm_rs, cudaStreamNonBlocking));
+      // the loop chain's bodies are captured from a high-priority stream and
+      // the rounds' from low-priority ones: captured kernels keep their
+      // stream's priority, and the graph runs with per-node priorities
+      CK(cudaStreamCreateWithPriority(&ctx->gm_cs, cudaStreamNonBlocking, prio_hi));
+      CK(cudaStreamCreateWithPriority(&ctx->gm_rs, cudaStreamNonBlocking, prio_lo));
       for (cudaStream_t &x : ctx->gm_bs) {
-        CK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithPriority(&x, cudaStreamNonBlocking, prio_lo));
       }
     }
     cudaGraph_t graph;
     CK(cudaGraphCreate(&graph, 0));
     ctx->gm_graph = graph;
-    cudaGraphConditionalHandle loop;
-    CK(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = loop;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t wnode;
-    CK(cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
     cudaStream_t cs = ctx->gm_cs, rs = ctx->gm_rs;
     std::vector<cudaEvent_t> evs;
+    struct EvList {
+      std::vector<cudaEvent_t> *v;
+      ~EvList() {
+        for (cudaEvent_t e : *v) {
+          cudaEventDestroy(e);
+        }
+      }
+    } ev_list{&evs};
     auto link = [&](cudaStream_t from, cudaStream_t to) -> int {
       cudaEvent_t e;
       CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -1216,31 +1246,54 @@ static int gm_compute(tmx_ctx *ctx) {
       CK(cudaStreamWaitEvent(to, e, 0));
       return 0;
     };
-    CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
-                                     cudaStreamCaptureModeRelaxed));
-    // the body's launches; any error ends the capture before it returns
-    auto capture_body = [&]() -> int {
-      tmx_launch_gm_begin(G, I, (const int32_t *)ctx->gm_m0.p, kmin, glf, cs);
-      if ((rc = link(cs, rs))) {
-        return rc;
+    // an IF node on `deps` whose body is captured from stream `s` by `body`
+    auto add_if = [&](cudaGraphConditionalHandle h, cudaGraphNode_t dep, cudaStream_t s,
+                      cudaGraphNode_t *node, const std::function<int()> &body) -> int {
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      CK(cudaGraphAddNode(node, graph, &dep, 1, &cp));
+      CK(cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed));
+      const int brc = body();
+      cudaGraph_t captured = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+      if (brc) {
+        return brc;
       }
-      // loop branch: one order step of every active grain
-      tmx_launch_gm_prep(G, I, (const int32_t *)ctx->act0.p, (int)n, (TmxSlot *)ctx->gm_slots.p,
-                         (TmxItem *)ctx->gm_items.p, cs);
-      tmx_launch_tables((const TmxSlot *)ctx->gm_slots.p, (int)n, (const TmxGrain *)ctx->grains.p,
-                        (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
-                        (const int64_t *)ctx->gl_off.p, (double *)ctx->gm_tab.p,
-                        (double *)ctx->gm_nsc.p, S.bessel_start, glf * K, K, cs);
-      const int tops[TMX_GM_BUCKETS] = {8, 16, 32, 64, TMX_MAX_NB};
-      for (int b = 0; b < 4; ++b) {
-        // (buckets of the m = 0 classes, size (k + 1) / 2, that some order reaches)
-        const int lo = (b == 0) ? 1 : tops[b - 1] + 1;
-        if (lo > (K + 1) / 2 || tops[b] < (kmin + 1) / 2) {
-          continue;
-        }
+      CK(ce);
+      return 0;
+    };
+    cudaGraphNode_t prev_loop = nullptr, prev_round = nullptr;
+    for (int k = kmin; k <= K; ++k) {
+      const int j = k - kmin;
+      const int in = (j & 1) ? 2 : 0;
+      const int out = 2 - in;
+      int32_t *act_in = (int32_t *)((j & 1) ? ctx->act1.p : ctx->act0.p);
+      int32_t *act_out = (int32_t *)((j & 1) ? ctx->act0.p : ctx->act1.p);
+      // ---- loop chain: order step k
+      cudaGraphConditionalHandle hl, hr;
+      CK(cudaGraphConditionalHandleCreate(&hl, graph, 0, cudaGraphCondAssignDefault));
+      cudaGraphNode_t e_node, l_node;
+      if (tmx_gm_add_cond(graph, prev_loop ? &prev_loop : nullptr, prev_loop ? 1 : 0, &e_node,
+                          G, in, hl, prio_hi)) {
+        return fail(ctx, TMX_ERR_CUDA, "graph: step condition node");
+      }
+      auto step_body = [&]() -> int {
+        tmx_launch_gm_begin(G, I, k, glf, m0_sets[j], in, out, cs);
+        tmx_launch_gm_prep(&G->cnt[in], I, act_in, (int)n, (TmxSlot *)ctx->gm_slots.p,
+                           (TmxItem *)ctx->gm_items.p, cs);
+        tmx_launch_tables_dev((const TmxSlot *)ctx->gm_slots.p, (int)n, &G->cnt[in],
+                              &I->ngauss, (const TmxGrain *)ctx->grains.p,
+                              (const double *)ctx->gl_x.p, (const double *)ctx->gl_w.p,
+                              (const int64_t *)ctx->gl_off.p, (double *)ctx->gm_tab.p,
+                              (double *)ctx->gm_nsc.p, S.bessel_start, K, cs);
         TmxBlockArgs B;
         B.items = (const TmxItem *)ctx->gm_items.p;
         B.nitems = (int)(4 * n);
+        B.range = I->m0_range;
         B.slots = (const TmxSlot *)ctx->gm_slots.p;
         B.grains = (const TmxGrain *)ctx->grains.p;
         B.tab = (const double *)ctx->gm_tab.p;
@@ -1251,21 +1304,16 @@ static int gm_compute(tmx_ctx *ctx) {
         B.tout = nullptr;
         B.diag = (cplx *)ctx->gm_diag.p;
         B.status = (int32_t *)ctx->status.p;
-        B.max_nb = std::min(tops[b], (K + 1) / 2);
+        B.max_nb = (k + 1) / 2;
         B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
-        B.family = ctx->dispatch[b];
-        B.gate = &I->bucket;
-        B.gate_value = b;
+        B.family = ctx->dispatch[gm_bucket(B.max_nb)];
         B.max_ctas = 148 * 8;
         tmx_launch_blocks(B, cs);
-      }
-      tmx_launch_converge((const int32_t *)ctx->act0.p, (int)n, (const TmxSlot *)ctx->gm_slots.p,
-                          (const cplx *)ctx->gm_diag.p, (TmxChainState *)ctx->state.p,
-                          S.tolerance, 0, K, (int32_t *)ctx->act1.p, &G->cnt[2],
-                          (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
-                          (int32_t *)ctx->done_pos.p, &G->cnt[1], &G->cnt[0], 0, cs,
-                          &I->order);
-      {
+        tmx_launch_converge(act_in, (int)n, (const TmxSlot *)ctx->gm_slots.p,
+                            (const cplx *)ctx->gm_diag.p, (TmxChainState *)ctx->state.p,
+                            S.tolerance, k, K, act_out, &G->cnt[out], (int32_t *)ctx->done.p,
+                            (int32_t *)ctx->done.p + n, (int32_t *)ctx->done_pos.p,
+                            &G->cnt[1], &G->cnt[in], 0, cs);
         TmxKeepArgs KA;
         KA.done_list = (const int32_t *)ctx->done.p;
         KA.done_ord = (const int32_t *)ctx->done.p + n;
@@ -1274,21 +1322,37 @@ static int gm_compute(tmx_ctx *ctx) {
         KA.next = (int32_t *)ctx->keep_ctl.p;
         KA.ticket = (unsigned *)ctx->keep_ctl.p + 1;
         KA.used = (unsigned long long *)ctx->keep_ctl.p + 1;
-        KA.order0 = 0;
-        KA.base[0] = TmxChainBase{};
+        KA.order0 = k;
+        TmxChainBase &kb = KA.base[0];
+        kb = TmxChainBase{};
+        kb.tab_stride = (int64_t)glf * k * k * TMX_NQ;
+        kb.nsc_stride = (int64_t)glf * k * TMX_NS;
+        kb.diag_stride = 2 * (int64_t)k;
+        kb.scr_stride = 2 * (int64_t)((k + 1) / 2) * ((k + 1) / 2);
         KA.tab = (const double *)ctx->gm_tab.p;
         KA.nsc = (const double *)ctx->gm_nsc.p;
         KA.arena = (double *)ctx->keep_arena.p;
         KA.cap = arena_cap;
         KA.keep_tab = (int64_t *)ctx->keep_tab.p;
         KA.keep_q = (int64_t *)ctx->keep_q.p;
-        KA.order0_dev = &I->order;
-        KA.base_dev = &I->base;
         tmx_launch_keep_tables(KA, (int)n, cs);
+        tmx_launch_gm_step_end(G, snap, outz, j, out, cs);
+        CK(cudaGetLastError());
+        return 0;
+      };
+      if ((rc = add_if(hl, e_node, cs, &l_node, step_body))) {
+        return rc;
       }
-      // round branch: every block of the grains that became final in the
-      // previous iteration, one launch per size bucket side by side
-      {
+      prev_loop = l_node;
+      // ---- round chain: the blocks of the grains final so far
+      CK(cudaGraphConditionalHandleCreate(&hr, graph, 0, cudaGraphCondAssignDefault));
+      cudaGraphNode_t f_node, r_node;
+      const cudaGraphNode_t fdeps[2] = {l_node, prev_round};
+      if (tmx_gm_add_decide(graph, fdeps, prev_round ? 2 : 1, &f_node, G, snap, outz, j,
+                            k == K ? 1 : 0, round_min, round_max, hr, prio_lo)) {
+        return fail(ctx, TMX_ERR_CUDA, "graph: round condition node");
+      }
+      auto round_body = [&]() -> int {
         TmxGmRoundArgs RA;
         RA.G = G;
         RA.done_list = (const int32_t *)ctx->done.p;
@@ -1309,68 +1373,69 @@ static int gm_compute(tmx_ctx *ctx) {
         RA.lu_cap = (unsigned long long)lu_cap;
         tmx_launch_gm_round(RA, rs);
         tmx_launch_gm_round_mid(G, rs);
-      }
-      for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
-        if (bcap[b] == 0) {
-          continue;
+        tmx_launch_gm_tzero(G, (const TmxSlot *)ctx->gm_rslots.p,
+                            (const int64_t *)ctx->gm_tsize.p, (cplx *)ctx->T.p, rs);
+        for (int b = TMX_GM_BUCKETS - 1; b >= 0; --b) {
+          if (bcap[b] == 0) {
+            continue;
+          }
+          cudaStream_t bs = ctx->gm_bs[b];
+          int lrc;
+          if ((lrc = link(rs, bs))) {
+            return lrc;
+          }
+          TmxBlockArgs R;
+          R.items = bitems[b];
+          R.nitems = bcap[b];
+          R.range = &G->rng[b][0];
+          R.slots = (const TmxSlot *)ctx->gm_rslots.p;
+          R.grains = (const TmxGrain *)ctx->grains.p;
+          R.tab = (const double *)ctx->keep_arena.p;
+          R.nsc = (const double *)ctx->keep_arena.p;
+          R.wig = (const double *)ctx->wig.p;
+          R.wig_off = (const int64_t *)ctx->wig_off.p;
+          R.scratch = (cplx *)ctx->gm_luscr.p;
+          R.tout = (cplx *)ctx->T.p;
+          R.diag = nullptr;
+          R.status = (int32_t *)ctx->status.p;
+          R.max_nb = nbmax_b[b];
+          R.chunk_nodes = tmx_host_chunk_nodes(R.max_nb);
+          R.lu = (cplx *)ctx->gm_lu.p;
+          R.family = ctx->dispatch[b];
+          R.max_ctas = TMX_GM_ROUND_CTAS;
+          tmx_launch_blocks(R, bs);
         }
-        cudaStream_t bs = ctx->gm_bs[b];
-        if ((rc = link(rs, bs))) {
-          return rc;
+        // (joined only after every bucket has forked, so that they run
+        // side by side)
+        for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
+          int lrc;
+          if (bcap[b] > 0 && (lrc = link(ctx->gm_bs[b], rs))) {
+            return lrc;
+          }
         }
-        TmxBlockArgs R;
-        R.items = bitems[b];
-        R.nitems = bcap[b];
-        R.range = &G->rng[b][0];
-        R.slots = (const TmxSlot *)ctx->gm_rslots.p;
-        R.grains = (const TmxGrain *)ctx->grains.p;
-        R.tab = (const double *)ctx->keep_arena.p;
-        R.nsc = (const double *)ctx->keep_arena.p;
-        R.wig = (const double *)ctx->wig.p;
-        R.wig_off = (const int64_t *)ctx->wig_off.p;
-        R.scratch = (cplx *)ctx->gm_luscr.p;
-        R.tout = (cplx *)ctx->T.p;
-        R.diag = nullptr;
-        R.status = (int32_t *)ctx->status.p;
-        R.max_nb = nbmax_b[b];
-        R.chunk_nodes = tmx_host_chunk_nodes(R.max_nb);
-        R.lu = (cplx *)ctx->gm_lu.p;
-        R.family = ctx->dispatch[b];
-        R.max_ctas = 148 * 16;
-        tmx_launch_blocks(R, bs);
-        if ((rc = link(bs, rs))) {
-          return rc;
-        }
-      }
-      tmx_launch_qsums((const TmxSlot *)ctx->gm_rslots.p, (int)n, (const cplx *)ctx->T.p,
-                       (double *)ctx->q.p, rs, &G->srng[0], 148 * 4);
-      if ((rc = link(rs, cs))) {
+        tmx_launch_qsums((const TmxSlot *)ctx->gm_rslots.p, (int)n, (const cplx *)ctx->T.p,
+                         (double *)ctx->q.p, rs, &G->srng[0], 148 * 4);
+        tmx_launch_gm_round_end(G, rs);
+        CK(cudaGetLastError());
+        return 0;
+      };
+      if ((rc = add_if(hr, f_node, rs, &r_node, round_body))) {
         return rc;
       }
-      tmx_launch_gm_swap(G, (const int32_t *)ctx->act1.p, (int32_t *)ctx->act0.p, (int)n, cs);
-      tmx_launch_gm_end(G, loop, cs);
-      return 0;
-    };
-    const int crc = capture_body();
-    cudaGraph_t captured = nullptr;
-    const cudaError_t ce = cudaStreamEndCapture(cs, &captured);
-    for (cudaEvent_t e : evs) {
-      cudaEventDestroy(e);
+      prev_round = r_node;
     }
-    if (crc) {
-      return crc;
-    }
-    CK(ce);
-    CK(cudaGraphInstantiate(&ctx->gm_exec, graph, 0));
+    CK(cudaGraphInstantiateWithFlags(&ctx->gm_exec, graph,
+                                     cudaGraphInstantiateFlagUseNodePriority));
     ctx->gm_key = key;
+    ctx->gm_body_kernels[0] = 7;
+    ctx->gm_body_kernels[1] = 5 + nbk;
   }
   // ---- this batch: initial state, the graph, the results
   TmxGState g0 = {};
-  g0.k = kmin;
-  g0.last_order = K;
-  g0.max_iter = K - kmin + 3;
   g0.cnt[0] = ctx->up_nact;
   CK(cudaMemcpyAsync(G, &g0, sizeof(g0), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(snap, 0xff, nsteps * sizeof(int32_t), st));
+  CK(cudaMemsetAsync(outz, 0, nsteps * sizeof(int32_t), st));
   CK(cudaMemcpyAsync(ctx->state.p, ctx->state0.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToDevice, st));
   CK(cudaMemcpyAsync(ctx->act0.p, ctx->actinit.p, ctx->up_nact * sizeof(int32_t),
@@ -1379,23 +1444,49 @@ static int gm_compute(tmx_ctx *ctx) {
   CK(cudaMemsetAsync(ctx->keep_ctl.p, 0, 32, st));
   CK(cudaMemsetAsync(ctx->gm_toff.p, 0xff, n * sizeof(int64_t), st));
   CK(cudaGraphLaunch(ctx->gm_exec, st));
-  LAUNCHED();
+  CK(cudaGetLastError());
+  // the per-grain results and the round items (for the gradients) follow
+  // the graph on the same stream: one synchronisation
   TmxGState g1;
   std::vector<TmxChainState> st0(n);
   std::vector<int64_t> toff(n);
+  std::vector<double> q2(2 * n);
+  std::vector<int32_t> stb(n);
   CK(cudaMemcpyAsync(&g1, G, sizeof(g1), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(st0.data(), ctx->state.p, n * sizeof(TmxChainState),
                      cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(toff.data(), ctx->gm_toff.p, n * sizeof(int64_t),
                      cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(q2.data(), ctx->q.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                     st));
+  CK(cudaMemcpyAsync(stb.data(), ctx->status.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     st));
+  {
+    // every bucket's item array at its capacity, largest bucket first (the
+    // fill counts are known only after the graph)
+    int64_t off = 0;
+    for (int b = TMX_GM_BUCKETS - 1; b >= 0; --b) {
+      if (bcap[b] > 0) {
+        CK(cudaMemcpyAsync((TmxItem *)ctx->gm_allitems.p + off, bitems[b],
+                           bcap[b] * sizeof(TmxItem), cudaMemcpyDeviceToDevice, st));
+      }
+      off += bcap[b];
+    }
+  }
   CK(cudaStreamSynchronize(st));
-  if (g1.overflow || g1.cnt[0] > 0 || g1.round_hi > g1.round_lo) {
-    // storage ran out (or the loop stopped early): grow the estimates and
+  // kernels the graph ran: the two control nodes of every order, the
+  // bodies of the steps and rounds that ran
+  ctx->launches += 2 * (int64_t)nsteps + (int64_t)g1.steps * ctx->gm_body_kernels[0] +
+                   (int64_t)g1.rounds * ctx->gm_body_kernels[1];
+  if (g1.overflow || g1.cnt[1] != ctx->up_nact || g1.round_lo != g1.cnt[1]) {
+    // storage ran out (or a grain was not finished): grow the estimates and
     // compute this batch in the host mode
     ctx->gm_t_hint = std::max<int64_t>(2 * t_cap, (int64_t)g1.t_used + (int64_t)g1.t_used / 4);
     ctx->gm_lu_hint = std::max<int64_t>(2 * lu_cap, (int64_t)g1.lu_used + (int64_t)g1.lu_used / 4);
     return 1;
   }
+  ctx->gm_counts[0] = g1.steps;
+  ctx->gm_counts[1] = g1.rounds;
   for (int64_t i = 0; i < n; ++i) {
     ctx->nmax_h[i] = st0[i].nmax;
     ctx->ngauss_h[i] = st0[i].ngauss;
@@ -1417,37 +1508,19 @@ static int gm_compute(tmx_ctx *ctx) {
   rec.lu = (cplx *)ctx->gm_lu.p;
   rec.scr_total = (int64_t)g1.lu_used;
   {
-    int64_t total = 0;
-    for (int b = 0; b < TMX_GM_BUCKETS; ++b) {
-      total += std::min(g1.fill[b], bcap[b]);
-    }
-    std::vector<TmxItem> items(total);
-    std::vector<TmxSlot> rsl(std::min<int64_t>(g1.nslots, n));
     int64_t off = 0;
     for (int b = TMX_GM_BUCKETS - 1; b >= 0; --b) {
       const int64_t c = std::min(g1.fill[b], bcap[b]);
       if (c > 0) {
-        CK(cudaMemcpyAsync(rec.items + off, bitems[b], c * sizeof(TmxItem),
-                           cudaMemcpyDeviceToDevice, st));
-        CK(cudaMemcpyAsync(items.data() + off, bitems[b], c * sizeof(TmxItem),
-                           cudaMemcpyDeviceToHost, st));
+        rec.seg.push_back({off, off + c, (int64_t)nbmax_b[b]});
       }
-      off += c;
-    }
-    if (!rsl.empty()) {
-      CK(cudaMemcpyAsync(rsl.data(), rec.slots, rsl.size() * sizeof(TmxSlot),
-                         cudaMemcpyDeviceToHost, st));
-    }
-    CK(cudaStreamSynchronize(st));
-    rec.nb.resize(total);
-    for (int64_t i = 0; i < total; ++i) {
-      rec.nb[i] = tmx_host_class_size(rsl[items[i].slot].nmax, items[i].m, items[i].cls);
+      off += bcap[b];
     }
   }
   ctx->rounds_kept.push_back(std::move(rec));
   ctx->gm_last_t = (int64_t)g1.t_used;
   ctx->sink_done = 0;
-  if ((rc = finish_blocks(ctx, (int64_t)g1.t_used, 1))) {
+  if ((rc = finish_blocks(ctx, (int64_t)g1.t_used, 1, &q2, &stb))) {
     return rc;
   }
   ctx->rounds_lu = true;

@@ -35,6 +35,14 @@ void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
                        int bessel_start, int ngmax, int nmax_max,
                        cudaStream_t stream);
 
+// device-driven form: slots [0, min(nslots, *nact)), each with *ng_dev nodes
+// and order <= nmax_max
+void tmx_launch_tables_dev(const TmxSlot *slots, int nslots, const int32_t *nact,
+                           const int32_t *ng_dev, const TmxGrain *grains,
+                           const double *gl_x, const double *gl_w,
+                           const int64_t *gl_off, double *tab, double *nsc,
+                           int bessel_start, int nmax_max, cudaStream_t stream);
+
 void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,
                        const double *gl_x, const int64_t *gl_off, double *out,
                        cudaStream_t stream);
@@ -109,19 +117,20 @@ void tmx_launch_converge(const int32_t *active, int nactive,
 #define TMX_GM_BUCKETS 5
 struct TmxGState {
   unsigned long long t_used, lu_used; // T-matrix and LU storage handed out
-  int32_t k;                          // order of the current iteration
-  int32_t last_order;                 // maximum_order - 1
-  int32_t iter, max_iter;
-  int32_t cnt[3];   // [0] active list length, [1] done-list length, [2] next list
-  int32_t round_lo, round_hi;         // done entries of this iteration's round
+  int32_t cnt[3];   // [0] list A length, [1] done-list length, [2] list B length
+  int32_t loop_done;                  // a step found its input list empty
+  int32_t snap_last;                  // done-list length after the latest step
+  int32_t steps, rounds;              // order steps run, rounds fired
+  int32_t round_lo, round_hi;         // done entries of the current round
   int32_t fill[TMX_GM_BUCKETS];       // items appended per size bucket
-  int32_t rng[TMX_GM_BUCKETS][2];     // this round's items per bucket
-  int32_t nslots, srng[2];            // round slots appended; this round's
+  int32_t rng[TMX_GM_BUCKETS][2];     // the current round's items per bucket
+  int32_t nslots, srng[2];            // round slots appended; the current round's
   int32_t overflow;                   // storage or arena ran out (bit mask)
 };
-// parameters of one iteration, written by k_gm_begin
+// parameters of one order step, written by k_gm_begin
 struct TmxGIter {
   int32_t order, ngauss, wig_n, bucket;
+  int32_t m0_range[2]; // the m = 0 items of the active slots: [0, 4 active)
   TmxChainBase base;
 };
 
@@ -140,15 +149,26 @@ struct TmxGmRoundArgs {
   int64_t *t_off;            // per grain: T-matrix offset
   unsigned long long t_cap, lu_cap;
 };
-void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, const int32_t *m0_sets, int min_order,
-                         int glf, cudaStream_t stream);
-void tmx_launch_gm_prep(const TmxGState *G, const TmxGIter *I, const int32_t *active, int n,
+// lists: `in` / `out` name the counts cnt[in] / cnt[out] of the step's input
+// and output lists
+void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, int k, int glf, int wig_n, int in, int out,
+                         cudaStream_t stream);
+void tmx_launch_gm_prep(const int32_t *nact, const TmxGIter *I, const int32_t *active, int n,
                         TmxSlot *slots, TmxItem *items, cudaStream_t stream);
+void tmx_launch_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out,
+                            cudaStream_t stream);
 void tmx_launch_gm_round(const TmxGmRoundArgs &a, cudaStream_t stream);
 void tmx_launch_gm_round_mid(TmxGState *G, cudaStream_t stream);
-void tmx_launch_gm_swap(const TmxGState *G, const int32_t *next, int32_t *cur, int n,
-                        cudaStream_t stream);
-void tmx_launch_gm_end(TmxGState *G, cudaGraphConditionalHandle loop, cudaStream_t stream);
+void tmx_launch_gm_tzero(const TmxGState *G, const TmxSlot *slots, const int64_t *tsize,
+                         double2 *T, cudaStream_t stream);
+void tmx_launch_gm_round_end(TmxGState *G, cudaStream_t stream);
+// the chains' control kernels as graph kernel nodes (0 or -1)
+int tmx_gm_add_cond(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd, cudaGraphNode_t *node,
+                    TmxGState *G, int in, cudaGraphConditionalHandle h, int priority);
+int tmx_gm_add_decide(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd,
+                      cudaGraphNode_t *node, TmxGState *G, const int32_t *snap,
+                      const int32_t *outz, int j, int last, int thr, int rmax,
+                      cudaGraphConditionalHandle h, int priority);
 
 // copies of the final-order tables of the grains that became final in one
 // group of orders, into the batch's table arena (k_keep_tables)

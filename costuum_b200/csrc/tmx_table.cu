@@ -1116,13 +1116,35 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
     const TmxSlot *slots;
     const double *tab, *nsc;
     cplx *lu;
-    const std::vector<int> *nb;
+    std::vector<std::array<int64_t, 3>> seg; // size buckets: [i0, i1), max class size
     int64_t scr;
+  };
+  // the class-size buckets of a round whose items are sorted by size,
+  // largest first
+  auto segments = [](const std::vector<int> &nb) {
+    std::vector<std::array<int64_t, 3>> seg;
+    const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
+    const int64_t nitems = (int64_t)nb.size();
+    int64_t i0 = 0;
+    for (int b = 0; b < 5; ++b) {
+      int64_t i1 = i0;
+      int mx = 0;
+      while (i1 < nitems && nb[i1] > edges[b + 1]) {
+        mx = std::max(mx, nb[i1]);
+        ++i1;
+      }
+      if (i1 > i0) {
+        seg.push_back({i0, i1, (int64_t)mx});
+      }
+      i0 = i1;
+    }
+    return seg;
   };
   std::vector<RoundView> views;
   if (ctx->rounds_lu) {
     for (const auto &r : ctx->rounds_kept) {
-      views.push_back({r.items, r.slots, r.tab, r.nsc, r.lu, &r.nb, r.scr_total});
+      views.push_back({r.items, r.slots, r.tab, r.nsc, r.lu,
+                       r.seg.empty() ? segments(r.nb) : r.seg, r.scr_total});
     }
   } else {
     if ((rc = ensure(ctx, ctx->lu, std::max<int64_t>(1, ctx->p2_scr_total) * sizeof(cplx)))) {
@@ -1130,7 +1152,7 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
     }
     views.push_back({(const TmxItem *)ctx->p2items.p, (const TmxSlot *)ctx->p2slots.p,
                      (const double *)ctx->p2tab.p, (const double *)ctx->p2nsc.p,
-                     (cplx *)ctx->lu.p, &ctx->p2_nb, ctx->p2_scr_total});
+                     (cplx *)ctx->lu.p, segments(ctx->p2_nb), ctx->p2_scr_total});
   }
   // each round's tangent scratch in its own region: the rounds' size
   // buckets run concurrently
@@ -1162,17 +1184,10 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   int glaunch = 0;
   int64_t scr_off = 0;
   for (const RoundView &v : views) {
-    const int64_t nitems = (int64_t)v.nb->size();
-    // the class-size buckets of the forward schedule (items sorted by size)
-    const int edges[] = {1 << 30, 64, 32, 16, 8, 0};
-    int64_t i0 = 0;
-    for (int b = 0; b < 5; ++b) {
-      int64_t i1 = i0;
-      while (i1 < nitems && (*v.nb)[i1] > edges[b + 1]) {
-        ++i1;
-      }
-      if (i1 > i0) {
-        const int max_nb = (*v.nb)[i0];
+    for (const auto &sg : v.seg) {
+      const int64_t i0 = sg[0], i1 = sg[1];
+      const int max_nb = (int)sg[2];
+      {
         const int gi = glaunch++ % 9;
         cudaStream_t gs = gstreams[gi];
         if (!gused[gi]) {
@@ -1228,7 +1243,6 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
           return rc;
         }
       }
-      i0 = i1;
     }
     scr_off += v.scr;
   }

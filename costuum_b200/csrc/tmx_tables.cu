@@ -136,37 +136,28 @@ __device__ static void bessel_j_complex(int nmax, int nstart, cplx z,
   }
 }
 
-// Grid (slot, node chunk, kind): kind 0 threads do the real-argument tables
-// and node scalars of node g, kind 1 threads the complex-argument tables, so
-// every warp runs one recurrence type.
 // Node scalars follow GaussBasedResources::execute (GaussBasedResources.hpp:
 // 132-152), get_r_dr_spheroid (SpecialFunctions.hpp:872-893) and
 // InteractionTask::execute (InteractionResource.hpp:478-527).
-__global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
-                         const TmxGrain *__restrict__ grains,
-                         const double *__restrict__ gl_x,
-                         const double *__restrict__ gl_w,
-                         const int64_t *__restrict__ gl_off, double *tab,
-                         double *nsc, int bessel_start, int rho_smem) {
-  // ratio buffers: a shared-memory column per thread (rho_smem rows), or
-  // the output slots themselves when the orders exceed rho_smem
-  extern __shared__ cplx trho[];
-  const int s = blockIdx.x;
-  if (s >= nslots) {
-    return;
-  }
-  const TmxSlot sl = slots[s];
+// Tables of node g of one slot; kind 0: real-argument tables and node
+// scalars, kind 1: complex-argument tables. Ratio columns in shared memory,
+// i < rho_smem: the complex recurrence uses the complex entries tid + nt i
+// of trho, the real one the doubles rtid + rnt i.
+__device__ __forceinline__ void table_node(const TmxSlot &sl,
+                                           const TmxGrain *__restrict__ grains,
+                                           const double *__restrict__ gl_x,
+                                           const double *__restrict__ gl_w,
+                                           const int64_t *__restrict__ gl_off,
+                                           double *tab, double *nsc,
+                                           int bessel_start, int rho_smem,
+                                           int g, int kind, cplx *trho, int tid,
+                                           int nt, int rtid, int rnt) {
   const TmxGrain G = grains[sl.grain];
   const int N = sl.nmax;
   const int ng = sl.ngauss;
   const double *x = gl_x + gl_off[ng];
   const double *w = gl_w + gl_off[ng];
-  const int kind = blockIdx.z;
   {
-    const int g = blockIdx.y * blockDim.x + threadIdx.x;
-    if (g >= ng) {
-      return;
-    }
     const double c = x[g];
     const double s2 = (1. - c) * (1. + c);
     const double sn = sqrt(s2);
@@ -209,8 +200,7 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       S[TMX_NS_PAD2] = 0.;
       if (N <= rho_smem) {
         bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
-                      TMX_NQ, reinterpret_cast<double *>(trho) + threadIdx.x,
-                      blockDim.x);
+                      TMX_NQ, reinterpret_cast<double *>(trho) + rtid, rnt);
       } else {
         bessel_j_real(N, bessel_nstart(bessel_start, N, kr), kr, T + TMX_Q_J,
                       TMX_NQ, T + TMX_Q_J, TMX_NQ);
@@ -220,12 +210,71 @@ __global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
       const cplx krmr = mkc(G.mr * G.k * r * G.r_ev, G.mi * G.k * r * G.r_ev);
       const int ns = bessel_nstart(bessel_start, N, hypot(krmr.x, krmr.y));
       if (N <= rho_smem) {
-        bessel_j_complex(N, ns, krmr, T + TMX_Q_JM_RE, TMX_NQ,
-                         trho + threadIdx.x, blockDim.x);
+        bessel_j_complex(N, ns, krmr, T + TMX_Q_JM_RE, TMX_NQ, trho + tid, nt);
       } else {
         bessel_j_complex(N, ns, krmr, T + TMX_Q_JM_RE, TMX_NQ,
                          reinterpret_cast<cplx *>(T + TMX_Q_JM_RE), TMX_NQ / 2);
       }
+    }
+  }
+}
+
+// Grid (slot, node chunk, kind): kind 0 threads do the real-argument tables
+// and node scalars of node g, kind 1 threads the complex-argument tables, so
+// every warp runs one recurrence type.
+__global__ void k_tables(const TmxSlot *__restrict__ slots, int nslots,
+                         const TmxGrain *__restrict__ grains,
+                         const double *__restrict__ gl_x,
+                         const double *__restrict__ gl_w,
+                         const int64_t *__restrict__ gl_off, double *tab,
+                         double *nsc, int bessel_start, int rho_smem) {
+  // ratio buffers: a shared-memory column per thread (rho_smem rows), or
+  // the output slots themselves when the orders exceed rho_smem
+  extern __shared__ cplx trho[];
+  const int s = blockIdx.x;
+  if (s >= nslots) {
+    return;
+  }
+  const TmxSlot sl = slots[s];
+  const int g = blockIdx.y * blockDim.x + threadIdx.x;
+  if (g >= sl.ngauss) {
+    return;
+  }
+  table_node(sl, grains, gl_x, gl_w, gl_off, tab, nsc, bessel_start, rho_smem, g,
+             blockIdx.z, trho, threadIdx.x, blockDim.x, threadIdx.x, blockDim.x);
+}
+
+// Device-driven form (CUDA graph): the slots [0, *nact) of one order, whose
+// count is known only on the device, as tasks of 32 nodes of one slot and
+// one kind, one per warp at a time over a fixed grid; every slot of the
+// launch has *ng_dev nodes. Same arithmetic per node as k_tables. The warps
+// of a CTA may run different kinds, so a thread's real ratios stay inside
+// its own complex column (every other double of it).
+__global__ void k_tables_dev(const TmxSlot *__restrict__ slots, int nslots,
+                             const int32_t *__restrict__ nact,
+                             const int32_t *__restrict__ ng_dev,
+                             const TmxGrain *__restrict__ grains,
+                             const double *__restrict__ gl_x,
+                             const double *__restrict__ gl_w,
+                             const int64_t *__restrict__ gl_off, double *tab,
+                             double *nsc, int bessel_start, int rho_smem) {
+  extern __shared__ cplx trho[];
+  const int ns = min(nslots, *nact);
+  const int ng = *ng_dev;
+  const int nch = (ng + 31) >> 5;
+  const int64_t ntask = (int64_t)ns * nch * 2;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  for (int64_t t = (int64_t)blockIdx.x * wpb + (threadIdx.x >> 5); t < ntask;
+       t += (int64_t)gridDim.x * wpb) {
+    const int s = (int)(t / (2 * nch));
+    const int rem = (int)(t - (int64_t)s * 2 * nch);
+    const int kind = rem & 1;
+    const int g = (rem >> 1) * 32 + lane;
+    const TmxSlot sl = slots[s];
+    if (g < sl.ngauss) {
+      table_node(sl, grains, gl_x, gl_w, gl_off, tab, nsc, bessel_start, rho_smem, g,
+                 kind, trho, threadIdx.x, blockDim.x, 2 * threadIdx.x, 2 * blockDim.x);
     }
   }
 }
@@ -346,6 +395,33 @@ void tmx_launch_tables(const TmxSlot *slots, int nslots, const TmxGrain *grains,
   k_tables<<<grid, threads, smem, stream>>>(slots, nslots, grains, gl_x, gl_w,
                                             gl_off, tab, nsc, bessel_start,
                                             rho_smem);
+}
+
+void tmx_launch_tables_dev(const TmxSlot *slots, int nslots, const int32_t *nact,
+                           const int32_t *ng_dev, const TmxGrain *grains,
+                           const double *gl_x, const double *gl_w,
+                           const int64_t *gl_off, double *tab, double *nsc,
+                           int bessel_start, int nmax_max, cudaStream_t stream) {
+  if (nslots <= 0) {
+    return;
+  }
+  // two warps per CTA; ratios in shared memory for orders up to 48
+  const int threads = 64;
+  const int rho_smem = std::max(1, std::min(48, nmax_max));
+  const size_t smem = (size_t)threads * rho_smem * sizeof(cplx);
+  static int attr_dev = -1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_tables_dev, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(64 * 48 * sizeof(cplx)));
+    attr_dev = dev;
+  }
+  // resident CTAs only (shared memory allows four per SM at orders >= 48)
+  const int blocks = 148 * 4;
+  k_tables_dev<<<blocks, threads, smem, stream>>>(slots, nslots, nact, ng_dev, grains,
+                                                  gl_x, gl_w, gl_off, tab, nsc,
+                                                  bessel_start, rho_smem);
 }
 
 void tmx_launch_wigner(const TmxWigJob *jobs, int njobs, int max_work,

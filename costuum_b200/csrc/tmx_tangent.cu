@@ -213,7 +213,8 @@ __global__ void __launch_bounds__(NT, MINB)
   const int m = item.m;
   const ClassDesc D = describe<TR>(N, m, item.cls);
   const int nb = D.nb;
-  if (nb <= 0 || nb > TMX_MAX_NB) {
+  // (shared memory is sized for classes of at most max_nb members)
+  if (nb <= 0 || nb > TMX_MAX_NB || nb > A.max_nb) {
     return;
   }
   const double *T = A.tab + sl.tab;

@@ -1,5 +1,5 @@
 """Device-driven batches (TMX_BATCH_GRAPH): the order loop and its block
-rounds as one CUDA graph whose WHILE node runs on the GPU.
+rounds as one CUDA graph of conditional nodes that the GPU runs by itself.
 
 The graph mode runs the same kernels on the same tables as the host-driven
 loop, only scheduled by the device, so every result must equal the host
@@ -7,9 +7,11 @@ mode's bit for bit: final orders, status bits, the six per-grain sums, every
 T-matrix and the gradients (which reuse the LU factors the graph's rounds
 kept). Covered: the bench distribution (orders up to 32, every size bucket
 up to 17..32 members), repeated batches on one context (the graph is built
-once per batch shape and reused), and a low maximum_order at which most
-grains stop unconverged at the last order (the loop's exit with grains still
-in flight and the final round after it).
+once per batch shape and reused) and a batch after another one of other
+grains (nothing may depend on what an earlier batch left in the buffers),
+and a low maximum_order at which most grains stop unconverged at the last
+order (the loop's exit with grains still in flight and the final round
+after it).
 """
 import numpy as np
 import pytest
@@ -24,10 +26,14 @@ SCHEDULE = dict(min_order=10, max_order=100, gauss_legendre_factor=2,
                 tolerance=1e-4)
 
 
-def _run(mode, r, lam, m, d, sched, reps=1):
+def _run(mode, r, lam, m, d, sched, reps=1, before=None):
     c = Context(0)
     try:
         c.set_batch_mode(mode)
+        if before is not None:
+            # another batch first: the compared one must not depend on what
+            # an earlier batch left in the context's buffers
+            c.tmatrix_batch(*before, **sched)
         out = []
         for _ in range(reps):
             res = c.tmatrix_batch(r, lam, m, d, **sched)
@@ -60,6 +66,16 @@ def test_graph_equals_host_bench_distribution():
         assert g["mode"] == Context.BATCH_GRAPH
         _same(g, host)
     assert (host["status"] == 0).all()
+
+
+def test_graph_after_other_batches_equals_host():
+    r, lam, m, d = H.config2_sample(1024, 34)
+    other = H.config2_sample(1500, 35)
+    host = _run(Context.BATCH_HOST, r, lam, m, d, SCHEDULE)[0]
+    graph = _run(Context.BATCH_GRAPH, r, lam, m, d, SCHEDULE, reps=2, before=other)
+    for g in graph:
+        assert g["mode"] == Context.BATCH_GRAPH
+        _same(g, host)
 
 
 def test_graph_equals_host_unconverged_at_last_order():

@@ -218,6 +218,45 @@ def flush_l2(buf):
     buf.zero_()
 
 
+BUCKETS = ["nb<=8", "9..16", "17..32", "33..64", "65..128"]
+
+
+def class_size(N, m, cls):
+    """Members of parity class `cls` of block m at order N (the work items of
+    the block kernels)."""
+    if m == 0:
+        n0 = 1 if cls & 1 else 2
+        return (N - n0) // 2 + 1 if N >= n0 else 0
+    na0 = m if (m & 1) == cls else m + 1
+    nb0 = m if (m & 1) == (cls ^ 1) else m + 1
+    r0 = (N - na0) // 2 + 1 if N >= na0 else 0
+    r1 = (N - nb0) // 2 + 1 if N >= nb0 else 0
+    return r0 + r1
+
+
+def bucket_flops(nmax, ngauss):
+    """Executed-flop model of the block kernels per class-size bucket for
+    every (m, class) item of the grains at their orders: assembly
+    8 t nb^2 ng (t = 2 terms for m = 0, 4 otherwise), LU 8/3 nb^3, the two
+    triangular solves 8 nb^3; and the items per bucket."""
+    fl = np.zeros(5)
+    cnt = np.zeros(5, np.int64)
+    orders, counts = np.unique(np.stack([nmax, ngauss], 1), axis=0, return_counts=True)
+    for (N, ng), c in zip(orders, counts):
+        if N <= 0:
+            continue
+        for m in range(N + 1):
+            for cls in range(4 if m == 0 else 2):
+                nb = class_size(int(N), m, cls)
+                if nb <= 0:
+                    continue
+                b = 0 if nb <= 8 else 1 if nb <= 16 else 2 if nb <= 32 else 3 if nb <= 64 else 4
+                t = 2.0 if m == 0 else 4.0
+                fl[b] += c * (8 * t * nb * nb * ng + (8.0 / 3.0) * nb ** 3 + 8.0 * nb ** 3)
+                cnt[b] += c
+    return fl, cnt
+
+
 def workload_config():
     """The workload both arms name in their JSON line."""
     return {"workload": "batched T-matrices, config-2 distribution "
@@ -347,17 +386,20 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         step_device()
-    # ---- device-resident timed region
+    # ---- device-resident timed region (no per-launch events in it: the
+    # kernel profile below runs on separate, untimed steps)
     sampler = ClockSampler(local)
     sampler.start()
-    lib.tmx_profile_enable(h, 1)
     launches0 = ctx.kernel_launches
     dist.barrier()
     torch.cuda.synchronize()
     total = 0.0
     host_t = []
+    step_ms = []
     for _ in range(args.steps):
-        total += step_device()
+        t = step_device()
+        step_ms.append(t)
+        total += t
         ht = np.zeros(4)
         lib.tmx_batch_host_times(h, P(ht))
         host_t.append(ht)
@@ -365,6 +407,20 @@ def run_ours(args):
     dist.barrier()
     launches = ctx.kernel_launches - launches0
     clocks = sampler.stop()
+    # ---- the same batch in the device-driven mode (one CUDA graph, no host
+    # synchronisation before the end of the batch), timed the same way
+    ctx.set_batch_mode(Context.BATCH_GRAPH)
+    for _ in range(max(2, args.warmup)):
+        step_device()
+    graph_ms = [step_device() for _ in range(args.steps)]
+    graph_mode_ok = ctx.last_batch_mode == Context.BATCH_GRAPH
+    ctx.set_batch_mode(Context.BATCH_HOST)
+    # ---- kernel profile: the same steps again with CUDA events around every
+    # block and table launch and the launch timeline (untimed)
+    lib.tmx_profile_enable(h, 1)
+    prof_total = 0.0
+    for _ in range(args.steps):
+        prof_total += step_device()
     bk_ms = np.zeros(1)
     bk_n = ctypes.c_int64()
     bk_fl = np.zeros(1)
@@ -569,19 +625,35 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.skip_extras:
         avg = averaging_leg(ctx, lib, dmma)
 
-    # roofline of the dominant kernel (block kernels: assembly + LU + solve),
-    # algorithmic flops of the per-grain model (every chain order and every
-    # m block as a full 2nb x 2nb assembly, LU and solve) over the summed
-    # CUDA-event time of the block launches
-    # DRAM bytes (read + write) per block launch from one ncu capture of
-    # this command (--steps 1 --warmup 3 --skip-cpu --skip-extras, metrics
-    # dram__bytes_read.sum and dram__bytes_write.sum): the mean over the 38
-    # block launches of the timed step, with L2 flushed before each launch
-    BLOCK_TRAFFIC_PER_LAUNCH = 30.76e6
-    bk_launches = max(1, bk_n.value)
+    # Roofline of the dominant kernel. The block launches of a live step
+    # overlap on several streams, so their event times are not kernel
+    # durations; the tuning pass above times each size bucket's launch alone
+    # (all of the bucket's items of the 4096 grains at their converged
+    # orders, one launch, CUDA events, serialised). The dominant kernel is
+    # the bucket launch with the longest time under the tuned table;
+    # achieved = its executed-flop model (bucket_flops) / that time. The step
+    # figure (model flops of the whole step over the step time) is beside it.
+    # DRAM bytes per item of the dominant kernel from one ncu capture of that
+    # launch on a 1024-grain case (profiles/k_blocks_warp_dmma_fixed_1024.md),
+    # scaled by its item count (traffic grows with the items: every item
+    # reads its own table rows and writes its own T block).
+    DMMA_BYTES_PER_ITEM = 10.29e3
     bk_s = bk_ms[0] * 1e-3
-    achieved = flops_survey * args.steps / bk_s / 1e12 if bk_s > 0 else 0.0
     executed = bk_fl[0] / bk_s / 1e12 if bk_s > 0 else 0.0
+    dominant, buckets_roof = None, []
+    if autotune is not None:
+        bfl, bcnt = bucket_flops(conv.nmax, conv.ngauss)
+        for b in range(5):
+            fam = table[b]
+            ms = float(tune_ms[b][fam])
+            if bcnt[b] == 0 or ms <= 0:
+                continue
+            row = {"bucket": BUCKETS[b], "family": Context.FAMILIES[fam],
+                   "items": int(bcnt[b]), "ms": ms, "gflop": bfl[b] / 1e9,
+                   "tflops": bfl[b] / (ms * 1e-3) / 1e12}
+            buckets_roof.append(row)
+            if dominant is None or ms > dominant["ms"]:
+                dominant = row
     out = None
     if rank == 0:
         cpu = None
@@ -604,28 +676,47 @@ def run_ours(args):
                             "T-matrix in host memory (tmatrices(), streamed "
                             "by the block rounds) + per-grain results"},
             "roofline": {"bound": "tensor",
-                         "kernel": "block kernels (k_blocks_warp, k_blocks): "
-                                   "assembly + LU + solve",
-                         "achieved": achieved, "peak": dmma,
-                         "unit": "TFLOP/s", "frac": achieved / dmma,
-                         "peak_kind": "measured FP64 DMMA (mma.sync m8n8k4 f64) "
-                                      "this run; DFMA peak %.1f" % dfma,
-                         "flops_model": "per-grain model: chain orders "
-                                        "F_asm(k,2k,4)+F_lu(2k)+F_solve(2k), m "
-                                        "blocks F_asm(N+1-m,2N,10)+F_lu+F_solve",
+                         "kernel": ("k_blocks_warp %s, classes %s: assembly + LU "
+                                    "+ solve" % (dominant["family"], dominant["bucket"])
+                                    if dominant else "block kernels"),
+                         "achieved": dominant["tflops"] if dominant else None,
+                         "peak": dmma, "unit": "TFLOP/s",
+                         "frac": dominant["tflops"] / dmma if dominant else None,
+                         "peak_kind": "measured FP64 DMMA (mma.sync m8n8k4 f64) this run "
+                                      "(of measured); DFMA peak %.1f" % dfma,
+                         "launch_ms": dominant["ms"] if dominant else None,
+                         "what": "one launch of the bucket's items of the 4096 grains "
+                                 "at their converged orders, timed alone with CUDA "
+                                 "events (tuning pass); executed-flop model",
+                         "buckets": buckets_roof,
+                         "traffic": (DMMA_BYTES_PER_ITEM * dominant["items"]
+                                     if dominant and dominant["family"] == "warp_dmma"
+                                     else None),
+                         "traffic_unit": "DRAM bytes per launch (ncu per-item figure "
+                                         "of a 1024-grain capture x items)",
+                         "flops_model_step": "per-grain model: chain orders "
+                                             "F_asm(k,2k,4)+F_lu(2k)+F_solve(2k), m "
+                                             "blocks F_asm(N+1-m,2N,10)+F_lu+F_solve",
                          "flops_per_step": flops_survey,
-                         "executed_tflops": executed,
-                         # launches of several streams overlap, so their summed
-                         # event time exceeds the step; the model flops over the
-                         # step time is the rate the whole step sustains
                          "step_tflops": flops_survey / (ms_step * 1e-3) / 1e12,
-                         "step_frac": flops_survey / (ms_step * 1e-3) / 1e12 / dmma,
-                         "launches": int(bk_n.value),
-                         "share_of_step": bk_ms[0] / max(total, 1e-9),
-                         "traffic": BLOCK_TRAFFIC_PER_LAUNCH,
-                         "traffic_unit": "bytes per block launch (ncu, cold L2)"},
-            "phases_ms_per_step": {"blocks": bk_ms[0] / args.steps,
-                                   "tables": tb_ms[0] / args.steps},
+                         "step_frac": flops_survey / (ms_step * 1e-3) / 1e12 / dmma},
+            "device_driven": {
+                "ms_per_step": float(np.median(graph_ms)),
+                "value": world * N_GRAINS / (float(np.median(graph_ms)) * 1e-3),
+                "mode_ok": bool(graph_mode_ok),
+                "host_syncs_per_batch": 1,
+                "what": "the same batch as one CUDA graph of conditional nodes "
+                        "(order steps and block rounds decided on the device), "
+                        "median of the same number of steps"},
+            "profiled_pass": {
+                "ms_per_step": prof_total / args.steps,
+                "block_launches": int(bk_n.value),
+                "block_event_ms_per_step": bk_ms[0] / args.steps,
+                "executed_tflops_over_event_time": executed,
+                "what": "the same steps again with CUDA events around every "
+                        "block and table launch (untimed); block launches "
+                        "overlap, so their summed event time exceeds the step"},
+            "phases_ms_per_step": {"tables": tb_ms[0] / args.steps},
             # host side of the timed steps (medians): the batch call's wall
             # time, the time it blocked on the order loop's events and the
             # final synchronisation, and its host set-up of block rounds

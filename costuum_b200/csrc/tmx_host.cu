@@ -183,6 +183,8 @@ static_assert(TMX_FAMILY_WARP_DFMA == TMX_BLOCKS_WARP_DFMA &&
 // largest class size of each dispatch bucket
 static const int kBucketTop[TMX_DISPATCH_BUCKETS] = {8, 16, 32, 64, TMX_MAX_NB};
 static const int32_t kDefaultDispatch[TMX_DISPATCH_BUCKETS] = {0, 1, 2, 3, 4};
+static const char *const kFamilyNames[TMX_DISPATCH_FAMILIES] = {"warp_dfma", "warp_dmma",
+                                                                "cta32", "cta64", "cta"};
 
 int tmx_host_class_size(int N, int m, int cls) {
   if (m == 0) {
@@ -2189,6 +2191,9 @@ int tmx_autotune(tmx_ctx *ctx, int64_t n, const double *r_ev,
     if (!any) {
       continue;
     }
+    // (a named range per family, so that a profiler can pick its launches)
+    const std::string range_name = "tmx_autotune_" + std::string(kFamilyNames[f]);
+    NvtxRange family_range(range_name.c_str());
     // one untimed batch, then reps timed ones
     for (int r = 0; r <= reps && rc == TMX_OK; ++r) {
       drop_tune_events(ctx);

@@ -201,8 +201,13 @@ struct tmx_ctx {
   DevBuf lu, dT, tscr, dTa, dS; // tangent buffers
   int o_nsj = 0, o_nqj = 0;     // per-grain observable job counts
   // events that order a free on `stream` after the work queued so far on the
-  // round streams and their bucket streams (stream2, stream3, aux[0..5])
-  cudaEvent_t drain_ev[8] = {};
+  // round streams, their bucket streams (stream2, stream3, aux[0..5]) and
+  // the copy stream
+  cudaEvent_t drain_ev[9] = {};
+  // device-to-host copies of streamed T-matrices (created with the first
+  // sink copy): a round's copy waits for the round, the rounds that follow
+  // on the same round stream do not wait for the copy
+  cudaStream_t copy_stream = nullptr;
   // page-locked host destination of the T-matrices (tmx_set_tmatrix_sink):
   // every block round copies its T range there as soon as its blocks are
   // done; sink_done = complex elements [0, sink_done) already copied for the
@@ -245,9 +250,10 @@ struct tmx_ctx {
 // block to the next allocation as soon as the free is complete in stream
 // order, so the free must come after those readers.
 static inline int order_after_rounds(tmx_ctx *ctx) {
-  cudaStream_t others[8] = {ctx->stream2, ctx->stream3, ctx->aux[0], ctx->aux[1],
-                            ctx->aux[2],  ctx->aux[3],  ctx->aux[4], ctx->aux[5]};
-  for (int i = 0; i < 8; ++i) {
+  cudaStream_t others[9] = {ctx->stream2, ctx->stream3, ctx->aux[0], ctx->aux[1],
+                            ctx->aux[2],  ctx->aux[3],  ctx->aux[4], ctx->aux[5],
+                            ctx->copy_stream};
+  for (int i = 0; i < 9; ++i) {
     if (!others[i]) {
       continue;
     }

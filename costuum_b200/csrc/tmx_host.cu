@@ -404,6 +404,9 @@ void tmx_destroy(tmx_ctx *ctx) {
       cudaStreamDestroy(x);
     }
   }
+  if (ctx->copy_stream) {
+    cudaStreamDestroy(ctx->copy_stream);
+  }
   if (ctx->pool) {
     cudaMemPoolDestroy(ctx->pool);
   }
@@ -844,14 +847,31 @@ static int run_blocks_round(tmx_ctx *ctx, const std::vector<int32_t> &p2,
   }
   tmx_launch_qsums(dslots, np2, (const cplx *)ctx->T.p, (double *)ctx->q.p, st);
   LAUNCHED();
-  // the round's T-matrices to the caller's page-locked sink, on the round's
-  // stream: the copy overlaps the order loop and the rounds that follow
+  // the round's T-matrices to the caller's page-locked sink, on the copy
+  // stream once the round is done: the copy overlaps the order loop and the
+  // rounds that follow, which do not wait for it (the batch's end does)
   if (ctx->sink && t_base == ctx->sink_done && t_total <= ctx->sink_cap &&
       t_total > t_base) {
+    if (!ctx->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    }
+    cudaEvent_t done;
+    CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CK(cudaEventRecord(done, st));
+    CK(cudaStreamWaitEvent(ctx->copy_stream, done, 0));
+    CK(cudaEventDestroy(done));
     CK(cudaMemcpyAsync(ctx->sink + 2 * t_base, (const cplx *)ctx->T.p + t_base,
                        (t_total - t_base) * sizeof(cplx), cudaMemcpyDeviceToHost,
-                       st));
+                       ctx->copy_stream));
     ctx->sink_done = t_total;
+    if (st == ctx->stream) {
+      // a round on the library stream ends its batch (a single round, or
+      // the last one): the batch's synchronisation covers the copy
+      CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+      CK(cudaEventRecord(done, ctx->copy_stream));
+      CK(cudaStreamWaitEvent(st, done, 0));
+      CK(cudaEventDestroy(done));
+    }
   }
   if (temp && ctx->keep_rounds) {
     tmx_ctx::RoundRec rec;
@@ -2041,6 +2061,10 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   CK(cudaStreamWaitEvent(st, rounds_done, 0));
   CK(cudaEventRecord(rounds_done, ctx->stream3));
   CK(cudaStreamWaitEvent(st, rounds_done, 0));
+  if (ctx->copy_stream) {
+    CK(cudaEventRecord(rounds_done, ctx->copy_stream));
+    CK(cudaStreamWaitEvent(st, rounds_done, 0));
+  }
   CK(cudaEventDestroy(rounds_done));
   if ((rc = finish_blocks(ctx, t_next, rounds + 1))) {
     return rc;
@@ -2357,6 +2381,9 @@ int tmx_set_tmatrix_sink(tmx_ctx *ctx, double *host, int64_t capacity) {
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream2));
   CK(cudaStreamSynchronize(ctx->stream3));
+  if (ctx->copy_stream) {
+    CK(cudaStreamSynchronize(ctx->copy_stream));
+  }
   ctx->sink = host;
   ctx->sink_cap = host ? capacity : 0;
   ctx->sink_done = 0;

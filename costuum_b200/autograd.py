@@ -57,7 +57,10 @@ class Extinction(torch.autograd.Function):
         # rounds kept their LU factors: only the tangent kernels run
         _, dq = tm.gradients(th, c)
         g = grad.detach().cpu().numpy().astype(np.float64)
-        gp = np.einsum("ntk,ntkp->np", g, dq)
+        # sum over angles and coefficients of grad * dq, per grain and
+        # parameter (one batched matrix-vector product)
+        n = g.shape[0]
+        gp = np.matmul(g.reshape(n, 1, -1), dq.reshape(n, -1, dq.shape[-1]))[:, 0, :]
         return (torch.as_tensor(gp, dtype=grad.dtype, device=grad.device),
                 None, None, None, None)
 

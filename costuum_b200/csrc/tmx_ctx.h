@@ -176,6 +176,9 @@ struct tmx_ctx {
     std::vector<double> thetas, coeffs;
     bool has_coeffs = false;
   } obs_key;
+  // o_S holds the amplitudes of the batch's T-matrices under the plan of
+  // obs_key (tmx_batch_observables); the gradients of the same plan reuse them
+  bool obs_s_valid = false;
   std::vector<int32_t> nmax_h, ngauss_h, status_h;
   std::vector<double> q_h;
   std::vector<int64_t> t_off_h;

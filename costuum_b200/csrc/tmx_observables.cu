@@ -741,16 +741,24 @@ void tmx_launch_orient_pairs(const TmxObsGrain *og, const int64_t *pstart,
   const size_t smem = (size_t)8 * wcap * nmat * sizeof(double2);
   const int64_t want = (npairs + 7) / 8;
   const int blocks = (int)std::min<int64_t>(want, 148 * 8);
-  if (nmat == 4) {
-    // four warps per CTA: the four matrices' buffers of 8 warps would
-    // leave room for one CTA per SM
+  if (nmat == 4 || nmat == 3) {
+    // four warps per CTA: the matrices' buffers of 8 warps would leave room
+    // for one CTA per SM
     const size_t smem4 = (size_t)4 * wcap * nmat * sizeof(double2);
     const int blocks4 = (int)std::min<int64_t>((npairs + 3) / 4, 148 * 16);
-    cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem4);
-    k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pstart, order, pmax, npairs,
-                                                       mats, coeffs, ncoef, cg_off, cg,
-                                                       cg_nmax, wcap, fold);
+    if (nmat == 4) {
+      cudaFuncSetAttribute(k_orient_pairs<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem4);
+      k_orient_pairs<4><<<blocks4, 128, smem4, stream>>>(og, pstart, order, pmax, npairs,
+                                                         mats, coeffs, ncoef, cg_off, cg,
+                                                         cg_nmax, wcap, fold);
+    } else {
+      cudaFuncSetAttribute(k_orient_pairs<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem4);
+      k_orient_pairs<3><<<blocks4, 128, smem4, stream>>>(og, pstart, order, pmax, npairs,
+                                                         mats, coeffs, ncoef, cg_off, cg,
+                                                         cg_nmax, wcap, fold);
+    }
   } else {
     cudaFuncSetAttribute(k_orient_pairs<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
@@ -774,6 +782,11 @@ int tmx_amp_grid(int nbmax, int nmat) {
                          (int)amp_smem(TMX_MAX_NB, 4));
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<4>, 256,
                                                   amp_smem(nbmax, 4));
+  } else if (nmat == 3) {
+    cudaFuncSetAttribute(k_amp<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)amp_smem(TMX_MAX_NB, 3));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_amp<3>, 256,
+                                                  amp_smem(nbmax, 3));
   } else {
     cudaFuncSetAttribute(k_amp<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)amp_smem(TMX_MAX_NB, 1));
@@ -804,6 +817,10 @@ void tmx_launch_amp(const TmxAmpGroup *groups, int ngroups, const TmxSJob *jobs,
   const int blocks = std::min(grid, ngroups);
   if (nmat == 4) {
     k_amp<4><<<blocks, 256, amp_smem(nbmax, 4), stream>>>(groups, ngroups, jobs, og,
+                                                          mats, angles, phis, xslot,
+                                                          nbmax, wpi, wtau, wnmax);
+  } else if (nmat == 3) {
+    k_amp<3><<<blocks, 256, amp_smem(nbmax, 3), stream>>>(groups, ngroups, jobs, og,
                                                           mats, angles, phis, xslot,
                                                           nbmax, wpi, wtau, wnmax);
   } else {

@@ -844,6 +844,7 @@ extern "C" int tmx_get_table(
                          cudaMemcpyHostToDevice, st));
     }
     if ((rc = upload_obs_plan(ctx, og, sj)) ||
+        (ctx->obs_s_valid = false, false) ||
         (rc = run_amplitudes(ctx, (const cplx *)ctx->T.p, t_total, ncoef,
                              (cplx *)ctx->o_S.p, s_total))) {
       return rc;
@@ -960,6 +961,7 @@ int batch_observable_setup(tmx_ctx *ctx, int ntheta, const double *thetas,
     return TMX_OK;
   }
   key.valid = false;
+  ctx->obs_s_valid = false;
   std::vector<TmxAngle> ang(ntheta);
   for (int i = 0; i < ntheta; ++i) {
     ang[i] = make_angle(cos(thetas[i]));
@@ -1073,10 +1075,12 @@ extern "C" int tmx_batch_observables(tmx_ctx *ctx, int32_t ntheta,
       (rc = ensure(ctx, ctx->o_gq, std::max<int64_t>(1, n * ntheta * 3) * sizeof(double)))) {
     return rc;
   }
+  ctx->obs_s_valid = false;
   if ((rc = batch_amplitudes(ctx, (const cplx *)ctx->T.p, ntheta, ncoef,
                              (cplx *)ctx->o_S.p))) {
     return rc;
   }
+  ctx->obs_s_valid = true;
   CK(cudaMemsetAsync(ctx->o_gq.p, 0, n * ntheta * 3 * sizeof(double), st));
   tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
                         (const TmxObsGrain *)ctx->o_og.p, (const cplx *)ctx->o_S.p,
@@ -1258,23 +1262,29 @@ extern "C" int tmx_batch_gradients(tmx_ctx *ctx, int32_t ntheta,
   }
   cplx *S = (cplx *)ctx->dS.p;
   const int64_t sz = n * ntheta * 4;
+  // the T-matrices' own amplitudes: those of tmx_batch_observables when it
+  // ran on this batch with the same plan (still in o_S), else computed here
+  const bool have_s = ctx->obs_s_valid;
+  const cplx *S0 = have_s ? (const cplx *)ctx->o_S.p : S;
   {
-    // T and its three tangents in one pass (shared angle and coupling work)
+    // the three tangents (and T) in one pass (shared angle and coupling work)
     const cplx *src[4] = {(const cplx *)ctx->T.p, (const cplx *)ctx->dT.p,
                           (const cplx *)ctx->dT.p + tt, (const cplx *)ctx->dT.p + 2 * tt};
     cplx *dst[4] = {S, S + sz, S + 2 * sz, S + 3 * sz};
-    if ((rc = run_amplitudes(ctx, src, 4, ctx->p2_t_total, ncoef, dst, n * ntheta))) {
+    const int k0 = have_s ? 1 : 0;
+    if ((rc = run_amplitudes(ctx, src + k0, 4 - k0, ctx->p2_t_total, ncoef, dst + k0,
+                             n * ntheta))) {
       return rc;
     }
   }
   CK(cudaMemsetAsync(ctx->o_gq.p, 0, n * ntheta * 3 * sizeof(double), st));
   CK(cudaMemsetAsync(ctx->o_gz.p, 0, n * ntheta * 12 * sizeof(double), st));
   tmx_launch_q_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
-                        (const TmxObsGrain *)ctx->o_og.p, S, nullptr, 0,
+                        (const TmxObsGrain *)ctx->o_og.p, S0, nullptr, 0,
                         (double *)ctx->o_gq.p, 3, 0, 1, st);
   LAUNCHED();
   tmx_launch_dq_epilogue((const TmxQJob *)ctx->o_qj.p, ctx->o_nqj,
-                         (const TmxObsGrain *)ctx->o_og.p, S, S + sz, S + 2 * sz,
+                         (const TmxObsGrain *)ctx->o_og.p, S0, S + sz, S + 2 * sz,
                          S + 3 * sz, (double *)ctx->o_gz.p, st);
   LAUNCHED();
   if (q) {
@@ -1478,6 +1488,7 @@ int plain_amplitudes(tmx_ctx *ctx, const std::vector<int32_t> &grain,
                        cudaMemcpyHostToDevice, st));
   }
   if ((rc = upload_obs_plan(ctx, og, sj)) ||
+      (ctx->obs_s_valid = false, false) ||
       (rc = run_amplitudes(ctx, (const cplx *)ctx->T.p, ctx->p2_t_total, 1,
                            (cplx *)ctx->o_S.p, nj))) {
     return rc;

@@ -285,3 +285,32 @@ def test_observable_plan_reuse():
         assert np.array_equal(got[1], want2[1])
     finally:
         ctx.close()
+
+
+def test_gradients_reuse_forward_amplitudes():
+    """After observables() on the same batch, angles and coefficients, the
+    gradient pass takes the T-matrices' amplitudes from that call and runs
+    the observable kernels on the three tangents only: q must then equal
+    observables() exactly, and q and dq must agree with a gradient pass that
+    computes all four (within 1e-12 of each coefficient's scale: the same
+    arithmetic per matrix, in kernels compiled for three or four)."""
+    from costuum_b200.tmatrix import Context
+    r, lam, m, d = H.config2_sample(256, 41)
+    co = _coeffs(2, 0.5)
+    c = Context(0)
+    try:
+        c.tmatrix_batch(r, lam, m, d, min_order=10, max_order=100,
+                        gauss_legendre_factor=2, tolerance=1e-4)
+        q_all, dq_all = c.gradients(THETAS, co)
+        q_all, dq_all = q_all.copy(), dq_all.copy()
+        c.tmatrix_batch(r, lam, m, d, min_order=10, max_order=100,
+                        gauss_legendre_factor=2, tolerance=1e-4)
+        q_obs = c.observables(THETAS, co).copy()
+        q_re, dq_re = c.gradients(THETAS, co)
+    finally:
+        c.close()
+    assert np.array_equal(q_re, q_obs)
+    scale_q = np.abs(q_all).max(axis=1, keepdims=True) + 1e-300
+    assert (np.abs(q_re - q_all) <= 1e-12 * scale_q).all()
+    scale = np.abs(dq_all).max(axis=(1, 2), keepdims=True) + 1e-300
+    assert (np.abs(dq_re - dq_all) <= 1e-12 * scale).all()

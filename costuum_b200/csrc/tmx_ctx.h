@@ -164,8 +164,12 @@ struct tmx_ctx {
   cudaStream_t gm_cs = nullptr, gm_rs = nullptr, gm_bs[TMX_GM_BUCKETS] = {};
   int64_t gm_t_hint = 0, gm_lu_hint = 0;
   int64_t gm_last_t = 0;
-  int gm_body_kernels[2] = {0, 0}; // kernels of one order step and of one round
   int gm_counts[2] = {0, 0};       // the last graph batch's order steps and rounds
+  // largest final order of the last batch and its schedule (min order, last
+  // order, Gauss-Legendre factor, tolerance): the device-driven graph's extent
+  int kmax_seen = 0;
+  int kmax_sched[3] = {0, 0, 0};
+  double kmax_tol = -1.;
   // host-side times of the last tmx_batch_compute (ms): wall time, time
   // blocked on the order loop's events and the final synchronisation, host
   // set-up of block rounds, and the number of order groups

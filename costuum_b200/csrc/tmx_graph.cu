@@ -11,19 +11,25 @@
 // The graph has two chains of conditional (IF) nodes, one node of each per
 // order k = min_order .. maximum_order - 1:
 //   loop chain (high priority)
-//     k_gm_cond       whether step k runs (a grain is still active)
+//     k_gm_cond       which form of step k runs, if any (a grain is still
+//                     active and k is not inside an earlier group of orders):
+//                     one order, or with few grains left 4 or 8 orders at
+//                     once as the host-driven loop speculates
 //     IF step k:      k_gm_begin (step parameters, next list emptied),
 //                     k_gm_prep (slots and m = 0 items of the active list),
 //                     k_tables_dev, the m = 0 block launch, k_converge,
 //                     k_keep_tables, k_gm_step_end (snapshot of the done list)
-//   round chain (low priority), node k after step k and round k - 1
+//   round chain (low priority), after step k, the previous round's formation
+//   and the round TMX_GM_RSLOTS orders earlier (rounds run in round slots
+//   k mod TMX_GM_RSLOTS, several at once)
 //     k_gm_decide     whether to run a round now: at least a threshold of
 //                     grains final and not yet in a round, or the loop over
-//     IF round k:     k_gm_round (slots and items of those grains, every m
+//     IF form k:      k_gm_round (slots and items of those grains, every m
 //                     and class, into per-size-bucket item arrays; T-matrix
 //                     and LU offsets), k_gm_round_mid, k_gm_tzero (their
-//                     T-matrices cleared), one block launch per size bucket
-//                     side by side, k_qsums, k_gm_round_end
+//                     T-matrices cleared)
+//     IF run k:       one block launch per size bucket side by side,
+//                     k_qsums, k_gm_round_end
 // Nothing in the loop chain waits for a round, so rounds run beside the
 // later orders, as the host-driven loop's rounds do on their streams; the
 // lists alternate between two buffers by the parity of k - min_order.
@@ -40,17 +46,47 @@
 
 // ------------------------------------------------------------- kernels --
 
-// whether order step k runs: a grain is left in its input list (count
-// cnt[in]) and no earlier step found the list empty
-__global__ void k_gm_cond(TmxGState *G, int in, cudaGraphConditionalHandle h) {
+// which form of order step k runs, if any: none while k is inside a group
+// of orders an earlier step evaluated (k < next_k) or once the input list
+// (count cnt[in]) is empty; else a group of 8 orders for at most 32 active
+// grains, of 4 orders for at most 128 (where the graph has those forms: the
+// group fits below the last order), one order otherwise -- the host-driven
+// loop's speculation rule
+__global__ void k_gm_cond(TmxGState *G, int in, int k, cudaGraphConditionalHandle h1,
+                          cudaGraphConditionalHandle h4, cudaGraphConditionalHandle h8,
+                          int has4, int has8) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
-  const bool run = !G->loop_done && G->cnt[in] > 0;
-  if (!run) {
-    G->loop_done = 1;
+  int form = 0;
+  if (k >= G->next_k && !G->loop_done) {
+    const int a = G->cnt[in];
+    if (a <= 0) {
+      G->loop_done = 1;
+    } else {
+      form = (has8 && a <= 32) ? 8 : (has4 && a <= 128) ? 4 : 1;
+    }
   }
-  cudaGraphSetConditional(h, run ? 1u : 0u);
+  // (a form the graph does not have has no IF node and no handle)
+  cudaGraphSetConditional(h1, form == 1 ? 1u : 0u);
+  if (has4) {
+    cudaGraphSetConditional(h4, form == 4 ? 1u : 0u);
+  }
+  if (has8) {
+    cudaGraphSetConditional(h8, form == 8 ? 1u : 0u);
+  }
+}
+
+// end of a group of orders: the grains still active after its last order
+// (list `out`) become the input list of the next step (list `in`, the same
+// parity: the group's length is even)
+__global__ void k_gm_relist(TmxGState *G, const int32_t *__restrict__ from, int32_t *to,
+                            int n, int in, int out) {
+  const int c = G->cnt[out];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < min(c, n);
+       p += gridDim.x * blockDim.x) {
+    to[p] = from[p];
+  }
 }
 
 // parameters of step k; the step's output list starts empty
@@ -111,14 +147,21 @@ __global__ void k_gm_prep(const int32_t *__restrict__ nact, const TmxGIter *__re
 
 // end of step j = k - min_order: the done list's length now (every entry
 // and its kept tables complete), and whether the output list is empty
-__global__ void k_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out) {
+__global__ void k_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out,
+                              int in, int next_k, int nk) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
   snap[j] = G->cnt[1];
   outz[j] = (G->cnt[out] == 0) ? 1 : 0;
+  if (in >= 0) {
+    // (a group: its surviving list was copied into list `in`)
+    G->cnt[in] = G->cnt[out];
+  }
   G->snap_last = G->cnt[1];
+  G->next_k = next_k;
   G->steps += 1;
+  G->kernels += nk; // the kernels of this step's body
 }
 
 // whether round j runs: the done entries that step j completed (or, if step
@@ -128,26 +171,30 @@ __global__ void k_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j,
 // last order)
 __global__ void k_gm_decide(TmxGState *G, const int32_t *__restrict__ snap,
                             const int32_t *__restrict__ outz, int j, int last, int thr,
-                            int rmax, cudaGraphConditionalHandle h) {
+                            int rmax, int rs, cudaGraphConditionalHandle hform,
+                            cudaGraphConditionalHandle hexec) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
   const bool ran = snap[j] >= 0;
   const int avail = ran ? snap[j] : G->snap_last;
   const bool ended = !ran || outz[j] != 0 || last != 0;
-  const int pending = avail - G->round_lo;
+  const int pending = avail - G->cursor;
   const bool fire = pending > 0 && (ended || pending >= thr);
   if (fire) {
-    G->round_hi = ended ? avail : min(avail, G->round_lo + rmax);
+    G->rlo[rs] = G->cursor;
+    G->rhi[rs] = ended ? avail : min(avail, G->cursor + rmax);
+    G->cursor = G->rhi[rs];
     for (int q = 0; q < TMX_GM_BUCKETS; ++q) {
-      G->rng[q][0] = G->fill[q];
-      G->rng[q][1] = G->fill[q];
+      G->rng[rs][q][0] = G->fill[q];
+      G->rng[rs][q][1] = G->fill[q];
     }
-    G->srng[0] = G->nslots;
-    G->srng[1] = G->nslots;
+    G->srng[rs][0] = G->nslots;
+    G->srng[rs][1] = G->nslots;
     G->rounds += 1;
   }
-  cudaGraphSetConditional(h, fire ? 1u : 0u);
+  cudaGraphSetConditional(hform, fire ? 1u : 0u);
+  cudaGraphSetConditional(hexec, fire ? 1u : 0u);
 }
 
 // The round: one thread per done entry of [round_lo, round_hi). A grain's
@@ -156,7 +203,7 @@ __global__ void k_gm_decide(TmxGState *G, const int32_t *__restrict__ snap,
 // their size bucket; its T-matrix and each item's LU factors get offsets
 // from bump counters. A grain without kept tables or beyond the T / LU
 // capacity sets the overflow flag (the host then recomputes the batch).
-__global__ void k_gm_round(TmxGState *G, const int32_t *__restrict__ done_list,
+__global__ void k_gm_round(TmxGState *G, int rs, const int32_t *__restrict__ done_list,
                            const int32_t *__restrict__ done_ord,
                            const int64_t *__restrict__ keep_tab,
                            const int32_t *__restrict__ tpl_off,
@@ -166,8 +213,8 @@ __global__ void k_gm_round(TmxGState *G, const int32_t *__restrict__ done_list,
                            TmxSlot *rslots, int nslot_cap, TmxItem *const *bitems,
                            const int32_t *__restrict__ bcap, int64_t *t_off,
                            unsigned long long t_cap, unsigned long long lu_cap) {
-  const int q = G->round_lo + blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= G->round_hi) {
+  const int q = G->rlo[rs] + blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= G->rhi[rs]) {
     return;
   }
   const int g = done_list[q];
@@ -232,23 +279,24 @@ __global__ void k_gm_round(TmxGState *G, const int32_t *__restrict__ done_list,
   }
 }
 
-__global__ void k_gm_round_mid(TmxGState *G) {
+__global__ void k_gm_round_mid(TmxGState *G, int rs) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
   for (int q = 0; q < TMX_GM_BUCKETS; ++q) {
-    G->rng[q][1] = G->fill[q];
+    G->rng[rs][q][1] = G->fill[q];
   }
-  G->srng[1] = G->nslots;
+  G->srng[rs][1] = G->nslots;
 }
 
 // The T-matrix ranges of the round's slots [srng[0], srng[1]) start at
 // zero: the parity classes write only their own entries of a block, the
 // others are zero by symmetry (the host-driven rounds clear their range the
 // same way). One CTA per slot at a time, 16-byte stores.
-__global__ void k_gm_tzero(const TmxGState *__restrict__ G, const TmxSlot *__restrict__ slots,
+__global__ void k_gm_tzero(const TmxGState *__restrict__ G, int rs,
+                           const TmxSlot *__restrict__ slots,
                            const int64_t *__restrict__ tsize, double2 *T) {
-  const int lo = G->srng[0], hi = G->srng[1];
+  const int lo = G->srng[rs][0], hi = G->srng[rs][1];
   for (int s = lo + blockIdx.x; s < hi; s += gridDim.x) {
     const TmxSlot sl = slots[s];
     if (sl.nmax <= 0) {
@@ -263,11 +311,11 @@ __global__ void k_gm_tzero(const TmxGState *__restrict__ G, const TmxSlot *__res
 }
 
 // the round's done entries are consumed
-__global__ void k_gm_round_end(TmxGState *G) {
+__global__ void k_gm_round_end(TmxGState *G, int nk) {
   if (threadIdx.x != 0 || blockIdx.x != 0) {
     return;
   }
-  G->round_lo = G->round_hi;
+  atomicAdd(&G->kernels, nk); // the kernels of this round's bodies
 }
 
 
@@ -284,27 +332,33 @@ void tmx_launch_gm_prep(const int32_t *nact, const TmxGIter *I, const int32_t *a
 }
 
 void tmx_launch_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out,
-                            cudaStream_t stream) {
-  k_gm_step_end<<<1, 32, 0, stream>>>(G, snap, outz, j, out);
+                            int in, int next_k, int nk, cudaStream_t stream) {
+  k_gm_step_end<<<1, 32, 0, stream>>>(G, snap, outz, j, out, in, next_k, nk);
+}
+
+void tmx_launch_gm_relist(TmxGState *G, const int32_t *from, int32_t *to, int n, int in,
+                          int out, cudaStream_t stream) {
+  k_gm_relist<<<std::max(1, std::min((n + 255) / 256, 148)), 256, 0, stream>>>(G, from, to,
+                                                                             n, in, out);
 }
 
 void tmx_launch_gm_round(const TmxGmRoundArgs &a, cudaStream_t stream) {
   k_gm_round<<<(a.n + 127) / 128, 128, 0, stream>>>(
-      a.G, a.done_list, a.done_ord, a.keep_tab, a.tpl_off, a.tpl, a.full_sets, a.tsize,
+      a.G, a.rs, a.done_list, a.done_ord, a.keep_tab, a.tpl_off, a.tpl, a.full_sets, a.tsize,
       a.glf, a.min_order, a.rslots, a.n, a.bitems, a.bcap, a.t_off, a.t_cap, a.lu_cap);
 }
 
-void tmx_launch_gm_round_mid(TmxGState *G, cudaStream_t stream) {
-  k_gm_round_mid<<<1, 32, 0, stream>>>(G);
+void tmx_launch_gm_round_mid(TmxGState *G, int rs, cudaStream_t stream) {
+  k_gm_round_mid<<<1, 32, 0, stream>>>(G, rs);
 }
 
-void tmx_launch_gm_tzero(const TmxGState *G, const TmxSlot *slots, const int64_t *tsize,
-                         double2 *T, cudaStream_t stream) {
-  k_gm_tzero<<<148 * 4, 256, 0, stream>>>(G, slots, tsize, T);
+void tmx_launch_gm_tzero(const TmxGState *G, int rs, const TmxSlot *slots,
+                         const int64_t *tsize, double2 *T, cudaStream_t stream) {
+  k_gm_tzero<<<148 * 4, 256, 0, stream>>>(G, rs, slots, tsize, T);
 }
 
-void tmx_launch_gm_round_end(TmxGState *G, cudaStream_t stream) {
-  k_gm_round_end<<<1, 32, 0, stream>>>(G);
+void tmx_launch_gm_round_end(TmxGState *G, int nk, cudaStream_t stream) {
+  k_gm_round_end<<<1, 32, 0, stream>>>(G, nk);
 }
 
 // The two control kernels of the top-level chains as graph kernel nodes
@@ -332,15 +386,18 @@ static int add_kernel_node(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd
 }
 
 int tmx_gm_add_cond(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd, cudaGraphNode_t *node,
-                    TmxGState *G, int in, cudaGraphConditionalHandle h, int priority) {
-  void *args[] = {&G, &in, &h};
+                    TmxGState *G, int in, int k, cudaGraphConditionalHandle h1,
+                    cudaGraphConditionalHandle h4, cudaGraphConditionalHandle h8, int has4,
+                    int has8, int priority) {
+  void *args[] = {&G, &in, &k, &h1, &h4, &h8, &has4, &has8};
   return add_kernel_node(g, deps, nd, node, (void *)k_gm_cond, args, priority);
 }
 
 int tmx_gm_add_decide(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd,
                       cudaGraphNode_t *node, TmxGState *G, const int32_t *snap,
-                      const int32_t *outz, int j, int last, int thr, int rmax,
-                      cudaGraphConditionalHandle h, int priority) {
-  void *args[] = {&G, &snap, &outz, &j, &last, &thr, &rmax, &h};
+                      const int32_t *outz, int j, int last, int thr, int rmax, int rs,
+                      cudaGraphConditionalHandle hform, cudaGraphConditionalHandle hexec,
+                      int priority) {
+  void *args[] = {&G, &snap, &outz, &j, &last, &thr, &rmax, &rs, &hform, &hexec};
   return add_kernel_node(g, deps, nd, node, (void *)k_gm_decide, args, priority);
 }

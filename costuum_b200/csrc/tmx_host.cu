@@ -1053,6 +1053,20 @@ int tmx_rerun_blocks(tmx_ctx *ctx) {
 #define TMX_GM_ROUND_CTAS (148 * 16)
 #endif
 
+// largest final order of the batch just computed, for the extent of the
+// next device-driven graph of the same schedule
+static void note_kmax(tmx_ctx *ctx) {
+  int km = 0;
+  for (int32_t v : ctx->nmax_h) {
+    km = std::max(km, (int)v);
+  }
+  ctx->kmax_seen = km;
+  ctx->kmax_sched[0] = ctx->up_sched.min_order;
+  ctx->kmax_sched[1] = ctx->up_sched.max_order - 1;
+  ctx->kmax_sched[2] = ctx->up_sched.gauss_legendre_factor;
+  ctx->kmax_tol = ctx->up_sched.tolerance;
+}
+
 static int gm_bucket(int nb) {
   return (nb <= 8) ? 0 : (nb <= 16) ? 1 : (nb <= 32) ? 2 : (nb <= 64) ? 3 : 4;
 }
@@ -1072,6 +1086,16 @@ static int gm_compute(tmx_ctx *ctx) {
   const double tab_per = (double)glf * K * K * TMX_NQ + (double)glf * K * TMX_NS + 32.;
   if (2. * tab_per * sizeof(double) * n > 24e9) {
     return 1;
+  }
+  // The graph's orders end 8 above the largest final order of the previous
+  // batch of the same schedule (the orders beyond it would only be skipped
+  // nodes at the ends of both chains); a batch with grains still active at
+  // that order runs again in the host-driven mode, whose orders then set the
+  // bound of the next graph. Convergence still uses the schedule's last order.
+  int Kg = K;
+  if (ctx->kmax_seen > 0 && ctx->kmax_sched[0] == kmin && ctx->kmax_sched[1] == K &&
+      ctx->kmax_sched[2] == glf && ctx->kmax_tol == S.tolerance) {
+    Kg = std::min(K, std::max(kmin, ctx->kmax_seen + 8));
   }
   // ---- tables shared by all grains: the quadrature and the m = 0 Wigner
   // set of every order of the loop, every m of every order a grain can end
@@ -1119,10 +1143,12 @@ static int gm_compute(tmx_ctx *ctx) {
     tsz[N] = tmx_tmatrix_size(N);
   }
   tpl_off[K + 1] = (int32_t)(tpl.size() / 2);
-  // T-matrix and LU storage: the last graph batch's use with a margin, else
-  // every grain at order 40 (at most every grain at the largest order)
+  // T-matrix and LU storage: the last batch's use (in either mode) with a
+  // margin, else every grain at order 40 (at most every grain at the
+  // largest order)
   const int kest = std::min(K, std::max(kmin, 40));
-  int64_t t_cap = std::max(ctx->gm_t_hint, ctx->gm_last_t + ctx->gm_last_t / 4);
+  const int64_t t_last = std::max(ctx->gm_last_t, ctx->p2_t_total);
+  int64_t t_cap = std::max(ctx->gm_t_hint, t_last + t_last / 4);
   if (t_cap <= 0) {
     t_cap = n * tsz[kest];
   }
@@ -1137,7 +1163,11 @@ static int gm_compute(tmx_ctx *ctx) {
   }
   const int cmK = (K + 1) / 2;
   const int64_t arena_cap = (int64_t)(tab_per * n);
-  const int nsteps = K - kmin + 1;
+  const int nsteps = Kg - kmin + 1;
+  // order-step slots: one per active grain, or a group's G orders of at most
+  // 32 (G = 8) or 128 (G = 4) grains
+  const int64_t ncap = std::max<int64_t>(
+      n, std::max<int64_t>(8 * std::min<int64_t>(n, 32), 4 * std::min<int64_t>(n, 128)));
   // rounds: at least round_min grains final while the loop runs (at most
   // round_max of them), as in the host-driven loop
   const int round_min = (int)std::max<int64_t>(256, ctx->up_nact / 16);
@@ -1153,12 +1183,12 @@ static int gm_compute(tmx_ctx *ctx) {
       (rc = ensure(ctx, ctx->keep_q, n * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->keep_ctl, 32)) ||
       (rc = ensure(ctx, ctx->keep_arena, arena_cap * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->gm_tab, n * (int64_t)glf * K * K * TMX_NQ * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->gm_nsc, n * (int64_t)glf * K * TMX_NS * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->gm_scr, 4 * n * 2 * (int64_t)cmK * cmK * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->gm_diag, n * 2 * (int64_t)K * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->gm_slots, n * sizeof(TmxSlot))) ||
-      (rc = ensure(ctx, ctx->gm_items, 4 * n * sizeof(TmxItem))) ||
+      (rc = ensure(ctx, ctx->gm_tab, ncap * (int64_t)glf * K * K * TMX_NQ * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_nsc, ncap * (int64_t)glf * K * TMX_NS * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_scr, 4 * ncap * 2 * (int64_t)cmK * cmK * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_diag, ncap * 2 * (int64_t)K * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_slots, ncap * sizeof(TmxSlot))) ||
+      (rc = ensure(ctx, ctx->gm_items, 4 * ncap * sizeof(TmxItem))) ||
       (rc = ensure(ctx, ctx->gm_rslots, n * sizeof(TmxSlot))) ||
       (rc = ensure(ctx, ctx->gm_bitems, btot * sizeof(TmxItem))) ||
       (rc = ensure(ctx, ctx->gm_allitems, btot * sizeof(TmxItem))) ||
@@ -1191,7 +1221,7 @@ static int gm_compute(tmx_ctx *ctx) {
   std::vector<uint64_t> key = {
       (uint64_t)n, (uint64_t)glf, (uint64_t)kmin, (uint64_t)K,
       (uint64_t)S.bessel_start, (uint64_t)t_cap, (uint64_t)lu_cap, (uint64_t)arena_cap,
-      (uint64_t)round_min, (uint64_t)round_max};
+      (uint64_t)round_min, (uint64_t)round_max, (uint64_t)Kg};
   uint64_t tol_bits;
   memcpy(&tol_bits, &S.tolerance, sizeof(tol_bits));
   key.push_back(tol_bits);
@@ -1288,19 +1318,30 @@ static int gm_compute(tmx_ctx *ctx) {
       CK(ce);
       return 0;
     };
-    cudaGraphNode_t prev_loop = nullptr, prev_round = nullptr;
-    for (int k = kmin; k <= K; ++k) {
+    std::vector<cudaGraphNode_t> prev_loop;
+    cudaGraphNode_t prev_form = nullptr, slot_exec[TMX_GM_RSLOTS] = {};
+    for (int k = kmin; k <= Kg; ++k) {
       const int j = k - kmin;
       const int in = (j & 1) ? 2 : 0;
       const int out = 2 - in;
       int32_t *act_in = (int32_t *)((j & 1) ? ctx->act1.p : ctx->act0.p);
       int32_t *act_out = (int32_t *)((j & 1) ? ctx->act0.p : ctx->act1.p);
-      // ---- loop chain: order step k
-      cudaGraphConditionalHandle hl, hr;
+      // ---- loop chain: order step k, in one of three forms: this order
+      // alone, or (few grains left) the group of orders k .. k + 3 or
+      // k .. k + 7 where it fits below the last order
+      const bool has4 = k + 3 <= Kg, has8 = k + 7 <= Kg;
+      cudaGraphConditionalHandle hl, h4 = 0, h8 = 0;
       CK(cudaGraphConditionalHandleCreate(&hl, graph, 0, cudaGraphCondAssignDefault));
+      if (has4) {
+        CK(cudaGraphConditionalHandleCreate(&h4, graph, 0, cudaGraphCondAssignDefault));
+      }
+      if (has8) {
+        CK(cudaGraphConditionalHandleCreate(&h8, graph, 0, cudaGraphCondAssignDefault));
+      }
       cudaGraphNode_t e_node, l_node;
-      if (tmx_gm_add_cond(graph, prev_loop ? &prev_loop : nullptr, prev_loop ? 1 : 0, &e_node,
-                          G, in, hl, prio_hi)) {
+      if (tmx_gm_add_cond(graph, prev_loop.empty() ? nullptr : prev_loop.data(),
+                          prev_loop.size(), &e_node, G, in, k, hl, h4, h8, has4 ? 1 : 0,
+                          has8 ? 1 : 0, prio_hi)) {
         return fail(ctx, TMX_ERR_CUDA, "graph: step condition node");
       }
       auto step_body = [&]() -> int {
@@ -1358,25 +1399,141 @@ static int gm_compute(tmx_ctx *ctx) {
         KA.keep_tab = (int64_t *)ctx->keep_tab.p;
         KA.keep_q = (int64_t *)ctx->keep_q.p;
         tmx_launch_keep_tables(KA, (int)n, cs);
-        tmx_launch_gm_step_end(G, snap, outz, j, out, cs);
+        tmx_launch_gm_step_end(G, snap, outz, j, out, -1, k + 1, 7, cs);
         CK(cudaGetLastError());
         return 0;
       };
       if ((rc = add_if(hl, e_node, cs, &l_node, step_body))) {
         return rc;
       }
-      prev_loop = l_node;
-      // ---- round chain: the blocks of the grains final so far
-      CK(cudaGraphConditionalHandleCreate(&hr, graph, 0, cudaGraphCondAssignDefault));
-      cudaGraphNode_t f_node, r_node;
-      const cudaGraphNode_t fdeps[2] = {l_node, prev_round};
-      if (tmx_gm_add_decide(graph, fdeps, prev_round ? 2 : 1, &f_node, G, snap, outz, j,
-                            k == K ? 1 : 0, round_min, round_max, hr, prio_lo)) {
+      prev_loop.assign(1, l_node);
+      // the group of orders k .. k + gk - 1 for at most `chunk` active
+      // grains, laid out as the host-driven loop's speculative groups: slots
+      // [s chunk, (s + 1) chunk) for order k + s, positions past the list's
+      // length empty; after the group its surviving list becomes the input
+      // list of order k + gk (the same parity)
+      auto group_body = [&](int gk, int chunk) -> int {
+        TmxChainBase base[TMX_MAX_GROUP];
+        int64_t tab_t = 0, nsc_t = 0, diag_t = 0, scr_t = 0;
+        for (int q = 0; q < gk; ++q) {
+          const int ks = k + q;
+          const int cm = (ks + 1) / 2;
+          TmxChainBase &b = base[q];
+          b.tab_stride = (int64_t)glf * ks * ks * TMX_NQ;
+          b.nsc_stride = (int64_t)glf * ks * TMX_NS;
+          b.diag_stride = 2 * (int64_t)ks;
+          b.scr_stride = 2 * (int64_t)cm * cm;
+          b.slot = q * chunk;
+          b.tab = tab_t;
+          b.nsc = nsc_t;
+          b.diag = diag_t;
+          b.scr = scr_t;
+          tab_t += chunk * b.tab_stride;
+          nsc_t += chunk * b.nsc_stride;
+          diag_t += chunk * b.diag_stride;
+          scr_t += 4 * chunk * b.scr_stride;
+        }
+        for (int q = 0; q < gk; ++q) {
+          tmx_launch_chain_prep(act_in, chunk, &G->cnt[in], 0, k + q, glf * (k + q),
+                                m0_sets[j + q], base[q], (TmxSlot *)ctx->gm_slots.p,
+                                (TmxItem *)ctx->gm_items.p, cs);
+        }
+        const int kl = k + gk - 1;
+        tmx_launch_tables((const TmxSlot *)ctx->gm_slots.p, gk * chunk,
+                          (const TmxGrain *)ctx->grains.p, (const double *)ctx->gl_x.p,
+                          (const double *)ctx->gl_w.p, (const int64_t *)ctx->gl_off.p,
+                          (double *)ctx->gm_tab.p, (double *)ctx->gm_nsc.p, S.bessel_start,
+                          glf * kl, kl, cs);
+        TmxBlockArgs B;
+        B.items = (const TmxItem *)ctx->gm_items.p;
+        B.nitems = 4 * gk * chunk;
+        B.slots = (const TmxSlot *)ctx->gm_slots.p;
+        B.grains = (const TmxGrain *)ctx->grains.p;
+        B.tab = (const double *)ctx->gm_tab.p;
+        B.nsc = (const double *)ctx->gm_nsc.p;
+        B.wig = (const double *)ctx->wig.p;
+        B.wig_off = (const int64_t *)ctx->wig_off.p;
+        B.scratch = (cplx *)ctx->gm_scr.p;
+        B.tout = nullptr;
+        B.diag = (cplx *)ctx->gm_diag.p;
+        B.status = (int32_t *)ctx->status.p;
+        B.max_nb = (kl + 1) / 2;
+        B.chunk_nodes = tmx_host_chunk_nodes(B.max_nb);
+        B.family = ctx->dispatch[gm_bucket(B.max_nb)];
+        tmx_launch_blocks(B, cs);
+        for (int q = 0; q < gk; ++q) {
+          // (the output list after the group is the one of its last order)
+          CK(cudaMemsetAsync(&G->cnt[out], 0, sizeof(int32_t), cs));
+          tmx_launch_converge(act_in, chunk, (const TmxSlot *)ctx->gm_slots.p + base[q].slot,
+                              (const cplx *)ctx->gm_diag.p, (TmxChainState *)ctx->state.p,
+                              S.tolerance, k + q, K, act_out, &G->cnt[out],
+                              (int32_t *)ctx->done.p, (int32_t *)ctx->done.p + n,
+                              (int32_t *)ctx->done_pos.p, &G->cnt[1], &G->cnt[in], 0, cs);
+        }
+        TmxKeepArgs KA;
+        KA.done_list = (const int32_t *)ctx->done.p;
+        KA.done_ord = (const int32_t *)ctx->done.p + n;
+        KA.done_pos = (const int32_t *)ctx->done_pos.p;
+        KA.counters = G->cnt;
+        KA.next = (int32_t *)ctx->keep_ctl.p;
+        KA.ticket = (unsigned *)ctx->keep_ctl.p + 1;
+        KA.used = (unsigned long long *)ctx->keep_ctl.p + 1;
+        KA.order0 = k;
+        for (int q = 0; q < gk; ++q) {
+          KA.base[q] = base[q];
+        }
+        KA.tab = (const double *)ctx->gm_tab.p;
+        KA.nsc = (const double *)ctx->gm_nsc.p;
+        KA.arena = (double *)ctx->keep_arena.p;
+        KA.cap = arena_cap;
+        KA.keep_tab = (int64_t *)ctx->keep_tab.p;
+        KA.keep_q = (int64_t *)ctx->keep_q.p;
+        tmx_launch_keep_tables(KA, (int)n, cs);
+        tmx_launch_gm_relist(G, act_out, act_in, (int)n, in, out, cs);
+        tmx_launch_gm_step_end(G, snap, outz, j, out, in, k + gk, 2 * gk + 5, cs);
+        CK(cudaGetLastError());
+        return 0;
+      };
+      for (int f = 0; f < 2; ++f) {
+        const int gk = f ? 8 : 4;
+        if (!(f ? has8 : has4)) {
+          continue;
+        }
+        cudaGraphNode_t g_node;
+        if ((rc = add_if(f ? h8 : h4, e_node, cs, &g_node,
+                         [&]() { return group_body(gk, (int)std::min<int64_t>(n, f ? 32 : 128)); }))) {
+          return rc;
+        }
+        prev_loop.push_back(g_node);
+      }
+      // ---- round chain: the blocks of the grains final so far. Rounds are
+      // formed one after another (item lists, T-matrix and LU offsets from
+      // shared counters) and run in round slots k mod TMX_GM_RSLOTS, so that
+      // a round's blocks overlap the next rounds' (the host-driven loop's
+      // rounds overlap on two streams); a slot is reused only after its
+      // previous round, TMX_GM_RSLOTS orders earlier, is done
+      const int rsl = j % TMX_GM_RSLOTS;
+      cudaGraphConditionalHandle hform, hexec;
+      CK(cudaGraphConditionalHandleCreate(&hform, graph, 0, cudaGraphCondAssignDefault));
+      CK(cudaGraphConditionalHandleCreate(&hexec, graph, 0, cudaGraphCondAssignDefault));
+      cudaGraphNode_t f_node, form_node, exec_node;
+      std::vector<cudaGraphNode_t> fdeps = prev_loop;
+      if (prev_form) {
+        fdeps.push_back(prev_form);
+      }
+      if (slot_exec[rsl]) {
+        // (the slot's previous round must be done before its state is reused)
+        fdeps.push_back(slot_exec[rsl]);
+      }
+      if (tmx_gm_add_decide(graph, fdeps.data(), fdeps.size(), &f_node, G, snap, outz, j,
+                            k == Kg ? 1 : 0, round_min, round_max, rsl, hform, hexec,
+                            prio_hi)) {
         return fail(ctx, TMX_ERR_CUDA, "graph: round condition node");
       }
-      auto round_body = [&]() -> int {
+      auto form_body = [&]() -> int {
         TmxGmRoundArgs RA;
         RA.G = G;
+        RA.rs = rsl;
         RA.done_list = (const int32_t *)ctx->done.p;
         RA.done_ord = (const int32_t *)ctx->done.p + n;
         RA.keep_tab = (const int64_t *)ctx->keep_tab.p;
@@ -1393,10 +1550,19 @@ static int gm_compute(tmx_ctx *ctx) {
         RA.t_off = (int64_t *)ctx->gm_toff.p;
         RA.t_cap = (unsigned long long)t_cap;
         RA.lu_cap = (unsigned long long)lu_cap;
-        tmx_launch_gm_round(RA, rs);
-        tmx_launch_gm_round_mid(G, rs);
-        tmx_launch_gm_tzero(G, (const TmxSlot *)ctx->gm_rslots.p,
-                            (const int64_t *)ctx->gm_tsize.p, (cplx *)ctx->T.p, rs);
+        tmx_launch_gm_round(RA, cs);
+        tmx_launch_gm_round_mid(G, rsl, cs);
+        tmx_launch_gm_tzero(G, rsl, (const TmxSlot *)ctx->gm_rslots.p,
+                            (const int64_t *)ctx->gm_tsize.p, (cplx *)ctx->T.p, cs);
+        CK(cudaGetLastError());
+        return 0;
+      };
+      // (the formation is short: its kernels run at the loop's priority, so
+      // that they do not queue behind the running round's blocks)
+      if ((rc = add_if(hform, f_node, cs, &form_node, form_body))) {
+        return rc;
+      }
+      auto exec_body = [&]() -> int {
         for (int b = TMX_GM_BUCKETS - 1; b >= 0; --b) {
           if (bcap[b] == 0) {
             continue;
@@ -1409,7 +1575,7 @@ static int gm_compute(tmx_ctx *ctx) {
           TmxBlockArgs R;
           R.items = bitems[b];
           R.nitems = bcap[b];
-          R.range = &G->rng[b][0];
+          R.range = &G->rng[rsl][b][0];
           R.slots = (const TmxSlot *)ctx->gm_rslots.p;
           R.grains = (const TmxGrain *)ctx->grains.p;
           R.tab = (const double *)ctx->keep_arena.p;
@@ -1436,25 +1602,25 @@ static int gm_compute(tmx_ctx *ctx) {
           }
         }
         tmx_launch_qsums((const TmxSlot *)ctx->gm_rslots.p, (int)n, (const cplx *)ctx->T.p,
-                         (double *)ctx->q.p, rs, &G->srng[0], 148 * 4);
-        tmx_launch_gm_round_end(G, rs);
+                         (double *)ctx->q.p, rs, &G->srng[rsl][0], 148 * 4);
+        tmx_launch_gm_round_end(G, 5 + nbk, rs);
         CK(cudaGetLastError());
         return 0;
       };
-      if ((rc = add_if(hr, f_node, rs, &r_node, round_body))) {
+      if ((rc = add_if(hexec, form_node, rs, &exec_node, exec_body))) {
         return rc;
       }
-      prev_round = r_node;
+      prev_form = form_node;
+      slot_exec[rsl] = exec_node;
     }
     CK(cudaGraphInstantiateWithFlags(&ctx->gm_exec, graph,
                                      cudaGraphInstantiateFlagUseNodePriority));
     ctx->gm_key = key;
-    ctx->gm_body_kernels[0] = 7;
-    ctx->gm_body_kernels[1] = 5 + nbk;
   }
   // ---- this batch: initial state, the graph, the results
   TmxGState g0 = {};
   g0.cnt[0] = ctx->up_nact;
+  g0.next_k = kmin;
   CK(cudaMemcpyAsync(G, &g0, sizeof(g0), cudaMemcpyHostToDevice, st));
   CK(cudaMemsetAsync(snap, 0xff, nsteps * sizeof(int32_t), st));
   CK(cudaMemsetAsync(outz, 0, nsteps * sizeof(int32_t), st));
@@ -1498,9 +1664,8 @@ static int gm_compute(tmx_ctx *ctx) {
   CK(cudaStreamSynchronize(st));
   // kernels the graph ran: the two control nodes of every order, the
   // bodies of the steps and rounds that ran
-  ctx->launches += 2 * (int64_t)nsteps + (int64_t)g1.steps * ctx->gm_body_kernels[0] +
-                   (int64_t)g1.rounds * ctx->gm_body_kernels[1];
-  if (g1.overflow || g1.cnt[1] != ctx->up_nact || g1.round_lo != g1.cnt[1]) {
+  ctx->launches += 2 * (int64_t)nsteps + (int64_t)g1.kernels;
+  if (g1.overflow || g1.cnt[1] != ctx->up_nact || g1.cursor != g1.cnt[1]) {
     // storage ran out (or a grain was not finished): grow the estimates and
     // compute this batch in the host mode
     ctx->gm_t_hint = std::max<int64_t>(2 * t_cap, (int64_t)g1.t_used + (int64_t)g1.t_used / 4);
@@ -1620,6 +1785,9 @@ int tmx_batch_compute(tmx_ctx *ctx) {
   if (ctx->batch_mode == TMX_BATCH_GRAPH) {
     rc = gm_compute(ctx);
     if (rc != 1) {
+      if (rc == TMX_OK) {
+        note_kmax(ctx);
+      }
       return rc;
     }
   }
@@ -2045,6 +2213,7 @@ int tmx_batch_compute(tmx_ctx *ctx) {
       p2.push_back((int32_t)i);
     }
   }
+  note_kmax(ctx);
   if (rounds == 0) {
     if ((rc = run_blocks(ctx, p2))) {
       return rc;

@@ -115,16 +115,23 @@ void tmx_launch_converge(const int32_t *active, int nactive,
 
 // state of the device-driven order loop (tmx_graph.cu), in device memory
 #define TMX_GM_BUCKETS 5
+#define TMX_GM_RSLOTS 8
 struct TmxGState {
   unsigned long long t_used, lu_used; // T-matrix and LU storage handed out
   int32_t cnt[3];   // [0] list A length, [1] done-list length, [2] list B length
   int32_t loop_done;                  // a step found its input list empty
+  int32_t next_k;                     // first order not yet evaluated
   int32_t snap_last;                  // done-list length after the latest step
   int32_t steps, rounds;              // order steps run, rounds fired
-  int32_t round_lo, round_hi;         // done entries of the current round
+  int32_t kernels;                    // kernels the steps' and rounds' bodies ran
+  int32_t cursor;                     // done entries handed to rounds so far
+  // rounds run in round slots r = k mod TMX_GM_RSLOTS, several at once: the
+  // done entries [rlo[r], rhi[r]) of slot r's round, its items per size
+  // bucket and its round slots
+  int32_t rlo[TMX_GM_RSLOTS], rhi[TMX_GM_RSLOTS];
   int32_t fill[TMX_GM_BUCKETS];       // items appended per size bucket
-  int32_t rng[TMX_GM_BUCKETS][2];     // the current round's items per bucket
-  int32_t nslots, srng[2];            // round slots appended; the current round's
+  int32_t rng[TMX_GM_RSLOTS][TMX_GM_BUCKETS][2];
+  int32_t nslots, srng[TMX_GM_RSLOTS][2]; // round slots appended; each slot's
   int32_t overflow;                   // storage or arena ran out (bit mask)
 };
 // parameters of one order step, written by k_gm_begin
@@ -137,6 +144,7 @@ struct TmxGIter {
 // the device-driven loop's kernels (tmx_graph.cu)
 struct TmxGmRoundArgs {
   TmxGState *G;
+  int rs;                    // round slot (0 .. TMX_GM_RSLOTS - 1)
   const int32_t *done_list, *done_ord;
   const int64_t *keep_tab;
   const int32_t *tpl_off, *tpl, *full_sets;
@@ -156,19 +164,24 @@ void tmx_launch_gm_begin(TmxGState *G, TmxGIter *I, int k, int glf, int wig_n, i
 void tmx_launch_gm_prep(const int32_t *nact, const TmxGIter *I, const int32_t *active, int n,
                         TmxSlot *slots, TmxItem *items, cudaStream_t stream);
 void tmx_launch_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j, int out,
-                            cudaStream_t stream);
+                            int in, int next_k, int nk, cudaStream_t stream);
+void tmx_launch_gm_relist(TmxGState *G, const int32_t *from, int32_t *to, int n, int in,
+                          int out, cudaStream_t stream);
 void tmx_launch_gm_round(const TmxGmRoundArgs &a, cudaStream_t stream);
-void tmx_launch_gm_round_mid(TmxGState *G, cudaStream_t stream);
-void tmx_launch_gm_tzero(const TmxGState *G, const TmxSlot *slots, const int64_t *tsize,
-                         double2 *T, cudaStream_t stream);
-void tmx_launch_gm_round_end(TmxGState *G, cudaStream_t stream);
+void tmx_launch_gm_round_mid(TmxGState *G, int rs, cudaStream_t stream);
+void tmx_launch_gm_tzero(const TmxGState *G, int rs, const TmxSlot *slots,
+                         const int64_t *tsize, double2 *T, cudaStream_t stream);
+void tmx_launch_gm_round_end(TmxGState *G, int nk, cudaStream_t stream);
 // the chains' control kernels as graph kernel nodes (0 or -1)
 int tmx_gm_add_cond(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd, cudaGraphNode_t *node,
-                    TmxGState *G, int in, cudaGraphConditionalHandle h, int priority);
+                    TmxGState *G, int in, int k, cudaGraphConditionalHandle h1,
+                    cudaGraphConditionalHandle h4, cudaGraphConditionalHandle h8, int has4,
+                    int has8, int priority);
 int tmx_gm_add_decide(cudaGraph_t g, const cudaGraphNode_t *deps, size_t nd,
                       cudaGraphNode_t *node, TmxGState *G, const int32_t *snap,
-                      const int32_t *outz, int j, int last, int thr, int rmax,
-                      cudaGraphConditionalHandle h, int priority);
+                      const int32_t *outz, int j, int last, int thr, int rmax, int rs,
+                      cudaGraphConditionalHandle hform, cudaGraphConditionalHandle hexec,
+                      int priority);
 
 // copies of the final-order tables of the grains that became final in one
 // group of orders, into the batch's table arena (k_keep_tables)

@@ -107,3 +107,29 @@ def test_graph_gradients_equal_host():
     (qh, (q2h, dqh)), (qg, (q2g, dqg)) = out[Context.BATCH_HOST], out[Context.BATCH_GRAPH]
     assert np.array_equal(qh, qg) and np.array_equal(q2h, q2g)
     assert np.array_equal(dqh, dqg)
+
+
+def test_graph_extent_from_previous_batch():
+    """The graph's orders end a margin above the previous batch's largest
+    final order. A batch that needs more orders than that is computed again
+    in the host-driven mode (same results), and the next graph covers it."""
+    small = H.config2_sample(300, 36, xmin=0.1, xmax=1.0)   # orders ~10-12
+    large = H.config2_sample(600, 37, xmin=5.0, xmax=10.0)  # orders up to ~32
+    host = _run(Context.BATCH_HOST, *large, SCHEDULE)[0]
+    c = Context(0)
+    try:
+        c.set_batch_mode(Context.BATCH_GRAPH)
+        c.tmatrix_batch(*small, **SCHEDULE)
+        modes = []
+        for _ in range(2):
+            res = c.tmatrix_batch(*large, **SCHEDULE)
+            flat, off = c.tmatrices()
+            got = dict(nmax=res.nmax.copy(), status=res.status.copy(), q=res.q.copy(),
+                       T=[flat[off[i]:off[i] + tmatrix_size(int(res.nmax[i]))].copy()
+                          if res.nmax[i] > 0 else None for i in range(res.n)])
+            _same(got, host)
+            modes.append(c.last_batch_mode)
+    finally:
+        c.close()
+    assert int(host["nmax"].max()) > 12 + 8
+    assert modes == [Context.BATCH_HOST, Context.BATCH_GRAPH]

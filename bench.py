@@ -38,6 +38,7 @@ SCHEDULE = dict(min_order=10, max_order=100, gauss_legendre_factor=2,
 CPU_SAMPLE = 1024
 # contexts (host threads) of the end-to-end measurement
 E2E_CONTEXTS = 3
+MODE_NAMES = {0: "host", 1: "graph"}
 
 
 def grains(n, seed):
@@ -386,6 +387,18 @@ def run_ours(args):
         _lib.check(h, lib.tmx_timer_stop(h, P(ms)), "timer")
         return float(ms[0])
 
+    # batch mode: the host-driven loop or the device-driven graph, whichever
+    # runs this workload faster on this box (measured on untimed steps; the
+    # host-driven mode depends on the host thread's speed, the graph not)
+    mode_ms = {}
+    for mode in (Context.BATCH_HOST, Context.BATCH_GRAPH):
+        ctx.set_batch_mode(mode)
+        for _ in range(2):
+            step_device()
+        mode_ms[mode] = float(np.median([step_device() for _ in range(3)]))
+    chosen = min(mode_ms, key=mode_ms.get)
+    other = Context.BATCH_GRAPH if chosen == Context.BATCH_HOST else Context.BATCH_HOST
+    ctx.set_batch_mode(chosen)
     for _ in range(args.warmup):
         step_device()
     # ---- device-resident timed region (no per-launch events in it: the
@@ -409,13 +422,13 @@ def run_ours(args):
     dist.barrier()
     launches = ctx.kernel_launches - launches0
     clocks = sampler.stop()
-    # ---- the same batch in the device-driven mode (one CUDA graph, no host
-    # synchronisation before the end of the batch), timed the same way
-    ctx.set_batch_mode(Context.BATCH_GRAPH)
+    chosen_ok = ctx.last_batch_mode == chosen
+    # ---- the same batch in the other mode, timed the same way
+    ctx.set_batch_mode(other)
     for _ in range(max(2, args.warmup)):
         step_device()
-    graph_ms = [step_device() for _ in range(args.steps)]
-    graph_mode_ok = ctx.last_batch_mode == Context.BATCH_GRAPH
+    other_ms = [step_device() for _ in range(args.steps)]
+    other_ok = ctx.last_batch_mode == other
     ctx.set_batch_mode(Context.BATCH_HOST)
     # ---- kernel profile: the same steps again with CUDA events around every
     # block and table launch and the launch timeline (untimed)
@@ -760,14 +773,19 @@ def run_ours(args):
                          "flops_per_step": flops_survey,
                          "step_tflops": flops_survey / (ms_step * 1e-3) / 1e12,
                          "step_frac": flops_survey / (ms_step * 1e-3) / 1e12 / dmma},
-            "device_driven": {
-                "ms_per_step": float(np.median(graph_ms)),
-                "value": world * N_GRAINS / (float(np.median(graph_ms)) * 1e-3),
-                "mode_ok": bool(graph_mode_ok),
-                "host_syncs_per_batch": 1,
-                "what": "the same batch as one CUDA graph of conditional nodes "
-                        "(order steps and block rounds decided on the device), "
-                        "median of the same number of steps"},
+            "batch_mode": {
+                "timed": MODE_NAMES[chosen], "ran_as_timed": bool(chosen_ok),
+                "untimed_median_ms": {MODE_NAMES[k]: v for k, v in mode_ms.items()},
+                "other": {"mode": MODE_NAMES[other],
+                          "ms_per_step": float(np.median(other_ms)),
+                          "value": world * N_GRAINS / (float(np.median(other_ms)) * 1e-3),
+                          "ran_as_asked": bool(other_ok)},
+                "what": "host: the order loop driven by the host thread one group "
+                        "of orders ahead, block rounds formed on the host; graph: "
+                        "one CUDA graph of conditional nodes, every decision on "
+                        "the device, one host synchronisation per batch. The "
+                        "timed steps use the mode that was faster on 3 untimed "
+                        "steps; the other is timed after them the same way"},
             "profiled_pass": {
                 "ms_per_step": prof_total / args.steps,
                 "block_launches": int(bk_n.value),

@@ -498,10 +498,13 @@ def run_ours(args):
     # tables per step exceed the 126 MB L2)
     pipe_ctx = [ctx] + [Context(local) for _ in range(E2E_CONTEXTS - 1)]
     for c in pipe_ctx:
-        c.set_batch_mode(Context.BATCH_GRAPH)
         if c is not ctx:
-            # page-locked destination of the download, as on the first one
+            # page-locked destination of the download, as on the first one;
+            # a first batch in the host-driven mode gives the graph its
+            # extent (the largest converged order) and its storage sizes
             c.stream_tmatrices(int(flat.size * 1.25) + 4096)
+            c.tmatrix_batch(r, lam, m, d, **SCHEDULE)
+        c.set_batch_mode(Context.BATCH_GRAPH)
         for _ in range(2):
             c.tmatrix_batch(r, lam, m, d, **SCHEDULE)
             c.tmatrices()

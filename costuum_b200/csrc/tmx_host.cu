@@ -1083,19 +1083,21 @@ static int gm_compute(tmx_ctx *ctx) {
       ctx->tuning) {
     return 1;
   }
-  const double tab_per = (double)glf * K * K * TMX_NQ + (double)glf * K * TMX_NS + 32.;
-  if (2. * tab_per * sizeof(double) * n > 24e9) {
-    return 1;
-  }
   // The graph's orders end 8 above the largest final order of the previous
   // batch of the same schedule (the orders beyond it would only be skipped
   // nodes at the ends of both chains); a batch with grains still active at
   // that order runs again in the host-driven mode, whose orders then set the
   // bound of the next graph. Convergence still uses the schedule's last order.
+  // The order steps' tables and the arena of final-order tables are sized
+  // for orders up to Kg.
   int Kg = K;
   if (ctx->kmax_seen > 0 && ctx->kmax_sched[0] == kmin && ctx->kmax_sched[1] == K &&
       ctx->kmax_sched[2] == glf && ctx->kmax_tol == S.tolerance) {
     Kg = std::min(K, std::max(kmin, ctx->kmax_seen + 8));
+  }
+  const double tab_per = (double)glf * Kg * Kg * TMX_NQ + (double)glf * Kg * TMX_NS + 32.;
+  if (2. * tab_per * sizeof(double) * n > 24e9) {
+    return 1;
   }
   // ---- tables shared by all grains: the quadrature and the m = 0 Wigner
   // set of every order of the loop, every m of every order a grain can end
@@ -1161,7 +1163,7 @@ static int gm_compute(tmx_ctx *ctx) {
     bcap[b] = (int32_t)std::min<int64_t>(n * bmax[b], (int64_t)1 << 30);
     btot += bcap[b];
   }
-  const int cmK = (K + 1) / 2;
+  const int cmK = (Kg + 1) / 2;
   const int64_t arena_cap = (int64_t)(tab_per * n);
   const int nsteps = Kg - kmin + 1;
   // order-step slots: one per active grain, or a group's G orders of at most
@@ -1183,10 +1185,10 @@ static int gm_compute(tmx_ctx *ctx) {
       (rc = ensure(ctx, ctx->keep_q, n * sizeof(int64_t))) ||
       (rc = ensure(ctx, ctx->keep_ctl, 32)) ||
       (rc = ensure(ctx, ctx->keep_arena, arena_cap * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->gm_tab, ncap * (int64_t)glf * K * K * TMX_NQ * sizeof(double))) ||
-      (rc = ensure(ctx, ctx->gm_nsc, ncap * (int64_t)glf * K * TMX_NS * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_tab, ncap * (int64_t)glf * Kg * Kg * TMX_NQ * sizeof(double))) ||
+      (rc = ensure(ctx, ctx->gm_nsc, ncap * (int64_t)glf * Kg * TMX_NS * sizeof(double))) ||
       (rc = ensure(ctx, ctx->gm_scr, 4 * ncap * 2 * (int64_t)cmK * cmK * sizeof(cplx))) ||
-      (rc = ensure(ctx, ctx->gm_diag, ncap * 2 * (int64_t)K * sizeof(cplx))) ||
+      (rc = ensure(ctx, ctx->gm_diag, ncap * 2 * (int64_t)Kg * sizeof(cplx))) ||
       (rc = ensure(ctx, ctx->gm_slots, ncap * sizeof(TmxSlot))) ||
       (rc = ensure(ctx, ctx->gm_items, 4 * ncap * sizeof(TmxItem))) ||
       (rc = ensure(ctx, ctx->gm_rslots, n * sizeof(TmxSlot))) ||

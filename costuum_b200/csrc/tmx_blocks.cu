@@ -477,9 +477,6 @@ __device__ __forceinline__ void block_item(const TmxBlockArgs &A, int it,
 template <int TR, int TC, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_blocks(TmxBlockArgs A, size_t smem_bytes) {
-  if (A.gate && *A.gate != A.gate_value) {
-    return;
-  }
   const int ilo = A.range ? A.range[0] : 0;
   const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
   for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {
@@ -764,9 +761,6 @@ __global__ void __launch_bounds__(128, MINB)
   const double *stgS = stg + TMX_WG * NBM * TMX_ROW;
   const int rt = lane >> 2;
   const int ct = lane & 3;
-  if (A.gate && *A.gate != A.gate_value) {
-    return;
-  }
   const int ilo = A.range ? A.range[0] : 0;
   const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
   for (int it = ilo + blockIdx.x * 4 + wib; it < ihi; it += gridDim.x * 4) {
@@ -1119,9 +1113,6 @@ __global__ void __launch_bounds__(128, 4) k_blocks_cta32(TmxBlockArgs A) {
   const int wib = tid >> 5;
   const int q = lane & 3;
   const int rr = lane >> 2;
-  if (A.gate && *A.gate != A.gate_value) {
-    return;
-  }
   const int ilo = A.range ? A.range[0] : 0;
   const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
   for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {
@@ -1387,9 +1378,6 @@ __global__ void __launch_bounds__(256, 1) k_blocks_cta64(TmxBlockArgs A) {
   const int wib = tid >> 5;
   const int q = lane & 3;
   const int rr = lane >> 2;
-  if (A.gate && *A.gate != A.gate_value) {
-    return;
-  }
   const int ilo = A.range ? A.range[0] : 0;
   const int ihi = A.range ? min(A.range[1], A.nitems) : A.nitems;
   for (int it = ilo + blockIdx.x; it < ihi; it += gridDim.x) {

@@ -156,7 +156,7 @@ struct tmx_ctx {
   // LU storage hints grown by a batch that outgrew them
   int batch_mode = TMX_BATCH_HOST, last_mode = TMX_BATCH_HOST;
   DevBuf gm_state, gm_iter, gm_tab, gm_nsc, gm_scr, gm_diag, gm_slots, gm_items,
-      gm_rslots, gm_bitems, gm_bptr, gm_bcap, gm_tpl, gm_tpl_off, gm_full, gm_m0,
+      gm_rslots, gm_bitems, gm_bptr, gm_bcap, gm_tpl, gm_tpl_off, gm_full,
       gm_tsize, gm_toff, gm_lu, gm_luscr, gm_allitems, gm_steps;
   cudaGraph_t gm_graph = nullptr;
   cudaGraphExec_t gm_exec = nullptr;

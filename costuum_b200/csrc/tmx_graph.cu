@@ -100,7 +100,6 @@ __global__ void k_gm_begin(TmxGState *G, TmxGIter *I, int k, int glf, int wig_n,
   it.ngauss = glf * k;
   it.wig_n = wig_n;
   const int cm = (k + 1) / 2;
-  it.bucket = (cm <= 8) ? 0 : (cm <= 16) ? 1 : (cm <= 32) ? 2 : (cm <= 64) ? 3 : 4;
   it.m0_range[0] = 0;
   it.m0_range[1] = 4 * G->cnt[in];
   TmxChainBase &b = it.base;

@@ -343,7 +343,7 @@ void tmx_destroy(tmx_ctx *ctx) {
   DevBuf *gm_bufs[] = {&ctx->gm_state, &ctx->gm_iter, &ctx->gm_tab, &ctx->gm_nsc,
                        &ctx->gm_scr, &ctx->gm_diag, &ctx->gm_slots, &ctx->gm_items,
                        &ctx->gm_rslots, &ctx->gm_bitems, &ctx->gm_bptr, &ctx->gm_bcap,
-                       &ctx->gm_tpl, &ctx->gm_tpl_off, &ctx->gm_full, &ctx->gm_m0,
+                       &ctx->gm_tpl, &ctx->gm_tpl_off, &ctx->gm_full,
                        &ctx->gm_tsize, &ctx->gm_toff, &ctx->gm_lu, &ctx->gm_luscr,
                        &ctx->gm_allitems, &ctx->gm_steps};
   for (DevBuf *b : gm_bufs) {

@@ -67,12 +67,9 @@ struct TmxBlockArgs {
                                // at the item's scratch offset (2 nb^2)
   int family = -1;             // tmx_block_family to run, -1: by max_nb
   // device-driven launches (CUDA graph): items [range[0], range[1]) of
-  // `items` (clamped to nitems) instead of [0, nitems); the launch does
-  // nothing unless *gate == gate_value; at most max_ctas CTAs (0: one item
-  // per warp or CTA)
+  // `items` (clamped to nitems) instead of [0, nitems); at most max_ctas
+  // CTAs (0: one item per warp or CTA)
   const int32_t *range = nullptr;
-  const int32_t *gate = nullptr;
-  int gate_value = 0;
   int max_ctas = 0;
 };
 // largest class size each tmx_block_family can run
@@ -136,7 +133,7 @@ struct TmxGState {
 };
 // parameters of one order step, written by k_gm_begin
 struct TmxGIter {
-  int32_t order, ngauss, wig_n, bucket;
+  int32_t order, ngauss, wig_n;
   int32_t m0_range[2]; // the m = 0 items of the active slots: [0, 4 active)
   TmxChainBase base;
 };

@@ -560,6 +560,23 @@ def run_ours(args):
         plain = {"value": nplain / (t_ms * 1e-3), "unit": "T-matrices/s",
                  "grains": nplain,
                  "what": "one grain per library call (same kernels, no batching)"}
+        # the same calls in the device-driven mode (after two untimed calls
+        # that build the one-grain graph)
+        ctx.set_batch_mode(Context.BATCH_GRAPH)
+        t_ms = 0.0
+        graph_calls = 0
+        for i in range(-2, nplain):
+            rr, ll, mm_, dd = grains(1, 5000 + max(i, 0))
+            lib.tmx_timer_start(h)
+            ctx.tmatrix_batch(rr, ll, mm_, dd, **SCHEDULE)
+            ms = ev()
+            lib.tmx_timer_stop(h, P(ms))
+            if i >= 0:
+                t_ms += float(ms[0])
+                graph_calls += int(ctx.last_batch_mode == Context.BATCH_GRAPH)
+        ctx.set_batch_mode(Context.BATCH_HOST)
+        plain["device_driven"] = {"value": nplain / (t_ms * 1e-3),
+                                  "calls_in_graph_mode": graph_calls}
         # ---- gradient pass vs forward pass on the same batch
         th = np.arccos(np.linspace(-1, 1, 32))
         sys.path.insert(0, os.path.join(ROOT, "oracle"))

@@ -170,6 +170,10 @@ struct tmx_ctx {
   int kmax_seen = 0;
   int kmax_sched[3] = {0, 0, 0};
   double kmax_tol = -1.;
+  // the last graph's extent (last order) and its schedule
+  int gm_kg = 0;
+  int gm_kg_sched[3] = {0, 0, 0};
+  double gm_kg_tol = -1.;
   // host-side times of the last tmx_batch_compute (ms): wall time, time
   // blocked on the order loop's events and the final synchronisation, host
   // set-up of block rounds, and the number of order groups

@@ -1090,11 +1090,23 @@ static int gm_compute(tmx_ctx *ctx) {
   // bound of the next graph. Convergence still uses the schedule's last order.
   // The order steps' tables and the arena of final-order tables are sized
   // for orders up to Kg.
+  // (The extent only grows while the schedule stays the same, so that
+  // batches of changing orders -- one grain per call, say -- reuse one graph
+  // instead of building one per extent.)
   int Kg = K;
   if (ctx->kmax_seen > 0 && ctx->kmax_sched[0] == kmin && ctx->kmax_sched[1] == K &&
       ctx->kmax_sched[2] == glf && ctx->kmax_tol == S.tolerance) {
     Kg = std::min(K, std::max(kmin, ctx->kmax_seen + 8));
+    if (ctx->gm_kg > 0 && ctx->gm_kg_sched[0] == kmin && ctx->gm_kg_sched[1] == K &&
+        ctx->gm_kg_sched[2] == glf && ctx->gm_kg_tol == S.tolerance) {
+      Kg = std::max(Kg, ctx->gm_kg);
+    }
   }
+  ctx->gm_kg = Kg;
+  ctx->gm_kg_sched[0] = kmin;
+  ctx->gm_kg_sched[1] = K;
+  ctx->gm_kg_sched[2] = glf;
+  ctx->gm_kg_tol = S.tolerance;
   const double tab_per = (double)glf * Kg * Kg * TMX_NQ + (double)glf * Kg * TMX_NS + 32.;
   if (2. * tab_per * sizeof(double) * n > 24e9) {
     return 1;
@@ -1154,8 +1166,13 @@ static int gm_compute(tmx_ctx *ctx) {
   if (t_cap <= 0) {
     t_cap = n * tsz[kest];
   }
+  // (at least what the T buffer already holds: the buffers only grow, and a
+  // stable capacity keeps the graph's key, and so the graph, from changing
+  // with every batch's T-matrix total)
+  t_cap = std::max<int64_t>(t_cap, (int64_t)(ctx->T.cap / sizeof(cplx)));
   t_cap = std::min(t_cap, n * tsz[K]);
   int64_t lu_cap = std::max(ctx->gm_lu_hint, (int64_t)((double)t_cap * lun[K] / tsz[K]) + 2 * n * K * K);
+  lu_cap = std::max<int64_t>(lu_cap, (int64_t)(ctx->gm_lu.cap / sizeof(cplx)));
   lu_cap = std::min(lu_cap, n * lun[K]);
   int32_t bcap[TMX_GM_BUCKETS];
   int64_t btot = 0;

@@ -111,15 +111,17 @@ def test_graph_gradients_equal_host():
 
 def test_graph_extent_from_previous_batch():
     """The graph's orders end a margin above the previous batch's largest
-    final order. A batch that needs more orders than that is computed again
-    in the host-driven mode (same results), and the next graph covers it."""
+    final order (and never shrink for the same schedule). A batch that needs
+    more orders than that is computed again in the host-driven mode (same
+    results), and the next graph covers it."""
     small = H.config2_sample(300, 36, xmin=0.1, xmax=1.0)   # orders ~10-12
     large = H.config2_sample(600, 37, xmin=5.0, xmax=10.0)  # orders up to ~32
     host = _run(Context.BATCH_HOST, *large, SCHEDULE)[0]
     c = Context(0)
     try:
-        c.set_batch_mode(Context.BATCH_GRAPH)
+        # the first batch (host-driven) sets the extent of the first graph
         c.tmatrix_batch(*small, **SCHEDULE)
+        c.set_batch_mode(Context.BATCH_GRAPH)
         modes = []
         for _ in range(2):
             res = c.tmatrix_batch(*large, **SCHEDULE)

@@ -160,7 +160,8 @@ __global__ void k_gm_step_end(TmxGState *G, int32_t *snap, int32_t *outz, int j,
   G->snap_last = G->cnt[1];
   G->next_k = next_k;
   G->steps += 1;
-  G->kernels += nk; // the kernels of this step's body
+  atomicAdd(&G->kernels, nk); // the kernels of this step's body (round
+                              // bodies running beside it add theirs too)
 }
 
 // whether round j runs: the done entries that step j completed (or, if step

@@ -135,3 +135,27 @@ def test_graph_extent_from_previous_batch():
         c.close()
     assert int(host["nmax"].max()) > 12 + 8
     assert modes == [Context.BATCH_HOST, Context.BATCH_GRAPH]
+
+
+def test_graph_few_grains_per_call():
+    """Calls of one to five grains (groups of eight orders from the first
+    step, fewer slots than the group layout's 32 per order): every call
+    equals the host-driven result, and all run as one graph (its extent only
+    grows within the schedule)."""
+    c = Context(0)
+    modes = []
+    try:
+        for i, k in enumerate((1, 3, 5, 2, 1)):
+            g = H.config2_sample(k, 60 + i)
+            host = _run(Context.BATCH_HOST, *g, SCHEDULE)[0]
+            c.set_batch_mode(Context.BATCH_GRAPH)
+            res = c.tmatrix_batch(*g, **SCHEDULE)
+            flat, off = c.tmatrices()
+            got = dict(nmax=res.nmax.copy(), status=res.status.copy(), q=res.q.copy(),
+                       T=[flat[off[j]:off[j] + tmatrix_size(int(res.nmax[j]))].copy()
+                          if res.nmax[j] > 0 else None for j in range(res.n)])
+            _same(got, host)
+            modes.append(c.last_batch_mode)
+    finally:
+        c.close()
+    assert modes.count(Context.BATCH_GRAPH) >= 3

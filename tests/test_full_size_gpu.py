@@ -101,6 +101,7 @@ def test_oracle_parity_on_order_extremes(full):
     pick.update(int(i) for i in rng.choice(N_GRAINS, 5, replace=False))
     pick.add(1234)  # conditioning-limited at the rounding level
     worst = 0.0
+    widened = 0  # grains within the sensitivity-scaled bound but above 1e-9
     for i in sorted(pick):
         N, ng = int(nm[i]), int(full["ngauss"][i])
         args = (full["r"][i], full["lam"], full["m"][i], full["d"][i], N, ng)
@@ -112,6 +113,8 @@ def test_oracle_parity_on_order_extremes(full):
         worst = max(worst, err / t_tol)
         print("grain %d order %d: T err %.3g (oracle sensitivity %.3g)" % (i, N, err, t_s))
         assert err <= t_tol, (i, N, err, t_s)
+        widened += int(err > H.T_TOL)
         for j in range(4):
             assert abs(full["q"][i, j] - q[j]) <= q_tol * abs(q[j]), (i, j, q_s)
-    print("worst T error / bound %.3g" % worst)
+    print("worst T error / bound %.3g; %d of %d grains above %.0e, within 4x the "
+          "oracle's own sensitivity" % (worst, widened, len(pick), H.T_TOL))
